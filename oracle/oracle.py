@@ -1,0 +1,253 @@
+"""ctypes wrapper of the CPU oracle (test infrastructure, not product code).
+
+The oracle is a C++ f64 restatement of voronota-ltr's tessellation hot path
+(``oracle/vt_oracle.cpp``).  Only the tests, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` load it, always as the checker or the timed CPU
+baseline.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libvt_oracle.so")
+_lib = None
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+
+
+def build() -> str:
+    """Compile the oracle shared library (make) and return its path."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        build()
+    L = ctypes.CDLL(_LIB_PATH)
+    vp = ctypes.c_void_p
+    L.vto_set_threads.argtypes = [ctypes.c_int]
+    L.vto_get_threads.restype = ctypes.c_int
+    L.vto_set_faithful_grid_update.argtypes = [ctypes.c_int]
+    L.vto_compute.argtypes = [_f64p, ctypes.c_uint64, ctypes.c_double, _f64p, _i32p, ctypes.c_uint64,
+                              ctypes.c_int, ctypes.POINTER(vp)]
+    L.vto_compute.restype = ctypes.c_int
+    for name in ("vto_num_balls", "vto_num_contacts", "vto_num_cells", "vto_num_neighbor_entries",
+                 "vto_num_pairs"):
+        getattr(L, name).argtypes = [vp]
+        getattr(L, name).restype = ctypes.c_uint64
+    L.vto_get_contacts.argtypes = [vp, _u64p, _u64p, _f64p, _f64p, _u8p]
+    L.vto_get_cells.argtypes = [vp, _u64p, _f64p, _f64p]
+    L.vto_get_neighbors.argtypes = [vp, _u64p, _u64p, _f64p]
+    L.vto_get_pairs.argtypes = [vp, _u64p, _u64p, _u8p, _f64p, _f64p, _u8p, _f64p, _f64p, _f64p, _f64p]
+    L.vto_free.argtypes = [vp]
+    L.vto_upd_create.argtypes = [ctypes.c_int]
+    L.vto_upd_create.restype = vp
+    L.vto_upd_destroy.argtypes = [vp]
+    L.vto_upd_init.argtypes = [vp, _f64p, ctypes.c_uint64, ctypes.c_double, _f64p]
+    L.vto_upd_update.argtypes = [vp, _f64p, ctypes.c_uint64]
+    L.vto_upd_update_with_changed.argtypes = [vp, _f64p, ctypes.c_uint64, _u64p, ctypes.c_uint64]
+    L.vto_upd_set_exclusion.argtypes = [vp, ctypes.c_uint64, ctypes.c_int]
+    L.vto_upd_restore.argtypes = [vp]
+    L.vto_upd_last_full_reinit.argtypes = [vp]
+    for name in ("vto_upd_num_changed", "vto_upd_num_affected"):
+        getattr(L, name).argtypes = [vp]
+        getattr(L, name).restype = ctypes.c_uint64
+    L.vto_upd_get_changed.argtypes = [vp, _u64p]
+    L.vto_upd_get_affected.argtypes = [vp, _u64p]
+    L.vto_upd_summary.argtypes = [vp]
+    L.vto_upd_summary.restype = vp
+    _lib = L
+    return L
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def pbox_vectors(periodic_box) -> np.ndarray | None:
+    """Lattice vectors (3x3) from a reference-style periodic box dict, or None.
+
+    ``{"corners": [(x1,y1,z1), (x2,y2,z2)]}`` maps to diagonal vectors as
+    PeriodicBox::from_corners (types.rs:304-310); ``{"vectors": [...]}`` is taken as is.
+    """
+    if periodic_box is None:
+        return None
+    if isinstance(periodic_box, np.ndarray):
+        return np.ascontiguousarray(periodic_box, dtype=np.float64).reshape(9)
+    if "corners" in periodic_box:
+        (x1, y1, z1), (x2, y2, z2) = periodic_box["corners"]
+        return np.array([x2 - x1, 0, 0, 0, y2 - y1, 0, 0, 0, z2 - z1], dtype=np.float64)
+    if "vectors" in periodic_box:
+        return np.ascontiguousarray(np.array(periodic_box["vectors"], dtype=np.float64).reshape(9))
+    raise ValueError("periodic_box must have 'corners' or 'vectors' key")
+
+
+@dataclass
+class OracleResult:
+    num_balls: int
+    contacts_a: np.ndarray
+    contacts_b: np.ndarray
+    contacts_area: np.ndarray
+    contacts_arc: np.ndarray
+    contacts_central: np.ndarray
+    cells_index: np.ndarray
+    cells_sas: np.ndarray
+    cells_vol: np.ndarray
+    nb_offsets: np.ndarray | None = None
+    nb_ids: np.ndarray | None = None
+    nb_values: np.ndarray | None = None
+    pairs: dict = field(default_factory=dict)
+
+    @property
+    def total_contact_area(self) -> float:
+        return float(np.sum(self.contacts_area))
+
+    @property
+    def total_sas_area(self) -> float:
+        return float(np.sum(self.cells_sas))
+
+    @property
+    def total_volume(self) -> float:
+        return float(np.sum(self.cells_vol))
+
+
+def _read_result(L, h, internals: bool) -> OracleResult:
+    nc = L.vto_num_contacts(h)
+    a = np.zeros(nc, np.uint64)
+    b = np.zeros(nc, np.uint64)
+    ar = np.zeros(nc, np.float64)
+    arc = np.zeros(nc, np.float64)
+    ce = np.zeros(nc, np.uint8)
+    L.vto_get_contacts(h, _p(a, _u64p), _p(b, _u64p), _p(ar, _f64p), _p(arc, _f64p), _p(ce, _u8p))
+    m = L.vto_num_cells(h)
+    ci = np.zeros(m, np.uint64)
+    cs = np.zeros(m, np.float64)
+    cv = np.zeros(m, np.float64)
+    L.vto_get_cells(h, _p(ci, _u64p), _p(cs, _f64p), _p(cv, _f64p))
+    res = OracleResult(int(L.vto_num_balls(h)), a, b, ar, arc, ce.astype(bool), ci, cs, cv)
+    if internals:
+        n = res.num_balls
+        ne = L.vto_num_neighbor_entries(h)
+        off = np.zeros(n + 1, np.uint64)
+        ids = np.zeros(ne, np.uint64)
+        vals = np.zeros(ne, np.float64)
+        L.vto_get_neighbors(h, _p(off, _u64p), _p(ids, _u64p), _p(vals, _f64p))
+        res.nb_offsets, res.nb_ids, res.nb_values = off, ids, vals
+        npairs = L.vto_num_pairs(h)
+        arrs = {k: np.zeros(npairs, np.uint64) for k in ("a", "b")}
+        arrs["valid"] = np.zeros(npairs, np.uint8)
+        arrs["central"] = np.zeros(npairs, np.uint8)
+        for k in ("area", "arc", "solid_a", "solid_b", "pyr_a", "pyr_b"):
+            arrs[k] = np.zeros(npairs, np.float64)
+        L.vto_get_pairs(h, _p(arrs["a"], _u64p), _p(arrs["b"], _u64p), _p(arrs["valid"], _u8p),
+                        _p(arrs["area"], _f64p), _p(arrs["arc"], _f64p), _p(arrs["central"], _u8p),
+                        _p(arrs["solid_a"], _f64p), _p(arrs["solid_b"], _f64p), _p(arrs["pyr_a"], _f64p),
+                        _p(arrs["pyr_b"], _f64p))
+        res.pairs = arrs
+    return res
+
+
+def set_threads(n: int) -> None:
+    lib().vto_set_threads(int(n))
+
+
+def get_threads() -> int:
+    return int(lib().vto_get_threads())
+
+
+def set_faithful_grid_update(on: bool) -> None:
+    lib().vto_set_faithful_grid_update(1 if on else 0)
+
+
+def compute(balls, probe: float, periodic_box=None, groups=None, contacts_only: bool = False,
+            internals: bool = False) -> OracleResult:
+    """compute_tessellation / compute_contacts_only on the CPU oracle."""
+    L = lib()
+    xyzr = np.ascontiguousarray(np.asarray(balls, dtype=np.float64).reshape(-1, 4))
+    n = xyzr.shape[0]
+    pb = pbox_vectors(periodic_box)
+    g = None if groups is None else np.ascontiguousarray(np.asarray(groups, dtype=np.int32))
+    h = ctypes.c_void_p()
+    rc = L.vto_compute(_p(xyzr, _f64p), n, float(probe), None if pb is None else _p(pb, _f64p),
+                       None if g is None else _p(g, _i32p), 0 if g is None else len(g),
+                       1 if contacts_only else 0, ctypes.byref(h))
+    if rc != 0:
+        raise RuntimeError(f"oracle failed: {rc}")
+    try:
+        return _read_result(L, h, internals)
+    finally:
+        L.vto_free(h)
+
+
+class OracleUpdateable:
+    """UpdateableTessellation restated on the CPU (updateable.rs)."""
+
+    def __init__(self, with_backup: bool = False):
+        self._L = lib()
+        self._h = ctypes.c_void_p(self._L.vto_upd_create(1 if with_backup else 0))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._L.vto_upd_destroy(self._h)
+            self._h = None
+
+    @staticmethod
+    def _xyzr(balls):
+        return np.ascontiguousarray(np.asarray(balls, dtype=np.float64).reshape(-1, 4))
+
+    def init(self, balls, probe: float, periodic_box=None) -> bool:
+        x = self._xyzr(balls)
+        pb = pbox_vectors(periodic_box)
+        return bool(self._L.vto_upd_init(self._h, _p(x, _f64p), x.shape[0], float(probe),
+                                         None if pb is None else _p(pb, _f64p)))
+
+    def update(self, balls) -> bool:
+        x = self._xyzr(balls)
+        return bool(self._L.vto_upd_update(self._h, _p(x, _f64p), x.shape[0]))
+
+    def update_with_changed(self, balls, changed_ids) -> bool:
+        x = self._xyzr(balls)
+        ids = np.ascontiguousarray(np.asarray(changed_ids, dtype=np.uint64))
+        return bool(self._L.vto_upd_update_with_changed(self._h, _p(x, _f64p), x.shape[0], _p(ids, _u64p),
+                                                        len(ids)))
+
+    def set_exclusion(self, idx: int, excluded: bool) -> bool:
+        return bool(self._L.vto_upd_set_exclusion(self._h, int(idx), 1 if excluded else 0))
+
+    def restore(self) -> bool:
+        return bool(self._L.vto_upd_restore(self._h))
+
+    def last_update_was_full_reinit(self) -> bool:
+        return bool(self._L.vto_upd_last_full_reinit(self._h))
+
+    def changed_ids(self) -> np.ndarray:
+        k = self._L.vto_upd_num_changed(self._h)
+        out = np.zeros(k, np.uint64)
+        self._L.vto_upd_get_changed(self._h, _p(out, _u64p))
+        return out
+
+    def affected_ids(self) -> np.ndarray:
+        k = self._L.vto_upd_num_affected(self._h)
+        out = np.zeros(k, np.uint64)
+        self._L.vto_upd_get_affected(self._h, _p(out, _u64p))
+        return out
+
+    def summary(self) -> OracleResult:
+        h = ctypes.c_void_p(self._L.vto_upd_summary(self._h))
+        try:
+            return _read_result(self._L, h, False)
+        finally:
+            self._L.vto_free(h)

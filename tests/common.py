@@ -1,0 +1,37 @@
+"""Shared fixtures and helpers for the test-suite."""
+import json
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+RING_17 = [  # the C++ API example ring (src/tessellation.rs:743-761)
+    (0.0, 0.0, 2.0, 1.0), (0.0, 1.0, 0.0, 0.5), (0.382683, 0.92388, 0.0, 0.5),
+    (0.707107, 0.707107, 0.0, 0.5), (0.92388, 0.382683, 0.0, 0.5), (1.0, 0.0, 0.0, 0.5),
+    (0.92388, -0.382683, 0.0, 0.5), (0.707107, -0.707107, 0.0, 0.5), (0.382683, -0.92388, 0.0, 0.5),
+    (0.0, -1.0, 0.0, 0.5), (-0.382683, -0.92388, 0.0, 0.5), (-0.707107, -0.707107, 0.0, 0.5),
+    (-0.92388, -0.382683, 0.0, 0.5), (-1.0, 0.0, 0.0, 0.5), (-0.92388, 0.382683, 0.0, 0.5),
+    (-0.707107, 0.707107, 0.0, 0.5), (-0.382683, 0.92388, 0.0, 0.5),
+]
+CENTRAL_POINTS = [[0.0, 0.0, 0.0], [2.5, 0.0, 0.0], [1.25, 2.0, 0.0], [1.25, 0.8, 2.0],
+                  [0.0, 2.5, 1.0], [2.5, 2.5, 1.0], [1.25, -1.5, 1.0], [3.5, 1.25, 1.0]]
+THREE_LINE = [(0.0, 0.0, 0.0, 1.0), (2.0, 0.0, 0.0, 1.0), (4.0, 0.0, 0.0, 1.0)]
+
+
+def goldens():
+    with open(os.path.join(GOLDEN, "goldens.json")) as f:
+        return json.load(f)
+
+
+def load_balls(name):
+    return np.load(os.path.join(GOLDEN, f"balls_{name}.npy"))
+
+
+def central_golden():
+    return np.load(os.path.join(GOLDEN, "central_golden.npy"))
+
+
+def contact_lookup(res_a, res_b, a, b):
+    idx = np.where((np.asarray(res_a) == a) & (np.asarray(res_b) == b))[0]
+    return int(idx[0]) if len(idx) else None
