@@ -1,0 +1,118 @@
+/*
+ * voronota_b200.h -- C ABI of the B200 radical-tessellation library (libvoronota_b200.so).
+ *
+ * Drop-in boundary for voronota-ltr's tessellation hot path.  Plain pointers and sizes,
+ * integer status codes, no exceptions across the ABI, nothing aborts.
+ *
+ * Balls are N x 4 row-major doubles (x, y, z, r) -- the layout of the reference's
+ * numpy input (src/python.rs:69-88) and of `&[Ball]` (src/types.rs:12-21).  A periodic
+ * box is 9 doubles: the lattice vectors a, b, c (PeriodicBox, src/types.rs:292-320;
+ * from_corners(min, max) is the diagonal box (max - min)).  Pass NULL for no box.
+ * Groups: optional int32 per ball; as in the reference (src/tessellation.rs:323-328)
+ * only ids below n_groups are compared.
+ *
+ * Ids are 32-bit: n must satisfy 27 * n < 2^32 (periodic image ids are (g+1) n + i).
+ * Inputs must be finite with r >= 0; anything else returns VT_ERR_INVALID (the
+ * reference accepts such inputs silently and returns meaningless results).
+ */
+#ifndef VORONOTA_B200_H
+#define VORONOTA_B200_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define VT_OK 0
+#define VT_ERR_INVALID 1   /* malformed input (NaN/inf, r < 0, n too large, null pointer) */
+#define VT_ERR_OOM 2       /* device or host allocation failed */
+#define VT_ERR_CUDA 3      /* CUDA runtime error (message: vt_last_error()) */
+#define VT_ERR_CAPACITY 4  /* a neighbour list or contour exceeded the kernels' capacity */
+#define VT_ERR_TIMEOUT 5   /* a bounded device wait expired */
+#define VT_ERR_NO_DEVICE 6 /* no CUDA device */
+
+/* arithmetic of the contact kernel */
+#define VT_FP64 0        /* plain FP64: the reference's arithmetic on the GPU */
+#define VT_FP32_FIXUP 1  /* FP32 bulk; pairs with a decision inside the FP32 error band
+                            are recomputed in FP64 */
+
+typedef struct vt_result vt_result; /* library-owned host result */
+typedef struct vt_engine vt_engine; /* device workspace + stream, one per device/thread */
+
+/* Replaces compute_tessellation(balls, probe, periodic_box, groups, false)
+ * (src/tessellation.rs:37-48).  Contacts come in the reference's output order: pair
+ * order, i.e. by id_a, then by a's neighbour order (src/tessellation.rs:298-319,
+ * 238-253); periodic contacts are deduplicated as deduplicate_periodic_contacts
+ * (src/tessellation.rs:527-601) with ids taken mod n.  Cells are ascending by index
+ * (src/tessellation.rs:649-657).  Uses a per-device engine shared by the process. */
+int vt_compute_tessellation(const double* xyzr, uint64_t n, double probe, const double* periodic_box9,
+                            const int32_t* groups, uint64_t n_groups, int precision, vt_result** out);
+
+/* Replaces compute_contacts_only (src/tessellation.rs:125-166): no cells; periodic
+ * contacts are canonicalised to (min, max) ids and deduplicated keeping the first in
+ * pair order (the reference's HashMap order is unspecified; pair order is a valid one). */
+int vt_compute_contacts_only(const double* xyzr, uint64_t n, double probe, const double* periodic_box9,
+                             const int32_t* groups, uint64_t n_groups, int precision, vt_result** out);
+
+/* Result accessors: TessellationResult + the Results trait (src/types.rs:187-269). */
+uint64_t vt_result_num_balls(const vt_result* r);
+uint64_t vt_result_num_contacts(const vt_result* r);
+uint64_t vt_result_num_cells(const vt_result* r);
+/* Copy out the contacts (arrays of num_contacts); any pointer may be NULL. */
+int vt_result_contacts(const vt_result* r, uint32_t* id_a, uint32_t* id_b, double* area, double* arc_length,
+                       uint8_t* central);
+/* Copy out the cells (arrays of num_cells); any pointer may be NULL. */
+int vt_result_cells(const vt_result* r, uint32_t* index, double* sas_area, double* volume);
+/* total_sas_area / total_volume / total_contact_area (src/types.rs:230-252), summed on
+ * the device in FP64 with a fixed reduction tree. */
+void vt_result_totals(const vt_result* r, double* total_sas_area, double* total_volume,
+                      double* total_contact_area);
+void vt_result_free(vt_result* r);
+
+/* ---- engine: explicit device, stream and device-resident inputs ---- */
+int vt_engine_create(int device, vt_engine** out);
+void vt_engine_destroy(vt_engine* e);
+/* cudaStream_t to run on (NULL: the engine's own stream). */
+int vt_engine_set_stream(vt_engine* e, void* stream);
+/* One tessellation on device-resident input (d_xyzr: N x 4 doubles on the engine's
+ * device; d_groups: device int32 or NULL).  The box is read from host memory.  Results
+ * stay in device memory until vt_engine_download / vt_engine_device_outputs. */
+int vt_engine_compute_device(vt_engine* e, const double* d_xyzr, uint64_t n, double probe,
+                             const double* periodic_box9, const int32_t* d_groups, uint64_t n_groups,
+                             int precision, int contacts_only);
+/* Same from host memory (copied in on the engine's stream). */
+int vt_engine_compute_host(vt_engine* e, const double* xyzr, uint64_t n, double probe,
+                           const double* periodic_box9, const int32_t* groups, uint64_t n_groups,
+                           int precision, int contacts_only);
+int vt_engine_download(vt_engine* e, vt_result** out);
+
+typedef struct vt_stats {
+    uint64_t num_balls, num_slots, num_entries, num_pairs, num_contacts, num_cells;
+    uint64_t num_fp64_redo;   /* FP32 pairs recomputed in FP64 */
+    uint64_t num_serial;      /* pairs recomputed by the serial (large-contour) kernel */
+    double total_sas_area, total_volume, total_contact_area;
+    uint32_t device_error_bits;
+} vt_stats;
+int vt_engine_stats(const vt_engine* e, vt_stats* out);
+
+typedef struct vt_device_outputs {
+    const uint32_t* id_a;
+    const uint32_t* id_b;
+    const double* area;
+    const double* arc_length;
+    const uint8_t* central;
+    const uint32_t* cell_index;
+    const double* cell_sas_area;
+    const double* cell_volume;
+    const double* totals; /* 3 doubles: sas area, volume, contact area */
+} vt_device_outputs;
+int vt_engine_device_outputs(const vt_engine* e, vt_device_outputs* out);
+
+/* Human-readable status, and the message of the calling thread's last error. */
+const char* vt_status_string(int status);
+const char* vt_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

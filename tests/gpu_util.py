@@ -1,0 +1,69 @@
+"""Helpers for comparing GPU results with the oracle."""
+import numpy as np
+
+import oracle as O
+import voronota_ltr as V
+
+
+def has_gpu() -> bool:
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def gpu(balls, probe, periodic_box=None, groups=None, precision="fp64", contacts_only=False):
+    if contacts_only:
+        return V.compute_contacts_only_result(balls, probe, periodic_box, groups, precision)
+    return V.compute_tessellation_result(balls, probe, periodic_box, groups, precision)
+
+
+def compare(g, o, precision, contacts_only=False, ordered=True):
+    """Pair sets and central bits bit-exact; values within the precision's tolerance.
+
+    FP64: |d| <= 1e-9 (1 + |x|) everywhere (only the summation order of the warp
+    reductions and CUDA's vs glibc's transcendentals differ).
+    FP32: per-contact |dA| <= 1e-3 A^2 and |d arc| <= 1e-3 A; per-cell |d| <= 1e-2;
+    total SAS area and total volume relative error <= 1e-6.
+    """
+    ga, gb = g.id_a.astype(np.int64), g.id_b.astype(np.int64)
+    oa, ob = o.contacts_a.astype(np.int64), o.contacts_b.astype(np.int64)
+    assert len(ga) == len(oa), f"contact count {len(ga)} vs oracle {len(oa)}"
+    if ordered:
+        go = np.arange(len(ga))
+        oo = np.arange(len(oa))
+    else:
+        go = np.lexsort((gb, ga))
+        oo = np.lexsort((ob, oa))
+    assert np.array_equal(ga[go], oa[oo]), "id_a differ"
+    assert np.array_equal(gb[go], ob[oo]), "id_b differ"
+    mism = np.nonzero(g.central[go] != o.contacts_central[oo])[0]
+    assert len(mism) == 0, f"central bits differ at {mism[:10]}"
+    if precision == "fp64":
+        tol_area = 1e-9 * (1 + np.abs(o.contacts_area[oo]))
+        tol_arc = 1e-9 * (1 + np.abs(o.contacts_arc[oo]))
+    else:
+        tol_area = tol_arc = 1e-3
+    da = np.abs(g.area[go] - o.contacts_area[oo])
+    dr = np.abs(g.arc_length[go] - o.contacts_arc[oo])
+    assert np.all(da <= tol_area), f"max |dA| {da.max()}"
+    assert np.all(dr <= tol_arc), f"max |d arc| {dr.max()}"
+    if contacts_only:
+        return {"max_dA": float(da.max(initial=0))}
+    assert np.array_equal(g.cell_index.astype(np.int64), o.cells_index.astype(np.int64)), "cell index sets differ"
+    if precision == "fp64":
+        ts = 1e-9 * (1 + np.abs(o.cells_sas))
+        tv = 1e-9 * (1 + np.abs(o.cells_vol))
+    else:
+        ts = tv = 1e-2
+    ds = np.abs(g.cell_sas_area - o.cells_sas)
+    dv = np.abs(g.cell_volume - o.cells_vol)
+    assert np.all(ds <= ts), f"max |d sas| {ds.max()}"
+    assert np.all(dv <= tv), f"max |d vol| {dv.max()}"
+    rs = abs(g.total_sas_area - o.total_sas_area) / max(abs(o.total_sas_area), 1e-300)
+    rv = abs(g.total_volume - o.total_volume) / max(abs(o.total_volume), 1e-300)
+    lim = 1e-11 if precision == "fp64" else 1e-6
+    assert rs <= lim, f"total SAS rel err {rs}"
+    assert rv <= lim, f"total volume rel err {rv}"
+    return {"max_dA": float(da.max(initial=0)), "rel_sas": rs, "rel_vol": rv}

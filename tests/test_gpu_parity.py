@@ -1,0 +1,176 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle and the reference
+goldens.  Pair sets and central bits must match the oracle bit for bit; values within
+the tolerances in gpu_util.compare (FP64: 1e-9 relative; FP32+fixup: |dA| <= 1e-3 A^2,
+total SAS / volume relative error <= 1e-6)."""
+import numpy as np
+import pytest
+
+import oracle as O
+import voronota_ltr as V
+from common import CENTRAL_POINTS, RING_17, THREE_LINE, central_golden, contact_lookup, goldens, load_balls
+from gpu_util import compare, gpu
+from voronota_ltr import workloads as W
+
+pytestmark = pytest.mark.gpu
+G = goldens()
+PRECISIONS = ["fp64", "fp32"]
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_cs_1x1_golden_and_oracle(prec):
+    g = G["cs_1x1"]
+    balls = load_balls("cs_1x1")
+    r = gpu(balls, g["probe"], precision=prec)
+    assert len(r.id_a) == g["contacts"] and len(r.cell_index) == g["cells"]
+    assert abs(r.total_contact_area - g["total_contact_area"]) < g["tol"]
+    assert abs(r.total_sas_area - g["total_sas_area"]) < g["tol"]
+    assert abs(r.total_volume - g["total_volume"]) < g["tol"]
+    k = contact_lookup(r.id_a, r.id_b, 0, 1)
+    assert abs(r.area[k] - g["contact_0_1_area"]) < g["contact_tol"]
+    compare(r, O.compute(balls, g["probe"]), prec)
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+@pytest.mark.parametrize("form", ["corners", "vectors"])
+def test_cs_1x1_periodic(prec, form):
+    g = G["cs_1x1_periodic"]
+    (x1, y1, z1), (x2, y2, z2) = g["corners"]
+    box = ({"corners": g["corners"]} if form == "corners"
+           else {"vectors": [(x2 - x1, 0, 0), (0, y2 - y1, 0), (0, 0, z2 - z1)]})
+    balls = load_balls("cs_1x1")
+    r = gpu(balls, g["probe"], periodic_box=box, precision=prec)
+    assert len(r.id_a) == g["contacts"] and len(r.cell_index) == g["cells"]
+    assert abs(r.total_contact_area - g["total_contact_area"]) < g["tol"]
+    assert abs(r.total_sas_area - g["total_sas_area"]) < g["tol"]
+    assert abs(r.total_volume - g["total_volume"]) < g["tol"]
+    compare(r, O.compute(balls, g["probe"], periodic_box=box), prec)
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_2zsk(prec):
+    balls = load_balls("2zsk")
+    r = gpu(balls, 1.4, precision=prec)
+    assert (len(r.id_a), len(r.cell_index)) == (23855, 3545)
+    compare(r, O.compute(balls, 1.4), prec)
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_3dlb(prec):
+    balls = load_balls("3dlb")
+    compare(gpu(balls, 1.4, precision=prec), O.compute(balls, 1.4), prec)
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_ring17_basic_and_periodic(prec):
+    g = G["ring17"]
+    r = gpu(RING_17, g["probe"], precision=prec)
+    assert len(r.id_a) == g["contacts"] and len(r.cell_index) == g["cells"]
+    cells = dict(zip(r.cell_index.tolist(), zip(r.cell_sas_area, r.cell_volume)))
+    assert abs(cells[0][0] - g["cell0_sas"]) < g["cell_tol"]
+    assert abs(cells[1][1] - g["cell1_vol"]) < g["cell_tol"]
+    compare(r, O.compute(RING_17, g["probe"]), prec)
+    gp = G["ring17_periodic"]
+    box = {"corners": gp["corners"]}
+    r = gpu(RING_17, gp["probe"], periodic_box=box, precision=prec)
+    k = contact_lookup(r.id_a, r.id_b, 0, 0)
+    assert k is not None and abs(r.area[k] - gp["self_contact_0_0_area"]) < gp["self_tol"]
+    compare(r, O.compute(RING_17, gp["probe"], periodic_box=box), prec)
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_centrality_golden(prec):
+    balls = [p + [1.5] for p in CENTRAL_POINTS]
+    r = gpu(balls, 1.4, precision=prec)
+    got = {(int(a), int(b)): bool(c) for a, b, c in zip(r.id_a, r.id_b, r.central)}
+    for a, b, c in central_golden():
+        assert got[(min(a, b), max(a, b))] == bool(c)
+    compare(r, O.compute(balls, 1.4), prec)
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_two_body_groups_contacts_only(prec):
+    g = G["two_body_groups"]
+    balls = [(0.0, 0.0, 0.0, 1.5), (1.0, 0.0, 0.0, 1.5), (4.0, 0.0, 0.0, 2.0), (5.0, 0.0, 0.0, 2.0)]
+    c = V.compute_contacts_only(balls, g["probe"], groups=[0, 0, 1, 1], precision=prec)
+    assert len(c) == 1 and (c[0]["id_a"], c[0]["id_b"]) == (1, 2)
+    assert abs(c[0]["area"] - g["area"]) < (g["tol"] if prec == "fp64" else 1e-3)
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_lattice_2k_config(prec):
+    balls = W.lattice_balls(2000, 0)
+    compare(gpu(balls, 1.4, precision=prec), O.compute(balls, 1.4), prec)
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_lattice_20k_groups_contacts_only(prec):
+    balls = W.lattice_balls(20000, 3)
+    groups = W.x_sign_groups(balls)
+    r = gpu(balls, 1.4, groups=groups, precision=prec, contacts_only=True)
+    compare(r, O.compute(balls, 1.4, groups=groups, contacts_only=True), prec, contacts_only=True)
+    r = gpu(balls, 1.4, groups=groups, precision=prec)
+    compare(r, O.compute(balls, 1.4, groups=groups), prec)
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_periodic_random_box(prec):
+    balls, side = W.periodic_box_balls(6000, 0.033, 1.52, seed=5)
+    box = {"corners": [(0, 0, 0), (side, side, side)]}
+    compare(gpu(balls, 1.4, periodic_box=box, precision=prec), O.compute(balls, 1.4, periodic_box=box), prec)
+    r = gpu(balls, 1.4, periodic_box=box, precision=prec, contacts_only=True)
+    compare(r, O.compute(balls, 1.4, periodic_box=box, contacts_only=True), prec, contacts_only=True)
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_edge_cases(prec):
+    for balls, probe in [
+        (np.zeros((0, 4)), 1.4),
+        ([(0.0, 0.0, 0.0, 1.0)], 0.5),
+        ([(0, 0, 0, 1.0), (10, 0, 0, 1.0)], 0.5),
+        ([(0, 0, 0, 1.0), (0, 0, 0, 0.5), (1, 0, 0, 1.0)], 0.5),  # hidden ball
+        ([(0, 0, 0, 1.0), (0, 0, 0, 1.0), (1.5, 0, 0, 1.0)], 0.5),  # identical balls
+        (THREE_LINE, 0.5),
+        ([(0, 0, 0, 1.0), (0.5, 0, 0, 1.0), (1, 0, 0, 1.0)], 1.0),
+        ([(0, 0, 0, 1), (0, 0, 1, 1), (0, 1, 0, 1), (0, 1, 1, 1), (1, 0, 0, 1), (1, 0, 1, 1), (1, 1, 0, 1),
+          (1, 1, 1, 1)], 2.0),
+    ]:
+        r = gpu(balls, probe, precision=prec)
+        compare(r, O.compute(balls, probe), prec)
+
+
+def test_invalid_input_raises():
+    for bad in ([(0, 0, float("nan"), 1.0)], [(0, 0, 0, -1.0)]):
+        with pytest.raises(V.VoronotaError) as ei:
+            V.compute_tessellation(bad, 1.4)
+        assert ei.value.status == V.VT_ERR_INVALID
+
+
+def test_fp32_large_lattice_pair_set_and_totals():
+    balls = W.lattice_balls(100000, 0)
+    o = O.compute(balls, 1.4)
+    stats = compare(gpu(balls, 1.4, precision="fp32"), o, "fp32")
+    assert stats["rel_sas"] <= 1e-6
+
+
+def test_engine_device_path_matches_host_path():
+    import torch
+    balls = W.lattice_balls(5000, 11)
+    e = V.Engine(0)
+    e.compute_host(balls, 1.4, precision="fp64")
+    h = e.download()
+    t = torch.from_numpy(balls).cuda()
+    e.compute_device(t.data_ptr(), len(balls), 1.4, precision="fp64")
+    torch.cuda.synchronize()
+    d = e.download()
+    assert np.array_equal(h.id_a, d.id_a) and np.array_equal(h.area, d.area)
+    assert np.array_equal(h.cell_sas_area, d.cell_sas_area)
+    e.close()
+
+
+def test_deterministic_reruns():
+    balls = W.lattice_balls(8000, 2)
+    for prec in PRECISIONS:
+        r1 = gpu(balls, 1.4, precision=prec)
+        r2 = gpu(balls, 1.4, precision=prec)
+        assert np.array_equal(r1.area, r2.area) and np.array_equal(r1.cell_sas_area, r2.cell_sas_area)
+        assert r1.total_sas_area == r2.total_sas_area

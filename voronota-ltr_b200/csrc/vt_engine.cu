@@ -1,0 +1,695 @@
+// vt_engine.cu -- host orchestration of the tessellation pipeline and the C ABI.
+//
+// One engine = one device, one stream, one grow-only workspace.  A call runs:
+//   prepare (R = r + probe, bbox)  -> [read bbox]  -> periodic images -> cell grid
+//   -> neighbour count -> scans -> [read E, P] -> neighbour fill + pair list
+//   -> contact kernel (FP64 or FP32) -> collect unsure/overflow -> FP64 recompute
+//   -> serial fallback -> cells -> dedup -> compaction -> totals -> [read counts]
+// Three small device->host reads size the next stage's buffers; everything else stays
+// on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/voronota_b200.h"
+#include "vt_pipeline.cuh"
+
+using namespace vt;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct CudaError {
+    int status;
+};
+
+#define VT_CUDA(call)                                                                      \
+    do {                                                                                   \
+        cudaError_t _e = (call);                                                           \
+        if (_e != cudaSuccess) {                                                           \
+            g_last_error = std::string(#call) + ": " + cudaGetErrorString(_e);            \
+            throw CudaError{_e == cudaErrorMemoryAllocation ? VT_ERR_OOM : VT_ERR_CUDA}; \
+        }                                                                                  \
+    } while (0)
+
+template <typename T>
+struct DBuf {
+    T* p = nullptr;
+    size_t cap = 0;
+    void ensure(size_t n) {
+        if (n <= cap && p) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        size_t c = std::max<size_t>(n + n / 4, 64);
+        VT_CUDA(cudaMalloc(&p, c * sizeof(T)));
+        cap = c;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+}  // namespace
+
+struct vt_result {
+    uint64_t num_balls = 0;
+    std::vector<uint32_t> a, b;
+    std::vector<double> area, arc;
+    std::vector<uint8_t> central;
+    std::vector<uint32_t> cell_index;
+    std::vector<double> cell_sas, cell_vol;
+    double totals[3] = {0, 0, 0};
+};
+
+struct vt_engine {
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t stream = nullptr;
+    // workspace
+    DBuf<double> xyzr;
+    DBuf<int32_t> groups;
+    DBuf<double4> sph, c_pos;
+    DBuf<uint32_t> slot_id, c_id, c_slot, cell_count, cell_start, cell_cursor;
+    DBuf<uint32_t> nb_cnt, nb_npair, nb_off, pair_off, nb_id, nb_slot;
+    DBuf<uint8_t> excluded;
+    DBuf<double> nb_val;
+    DBuf<int32_t> nb_pair;
+    DBuf<float4> nb_rel;
+    DBuf<uint32_t> pair_a, pair_e;
+    DBuf<uint8_t> p_status, p_central;
+    DBuf<double> p_area, p_arc, p_sa_a, p_sa_b, p_pv_a, p_pv_b;
+    DBuf<uint32_t> redo_list, serial_list, keep, keep_off, cell_off, flags32;
+    DBuf<double> serial_scratch;
+    DBuf<uint8_t> cell_flag;
+    DBuf<double> cell_sas, cell_vol;
+    DBuf<uint32_t> out_a, out_b, out_cell_index;
+    DBuf<double> out_area, out_arc, out_cell_sas, out_cell_vol;
+    DBuf<uint8_t> out_central;
+    DBuf<double> totals, partials;
+    DBuf<uint32_t> words;  // [0] err, [1] zero, [2] nslots, [3] redo count, [4] serial count
+    DBuf<BBox> bbox_parts, bbox;
+    DBuf<uint32_t> img_cnt, img_off, scan_tmp;
+    // pinned readback
+    uint32_t* h_words = nullptr;  // 8 words
+    BBox* h_bbox = nullptr;
+    // state of the last call
+    vt_stats stats{};
+    bool contacts_only = false;
+    bool have_result = false;
+    DevBufs bufs{};
+
+    void init(int dev) {
+        device = dev;
+        VT_CUDA(cudaSetDevice(dev));
+        VT_CUDA(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+        stream = own;
+        VT_CUDA(cudaMallocHost(&h_words, 16 * sizeof(uint32_t)));
+        VT_CUDA(cudaMallocHost(&h_bbox, sizeof(BBox)));
+        words.ensure(16);
+        totals.ensure(4);
+        partials.ensure(148 * 3 + 8);
+        bbox.ensure(1);
+        bbox_parts.ensure(1024);
+        set_hex_table();
+        VT_CUDA(cudaGetLastError());
+    }
+    ~vt_engine() {
+        cudaSetDevice(device);
+        if (own) cudaStreamSynchronize(own);
+        DBuf<double>* dd[] = {&xyzr, &nb_val, &p_area, &p_arc, &p_sa_a, &p_sa_b, &p_pv_a, &p_pv_b, &serial_scratch,
+                              &cell_sas, &cell_vol, &out_area, &out_arc, &out_cell_sas, &out_cell_vol, &totals,
+                              &partials};
+        for (auto* b : dd) b->release();
+        DBuf<uint32_t>* du[] = {&slot_id, &c_id, &c_slot, &cell_count, &cell_start, &cell_cursor, &nb_cnt,
+                                &nb_npair, &nb_off, &pair_off, &nb_id, &nb_slot, &pair_a, &pair_e, &redo_list,
+                                &serial_list, &keep, &keep_off, &cell_off, &flags32, &out_a, &out_b,
+                                &out_cell_index, &words, &img_cnt, &img_off, &scan_tmp};
+        for (auto* b : du) b->release();
+        groups.release();
+        sph.release();
+        c_pos.release();
+        excluded.release();
+        nb_pair.release();
+        nb_rel.release();
+        p_status.release();
+        p_central.release();
+        cell_flag.release();
+        out_central.release();
+        bbox_parts.release();
+        bbox.release();
+        if (h_words) cudaFreeHost(h_words);
+        if (h_bbox) cudaFreeHost(h_bbox);
+        if (own) cudaStreamDestroy(own);
+    }
+
+    void sync() { VT_CUDA(cudaStreamSynchronize(stream)); }
+
+    void ensure_scan(size_t n) { scan_tmp.ensure(scan_tmp_words_needed(n) + 8); }
+
+    int run(const double* d_in, uint64_t n64, double probe, const double* pbox9, const int32_t* d_groups,
+            uint64_t n_groups, int precision, int contacts_only_) {
+        VT_CUDA(cudaSetDevice(device));
+        contacts_only = contacts_only_ != 0;
+        have_result = false;
+        stats = vt_stats{};
+        stats.num_balls = n64;
+        if (n64 == 0) {  // tessellation.rs:131-133, 205-207
+            have_result = true;
+            return VT_OK;
+        }
+        const uint32_t n = (uint32_t)n64;
+        const bool periodic = pbox9 != nullptr;
+        const size_t max_slots = periodic ? (size_t)n * 27 : (size_t)n;
+        DevBufs& b = bufs;
+        b = DevBufs{};
+        b.n = n;
+        b.periodic = periodic ? 1 : 0;
+        if (periodic)
+            for (int k = 0; k < 9; ++k) b.pbox[k] = pbox9[k];
+        b.groups = d_groups;
+        b.n_groups = d_groups ? n_groups : 0;
+
+        sph.ensure(max_slots);
+        slot_id.ensure(max_slots);
+        b.sph = sph.p;
+        b.slot_id = slot_id.p;
+        b.err = words.p;
+        b.d_nslots = words.p + 2;
+        b.d_redo_count = words.p + 3;
+        b.d_serial_count = words.p + 4;
+        VT_CUDA(cudaMemsetAsync(words.p, 0, 16 * sizeof(uint32_t), stream));
+
+        // 1. prepare + bounding box
+        int nblk = (int)std::min<size_t>((n + 255) / 256, 1024);
+        launch_prepare(b, d_in, probe, bbox_parts.p, nblk, stream);
+        launch_bbox_final(bbox_parts.p, nblk, bbox.p, stream);
+        VT_CUDA(cudaMemcpyAsync(h_bbox, bbox.p, sizeof(BBox), cudaMemcpyDeviceToHost, stream));
+        sync();
+        const BBox bb = *h_bbox;
+        for (int k = 0; k < 3; ++k)
+            if (!std::isfinite(bb.mn[k]) || !std::isfinite(bb.mx[k])) {
+                g_last_error = "non-finite coordinates";
+                return VT_ERR_INVALID;
+            }
+        // cell edge >= 2 max R + margin: intersecting balls lie in adjacent cells
+        // (the reference uses max(2R + 0.25), spheres_searcher.rs:74-77)
+        double reach = std::max(2.0 * bb.max_r + 0.25, 1.0);
+
+        // 2. periodic images within reach of the structure
+        if (periodic) {
+            img_cnt.ensure(n);
+            img_off.ensure(n + 1);
+            ensure_scan(n);
+            launch_images(b, reach, bbox.p, img_cnt.p, img_off.p, scan_tmp.p, scan_tmp.cap, stream);
+        } else {
+            VT_CUDA(cudaMemcpyAsync(b.d_nslots, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        }
+
+        // 3. grid over the extended box (cells of edge >= reach)
+        GridDev g;
+        double ext[3], cell = reach;
+        for (int k = 0; k < 3; ++k) ext[k] = (bb.mx[k] - bb.mn[k]) + 2.0 * reach;
+        double vol_cells = 1.0;
+        auto dims_for = [&](double c, int* d) {
+            for (int k = 0; k < 3; ++k) d[k] = (int)std::floor(ext[k] / c) + 1;
+        };
+        int dd[3];
+        dims_for(cell, dd);
+        vol_cells = (double)dd[0] * dd[1] * dd[2];
+        const double max_cells = 8.0 * (double)max_slots + 4096.0;
+        while (vol_cells > max_cells) {  // sparse inputs: coarser cells keep the grid O(n)
+            cell *= std::cbrt(vol_cells / max_cells) * 1.01;
+            dims_for(cell, dd);
+            vol_cells = (double)dd[0] * dd[1] * dd[2];
+        }
+        g.cell = cell;
+        g.ox = bb.mn[0] - reach;
+        g.oy = bb.mn[1] - reach;
+        g.oz = bb.mn[2] - reach;
+        g.dx = dd[0];
+        g.dy = dd[1];
+        g.dz = dd[2];
+        b.grid = g;
+        const uint32_t ncell = (uint32_t)(dd[0] * (uint64_t)dd[1] * dd[2]);
+        cell_count.ensure(ncell);
+        cell_start.ensure(ncell + 1);
+        cell_cursor.ensure(ncell);
+        c_pos.ensure(max_slots);
+        c_id.ensure(max_slots);
+        c_slot.ensure(max_slots);
+        b.cell_count = cell_count.p;
+        b.cell_start = cell_start.p;
+        b.cell_cursor = cell_cursor.p;
+        b.c_pos = c_pos.p;
+        b.c_id = c_id.p;
+        b.c_slot = c_slot.p;
+        ensure_scan(std::max<size_t>(ncell, n) + 1);
+        launch_grid(b, ncell, (uint32_t)max_slots, scan_tmp.p, scan_tmp.cap, stream);
+
+        // 4. neighbour counts
+        nb_cnt.ensure(n);
+        nb_npair.ensure(n);
+        excluded.ensure(n);
+        nb_off.ensure(n + 1);
+        pair_off.ensure(n + 1);
+        b.nb_cnt = nb_cnt.p;
+        b.nb_npair = nb_npair.p;
+        b.excluded = excluded.p;
+        b.nb_off = nb_off.p;
+        b.pair_off = pair_off.p;
+        launch_search_count(b, stream);
+        scan_u32(nb_cnt.p, nb_off.p, n, scan_tmp.p, stream);
+        scan_u32(nb_npair.p, pair_off.p, n, scan_tmp.p, stream);
+        VT_CUDA(cudaMemcpyAsync(h_words + 0, nb_off.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        VT_CUDA(cudaMemcpyAsync(h_words + 1, pair_off.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        VT_CUDA(cudaMemcpyAsync(h_words + 2, words.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        VT_CUDA(cudaMemcpyAsync(h_words + 3, b.d_nslots, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        sync();
+        const uint32_t E = h_words[0], P = h_words[1];
+        stats.num_entries = E;
+        stats.num_pairs = P;
+        stats.num_slots = h_words[3];
+        if (h_words[2] & kErrNeighborCap) {
+            g_last_error = "a ball has more than 256 neighbour candidates";
+            stats.device_error_bits = h_words[2];
+            return VT_ERR_CAPACITY;
+        }
+
+        // 5. neighbour lists + pair list
+        const bool fp32 = precision == VT_FP32_FIXUP;
+        nb_id.ensure(E);
+        nb_slot.ensure(E);
+        nb_val.ensure(E);
+        nb_pair.ensure(E);
+        if (fp32) nb_rel.ensure(E);
+        pair_a.ensure(P);
+        pair_e.ensure(P);
+        b.nb_id = nb_id.p;
+        b.nb_slot = nb_slot.p;
+        b.nb_val = nb_val.p;
+        b.nb_pair = nb_pair.p;
+        b.nb_rel = fp32 ? nb_rel.p : nullptr;
+        b.pair_a = pair_a.p;
+        b.pair_e = pair_e.p;
+        launch_search_fill(b, fp32 ? 1 : 0, stream);
+
+        // 6. contacts
+        p_status.ensure(P);
+        p_central.ensure(P);
+        p_area.ensure(P);
+        p_arc.ensure(P);
+        p_sa_a.ensure(P);
+        p_sa_b.ensure(P);
+        p_pv_a.ensure(P);
+        p_pv_b.ensure(P);
+        redo_list.ensure(P);
+        serial_list.ensure(P);
+        const uint32_t serial_slots = 2048;
+        serial_scratch.ensure((size_t)serial_slots * kSerialCap * 6);
+        b.p_status = p_status.p;
+        b.p_central = p_central.p;
+        b.p_area = p_area.p;
+        b.p_arc = p_arc.p;
+        b.p_sa_a = p_sa_a.p;
+        b.p_sa_b = p_sa_b.p;
+        b.p_pv_a = p_pv_a.p;
+        b.p_pv_b = p_pv_b.p;
+        b.redo_list = redo_list.p;
+        b.serial_list = serial_list.p;
+        b.serial_scratch = serial_scratch.p;
+        b.serial_slots = serial_slots;
+        const int full = contacts_only ? 0 : 1;
+        if (P > 0) {
+            if (fp32) {
+                launch_contact_f32(b, P, full, stream);
+                launch_collect_redo(b, P, stream);
+                launch_contact_f64(b, P, full, 1, stream);
+            } else {
+                launch_contact_f64(b, P, full, 0, stream);
+            }
+            VT_CUDA(cudaMemcpyAsync(h_words + 4, b.d_redo_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+            launch_collect_redo(b, P, stream);
+            launch_contact_serial(b, P, full, stream);
+        }
+
+        // 7. cells, dedup, compaction, totals
+        cell_flag.ensure(n);
+        cell_sas.ensure(n);
+        cell_vol.ensure(n);
+        keep.ensure(P + 1);
+        keep_off.ensure(P + 1);
+        cell_off.ensure(n + 1);
+        flags32.ensure(n);
+        out_a.ensure(P);
+        out_b.ensure(P);
+        out_area.ensure(P);
+        out_arc.ensure(P);
+        out_central.ensure(P);
+        out_cell_index.ensure(n);
+        out_cell_sas.ensure(n);
+        out_cell_vol.ensure(n);
+        b.cell_flag = cell_flag.p;
+        b.cell_sas = cell_sas.p;
+        b.cell_vol = cell_vol.p;
+        b.keep = keep.p;
+        b.keep_off = keep_off.p;
+        b.cell_off = cell_off.p;
+        b.params_u = flags32.p;
+        b.out_a = out_a.p;
+        b.out_b = out_b.p;
+        b.out_area = out_area.p;
+        b.out_arc = out_arc.p;
+        b.out_central = out_central.p;
+        b.out_cell_index = out_cell_index.p;
+        b.out_cell_sas = out_cell_sas.p;
+        b.out_cell_vol = out_cell_vol.p;
+        b.totals = totals.p;
+        b.partials = partials.p;
+        b.zero_word = words.p + 1;
+        ensure_scan(std::max<size_t>(P, n) + 1);
+        if (!contacts_only) launch_cells(b, stream);
+        launch_dedup(b, P, contacts_only ? 1 : 0, stream);
+        launch_compact(b, P, contacts_only ? 1 : 0, scan_tmp.p, scan_tmp.cap, stream);
+        launch_totals(b, P, contacts_only ? 1 : 0, stream);
+
+        VT_CUDA(cudaMemcpyAsync(h_words + 5, keep_off.p + P, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        if (!contacts_only)
+            VT_CUDA(cudaMemcpyAsync(h_words + 6, cell_off.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        VT_CUDA(cudaMemcpyAsync(h_words + 7, words.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        VT_CUDA(cudaMemcpyAsync(h_words + 8, b.d_serial_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        double h_tot[3];
+        VT_CUDA(cudaMemcpyAsync(h_tot, totals.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        sync();
+        VT_CUDA(cudaGetLastError());
+        stats.num_contacts = P > 0 ? h_words[5] : 0;
+        stats.num_cells = contacts_only ? 0 : h_words[6];
+        stats.num_fp64_redo = (P > 0 && fp32) ? h_words[4] : 0;
+        stats.num_serial = P > 0 ? h_words[8] : 0;
+        stats.device_error_bits = h_words[7];
+        stats.total_sas_area = contacts_only ? 0.0 : h_tot[0];
+        stats.total_volume = contacts_only ? 0.0 : h_tot[1];
+        stats.total_contact_area = h_tot[2];
+        if (h_words[7] & (kErrOverflow | kErrNeighborCap)) {
+            g_last_error = "contour or neighbour capacity exceeded";
+            return VT_ERR_CAPACITY;
+        }
+        if (h_words[7] & kErrInvalid) {
+            g_last_error = "non-finite input or negative radius";
+            return VT_ERR_INVALID;
+        }
+        have_result = true;
+        return VT_OK;
+    }
+
+    int download(vt_result** out) {
+        if (!have_result) {
+            g_last_error = "no result";
+            return VT_ERR_INVALID;
+        }
+        VT_CUDA(cudaSetDevice(device));
+        std::unique_ptr<vt_result> r(new vt_result());
+        r->num_balls = stats.num_balls;
+        const size_t C = stats.num_contacts, M = stats.num_cells;
+        r->a.resize(C);
+        r->b.resize(C);
+        r->area.resize(C);
+        r->arc.resize(C);
+        r->central.resize(C);
+        r->cell_index.resize(M);
+        r->cell_sas.resize(M);
+        r->cell_vol.resize(M);
+        if (C) {
+            VT_CUDA(cudaMemcpyAsync(r->a.data(), out_a.p, C * 4, cudaMemcpyDeviceToHost, stream));
+            VT_CUDA(cudaMemcpyAsync(r->b.data(), out_b.p, C * 4, cudaMemcpyDeviceToHost, stream));
+            VT_CUDA(cudaMemcpyAsync(r->area.data(), out_area.p, C * 8, cudaMemcpyDeviceToHost, stream));
+            VT_CUDA(cudaMemcpyAsync(r->arc.data(), out_arc.p, C * 8, cudaMemcpyDeviceToHost, stream));
+            VT_CUDA(cudaMemcpyAsync(r->central.data(), out_central.p, C, cudaMemcpyDeviceToHost, stream));
+        }
+        if (M) {
+            VT_CUDA(cudaMemcpyAsync(r->cell_index.data(), out_cell_index.p, M * 4, cudaMemcpyDeviceToHost, stream));
+            VT_CUDA(cudaMemcpyAsync(r->cell_sas.data(), out_cell_sas.p, M * 8, cudaMemcpyDeviceToHost, stream));
+            VT_CUDA(cudaMemcpyAsync(r->cell_vol.data(), out_cell_vol.p, M * 8, cudaMemcpyDeviceToHost, stream));
+        }
+        sync();
+        r->totals[0] = stats.total_sas_area;
+        r->totals[1] = stats.total_volume;
+        r->totals[2] = stats.total_contact_area;
+        *out = r.release();
+        return VT_OK;
+    }
+};
+
+namespace {
+
+int validate_host(const double* xyzr, uint64_t n, double probe, const double* pbox9, const int32_t* groups,
+                  uint64_t n_groups) {
+    if (n > 0 && !xyzr) {
+        g_last_error = "null balls pointer";
+        return VT_ERR_INVALID;
+    }
+    if (n_groups > 0 && !groups) {
+        g_last_error = "null groups pointer";
+        return VT_ERR_INVALID;
+    }
+    if (n >= (uint64_t)0xffffffffu / 27u) {
+        g_last_error = "too many balls for 32-bit ids";
+        return VT_ERR_INVALID;
+    }
+    if (!std::isfinite(probe)) {
+        g_last_error = "non-finite probe";
+        return VT_ERR_INVALID;
+    }
+    if (pbox9)
+        for (int k = 0; k < 9; ++k)
+            if (!std::isfinite(pbox9[k])) {
+                g_last_error = "non-finite periodic box";
+                return VT_ERR_INVALID;
+            }
+    for (uint64_t i = 0; i < n; ++i) {
+        const double* v = xyzr + 4 * i;
+        if (!std::isfinite(v[0]) || !std::isfinite(v[1]) || !std::isfinite(v[2]) || !std::isfinite(v[3]) ||
+            v[3] < 0.0) {
+            g_last_error = "ball " + std::to_string(i) + ": non-finite value or negative radius";
+            return VT_ERR_INVALID;
+        }
+    }
+    return VT_OK;
+}
+
+std::mutex g_engines_mu;
+std::vector<std::unique_ptr<vt_engine>> g_engines;
+std::vector<std::unique_ptr<std::mutex>> g_engine_mu;
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        return f();
+    } catch (const CudaError& e) {
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return VT_ERR_OOM;
+    } catch (...) {
+        g_last_error = "unexpected exception";
+        return VT_ERR_CUDA;
+    }
+}
+
+int host_compute(vt_engine* e, const double* xyzr, uint64_t n, double probe, const double* pbox9,
+                 const int32_t* groups, uint64_t n_groups, int precision, int contacts_only) {
+    int st = validate_host(xyzr, n, probe, pbox9, groups, n_groups);
+    if (st != VT_OK) return st;
+    if (precision != VT_FP64 && precision != VT_FP32_FIXUP) {
+        g_last_error = "unknown precision";
+        return VT_ERR_INVALID;
+    }
+    VT_CUDA(cudaSetDevice(e->device));
+    const double* d_in = nullptr;
+    const int32_t* d_g = nullptr;
+    if (n) {
+        e->xyzr.ensure(4 * n);
+        VT_CUDA(cudaMemcpyAsync(e->xyzr.p, xyzr, 4 * n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+        d_in = e->xyzr.p;
+    }
+    if (groups && n_groups) {
+        e->groups.ensure(n_groups);
+        VT_CUDA(cudaMemcpyAsync(e->groups.p, groups, n_groups * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                e->stream));
+        d_g = e->groups.p;
+    }
+    return e->run(d_in, n, probe, pbox9, d_g, n_groups, precision, contacts_only);
+}
+
+int stateless(const double* xyzr, uint64_t n, double probe, const double* pbox9, const int32_t* groups,
+              uint64_t n_groups, int precision, int contacts_only, vt_result** out) {
+    if (!out) {
+        g_last_error = "null result pointer";
+        return VT_ERR_INVALID;
+    }
+    *out = nullptr;
+    return guarded([&]() -> int {
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+            g_last_error = "no CUDA device";
+            return VT_ERR_NO_DEVICE;
+        }
+        int dev = 0;
+        VT_CUDA(cudaGetDevice(&dev));
+        vt_engine* e;
+        std::mutex* mu;
+        {
+            std::lock_guard<std::mutex> lk(g_engines_mu);
+            if ((int)g_engines.size() < ndev) {
+                g_engines.resize(ndev);
+                g_engine_mu.resize(ndev);
+            }
+            if (!g_engines[dev]) {
+                std::unique_ptr<vt_engine> ne(new vt_engine());
+                ne->init(dev);
+                g_engines[dev] = std::move(ne);
+                g_engine_mu[dev].reset(new std::mutex());
+            }
+            e = g_engines[dev].get();
+            mu = g_engine_mu[dev].get();
+        }
+        std::lock_guard<std::mutex> lk(*mu);
+        int st = host_compute(e, xyzr, n, probe, pbox9, groups, n_groups, precision, contacts_only);
+        if (st != VT_OK) return st;
+        return e->download(out);
+    });
+}
+
+}  // namespace
+
+extern "C" {
+
+int vt_compute_tessellation(const double* xyzr, uint64_t n, double probe, const double* periodic_box9,
+                            const int32_t* groups, uint64_t n_groups, int precision, vt_result** out) {
+    return stateless(xyzr, n, probe, periodic_box9, groups, n_groups, precision, 0, out);
+}
+int vt_compute_contacts_only(const double* xyzr, uint64_t n, double probe, const double* periodic_box9,
+                             const int32_t* groups, uint64_t n_groups, int precision, vt_result** out) {
+    return stateless(xyzr, n, probe, periodic_box9, groups, n_groups, precision, 1, out);
+}
+
+uint64_t vt_result_num_balls(const vt_result* r) { return r ? r->num_balls : 0; }
+uint64_t vt_result_num_contacts(const vt_result* r) { return r ? r->a.size() : 0; }
+uint64_t vt_result_num_cells(const vt_result* r) { return r ? r->cell_index.size() : 0; }
+int vt_result_contacts(const vt_result* r, uint32_t* a, uint32_t* b, double* area, double* arc, uint8_t* central) {
+    if (!r) return VT_ERR_INVALID;
+    size_t C = r->a.size();
+    if (C == 0) return VT_OK;
+    if (a) std::memcpy(a, r->a.data(), C * 4);
+    if (b) std::memcpy(b, r->b.data(), C * 4);
+    if (area) std::memcpy(area, r->area.data(), C * 8);
+    if (arc) std::memcpy(arc, r->arc.data(), C * 8);
+    if (central) std::memcpy(central, r->central.data(), C);
+    return VT_OK;
+}
+int vt_result_cells(const vt_result* r, uint32_t* index, double* sas, double* vol) {
+    if (!r) return VT_ERR_INVALID;
+    size_t M = r->cell_index.size();
+    if (M == 0) return VT_OK;
+    if (index) std::memcpy(index, r->cell_index.data(), M * 4);
+    if (sas) std::memcpy(sas, r->cell_sas.data(), M * 8);
+    if (vol) std::memcpy(vol, r->cell_vol.data(), M * 8);
+    return VT_OK;
+}
+void vt_result_totals(const vt_result* r, double* s, double* v, double* c) {
+    if (!r) return;
+    if (s) *s = r->totals[0];
+    if (v) *v = r->totals[1];
+    if (c) *c = r->totals[2];
+}
+void vt_result_free(vt_result* r) { delete r; }
+
+int vt_engine_create(int device, vt_engine** out) {
+    if (!out) return VT_ERR_INVALID;
+    *out = nullptr;
+    return guarded([&]() -> int {
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+            g_last_error = "no CUDA device";
+            return VT_ERR_NO_DEVICE;
+        }
+        if (device < 0 || device >= ndev) {
+            g_last_error = "bad device index";
+            return VT_ERR_INVALID;
+        }
+        std::unique_ptr<vt_engine> e(new vt_engine());
+        e->init(device);
+        *out = e.release();
+        return VT_OK;
+    });
+}
+void vt_engine_destroy(vt_engine* e) { delete e; }
+int vt_engine_set_stream(vt_engine* e, void* stream) {
+    if (!e) return VT_ERR_INVALID;
+    e->stream = stream ? (cudaStream_t)stream : e->own;
+    return VT_OK;
+}
+int vt_engine_compute_device(vt_engine* e, const double* d_xyzr, uint64_t n, double probe, const double* pbox9,
+                             const int32_t* d_groups, uint64_t n_groups, int precision, int contacts_only) {
+    if (!e || (n && !d_xyzr)) return VT_ERR_INVALID;
+    if (n >= (uint64_t)0xffffffffu / 27u) {
+        g_last_error = "too many balls for 32-bit ids";
+        return VT_ERR_INVALID;
+    }
+    if (precision != VT_FP64 && precision != VT_FP32_FIXUP) return VT_ERR_INVALID;
+    return guarded([&]() { return e->run(d_xyzr, n, probe, pbox9, d_groups, n_groups, precision, contacts_only); });
+}
+int vt_engine_compute_host(vt_engine* e, const double* xyzr, uint64_t n, double probe, const double* pbox9,
+                           const int32_t* groups, uint64_t n_groups, int precision, int contacts_only) {
+    if (!e) return VT_ERR_INVALID;
+    return guarded(
+        [&]() { return host_compute(e, xyzr, n, probe, pbox9, groups, n_groups, precision, contacts_only); });
+}
+int vt_engine_download(vt_engine* e, vt_result** out) {
+    if (!e || !out) return VT_ERR_INVALID;
+    *out = nullptr;
+    return guarded([&]() { return e->download(out); });
+}
+int vt_engine_stats(const vt_engine* e, vt_stats* out) {
+    if (!e || !out) return VT_ERR_INVALID;
+    *out = e->stats;
+    return VT_OK;
+}
+int vt_engine_device_outputs(const vt_engine* e, vt_device_outputs* o) {
+    if (!e || !o || !e->have_result) return VT_ERR_INVALID;
+    o->id_a = e->out_a.p;
+    o->id_b = e->out_b.p;
+    o->area = e->out_area.p;
+    o->arc_length = e->out_arc.p;
+    o->central = e->out_central.p;
+    o->cell_index = e->out_cell_index.p;
+    o->cell_sas_area = e->out_cell_sas.p;
+    o->cell_volume = e->out_cell_vol.p;
+    o->totals = e->totals.p;
+    return VT_OK;
+}
+const char* vt_status_string(int s) {
+    switch (s) {
+        case VT_OK: return "ok";
+        case VT_ERR_INVALID: return "invalid input";
+        case VT_ERR_OOM: return "out of memory";
+        case VT_ERR_CUDA: return "CUDA error";
+        case VT_ERR_CAPACITY: return "capacity exceeded";
+        case VT_ERR_TIMEOUT: return "device wait timed out";
+        case VT_ERR_NO_DEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+const char* vt_last_error(void) { return g_last_error.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,739 @@
+// vt_pipeline.cu -- grid build, neighbour search, pair list, cells, periodic dedup,
+// output compaction and totals.  All arithmetic here is FP64 and follows the reference
+// operation by operation (compiled with --fmad=false).
+#include <cfloat>
+
+#include "vt_geom.cuh"
+#include "vt_pipeline.cuh"
+
+namespace vt {
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kSearchWarps = 4;  // warps per block of the search kernels
+constexpr int kCellWarps = 8;
+
+__device__ __forceinline__ Sph<double> sph_of(double4 v) { return {{v.x, v.y, v.z}, v.w}; }
+
+// ---- prepare: R = r + probe (types.rs:58-63) and the bounding-box partials ----
+__global__ void k_prepare(const double* __restrict__ xyzr, uint32_t n, double probe, double4* __restrict__ sph,
+                          uint32_t* __restrict__ slot_id, BBox* __restrict__ partials, uint32_t* __restrict__ err) {
+    __shared__ double s[7][kBlock];
+    double mn0 = DBL_MAX, mn1 = DBL_MAX, mn2 = DBL_MAX, mx0 = -DBL_MAX, mx1 = -DBL_MAX, mx2 = -DBL_MAX, mr = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double x = xyzr[4 * (size_t)i], y = xyzr[4 * (size_t)i + 1], z = xyzr[4 * (size_t)i + 2];
+        double r = xyzr[4 * (size_t)i + 3];
+        double R = r + probe;
+        if (!isfinite(x) || !isfinite(y) || !isfinite(z) || !isfinite(r) || r < 0.0) atomicOr(err, (uint32_t)kErrInvalid);
+        sph[i] = make_double4(x, y, z, R);
+        slot_id[i] = i;
+        mn0 = fmin(mn0, x);
+        mn1 = fmin(mn1, y);
+        mn2 = fmin(mn2, z);
+        mx0 = fmax(mx0, x);
+        mx1 = fmax(mx1, y);
+        mx2 = fmax(mx2, z);
+        mr = fmax(mr, R);
+    }
+    int t = threadIdx.x;
+    s[0][t] = mn0;
+    s[1][t] = mn1;
+    s[2][t] = mn2;
+    s[3][t] = mx0;
+    s[4][t] = mx1;
+    s[5][t] = mx2;
+    s[6][t] = mr;
+    __syncthreads();
+    for (int o = kBlock / 2; o > 0; o >>= 1) {
+        if (t < o) {
+            for (int k = 0; k < 3; ++k) s[k][t] = fmin(s[k][t], s[k][t + o]);
+            for (int k = 3; k < 7; ++k) s[k][t] = fmax(s[k][t], s[k][t + o]);
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        BBox b;
+        for (int k = 0; k < 3; ++k) {
+            b.mn[k] = s[k][0];
+            b.mx[k] = s[k + 3][0];
+        }
+        b.max_r = s[6][0];
+        partials[blockIdx.x] = b;
+    }
+}
+
+__global__ void k_bbox_final(const BBox* __restrict__ p, int nb, BBox* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    BBox b = p[0];
+    for (int i = 1; i < nb; ++i) {
+        for (int k = 0; k < 3; ++k) {
+            b.mn[k] = fmin(b.mn[k], p[i].mn[k]);
+            b.mx[k] = fmax(b.mx[k], p[i].mx[k]);
+        }
+        b.max_r = fmax(b.max_r, p[i].max_r);
+    }
+    *out = b;
+}
+
+// ---- periodic images (types.rs:323-375): only images within `reach` of the balls'
+// bounding box can intersect a ball, so only those are materialised.
+__device__ __forceinline__ void neighbor_shift(int g, int& sx, int& sy, int& sz) {
+    int k = g < 13 ? g : g + 1;  // NEIGHBOR_SHIFTS skips the origin (index 13 of 27)
+    sx = k / 9 - 1;
+    sy = (k / 3) % 3 - 1;
+    sz = k % 3 - 1;
+}
+__device__ __forceinline__ double4 shift_sphere(double4 s, const double* pb, double wa, double wb, double wc) {
+    // PeriodicBox::shift_sphere (types.rs:323-347): c.mul_add(wc, b.mul_add(wb, a.mul_add(wa, x)))
+    return make_double4(fma(pb[6], wc, fma(pb[3], wb, fma(pb[0], wa, s.x))),
+                        fma(pb[7], wc, fma(pb[4], wb, fma(pb[1], wa, s.y))),
+                        fma(pb[8], wc, fma(pb[5], wb, fma(pb[2], wa, s.z))), s.w);
+}
+struct PBoxArg {
+    double v[9];
+};
+__device__ __forceinline__ bool in_reach(double4 p, const BBox& bb, double reach) {
+    return p.x >= bb.mn[0] - reach && p.x <= bb.mx[0] + reach && p.y >= bb.mn[1] - reach &&
+           p.y <= bb.mx[1] + reach && p.z >= bb.mn[2] - reach && p.z <= bb.mx[2] + reach;
+}
+__global__ void k_image_count(const double4* __restrict__ sph, uint32_t n, PBoxArg pb, const BBox* __restrict__ bb,
+                              double reach, uint32_t* __restrict__ cnt) {
+    BBox b = *bb;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        double4 s = sph[j];
+        uint32_t c = 0;
+        for (int g = 0; g < 26; ++g) {
+            int sx, sy, sz;
+            neighbor_shift(g, sx, sy, sz);
+            if (in_reach(shift_sphere(s, pb.v, sx, sy, sz), b, reach)) ++c;
+        }
+        cnt[j] = c;
+    }
+}
+__global__ void k_image_fill(double4* __restrict__ sph, uint32_t* __restrict__ slot_id, uint32_t n, PBoxArg pb,
+                             const BBox* __restrict__ bb, double reach, const uint32_t* __restrict__ off,
+                             uint32_t* __restrict__ d_nslots) {
+    BBox b = *bb;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        double4 s = sph[j];
+        uint32_t o = n + off[j];
+        for (int g = 0; g < 26; ++g) {
+            int sx, sy, sz;
+            neighbor_shift(g, sx, sy, sz);
+            double4 p = shift_sphere(s, pb.v, sx, sy, sz);
+            if (in_reach(p, b, reach)) {
+                sph[o] = p;
+                slot_id[o] = (uint32_t)(g + 1) * n + j;
+                ++o;
+            }
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d_nslots = n + off[n];
+}
+
+// ---- uniform grid: counting sort of the slots by cell ----
+__device__ __forceinline__ int cell_coord(double x, double o, double cell, int d) {
+    double f = floor((x - o) / cell);
+    int c = f < 0.0 ? 0 : (f > (double)(d - 1) ? d - 1 : (int)f);
+    return c;
+}
+__device__ __forceinline__ uint32_t cell_key(const GridDev& g, int x, int y, int z) {
+    return (uint32_t)x + (uint32_t)g.dx * ((uint32_t)y + (uint32_t)g.dy * (uint32_t)z);
+}
+__device__ __forceinline__ uint32_t slot_cell(const GridDev& g, double4 p) {
+    return cell_key(g, cell_coord(p.x, g.ox, g.cell, g.dx), cell_coord(p.y, g.oy, g.cell, g.dy),
+                    cell_coord(p.z, g.oz, g.cell, g.dz));
+}
+__global__ void k_cell_hist(const double4* __restrict__ sph, const uint32_t* __restrict__ d_nslots, GridDev g,
+                            uint32_t* __restrict__ cnt) {
+    uint32_t ns = *d_nslots;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < ns; s += gridDim.x * blockDim.x)
+        atomicAdd(&cnt[slot_cell(g, sph[s])], 1u);
+}
+__global__ void k_cell_scatter(const double4* __restrict__ sph, const uint32_t* __restrict__ slot_id,
+                               const uint32_t* __restrict__ d_nslots, GridDev g, uint32_t* __restrict__ cursor,
+                               double4* __restrict__ c_pos, uint32_t* __restrict__ c_id, uint32_t* __restrict__ c_slot) {
+    uint32_t ns = *d_nslots;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < ns; s += gridDim.x * blockDim.x) {
+        double4 p = sph[s];
+        uint32_t at = atomicAdd(&cursor[slot_cell(g, p)], 1u);
+        c_pos[at] = p;
+        c_id[at] = slot_id[s];
+        c_slot[at] = s;
+    }
+}
+
+// ---- neighbour search: find_colliding_ids (spheres_searcher.rs:253-326), one warp per
+// ball over the 3x3x3 cell stencil (9 contiguous rows of 3 cells in key order).
+__device__ __forceinline__ bool same_group(const int32_t* g, uint64_t ng, uint32_t a, uint32_t b) {
+    return g != nullptr && a < ng && b < ng && g[a] == g[b];  // tessellation.rs:323-328
+}
+__device__ __forceinline__ bool vless(double va, uint32_t ia, double vb, uint32_t ib) {
+    // ValuedId::cmp (types.rs:176-184): by value, ties and NaN by index
+    if (va < vb) return true;
+    if (va > vb) return false;
+    return ia < ib;
+}
+
+template <bool FILL>
+__global__ void __launch_bounds__(kSearchWarps * 32) k_search(DevBufs b, int want_rel) {
+    __shared__ double s_val[kSearchWarps][kSortCap];
+    __shared__ uint32_t s_id[kSearchWarps][kSortCap];
+    __shared__ uint32_t s_slot[kSearchWarps][kSortCap];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const GridDev g = b.grid;
+    const uint32_t n = b.n;
+    Dec<double, false> d;
+    for (uint32_t i = blockIdx.x * kSearchWarps + w; i < n; i += gridDim.x * kSearchWarps) {
+        const double4 A4 = b.sph[i];
+        const Sph<double> A = sph_of(A4);
+        int cx = cell_coord(A4.x, g.ox, g.cell, g.dx), cy = cell_coord(A4.y, g.oy, g.cell, g.dy),
+            cz = cell_coord(A4.z, g.oz, g.cell, g.dz);
+        uint32_t rbeg = 0, rcnt = 0;
+        if (lane < 9) {
+            int y = cy + lane / 3 - 1, z = cz + lane % 3 - 1;
+            if (y >= 0 && y < g.dy && z >= 0 && z < g.dz) {
+                int x0 = cx > 0 ? cx - 1 : 0, x1 = cx + 1 < g.dx ? cx + 1 : g.dx - 1;
+                rbeg = b.cell_start[cell_key(g, x0, y, z)];
+                rcnt = b.cell_start[cell_key(g, x1, y, z) + 1] - rbeg;
+            }
+        }
+        uint32_t incl = rcnt;
+        for (int o = 1; o < 16; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        uint32_t total = __shfl_sync(0xffffffffu, incl, 8);
+        uint32_t r_incl[9], r_beg[9];
+#pragma unroll
+        for (int r = 0; r < 9; ++r) {
+            r_incl[r] = __shfl_sync(0xffffffffu, incl, r);
+            r_beg[r] = __shfl_sync(0xffffffffu, rbeg, r);
+        }
+        uint32_t hits = 0;
+        bool hidden = false;
+        for (uint32_t t0 = 0; t0 < total && !hidden; t0 += 32) {
+            uint32_t t = t0 + lane;
+            bool hit = false, hid = false;
+            double val = 0.0;
+            uint32_t cid = 0, cslot = 0;
+            if (t < total) {
+                int r = 0;
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    if (r_incl[k] <= t) r = k + 1;
+                uint32_t prev = r == 0 ? 0 : r_incl[r - 1];
+                uint32_t idx = r_beg[r] + (t - prev);
+                cid = b.c_id[idx];
+                if (cid != i) {
+                    const Sph<double> C = sph_of(b.c_pos[idx]);
+                    if (sphere_intersects(d, A, C, 0.0)) {
+                        // hidden central ball (spheres_searcher.rs:295-303)
+                        bool eqs = fabs(C.r - A.r) <= kEps && fabs(C.c.x - A.c.x) <= kEps &&
+                                   fabs(C.c.y - A.c.y) <= kEps && fabs(C.c.z - A.c.z) <= kEps;
+                        if (sphere_contains(d, C, A, 0.0, 0.0) && (!eqs || i > cid)) {
+                            hid = true;
+                        } else if (!sphere_contains(d, A, C, 0.0, 0.0)) {  // :305-310
+                            hit = true;
+                            val = dist_to_ic_center(A, C);  // :312-316
+                            cslot = b.c_slot[idx];
+                        }
+                    }
+                }
+            }
+            if (__any_sync(0xffffffffu, hid)) {
+                hidden = true;
+                break;
+            }
+            unsigned m = __ballot_sync(0xffffffffu, hit);
+            uint32_t pos = hits + __popc(m & ((1u << lane) - 1u));
+            if (FILL && hit && pos < (uint32_t)kSortCap) {
+                s_val[w][pos] = val;
+                s_id[w][pos] = cid;
+                s_slot[w][pos] = cslot;
+            }
+            if (!FILL && hit && pos < (uint32_t)kSortCap) s_id[w][pos] = cid;
+            hits += __popc(m);
+        }
+        uint32_t cnt = hidden ? 0 : hits;
+        if (cnt > (uint32_t)kSortCap) {
+            if (lane == 0) atomicOr(b.err, (uint32_t)kErrNeighborCap);
+            cnt = 0;
+        }
+        __syncwarp();
+        if (!FILL) {
+            uint32_t np = 0;
+            for (uint32_t e = lane; e < cnt; e += 32) {
+                uint32_t bid = s_id[w][e];
+                uint32_t bc = b.periodic ? bid % n : bid;
+                bool gen = !same_group(b.groups, b.n_groups, i, bc) && ((b.periodic && bid >= n) || i < bid);
+                np += gen ? 1u : 0u;
+            }
+            for (int o = 16; o > 0; o >>= 1) np += __shfl_xor_sync(0xffffffffu, np, o);
+            if (lane == 0) {
+                b.nb_cnt[i] = cnt;
+                b.nb_npair[i] = np;
+                b.excluded[i] = hidden ? 1 : 0;
+            }
+            __syncwarp();
+            continue;
+        }
+        // bitonic sort of (value, id) (spheres_searcher.rs:324)
+        uint32_t n2 = 2;
+        while (n2 < cnt) n2 <<= 1;
+        for (uint32_t e = cnt + lane; e < n2; e += 32) {
+            s_val[w][e] = INFINITY;
+            s_id[w][e] = 0xffffffffu;
+            s_slot[w][e] = 0;
+        }
+        __syncwarp();
+        if (cnt > 1) {
+            for (uint32_t k = 2; k <= n2; k <<= 1) {
+                for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
+                    for (uint32_t t = lane; t < n2; t += 32) {
+                        uint32_t ixj = t ^ jj;
+                        if (ixj > t) {
+                            bool up = (t & k) == 0;
+                            double vt = s_val[w][t], vx = s_val[w][ixj];
+                            uint32_t it = s_id[w][t], ix = s_id[w][ixj];
+                            bool sw = up ? vless(vx, ix, vt, it) : vless(vt, it, vx, ix);
+                            if (sw) {
+                                s_val[w][t] = vx;
+                                s_val[w][ixj] = vt;
+                                s_id[w][t] = ix;
+                                s_id[w][ixj] = it;
+                                uint32_t st = s_slot[w][t];
+                                s_slot[w][t] = s_slot[w][ixj];
+                                s_slot[w][ixj] = st;
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+        const uint32_t off = b.nb_off[i];
+        uint32_t prank = b.pair_off[i];
+        for (uint32_t e0 = 0; e0 < cnt; e0 += 32) {
+            uint32_t e = e0 + lane;
+            bool gen = false;
+            uint32_t bid = 0, bslot = 0;
+            if (e < cnt) {
+                bid = s_id[w][e];
+                bslot = s_slot[w][e];
+                uint32_t bc = b.periodic ? bid % n : bid;
+                gen = !same_group(b.groups, b.n_groups, i, bc) && ((b.periodic && bid >= n) || i < bid);
+            }
+            unsigned m = __ballot_sync(0xffffffffu, gen);
+            if (e < cnt) {
+                b.nb_id[off + e] = bid;
+                b.nb_slot[off + e] = bslot;
+                b.nb_val[off + e] = s_val[w][e];
+                int32_t pidx = -1;
+                if (gen) {
+                    pidx = (int32_t)(prank + __popc(m & ((1u << lane) - 1u)));
+                    b.pair_a[pidx] = i;
+                    b.pair_e[pidx] = off + e;
+                }
+                b.nb_pair[off + e] = pidx;
+                if (want_rel) {
+                    double4 C = b.sph[bslot];
+                    b.nb_rel[off + e] = make_float4((float)(C.x - A4.x), (float)(C.y - A4.y), (float)(C.z - A4.z),
+                                                    (float)C.w);
+                }
+            }
+            prank += __popc(m);
+        }
+        __syncwarp();
+    }
+}
+
+// ---- cells: compute_cells (tessellation.rs:607-658) as a per-ball warp reduction ----
+__device__ __forceinline__ double wsum_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__global__ void __launch_bounds__(kCellWarps * 32) k_cells(DevBufs b) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t n = b.n;
+    for (uint32_t i = blockIdx.x * kCellWarps + w; i < n; i += gridDim.x * kCellWarps) {
+        const uint32_t cnt = b.nb_cnt[i], off = b.nb_off[i];
+        const double4 Si = b.sph[i];
+        double area = 0, arc = 0, spos = 0, sneg = 0, ppos = 0, pneg = 0;
+        uint32_t count = 0;
+        for (uint32_t e = lane; e < cnt; e += 32) {
+            uint32_t j = b.nb_id[off + e];
+            int32_t p = -1;
+            bool side_a = true;
+            if ((b.periodic && j >= n) || j > i) {
+                p = b.nb_pair[off + e];
+            } else {
+                // mirror entry: i in j's sorted list, located by its (value, id) key
+                double v = dist_to_ic_center(sph_of(b.sph[j]), sph_of(Si));
+                uint32_t lo = b.nb_off[j], hi = lo + b.nb_cnt[j];
+                while (lo < hi) {
+                    uint32_t mid = (lo + hi) >> 1;
+                    if (vless(b.nb_val[mid], b.nb_id[mid], v, i))
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                if (lo < b.nb_off[j] + b.nb_cnt[j] && b.nb_id[lo] == i) {
+                    p = b.nb_pair[lo];
+                    side_a = false;
+                }
+            }
+            if (p >= 0 && (b.p_status[p] & kValid)) {
+                double sa = side_a ? b.p_sa_a[p] : b.p_sa_b[p];
+                double pv = side_a ? b.p_pv_a[p] : b.p_pv_b[p];
+                ++count;
+                area += b.p_area[p];
+                arc += b.p_arc[p];
+                spos += fmax(sa, 0.0);
+                sneg -= fmin(sa, 0.0);
+                ppos += fmax(pv, 0.0);
+                pneg -= fmin(pv, 0.0);
+            }
+        }
+        area = wsum_d(area);
+        arc = wsum_d(arc);
+        spos = wsum_d(spos);
+        sneg = wsum_d(sneg);
+        ppos = wsum_d(ppos);
+        pneg = wsum_d(pneg);
+        for (int o = 16; o > 0; o >>= 1) count += __shfl_xor_sync(0xffffffffu, count, o);
+        if (lane == 0) {
+            const double r = Si.w;
+            uint8_t flag = 0;
+            double sas = 0.0, vol = 0.0;
+            if (count > 0) {  // CellContactSummary::compute_sas (types.rs:623-663)
+                flag = 1;
+                double diff = fabs(spos - sneg);
+                if (arc > 0.0 && diff > 1e-10) {
+                    if (spos > sneg) {
+                        sas = fma(4.0, kPi, -fmax(spos - sneg, 0.0)) * r * r;
+                    } else {
+                        sas = fmax(sneg - spos, 0.0) * r * r;
+                    }
+                    vol = (sas * r / 3.0) + ppos - pneg;
+                    double full = 4.0 / 3.0 * kPi * r * r * r;
+                    if (vol > full) {
+                        sas = 0.0;
+                        vol = ppos - pneg;
+                    }
+                } else {
+                    vol = ppos - pneg;
+                }
+            } else if (cnt == 0) {  // compute_sas_detached (types.rs:666-675)
+                flag = 1;
+                sas = 4.0 * kPi * r * r;
+                vol = sas * r / 3.0;
+            }
+            b.cell_flag[i] = flag;
+            b.cell_sas[i] = sas;
+            b.cell_vol[i] = vol;
+        }
+    }
+}
+
+// ---- periodic dedup ----
+// Full tessellation: compute_canonical_ids (tessellation.rs:556-601) keeps, among the
+// boundary contacts (an id >= n), the first one in pair order per unordered canonical
+// pair.  Contacts-only: deduplicate_and_canonicalize_contacts (tessellation.rs:172-188)
+// keeps the first contact per canonical pair among all contacts.  Pair order is a-major,
+// so earlier contacts with the same key sit in a's range before p or, when the canonical
+// partner c is smaller than a, anywhere in c's range.
+__device__ __forceinline__ bool earlier_same_key(const DevBufs& b, uint32_t lo, uint32_t hi, uint32_t want,
+                                                 bool boundary_only) {
+    const uint32_t n = b.n;
+    for (uint32_t q = lo; q < hi; ++q) {
+        if (!(b.p_status[q] & kValid)) continue;
+        uint32_t bid = b.nb_id[b.pair_e[q]];
+        if (boundary_only && bid < n) continue;
+        if (bid % n == want) return true;
+    }
+    return false;
+}
+__global__ void k_dedup(DevBufs b, uint32_t P, int contacts_only) {
+    const uint32_t n = b.n;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+        uint32_t keep = 0;
+        if (b.p_status[p] & kValid) {
+            keep = 1;
+            uint32_t a = b.pair_a[p];
+            uint32_t bid = b.nb_id[b.pair_e[p]];
+            bool boundary = bid >= n;
+            if (contacts_only || boundary) {
+                uint32_t c = bid % n;
+                bool bo = !contacts_only;
+                if (earlier_same_key(b, b.pair_off[a], p, c, bo)) keep = 0;
+                if (keep && c < a && earlier_same_key(b, b.pair_off[c], b.pair_off[c + 1], a, bo)) keep = 0;
+            }
+        }
+        b.keep[p] = keep;
+    }
+}
+__global__ void k_keep_plain(DevBufs b, uint32_t P) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x)
+        b.keep[p] = (b.p_status[p] & kValid) ? 1u : 0u;
+}
+__global__ void k_cell_keep(DevBufs b, uint32_t* flags32) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.n; i += gridDim.x * blockDim.x)
+        flags32[i] = b.cell_flag[i];
+}
+
+// ---- output compaction (pair order, which is the reference's output order) ----
+__global__ void k_compact_contacts(DevBufs b, uint32_t P, int contacts_only) {
+    const uint32_t n = b.n;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+        uint32_t o = b.keep_off[p];
+        if (b.keep_off[p + 1] == o) continue;
+        uint32_t a = b.pair_a[p];
+        uint32_t bid = b.nb_id[b.pair_e[p]];
+        uint32_t ia = a, ib = bid;
+        if (b.periodic) {
+            ia = a % n;
+            ib = bid % n;
+            if (contacts_only && ib < ia) {  // canonical (min, max)
+                uint32_t t = ia;
+                ia = ib;
+                ib = t;
+            }
+        }
+        b.out_a[o] = ia;
+        b.out_b[o] = ib;
+        b.out_area[o] = b.p_area[p];
+        b.out_arc[o] = b.p_arc[p];
+        b.out_central[o] = b.p_central[p];
+    }
+}
+__global__ void k_compact_cells(DevBufs b) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.n; i += gridDim.x * blockDim.x) {
+        uint32_t o = b.cell_off[i];
+        if (b.cell_off[i + 1] == o) continue;
+        b.out_cell_index[o] = i;
+        b.out_cell_sas[o] = b.cell_sas[i];
+        b.out_cell_vol[o] = b.cell_vol[i];
+    }
+}
+
+// ---- deterministic totals: fixed grid, fixed tree ----
+constexpr int kSumBlocks = 148;
+__global__ void k_partial_sums(const double* __restrict__ x0, const uint32_t* __restrict__ cnt0,
+                               const double* __restrict__ x1, const double* __restrict__ x2,
+                               const uint32_t* __restrict__ cnt1, double* __restrict__ partials) {
+    __shared__ double s[3][kBlock];
+    uint32_t c0 = *cnt0, c1 = *cnt1;
+    double a0 = 0, a1 = 0, a2 = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c0; i += gridDim.x * blockDim.x) a0 += x0[i];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c1; i += gridDim.x * blockDim.x) {
+        a1 += x1[i];
+        a2 += x2[i];
+    }
+    int t = threadIdx.x;
+    s[0][t] = a0;
+    s[1][t] = a1;
+    s[2][t] = a2;
+    __syncthreads();
+    for (int o = kBlock / 2; o > 0; o >>= 1) {
+        if (t < o)
+            for (int k = 0; k < 3; ++k) s[k][t] += s[k][t + o];
+        __syncthreads();
+    }
+    if (t < 3) partials[blockIdx.x * 3 + t] = s[t][0];
+}
+__global__ void k_final_sums(const double* __restrict__ partials, double* __restrict__ totals) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double a = 0, s = 0, v = 0;
+    for (int k = 0; k < kSumBlocks; ++k) {
+        a += partials[3 * k];
+        s += partials[3 * k + 1];
+        v += partials[3 * k + 2];
+    }
+    totals[0] = s;
+    totals[1] = v;
+    totals[2] = a;
+}
+
+// ---- pairs that must be recomputed (FP32 unsure -> FP64 warp; overflow -> serial) ----
+__global__ void k_collect_redo(DevBufs b, uint32_t P) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+        uint8_t st = b.p_status[p];
+        if (st & kOverflow) {
+            uint32_t at = atomicAdd(b.d_serial_count, 1u);
+            b.serial_list[at] = p;
+        } else if (st & kUnsure) {
+            uint32_t at = atomicAdd(b.d_redo_count, 1u);
+            b.redo_list[at] = p;
+        }
+    }
+}
+
+// ---- exclusive scan of u32 (3 phases: tile sums, scan of tile sums, tile scan) ----
+constexpr int kScanThreads = 1024;
+constexpr int kScanPer = 4;
+constexpr int kTile = kScanThreads * kScanPer;
+
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* total) {
+    __shared__ uint32_t ws[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += t;
+    }
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t y = lane < (int)(blockDim.x >> 5) ? ws[lane] : 0u;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += t;
+        }
+        ws[lane] = y;
+    }
+    __syncthreads();
+    uint32_t before = w > 0 ? ws[w - 1] : 0u;
+    *total = ws[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return before + x - v;
+}
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const uint32_t* __restrict__ in, size_t n,
+                                                             uint32_t* __restrict__ tile_sums) {
+    size_t base = (size_t)blockIdx.x * kTile + (size_t)threadIdx.x * kScanPer;
+    uint32_t s = 0;
+    for (int k = 0; k < kScanPer; ++k)
+        if (base + k < n) s += in[base + k];
+    uint32_t total;
+    block_excl_scan(s, &total);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(uint32_t* __restrict__ sums, size_t ntiles) {
+    // single block: exclusive scan of the tile sums in chunks, carrying the prefix
+    uint32_t carry = 0;
+    for (size_t base = 0; base < ntiles; base += kScanThreads) {
+        size_t i = base + threadIdx.x;
+        uint32_t v = i < ntiles ? sums[i] : 0u;
+        uint32_t total;
+        uint32_t ex = block_excl_scan(v, &total);
+        if (i < ntiles) sums[i] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) sums[ntiles] = carry;
+}
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(const uint32_t* __restrict__ in, size_t n,
+                                                             const uint32_t* __restrict__ tile_off,
+                                                             uint32_t* __restrict__ out, size_t ntiles) {
+    size_t base = (size_t)blockIdx.x * kTile + (size_t)threadIdx.x * kScanPer;
+    uint32_t v[kScanPer];
+    uint32_t s = 0;
+    for (int k = 0; k < kScanPer; ++k) {
+        v[k] = base + k < n ? in[base + k] : 0u;
+        s += v[k];
+    }
+    uint32_t total;
+    uint32_t ex = block_excl_scan(s, &total) + tile_off[blockIdx.x];
+    for (int k = 0; k < kScanPer; ++k) {
+        if (base + k < n) out[base + k] = ex;
+        ex += v[k];
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = tile_off[ntiles];
+}
+
+int grid_for(size_t n, int block, int cap = 148 * 16) {
+    size_t g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > (size_t)cap) g = cap;
+    return (int)g;
+}
+
+}  // namespace
+
+size_t scan_tmp_words_needed(size_t n) { return (n + kTile - 1) / kTile + 2; }
+
+void scan_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* tmp, cudaStream_t s) {
+    size_t ntiles = (n + kTile - 1) / kTile;
+    if (ntiles == 0) {
+        cudaMemsetAsync(out, 0, sizeof(uint32_t), s);
+        return;
+    }
+    k_scan_tiles<<<(unsigned)ntiles, kScanThreads, 0, s>>>(in, n, tmp);
+    k_scan_sums<<<1, kScanThreads, 0, s>>>(tmp, ntiles);
+    k_scan_apply<<<(unsigned)ntiles, kScanThreads, 0, s>>>(in, n, tmp, out, ntiles);
+}
+
+void launch_prepare(const DevBufs& b, const double* d_xyzr, double probe, BBox* d_parts, int nblocks,
+                    cudaStream_t s) {
+    k_prepare<<<nblocks, kBlock, 0, s>>>(d_xyzr, b.n, probe, b.sph, b.slot_id, d_parts, b.err);
+}
+void launch_bbox_final(const BBox* parts, int nblocks, BBox* out, cudaStream_t s) {
+    k_bbox_final<<<1, 32, 0, s>>>(parts, nblocks, out);
+}
+void launch_images(const DevBufs& b, double reach, const BBox* d_bbox, uint32_t* img_cnt, uint32_t* img_off,
+                   uint32_t* scan_tmp, size_t, cudaStream_t s) {
+    PBoxArg pb;
+    for (int k = 0; k < 9; ++k) pb.v[k] = b.pbox[k];
+    int gb = grid_for(b.n, kBlock);
+    k_image_count<<<gb, kBlock, 0, s>>>(b.sph, b.n, pb, d_bbox, reach, img_cnt);
+    scan_u32(img_cnt, img_off, b.n, scan_tmp, s);
+    k_image_fill<<<gb, kBlock, 0, s>>>(b.sph, b.slot_id, b.n, pb, d_bbox, reach, img_off, b.d_nslots);
+}
+void launch_grid(const DevBufs& b, uint32_t ncell, uint32_t max_slots, uint32_t* scan_tmp, size_t, cudaStream_t s) {
+    cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * ncell, s);
+    int gb = grid_for(max_slots, kBlock);
+    k_cell_hist<<<gb, kBlock, 0, s>>>(b.sph, b.d_nslots, b.grid, b.cell_count);
+    scan_u32(b.cell_count, b.cell_start, ncell, scan_tmp, s);
+    cudaMemcpyAsync(b.cell_cursor, b.cell_start, sizeof(uint32_t) * ncell, cudaMemcpyDeviceToDevice, s);
+    k_cell_scatter<<<gb, kBlock, 0, s>>>(b.sph, b.slot_id, b.d_nslots, b.grid, b.cell_cursor, b.c_pos, b.c_id,
+                                         b.c_slot);
+}
+void launch_search_count(const DevBufs& b, cudaStream_t s) {
+    int gb = grid_for(b.n, kSearchWarps, 148 * 64);
+    k_search<false><<<gb, kSearchWarps * 32, 0, s>>>(b, 0);
+}
+void launch_search_fill(const DevBufs& b, int want_rel, cudaStream_t s) {
+    int gb = grid_for(b.n, kSearchWarps, 148 * 64);
+    k_search<true><<<gb, kSearchWarps * 32, 0, s>>>(b, want_rel);
+}
+void launch_cells(const DevBufs& b, cudaStream_t s) {
+    int gb = grid_for(b.n, kCellWarps, 148 * 32);
+    k_cells<<<gb, kCellWarps * 32, 0, s>>>(b);
+}
+void launch_dedup(const DevBufs& b, uint32_t P, int contacts_only, cudaStream_t s) {
+    int gb = grid_for(P, kBlock);
+    if (b.periodic)
+        k_dedup<<<gb, kBlock, 0, s>>>(b, P, contacts_only);
+    else
+        k_keep_plain<<<gb, kBlock, 0, s>>>(b, P);
+}
+void launch_compact(const DevBufs& b, uint32_t P, int contacts_only, uint32_t* scan_tmp, size_t, cudaStream_t s) {
+    scan_u32(b.keep, b.keep_off, P, scan_tmp, s);
+    k_compact_contacts<<<grid_for(P, kBlock), kBlock, 0, s>>>(b, P, contacts_only);
+    if (!contacts_only) {
+        // cell flags (u8) widened into the keep buffer's tail is avoided: use params_u
+        k_cell_keep<<<grid_for(b.n, kBlock), kBlock, 0, s>>>(b, b.params_u);
+        scan_u32(b.params_u, b.cell_off, b.n, scan_tmp, s);
+        k_compact_cells<<<grid_for(b.n, kBlock), kBlock, 0, s>>>(b);
+    }
+}
+void launch_totals(const DevBufs& b, uint32_t P, int contacts_only, cudaStream_t s) {
+    const uint32_t* ccount = b.keep_off + P;
+    const uint32_t* ncell = contacts_only ? b.keep_off + P : b.cell_off + b.n;
+    if (contacts_only) {
+        // no cells: the cell sums read zero elements from a zero count
+        k_partial_sums<<<kSumBlocks, kBlock, 0, s>>>(b.out_area, ccount, b.out_area, b.out_area, b.zero_word,
+                                                     b.partials);
+    } else {
+        k_partial_sums<<<kSumBlocks, kBlock, 0, s>>>(b.out_area, ccount, b.out_cell_sas, b.out_cell_vol, ncell,
+                                                     b.partials);
+    }
+    k_final_sums<<<1, 32, 0, s>>>(b.partials, b.totals);
+}
+void launch_collect_redo(const DevBufs& b, uint32_t P, cudaStream_t s) {
+    cudaMemsetAsync(b.d_redo_count, 0, sizeof(uint32_t), s);
+    cudaMemsetAsync(b.d_serial_count, 0, sizeof(uint32_t), s);
+    k_collect_redo<<<grid_for(P, kBlock), kBlock, 0, s>>>(b, P);
+}
+
+}  // namespace vt

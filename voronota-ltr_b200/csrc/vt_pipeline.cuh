@@ -1,0 +1,147 @@
+// vt_pipeline.cuh -- device buffers and kernel launchers of the tessellation pipeline.
+//
+// Data layout in HBM (n balls, m periodic images, E neighbour entries, P pairs):
+//   sph      double4[n + m]  x, y, z, R (= r + probe) per slot; slots 0..n-1 are the balls,
+//                            slots n.. the periodic images within reach of the structure
+//   slot_id  u32[n + m]      reference id of the slot: i for balls, (g+1) n + j for the image
+//                            of ball j under NEIGHBOR_SHIFTS[g] (types.rs:351-375)
+//   grid     cell_start u32[ncell+1], c_pos double4 / c_id u32 / c_slot u32 [n + m]
+//            (slots sorted by cell: a counting sort on the cell key)
+//   CSR      nb_off u32[n+1]; nb_id, nb_slot u32[E]; nb_val f64[E]; nb_pair i32[E];
+//            nb_rel float4[E] (FP32 path: neighbour centre relative to the ball, and R)
+//   pairs    pair_a u32[P], pair_e u32[P] (CSR entry of b in a's list)
+//   per pair status u8, area, arc, solid angles a/b, pyramid volumes a/b f64, central u8
+//   cells    cell_flag u8[n], cell_sas f64[n], cell_vol f64[n]
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vt {
+
+// Error bits written by kernels into the engine's device status word.
+enum DevErr : uint32_t {
+    kErrNeighborCap = 1u,  // a ball has more neighbour candidates than the sort buffer holds
+    kErrOverflow = 2u,     // a contour exceeded the serial fallback's capacity
+    kErrIdRange = 4u,      // ids do not fit 32 bits
+    kErrInvalid = 8u,      // non-finite input value or negative radius
+};
+
+// Per-pair status bits.
+enum PairStatus : uint8_t {
+    kValid = 1,     // contact exists (area > 0)
+    kUnsure = 2,    // FP32 decision inside the band: recompute in FP64
+    kOverflow = 4,  // contour needed more than 32 points: recompute serially
+};
+
+constexpr int kSortCap = 256;       // neighbour list capacity of the warp sort buffer
+constexpr int kSerialCap = 256;     // contour capacity of the serial fallback
+
+struct GridDev {
+    double ox, oy, oz, cell;
+    int dx, dy, dz;
+};
+
+struct DevBufs {
+    // inputs / slots
+    double4* sph;
+    uint32_t* slot_id;
+    const int32_t* groups;
+    uint64_t n_groups;
+    uint32_t n;
+    uint32_t* d_nslots;  // device count of slots (n + images)
+    int periodic;
+    double pbox[9];
+    // grid
+    GridDev grid;
+    uint32_t* cell_count;
+    uint32_t* cell_start;
+    uint32_t* cell_cursor;
+    double4* c_pos;
+    uint32_t* c_id;
+    uint32_t* c_slot;
+    // CSR
+    uint32_t* nb_cnt;
+    uint32_t* nb_npair;
+    uint8_t* excluded;
+    uint32_t* nb_off;
+    uint32_t* pair_off;
+    uint32_t* nb_id;
+    uint32_t* nb_slot;
+    double* nb_val;
+    int32_t* nb_pair;
+    float4* nb_rel;
+    // pairs
+    uint32_t* pair_a;
+    uint32_t* pair_e;
+    uint8_t* p_status;
+    double* p_area;
+    double* p_arc;
+    uint8_t* p_central;
+    double* p_sa_a;
+    double* p_sa_b;
+    double* p_pv_a;
+    double* p_pv_b;
+    // recompute lists
+    uint32_t* redo_list;
+    uint32_t* d_redo_count;
+    uint32_t* serial_list;
+    uint32_t* d_serial_count;
+    double* serial_scratch;  // kSerialCap * 7 doubles per fallback slot
+    uint32_t serial_slots;
+    // cells
+    uint8_t* cell_flag;
+    double* cell_sas;
+    double* cell_vol;
+    // output compaction
+    uint32_t* keep;      // per pair 0/1, then scanned
+    uint32_t* keep_off;  // P+1
+    uint32_t* cell_off;  // n+1
+    uint32_t* out_a;
+    uint32_t* out_b;
+    double* out_area;
+    double* out_arc;
+    uint8_t* out_central;
+    uint32_t* out_cell_index;
+    double* out_cell_sas;
+    double* out_cell_vol;
+    double* totals;     // 3: sas, volume, contact area
+    double* partials;   // reduction scratch
+    uint32_t* err;        // device error bits
+    uint32_t* zero_word;  // a device word that stays 0 (an empty count)
+    uint32_t* params_u;   // n words of scratch (cell flags widened for the scan)
+};
+
+// Host-visible bounding-box reduction result.
+struct BBox {
+    double mn[3], mx[3], max_r;
+};
+
+// ---- launchers (vt_pipeline.cu) ----
+void launch_prepare(const DevBufs& b, const double* d_xyzr, double probe, BBox* d_bbox_partials, int nblocks,
+                    cudaStream_t s);
+void launch_bbox_final(const BBox* partials, int nblocks, BBox* out, cudaStream_t s);
+void launch_images(const DevBufs& b, double reach, const BBox* d_bbox, uint32_t* img_cnt, uint32_t* img_off,
+                   uint32_t* scan_tmp, size_t scan_tmp_words, cudaStream_t s);
+void launch_grid(const DevBufs& b, uint32_t ncell, uint32_t max_slots, uint32_t* scan_tmp, size_t scan_tmp_words,
+                 cudaStream_t s);
+void launch_search_count(const DevBufs& b, cudaStream_t s);
+void launch_search_fill(const DevBufs& b, int want_rel, cudaStream_t s);
+void launch_cells(const DevBufs& b, cudaStream_t s);
+void launch_dedup(const DevBufs& b, uint32_t P, int contacts_only, cudaStream_t s);
+void launch_compact(const DevBufs& b, uint32_t P, int contacts_only, uint32_t* scan_tmp, size_t scan_tmp_words,
+                    cudaStream_t s);
+void launch_totals(const DevBufs& b, uint32_t P, int contacts_only, cudaStream_t s);
+void launch_collect_redo(const DevBufs& b, uint32_t P, cudaStream_t s);
+size_t scan_tmp_words_needed(size_t n);
+void scan_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* tmp, cudaStream_t s);
+
+// ---- contact kernels (vt_contact64.cu / vt_contact32.cu) ----
+// mode: 0 = all pairs; 1 = pairs listed in redo_list (count on device)
+void launch_contact_f64(const DevBufs& b, uint32_t P, int full, int from_list, cudaStream_t s);
+void launch_contact_f32(const DevBufs& b, uint32_t P, int full, cudaStream_t s);
+void launch_contact_serial(const DevBufs& b, uint32_t P, int full, cudaStream_t s);
+// Upload the FP64 hexagon rotation table (sin/cos from the host C library) to the
+// current device; call once per device before the first FP64 contact launch.
+void set_hex_table();
+
+}  // namespace vt

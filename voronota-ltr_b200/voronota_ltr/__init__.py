@@ -1,0 +1,345 @@
+"""B200 radical tessellation -- Python front end mirroring voronota-ltr's bindings.
+
+``compute_tessellation`` takes the same arguments and returns the same dict as the
+reference's PyO3 function (src/python.rs:238-264, result_to_dict :189-210):
+balls as a list of (x, y, z, r) tuples / lists / {x, y, z, r} dicts or an (N, 4) numpy
+array; ``periodic_box`` as ``{"corners": [...]}`` or ``{"vectors": [...]}``; optional
+``groups``.  The work runs on the GPU through the C ABI of ``libvoronota_b200.so``
+(include/voronota_b200.h); there is no CPU fallback -- without the library or a CUDA
+device every call raises.
+
+Extra keyword: ``precision`` -- ``"fp32"`` (FP32 bulk geometry with FP64 recomputation
+of every pair whose decisions fall inside the FP32 error band; default) or ``"fp64"``
+(the reference's f64 arithmetic on the GPU).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Any
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libvoronota_b200.so")
+
+VT_OK = 0
+VT_ERR_INVALID = 1
+VT_ERR_OOM = 2
+VT_ERR_CUDA = 3
+VT_ERR_CAPACITY = 4
+VT_ERR_TIMEOUT = 5
+VT_ERR_NO_DEVICE = 6
+VT_FP64 = 0
+VT_FP32_FIXUP = 1
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_vp = ctypes.c_void_p
+
+
+class VoronotaError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+class VtStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in (
+        "num_balls", "num_slots", "num_entries", "num_pairs", "num_contacts", "num_cells",
+        "num_fp64_redo", "num_serial")] + [
+        ("total_sas_area", ctypes.c_double), ("total_volume", ctypes.c_double),
+        ("total_contact_area", ctypes.c_double), ("device_error_bits", ctypes.c_uint32)]
+
+
+class VtDeviceOutputs(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in (
+        "id_a", "id_b", "area", "arc_length", "central", "cell_index", "cell_sas_area",
+        "cell_volume", "totals")]
+
+
+_lib = None
+
+
+def library():
+    """Load libvoronota_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise VoronotaError(VT_ERR_CUDA, f"{LIB_PATH} is missing: build it with voronota-ltr_b200/build.py")
+    L = ctypes.CDLL(LIB_PATH)
+    args7 = [_f64p, ctypes.c_uint64, ctypes.c_double, _f64p, _i32p, ctypes.c_uint64, ctypes.c_int]
+    for name in ("vt_compute_tessellation", "vt_compute_contacts_only"):
+        f = getattr(L, name)
+        f.argtypes = args7 + [ctypes.POINTER(_vp)]
+        f.restype = ctypes.c_int
+    for name in ("vt_result_num_balls", "vt_result_num_contacts", "vt_result_num_cells"):
+        getattr(L, name).argtypes = [_vp]
+        getattr(L, name).restype = ctypes.c_uint64
+    L.vt_result_contacts.argtypes = [_vp, _u32p, _u32p, _f64p, _f64p, _u8p]
+    L.vt_result_cells.argtypes = [_vp, _u32p, _f64p, _f64p]
+    L.vt_result_totals.argtypes = [_vp, _f64p, _f64p, _f64p]
+    L.vt_result_totals.restype = None
+    L.vt_result_free.argtypes = [_vp]
+    L.vt_result_free.restype = None
+    L.vt_engine_create.argtypes = [ctypes.c_int, ctypes.POINTER(_vp)]
+    L.vt_engine_destroy.argtypes = [_vp]
+    L.vt_engine_destroy.restype = None
+    L.vt_engine_set_stream.argtypes = [_vp, _vp]
+    L.vt_engine_compute_device.argtypes = [_vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double, _f64p,
+                                           ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
+    L.vt_engine_compute_host.argtypes = [_vp, _f64p, ctypes.c_uint64, ctypes.c_double, _f64p, _i32p,
+                                         ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
+    L.vt_engine_download.argtypes = [_vp, ctypes.POINTER(_vp)]
+    L.vt_engine_stats.argtypes = [_vp, ctypes.POINTER(VtStats)]
+    L.vt_engine_device_outputs.argtypes = [_vp, ctypes.POINTER(VtDeviceOutputs)]
+    L.vt_status_string.argtypes = [ctypes.c_int]
+    L.vt_status_string.restype = ctypes.c_char_p
+    L.vt_last_error.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def _check(status: int) -> None:
+    if status != VT_OK:
+        L = library()
+        msg = L.vt_last_error().decode(errors="replace") or L.vt_status_string(status).decode()
+        raise VoronotaError(status, msg)
+
+
+def _precision_code(precision) -> int:
+    if precision in ("fp32", VT_FP32_FIXUP, "fp32_fixup"):
+        return VT_FP32_FIXUP
+    if precision in ("fp64", VT_FP64):
+        return VT_FP64
+    raise ValueError("precision must be 'fp32' or 'fp64'")
+
+
+# ---- input parsing (src/python.rs:21-120) ----
+def _ball_from_sequence(seq, type_name):
+    if len(seq) != 4:
+        raise ValueError(f"ball {type_name} must have 4 elements (x, y, z, r)")
+    return [float(seq[0]), float(seq[1]), float(seq[2]), float(seq[3])]
+
+
+def _parse_single_ball(obj):
+    if isinstance(obj, dict):
+        try:
+            return [float(obj["x"]), float(obj["y"]), float(obj["z"]), float(obj["r"])]
+        except KeyError as e:
+            raise KeyError(f"missing '{e.args[0]}'") from None
+    if isinstance(obj, tuple):
+        return _ball_from_sequence(obj, "tuple")
+    if isinstance(obj, list):
+        return _ball_from_sequence(obj, "list")
+    raise TypeError("ball must be tuple (x,y,z,r), list [x,y,z,r], or dict {x,y,z,r}")
+
+
+def parse_balls(obj) -> np.ndarray:
+    """(N, 4) contiguous float64 array from any accepted ball form."""
+    if isinstance(obj, np.ndarray):
+        if obj.ndim != 2 or obj.shape[1] != 4:
+            raise ValueError("numpy array must have shape (N, 4) for (x, y, z, r)")
+        return np.ascontiguousarray(obj, dtype=np.float64)
+    if not isinstance(obj, list):
+        raise TypeError("balls must be a list or a numpy array")
+    if len(obj) == 0:
+        return np.zeros((0, 4), np.float64)
+    return np.ascontiguousarray(np.array([_parse_single_ball(b) for b in obj], dtype=np.float64))
+
+
+def parse_periodic_box(obj) -> np.ndarray:
+    """9 doubles (lattice vectors a, b, c) from a corners / vectors dict (python.rs:90-120)."""
+    if not isinstance(obj, dict):
+        raise TypeError("periodic_box must be a dict")
+    if "corners" in obj:
+        c = [tuple(float(v) for v in p) for p in obj["corners"]]
+        if len(c) != 2:
+            raise ValueError("corners must have exactly 2 points")
+        (x1, y1, z1), (x2, y2, z2) = c
+        # PeriodicBox::from_corners (types.rs:304-310)
+        return np.array([x2 - x1, 0.0, 0.0, 0.0, y2 - y1, 0.0, 0.0, 0.0, z2 - z1], dtype=np.float64)
+    if "vectors" in obj:
+        v = [tuple(float(x) for x in p) for p in obj["vectors"]]
+        if len(v) != 3:
+            raise ValueError("vectors must have exactly 3 direction vectors")
+        return np.ascontiguousarray(np.array(v, dtype=np.float64).reshape(9))
+    raise ValueError("periodic_box must have 'corners' or 'vectors' key")
+
+
+def _groups_array(groups):
+    if groups is None:
+        return None
+    return np.ascontiguousarray(np.asarray(groups, dtype=np.int32).reshape(-1))
+
+
+class Result:
+    """Host copy of a tessellation result (numpy arrays)."""
+
+    def __init__(self, num_balls, id_a, id_b, area, arc_length, central, cell_index, cell_sas, cell_volume,
+                 totals):
+        self.num_balls = int(num_balls)
+        self.id_a, self.id_b = id_a, id_b
+        self.area, self.arc_length, self.central = area, arc_length, central
+        self.cell_index, self.cell_sas_area, self.cell_volume = cell_index, cell_sas, cell_volume
+        self.total_sas_area, self.total_volume, self.total_contact_area = totals
+
+    @classmethod
+    def from_handle(cls, L, h):
+        nc = L.vt_result_num_contacts(h)
+        a = np.empty(nc, np.uint32)
+        b = np.empty(nc, np.uint32)
+        ar = np.empty(nc, np.float64)
+        arc = np.empty(nc, np.float64)
+        ce = np.empty(nc, np.uint8)
+        _check(L.vt_result_contacts(h, a.ctypes.data_as(_u32p), b.ctypes.data_as(_u32p), ar.ctypes.data_as(_f64p),
+                                    arc.ctypes.data_as(_f64p), ce.ctypes.data_as(_u8p)))
+        m = L.vt_result_num_cells(h)
+        ci = np.empty(m, np.uint32)
+        cs = np.empty(m, np.float64)
+        cv = np.empty(m, np.float64)
+        _check(L.vt_result_cells(h, ci.ctypes.data_as(_u32p), cs.ctypes.data_as(_f64p), cv.ctypes.data_as(_f64p)))
+        t = (ctypes.c_double(), ctypes.c_double(), ctypes.c_double())
+        L.vt_result_totals(h, ctypes.byref(t[0]), ctypes.byref(t[1]), ctypes.byref(t[2]))
+        return cls(L.vt_result_num_balls(h), a, b, ar, arc, ce.astype(bool), ci, cs, cv,
+                   (t[0].value, t[1].value, t[2].value))
+
+    def sas_areas(self):
+        """Per-ball SAS area or None (Results::sas_areas, types.rs:207-213)."""
+        out = [None] * self.num_balls
+        for i, s in zip(self.cell_index.tolist(), self.cell_sas_area.tolist()):
+            out[i] = s
+        return out
+
+    def volumes(self):
+        """Per-ball volume or None (Results::volumes, types.rs:222-228)."""
+        out = [None] * self.num_balls
+        for i, v in zip(self.cell_index.tolist(), self.cell_volume.tolist()):
+            out[i] = v
+        return out
+
+    def to_dict(self) -> dict[str, Any]:
+        """The reference's result dict (python.rs:189-210)."""
+        contacts = [{"id_a": a, "id_b": b, "area": ar, "arc_length": arc, "central": ce}
+                    for a, b, ar, arc, ce in zip(self.id_a.tolist(), self.id_b.tolist(), self.area.tolist(),
+                                                 self.arc_length.tolist(), self.central.tolist())]
+        cells = [{"index": i, "sas_area": s, "volume": v}
+                 for i, s, v in zip(self.cell_index.tolist(), self.cell_sas_area.tolist(),
+                                    self.cell_volume.tolist())]
+        return {"num_balls": self.num_balls, "contacts": contacts, "cells": cells,
+                "total_sas_area": self.total_sas_area, "total_volume": self.total_volume,
+                "total_contact_area": self.total_contact_area}
+
+
+def _run(fn_name, balls, probe, periodic_box, groups, precision) -> Result:
+    L = library()
+    x = parse_balls(balls)
+    pb = None if periodic_box is None else parse_periodic_box(periodic_box)
+    g = _groups_array(groups)
+    h = _vp()
+    st = getattr(L, fn_name)(x.ctypes.data_as(_f64p), x.shape[0], float(probe),
+                             None if pb is None else pb.ctypes.data_as(_f64p),
+                             None if g is None else g.ctypes.data_as(_i32p), 0 if g is None else len(g),
+                             _precision_code(precision), ctypes.byref(h))
+    _check(st)
+    try:
+        return Result.from_handle(L, h)
+    finally:
+        L.vt_result_free(h)
+
+
+def compute_tessellation_result(balls, probe, periodic_box=None, groups=None, precision="fp32") -> Result:
+    """compute_tessellation returning a :class:`Result` of numpy arrays."""
+    return _run("vt_compute_tessellation", balls, probe, periodic_box, groups, precision)
+
+
+def compute_tessellation(balls, probe, periodic_box=None, groups=None, with_cell_vertices=False,
+                         precision="fp32") -> dict[str, Any]:
+    """Radical tessellation of balls (python.rs:238-264); returns the reference's dict."""
+    if with_cell_vertices:
+        raise NotImplementedError("with_cell_vertices (tessellation network) is not part of the GPU path")
+    return compute_tessellation_result(balls, probe, periodic_box, groups, precision).to_dict()
+
+
+def compute_contacts_only(balls, probe, periodic_box=None, groups=None, precision="fp32") -> list[dict]:
+    """compute_contacts_only (tessellation.rs:125-166): list of contact dicts."""
+    r = _run("vt_compute_contacts_only", balls, probe, periodic_box, groups, precision)
+    return r.to_dict()["contacts"]
+
+
+def compute_contacts_only_result(balls, probe, periodic_box=None, groups=None, precision="fp32") -> Result:
+    return _run("vt_compute_contacts_only", balls, probe, periodic_box, groups, precision)
+
+
+class Engine:
+    """Explicit engine: a device, a stream and a reusable device workspace.
+
+    ``compute_device`` takes a device pointer (e.g. ``tensor.data_ptr()`` of a contiguous
+    float64 CUDA tensor of shape (N, 4)); results stay on the device until
+    ``download()``.
+    """
+
+    def __init__(self, device: int = 0):
+        self._L = library()
+        self._h = _vp()
+        _check(self._L.vt_engine_create(int(device), ctypes.byref(self._h)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.vt_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_stream(self, stream_ptr: int | None):
+        _check(self._L.vt_engine_set_stream(self._h, stream_ptr))
+
+    def compute_device(self, d_xyzr_ptr: int, n: int, probe: float, periodic_box=None, d_groups_ptr: int = 0,
+                       n_groups: int = 0, precision="fp32", contacts_only: bool = False):
+        pb = None if periodic_box is None else (periodic_box if isinstance(periodic_box, np.ndarray)
+                                                else parse_periodic_box(periodic_box))
+        if pb is not None:
+            pb = np.ascontiguousarray(pb, dtype=np.float64).reshape(9)
+        self._pb_keep = pb
+        _check(self._L.vt_engine_compute_device(self._h, d_xyzr_ptr, int(n), float(probe),
+                                                None if pb is None else pb.ctypes.data_as(_f64p),
+                                                d_groups_ptr or None, int(n_groups), _precision_code(precision),
+                                                1 if contacts_only else 0))
+
+    def compute_host(self, balls, probe, periodic_box=None, groups=None, precision="fp32",
+                     contacts_only=False):
+        x = parse_balls(balls)
+        pb = None if periodic_box is None else parse_periodic_box(periodic_box)
+        g = _groups_array(groups)
+        _check(self._L.vt_engine_compute_host(self._h, x.ctypes.data_as(_f64p), x.shape[0], float(probe),
+                                              None if pb is None else pb.ctypes.data_as(_f64p),
+                                              None if g is None else g.ctypes.data_as(_i32p),
+                                              0 if g is None else len(g), _precision_code(precision),
+                                              1 if contacts_only else 0))
+
+    def stats(self) -> VtStats:
+        s = VtStats()
+        _check(self._L.vt_engine_stats(self._h, ctypes.byref(s)))
+        return s
+
+    def device_outputs(self) -> VtDeviceOutputs:
+        o = VtDeviceOutputs()
+        _check(self._L.vt_engine_device_outputs(self._h, ctypes.byref(o)))
+        return o
+
+    def download(self) -> Result:
+        h = _vp()
+        _check(self._L.vt_engine_download(self._h, ctypes.byref(h)))
+        try:
+            return Result.from_handle(self._L, h)
+        finally:
+            self._L.vt_result_free(h)
+
+
+__all__ = ["compute_tessellation", "compute_tessellation_result", "compute_contacts_only",
+           "compute_contacts_only_result", "Engine", "Result", "VoronotaError", "library", "parse_balls",
+           "parse_periodic_box"]
