@@ -1,0 +1,338 @@
+"""Benchmark: radical tessellation of a 100,000-ball structure on B200.
+
+Workload (the configuration the headline metric is quoted on): 100,000 balls from the
+seeded jittered-lattice generator (2.9 A spacing, +/-0.4 A jitter, protein-like radius
+mix; voronota_ltr.workloads.lattice_balls), probe 1.4, compute_tessellation, FP32 bulk
+geometry with FP64 recomputation of band pairs.  One step = one full tessellation
+(grid, neighbour lists, contacts, cells, compaction, totals).
+
+  value  balls/s with the input resident in HBM (engine API, per-step CUDA events on the
+         launching stream; a 256 MiB buffer is written between steps, outside the
+         events, to flush the 126 MB L2)
+  e2e    balls/s through the public C ABI (vt_compute_tessellation via the Python
+         front end) from pinned host memory, results copied back to host arrays
+  roofline  the contact kernel (the dominant kernel): algorithmic bytes per launch /
+         its CUDA-event duration, against the measured HBM copy bandwidth
+  cpu_baseline  the CPU oracle (a restatement of the reference's Rust code; Rust is not
+         in this image) on the host cores
+
+With torchrun (N > 1) each rank tessellates its own structure (seed = rank): independent
+replicas, no collective on the data path; value = all ranks' balls / max-over-ranks time.
+
+``--impl reference`` times the reference's algorithm on the host cores instead (the CPU
+oracle port: the Rust reference cannot be built here) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (os.path.join(ROOT, "voronota-ltr_b200"), os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+
+N_BALLS = 100_000
+PROBE = 1.4
+METRIC = "balls/s (FP32+FP64 fixup tessellation, 100k-ball structure)"
+UNIT = "balls/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_BALLS)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return ap.parse_args()
+
+
+def workload(n, seed):
+    from voronota_ltr import workloads as W
+
+    return W.lattice_balls(n, seed)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """Bytes per contact-kernel launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "contact_kernel_fp32_100k.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", f"vt_clocks_{os.getpid()}_{device}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(balls, seconds=12.0):
+    """The CPU oracle on all host cores: balls/s over repeated full tessellations."""
+    import oracle as O
+
+    O.set_threads(0)
+    cores = O.get_threads()
+    O.compute(balls, PROBE)  # warm-up
+    times = []
+    t_end = time.perf_counter() + seconds
+    while len(times) < 2 or (time.perf_counter() < t_end and len(times) < 20):
+        t0 = time.perf_counter()
+        O.compute(balls, PROBE)
+        times.append(time.perf_counter() - t0)
+    med = statistics.median(times)
+    return {"value": len(balls) / med, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{len(times)} full tessellations of the {len(balls)}-ball structure, median time"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle as O
+
+    balls = workload(args.n, 0)
+    O.set_threads(0)
+    cores = O.get_threads()
+    for _ in range(args.warmup):
+        O.compute(balls, PROBE)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.compute(balls, PROBE)
+        times.append(time.perf_counter() - t0)
+    mean = sum(times) / len(times)
+    value = args.n / mean
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"lattice {args.n} balls, probe 1.4, compute_tessellation", "balls": args.n,
+                   "probe": PROBE},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} full tessellations of the {args.n}-ball structure"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "CPU oracle (C++ restatement of the reference's Rust code, std::thread over all host "
+                "cores); the Rust reference cannot be compiled in this image",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    import voronota_ltr as V
+
+    balls = workload(args.n, rank)
+    d_xyzr = torch.from_numpy(balls).cuda()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    eng = V.Engine(local)
+    eng.set_stream(stream.cuda_stream)
+    eng.set_timing(True)
+
+    def device_leg(precision, steps, warmup, sample_clocks):
+        for _ in range(warmup):
+            eng.compute_device(d_xyzr.data_ptr(), args.n, PROBE, precision=precision)
+        barrier()
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.start()
+        step_ms, contact_ms, launches = [], [], 0
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            eng.compute_device(d_xyzr.data_ptr(), args.n, PROBE, precision=precision)
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            contact_ms.append(eng.stage_times()["contact"])
+            launches += int(eng.stats().num_kernel_launches)
+        barrier()
+        wall = time.perf_counter() - t0
+        clocks = sampler.stop() if sampler else None
+        st = eng.stats()
+        return {"mean_ms": sum(step_ms) / len(step_ms), "contact_ms": sum(contact_ms) / len(contact_ms),
+                "launches": launches, "wall_s": wall, "clocks": clocks, "stats": st,
+                "stages": eng.stage_times()}
+
+    fp32 = device_leg("fp32", args.steps, args.warmup, True)
+    mean_ms = max_over_ranks(fp32["mean_ms"])
+    value = world * args.n / (mean_ms * 1e-3)
+
+    fp64 = None
+    if not args.no_fp64:
+        fp64 = device_leg("fp64", max(3, args.steps // 2), max(1, args.warmup // 2), False)
+        fp64_ms = max_over_ranks(fp64["mean_ms"])
+
+    # e2e through the public API from pinned host memory
+    pinned = torch.from_numpy(balls).pin_memory()
+    host = pinned.numpy()
+    for _ in range(max(1, args.warmup)):
+        V.compute_tessellation_result(host, PROBE, precision="fp32")
+    barrier()
+    e2e_t = []
+    res = None
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        res = V.compute_tessellation_result(host, PROBE, precision="fp32")
+        e2e_t.append(time.perf_counter() - t0)
+    barrier()
+    e2e_ms = max_over_ranks(1e3 * sum(e2e_t) / len(e2e_t))
+    C, M = len(res.id_a), len(res.cell_index)
+    d2h = C * (4 + 4 + 8 + 8 + 1) + M * (4 + 8 + 8) + 3 * 8
+    h2d = balls.nbytes
+
+    st = fp32["stats"]
+    P, E = int(st.num_pairs), int(st.num_entries)
+    alg_bytes = 58 * P + 20 * E + 40 * args.n
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / (fp32["contact_ms"] * 1e-3) / 1e9
+    traffic = profiled_traffic()
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_baseline(balls)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (f64 band fixups, f64 reductions)", "data": "synthetic",
+            "config": {"workload": f"lattice {args.n} balls per GPU, probe 1.4, compute_tessellation, FP32+fixup",
+                       "balls_per_gpu": args.n, "probe": PROBE, "parallelism": f"replicas x{world}",
+                       "l2": "256 MiB buffer written between timed steps (outside the per-step events)"},
+            "e2e": {"value": world * args.n / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": "k_contact32",
+                         "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": fp32["contact_ms"],
+                         "peak_source": peak_kind},
+            "cpu_baseline": cpu,
+            "clocks": fp32["clocks"],
+            "gpu_launches": fp32["launches"],
+            "fp64_value": (world * args.n / (fp64_ms * 1e-3)) if fp64 else None,
+            "speedup_vs_fp64": (fp64_ms / mean_ms) if fp64 else None,
+            "counts": {"pairs": P, "neighbor_entries": E, "contacts": int(st.num_contacts),
+                       "cells": int(st.num_cells), "fp64_redo_pairs": int(st.num_fp64_redo),
+                       "serial_pairs": int(st.num_serial)},
+            "stages_ms_fp32": {k: round(v, 4) for k, v in fp32["stages"].items()},
+            "stages_ms_fp64": {k: round(v, 4) for k, v in fp64["stages"].items()} if fp64 else None,
+            "wall_s_timed_region": fp32["wall_s"],
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

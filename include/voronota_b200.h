@@ -92,8 +92,18 @@ typedef struct vt_stats {
     uint64_t num_serial;      /* pairs recomputed by the serial (large-contour) kernel */
     double total_sas_area, total_volume, total_contact_area;
     uint32_t device_error_bits;
+    uint64_t num_kernel_launches; /* kernels this library launched during the call */
 } vt_stats;
 int vt_engine_stats(const vt_engine* e, vt_stats* out);
+
+/* Per-stage device times (CUDA events on the engine's stream) of the last call, when
+ * timing is on:  [0] prepare  [1] periodic images  [2] grid  [3] neighbour count
+ * [4] neighbour fill  [5] contact kernel  [6] FP64 recompute  [7] serial fallback
+ * [8] cells  [9] dedup/compaction/totals  [10] whole call (first to last event,
+ * including the waits for the three small device->host reads).  Unused stages are 0. */
+#define VT_NUM_STAGES 11
+int vt_engine_set_timing(vt_engine* e, int on);
+int vt_engine_stage_times(const vt_engine* e, double* ms);
 
 typedef struct vt_device_outputs {
     const uint32_t* id_a;

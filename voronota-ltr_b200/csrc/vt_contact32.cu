@@ -67,6 +67,7 @@ void launch_contact_f32(const DevBufs& b, uint32_t P, int full, cudaStream_t s) 
         k_contact32<true><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P);
     else
         k_contact32<false><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P);
+    count_launch();
 }
 
 }  // namespace vt

@@ -414,12 +414,13 @@ void launch_contact_f64(const DevBufs& b, uint32_t P, int full, int from_list, c
         k_contact64<true><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, from_list);
     else
         k_contact64<false><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, from_list);
+    count_launch();
 }
 
 void launch_contact_serial(const DevBufs& b, uint32_t, int full, cudaStream_t s) {
     unsigned threads = 128;
     unsigned blocks = (b.serial_slots + threads - 1) / threads;
-    k_contact_serial<<<blocks, threads, 0, s>>>(b, full);
+    k_contact_serial<<<blocks, threads, 0, s>>>(b, full); count_launch();
 }
 
 }  // namespace vt

@@ -103,6 +103,29 @@ struct vt_engine {
     // pinned readback
     uint32_t* h_words = nullptr;  // 8 words
     BBox* h_bbox = nullptr;
+    // stage timing
+    bool timing = false;
+    cudaEvent_t ev0[VT_NUM_STAGES] = {}, ev1[VT_NUM_STAGES] = {};
+    bool used[VT_NUM_STAGES] = {};
+    double stage_ms[VT_NUM_STAGES] = {};
+    void t_begin(int k) {
+        if (!timing) return;
+        VT_CUDA(cudaEventRecord(ev0[k], stream));
+        used[k] = true;
+    }
+    void t_end(int k) {
+        if (timing) VT_CUDA(cudaEventRecord(ev1[k], stream));
+    }
+    void t_collect() {
+        for (int k = 0; k < VT_NUM_STAGES; ++k) {
+            stage_ms[k] = 0.0;
+            if (timing && used[k]) {
+                float ms = 0.f;
+                VT_CUDA(cudaEventElapsedTime(&ms, ev0[k], ev1[k]));
+                stage_ms[k] = ms;
+            }
+        }
+    }
     // state of the last call
     vt_stats stats{};
     bool contacts_only = false;
@@ -123,6 +146,10 @@ struct vt_engine {
         bbox_parts.ensure(1024);
         set_hex_table();
         VT_CUDA(cudaGetLastError());
+        for (int k = 0; k < VT_NUM_STAGES; ++k) {
+            VT_CUDA(cudaEventCreate(&ev0[k]));
+            VT_CUDA(cudaEventCreate(&ev1[k]));
+        }
     }
     ~vt_engine() {
         cudaSetDevice(device);
@@ -150,6 +177,10 @@ struct vt_engine {
         bbox.release();
         if (h_words) cudaFreeHost(h_words);
         if (h_bbox) cudaFreeHost(h_bbox);
+        for (int k = 0; k < VT_NUM_STAGES; ++k) {
+            if (ev0[k]) cudaEventDestroy(ev0[k]);
+            if (ev1[k]) cudaEventDestroy(ev1[k]);
+        }
         if (own) cudaStreamDestroy(own);
     }
 
@@ -164,6 +195,11 @@ struct vt_engine {
         have_result = false;
         stats = vt_stats{};
         stats.num_balls = n64;
+        const uint64_t launches0 = launch_count();
+        for (int k = 0; k < VT_NUM_STAGES; ++k) {
+            used[k] = false;
+            stage_ms[k] = 0.0;
+        }
         if (n64 == 0) {  // tessellation.rs:131-133, 205-207
             have_result = true;
             return VT_OK;
@@ -191,9 +227,12 @@ struct vt_engine {
         VT_CUDA(cudaMemsetAsync(words.p, 0, 16 * sizeof(uint32_t), stream));
 
         // 1. prepare + bounding box
+        t_begin(10);
         int nblk = (int)std::min<size_t>((n + 255) / 256, 1024);
+        t_begin(0);
         launch_prepare(b, d_in, probe, bbox_parts.p, nblk, stream);
         launch_bbox_final(bbox_parts.p, nblk, bbox.p, stream);
+        t_end(0);
         VT_CUDA(cudaMemcpyAsync(h_bbox, bbox.p, sizeof(BBox), cudaMemcpyDeviceToHost, stream));
         sync();
         const BBox bb = *h_bbox;
@@ -211,7 +250,9 @@ struct vt_engine {
             img_cnt.ensure(n);
             img_off.ensure(n + 1);
             ensure_scan(n);
+            t_begin(1);
             launch_images(b, reach, bbox.p, img_cnt.p, img_off.p, scan_tmp.p, scan_tmp.cap, stream);
+            t_end(1);
         } else {
             VT_CUDA(cudaMemcpyAsync(b.d_nslots, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
         }
@@ -255,7 +296,9 @@ struct vt_engine {
         b.c_id = c_id.p;
         b.c_slot = c_slot.p;
         ensure_scan(std::max<size_t>(ncell, n) + 1);
+        t_begin(2);
         launch_grid(b, ncell, (uint32_t)max_slots, scan_tmp.p, scan_tmp.cap, stream);
+        t_end(2);
 
         // 4. neighbour counts
         nb_cnt.ensure(n);
@@ -268,9 +311,11 @@ struct vt_engine {
         b.excluded = excluded.p;
         b.nb_off = nb_off.p;
         b.pair_off = pair_off.p;
+        t_begin(3);
         launch_search_count(b, stream);
         scan_u32(nb_cnt.p, nb_off.p, n, scan_tmp.p, stream);
         scan_u32(nb_npair.p, pair_off.p, n, scan_tmp.p, stream);
+        t_end(3);
         VT_CUDA(cudaMemcpyAsync(h_words + 0, nb_off.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         VT_CUDA(cudaMemcpyAsync(h_words + 1, pair_off.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         VT_CUDA(cudaMemcpyAsync(h_words + 2, words.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
@@ -302,7 +347,9 @@ struct vt_engine {
         b.nb_rel = fp32 ? nb_rel.p : nullptr;
         b.pair_a = pair_a.p;
         b.pair_e = pair_e.p;
+        t_begin(4);
         launch_search_fill(b, fp32 ? 1 : 0, stream);
+        t_end(4);
 
         // 6. contacts
         p_status.ensure(P);
@@ -332,15 +379,23 @@ struct vt_engine {
         const int full = contacts_only ? 0 : 1;
         if (P > 0) {
             if (fp32) {
+                t_begin(5);
                 launch_contact_f32(b, P, full, stream);
+                t_end(5);
+                t_begin(6);
                 launch_collect_redo(b, P, stream);
                 launch_contact_f64(b, P, full, 1, stream);
+                t_end(6);
             } else {
+                t_begin(5);
                 launch_contact_f64(b, P, full, 0, stream);
+                t_end(5);
             }
             VT_CUDA(cudaMemcpyAsync(h_words + 4, b.d_redo_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+            t_begin(7);
             launch_collect_redo(b, P, stream);
             launch_contact_serial(b, P, full, stream);
+            t_end(7);
         }
 
         // 7. cells, dedup, compaction, totals
@@ -378,10 +433,17 @@ struct vt_engine {
         b.partials = partials.p;
         b.zero_word = words.p + 1;
         ensure_scan(std::max<size_t>(P, n) + 1);
-        if (!contacts_only) launch_cells(b, stream);
+        if (!contacts_only) {
+            t_begin(8);
+            launch_cells(b, stream);
+            t_end(8);
+        }
+        t_begin(9);
         launch_dedup(b, P, contacts_only ? 1 : 0, stream);
         launch_compact(b, P, contacts_only ? 1 : 0, scan_tmp.p, scan_tmp.cap, stream);
         launch_totals(b, P, contacts_only ? 1 : 0, stream);
+        t_end(9);
+        t_end(10);
 
         VT_CUDA(cudaMemcpyAsync(h_words + 5, keep_off.p + P, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         if (!contacts_only)
@@ -392,6 +454,8 @@ struct vt_engine {
         VT_CUDA(cudaMemcpyAsync(h_tot, totals.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
         sync();
         VT_CUDA(cudaGetLastError());
+        t_collect();
+        stats.num_kernel_launches = launch_count() - launches0;
         stats.num_contacts = P > 0 ? h_words[5] : 0;
         stats.num_cells = contacts_only ? 0 : h_words[6];
         stats.num_fp64_redo = (P > 0 && fp32) ? h_words[4] : 0;
@@ -663,6 +727,16 @@ int vt_engine_download(vt_engine* e, vt_result** out) {
 int vt_engine_stats(const vt_engine* e, vt_stats* out) {
     if (!e || !out) return VT_ERR_INVALID;
     *out = e->stats;
+    return VT_OK;
+}
+int vt_engine_set_timing(vt_engine* e, int on) {
+    if (!e) return VT_ERR_INVALID;
+    e->timing = on != 0;
+    return VT_OK;
+}
+int vt_engine_stage_times(const vt_engine* e, double* ms) {
+    if (!e || !ms) return VT_ERR_INVALID;
+    for (int k = 0; k < VT_NUM_STAGES; ++k) ms[k] = e->stage_ms[k];
     return VT_OK;
 }
 int vt_engine_device_outputs(const vt_engine* e, vt_device_outputs* o) {

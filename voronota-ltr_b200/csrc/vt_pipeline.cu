@@ -1,6 +1,7 @@
 // vt_pipeline.cu -- grid build, neighbour search, pair list, cells, periodic dedup,
 // output compaction and totals.  All arithmetic here is FP64 and follows the reference
 // operation by operation (compiled with --fmad=false).
+#include <atomic>
 #include <cfloat>
 
 #include "vt_geom.cuh"
@@ -648,7 +649,12 @@ int grid_for(size_t n, int block, int cap = 148 * 16) {
     return (int)g;
 }
 
+std::atomic<uint64_t> g_launches{0};
+
 }  // namespace
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 size_t scan_tmp_words_needed(size_t n) { return (n + kTile - 1) / kTile + 2; }
 
@@ -658,47 +664,47 @@ void scan_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* tmp, cudaSt
         cudaMemsetAsync(out, 0, sizeof(uint32_t), s);
         return;
     }
-    k_scan_tiles<<<(unsigned)ntiles, kScanThreads, 0, s>>>(in, n, tmp);
-    k_scan_sums<<<1, kScanThreads, 0, s>>>(tmp, ntiles);
-    k_scan_apply<<<(unsigned)ntiles, kScanThreads, 0, s>>>(in, n, tmp, out, ntiles);
+    k_scan_tiles<<<(unsigned)ntiles, kScanThreads, 0, s>>>(in, n, tmp); count_launch();
+    k_scan_sums<<<1, kScanThreads, 0, s>>>(tmp, ntiles); count_launch();
+    k_scan_apply<<<(unsigned)ntiles, kScanThreads, 0, s>>>(in, n, tmp, out, ntiles); count_launch();
 }
 
 void launch_prepare(const DevBufs& b, const double* d_xyzr, double probe, BBox* d_parts, int nblocks,
                     cudaStream_t s) {
-    k_prepare<<<nblocks, kBlock, 0, s>>>(d_xyzr, b.n, probe, b.sph, b.slot_id, d_parts, b.err);
+    k_prepare<<<nblocks, kBlock, 0, s>>>(d_xyzr, b.n, probe, b.sph, b.slot_id, d_parts, b.err); count_launch();
 }
 void launch_bbox_final(const BBox* parts, int nblocks, BBox* out, cudaStream_t s) {
-    k_bbox_final<<<1, 32, 0, s>>>(parts, nblocks, out);
+    k_bbox_final<<<1, 32, 0, s>>>(parts, nblocks, out); count_launch();
 }
 void launch_images(const DevBufs& b, double reach, const BBox* d_bbox, uint32_t* img_cnt, uint32_t* img_off,
                    uint32_t* scan_tmp, size_t, cudaStream_t s) {
     PBoxArg pb;
     for (int k = 0; k < 9; ++k) pb.v[k] = b.pbox[k];
     int gb = grid_for(b.n, kBlock);
-    k_image_count<<<gb, kBlock, 0, s>>>(b.sph, b.n, pb, d_bbox, reach, img_cnt);
+    k_image_count<<<gb, kBlock, 0, s>>>(b.sph, b.n, pb, d_bbox, reach, img_cnt); count_launch();
     scan_u32(img_cnt, img_off, b.n, scan_tmp, s);
-    k_image_fill<<<gb, kBlock, 0, s>>>(b.sph, b.slot_id, b.n, pb, d_bbox, reach, img_off, b.d_nslots);
+    k_image_fill<<<gb, kBlock, 0, s>>>(b.sph, b.slot_id, b.n, pb, d_bbox, reach, img_off, b.d_nslots); count_launch();
 }
 void launch_grid(const DevBufs& b, uint32_t ncell, uint32_t max_slots, uint32_t* scan_tmp, size_t, cudaStream_t s) {
     cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * ncell, s);
     int gb = grid_for(max_slots, kBlock);
-    k_cell_hist<<<gb, kBlock, 0, s>>>(b.sph, b.d_nslots, b.grid, b.cell_count);
+    k_cell_hist<<<gb, kBlock, 0, s>>>(b.sph, b.d_nslots, b.grid, b.cell_count); count_launch();
     scan_u32(b.cell_count, b.cell_start, ncell, scan_tmp, s);
     cudaMemcpyAsync(b.cell_cursor, b.cell_start, sizeof(uint32_t) * ncell, cudaMemcpyDeviceToDevice, s);
     k_cell_scatter<<<gb, kBlock, 0, s>>>(b.sph, b.slot_id, b.d_nslots, b.grid, b.cell_cursor, b.c_pos, b.c_id,
-                                         b.c_slot);
+                                         b.c_slot); count_launch();
 }
 void launch_search_count(const DevBufs& b, cudaStream_t s) {
     int gb = grid_for(b.n, kSearchWarps, 148 * 64);
-    k_search<false><<<gb, kSearchWarps * 32, 0, s>>>(b, 0);
+    k_search<false><<<gb, kSearchWarps * 32, 0, s>>>(b, 0); count_launch();
 }
 void launch_search_fill(const DevBufs& b, int want_rel, cudaStream_t s) {
     int gb = grid_for(b.n, kSearchWarps, 148 * 64);
-    k_search<true><<<gb, kSearchWarps * 32, 0, s>>>(b, want_rel);
+    k_search<true><<<gb, kSearchWarps * 32, 0, s>>>(b, want_rel); count_launch();
 }
 void launch_cells(const DevBufs& b, cudaStream_t s) {
     int gb = grid_for(b.n, kCellWarps, 148 * 32);
-    k_cells<<<gb, kCellWarps * 32, 0, s>>>(b);
+    k_cells<<<gb, kCellWarps * 32, 0, s>>>(b); count_launch();
 }
 void launch_dedup(const DevBufs& b, uint32_t P, int contacts_only, cudaStream_t s) {
     int gb = grid_for(P, kBlock);
@@ -706,15 +712,16 @@ void launch_dedup(const DevBufs& b, uint32_t P, int contacts_only, cudaStream_t 
         k_dedup<<<gb, kBlock, 0, s>>>(b, P, contacts_only);
     else
         k_keep_plain<<<gb, kBlock, 0, s>>>(b, P);
+    count_launch();
 }
 void launch_compact(const DevBufs& b, uint32_t P, int contacts_only, uint32_t* scan_tmp, size_t, cudaStream_t s) {
     scan_u32(b.keep, b.keep_off, P, scan_tmp, s);
-    k_compact_contacts<<<grid_for(P, kBlock), kBlock, 0, s>>>(b, P, contacts_only);
+    k_compact_contacts<<<grid_for(P, kBlock), kBlock, 0, s>>>(b, P, contacts_only); count_launch();
     if (!contacts_only) {
         // cell flags (u8) widened into the keep buffer's tail is avoided: use params_u
-        k_cell_keep<<<grid_for(b.n, kBlock), kBlock, 0, s>>>(b, b.params_u);
+        k_cell_keep<<<grid_for(b.n, kBlock), kBlock, 0, s>>>(b, b.params_u); count_launch();
         scan_u32(b.params_u, b.cell_off, b.n, scan_tmp, s);
-        k_compact_cells<<<grid_for(b.n, kBlock), kBlock, 0, s>>>(b);
+        k_compact_cells<<<grid_for(b.n, kBlock), kBlock, 0, s>>>(b); count_launch();
     }
 }
 void launch_totals(const DevBufs& b, uint32_t P, int contacts_only, cudaStream_t s) {
@@ -723,17 +730,17 @@ void launch_totals(const DevBufs& b, uint32_t P, int contacts_only, cudaStream_t
     if (contacts_only) {
         // no cells: the cell sums read zero elements from a zero count
         k_partial_sums<<<kSumBlocks, kBlock, 0, s>>>(b.out_area, ccount, b.out_area, b.out_area, b.zero_word,
-                                                     b.partials);
+                                                     b.partials); count_launch();
     } else {
         k_partial_sums<<<kSumBlocks, kBlock, 0, s>>>(b.out_area, ccount, b.out_cell_sas, b.out_cell_vol, ncell,
-                                                     b.partials);
+                                                     b.partials); count_launch();
     }
-    k_final_sums<<<1, 32, 0, s>>>(b.partials, b.totals);
+    k_final_sums<<<1, 32, 0, s>>>(b.partials, b.totals); count_launch();
 }
 void launch_collect_redo(const DevBufs& b, uint32_t P, cudaStream_t s) {
     cudaMemsetAsync(b.d_redo_count, 0, sizeof(uint32_t), s);
     cudaMemsetAsync(b.d_serial_count, 0, sizeof(uint32_t), s);
-    k_collect_redo<<<grid_for(P, kBlock), kBlock, 0, s>>>(b, P);
+    k_collect_redo<<<grid_for(P, kBlock), kBlock, 0, s>>>(b, P); count_launch();
 }
 
 }  // namespace vt

@@ -116,6 +116,10 @@ struct BBox {
     double mn[3], mx[3], max_r;
 };
 
+// Host-side count of kernel launches issued by this library (all devices, all engines).
+void count_launch();
+uint64_t launch_count();
+
 // ---- launchers (vt_pipeline.cu) ----
 void launch_prepare(const DevBufs& b, const double* d_xyzr, double probe, BBox* d_bbox_partials, int nblocks,
                     cudaStream_t s);

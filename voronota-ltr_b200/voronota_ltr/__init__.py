@@ -51,7 +51,11 @@ class VtStats(ctypes.Structure):
         "num_balls", "num_slots", "num_entries", "num_pairs", "num_contacts", "num_cells",
         "num_fp64_redo", "num_serial")] + [
         ("total_sas_area", ctypes.c_double), ("total_volume", ctypes.c_double),
-        ("total_contact_area", ctypes.c_double), ("device_error_bits", ctypes.c_uint32)]
+        ("total_contact_area", ctypes.c_double), ("device_error_bits", ctypes.c_uint32),
+        ("num_kernel_launches", ctypes.c_uint64)]
+
+STAGES = ("prepare", "images", "grid", "neighbor_count", "neighbor_fill", "contact", "fp64_recompute",
+          "serial_fallback", "cells", "output", "call")
 
 
 class VtDeviceOutputs(ctypes.Structure):
@@ -96,6 +100,8 @@ def library():
     L.vt_engine_download.argtypes = [_vp, ctypes.POINTER(_vp)]
     L.vt_engine_stats.argtypes = [_vp, ctypes.POINTER(VtStats)]
     L.vt_engine_device_outputs.argtypes = [_vp, ctypes.POINTER(VtDeviceOutputs)]
+    L.vt_engine_set_timing.argtypes = [_vp, ctypes.c_int]
+    L.vt_engine_stage_times.argtypes = [_vp, _f64p]
     L.vt_status_string.argtypes = [ctypes.c_int]
     L.vt_status_string.restype = ctypes.c_char_p
     L.vt_last_error.restype = ctypes.c_char_p
@@ -325,6 +331,14 @@ class Engine:
         s = VtStats()
         _check(self._L.vt_engine_stats(self._h, ctypes.byref(s)))
         return s
+
+    def set_timing(self, on: bool = True):
+        _check(self._L.vt_engine_set_timing(self._h, 1 if on else 0))
+
+    def stage_times(self) -> dict:
+        buf = (ctypes.c_double * len(STAGES))()
+        _check(self._L.vt_engine_stage_times(self._h, buf))
+        return dict(zip(STAGES, list(buf)))
 
     def device_outputs(self) -> VtDeviceOutputs:
         o = VtDeviceOutputs()
