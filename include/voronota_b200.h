@@ -118,6 +118,38 @@ typedef struct vt_device_outputs {
 } vt_device_outputs;
 int vt_engine_device_outputs(const vt_engine* e, vt_device_outputs* out);
 
+/* ---- contact descriptors without device allocation ----
+ * No counterpart in the reference: an entry point for callers that cannot call
+ * cudaMalloc/cudaFree while they run (a custom call inside a framework whose allocator
+ * owns the device, a real-time loop that must not hit the allocator, a plugin host that
+ * only hands out pre-allocated buffers).  It runs the serial contour kernel
+ * (construct_contact_descriptor for each pair; no neighbour search) with its scratch in a
+ * static device array of VT_NOALLOC_SCRATCH_BYTES that every GPU loading this library
+ * holds until the process exits; it allocates nothing.
+ *
+ * All pointers are device memory on the current device.  d_spheres: num_spheres x 4
+ * doubles (x, y, z, R with R = r + probe).  Neighbour lists are per sphere: sphere a's
+ * list is d_nb_index[d_nb_offsets[a] .. d_nb_offsets[a+1]) in find_colliding_ids order
+ * (sorted by distance to the intersection-circle centre, then index).  Pair k is
+ * (d_pair_a[k], d_pair_b[k]).  Outputs per pair: status (1 contact, 0 none), area, arc
+ * length, central, and, if d_solid_a is not NULL, solid angles and pyramid volumes (all
+ * four or none).  Results equal the regular FP64 path's for the same lists.
+ *
+ * Limit: every listed a must have at most VT_NOALLOC_MAX_NEIGHBORS neighbours (the
+ * scratch holds 128 contour points per pair); otherwise the call returns
+ * VT_ERR_CAPACITY before computing anything.  The first call on a device looks up the
+ * scratch's device address and uploads a small table, so make it before any stream
+ * capture.  Calls share the one scratch array: calls that overlap on the GPU race and
+ * must be serialised (one stream, or host-side ordering).  The call returns after its
+ * work on `stream` (a cudaStream_t, NULL for the default stream) has finished. */
+#define VT_NOALLOC_MAX_NEIGHBORS 57
+#define VT_NOALLOC_SCRATCH_BYTES 6291712
+int vt_contact_descriptors_noalloc(const double* d_spheres, uint64_t num_spheres, const uint32_t* d_nb_offsets,
+                                   const uint32_t* d_nb_index, const uint32_t* d_pair_a, const uint32_t* d_pair_b,
+                                   uint64_t num_pairs, uint8_t* d_status, double* d_area, double* d_arc_length,
+                                   uint8_t* d_central, double* d_solid_a, double* d_solid_b, double* d_pyramid_a,
+                                   double* d_pyramid_b, void* stream);
+
 /* Human-readable status, and the message of the calling thread's last error. */
 const char* vt_status_string(int status);
 const char* vt_last_error(void);

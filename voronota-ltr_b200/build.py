@@ -24,6 +24,7 @@ UNITS = {
     "vt_contact64.cu": ["--fmad=false"],
     "vt_contact32.cu": [],
     "vt_engine.cu": ["--fmad=false"],
+    "vt_noalloc.cu": ["--fmad=false"],
 }
 
 

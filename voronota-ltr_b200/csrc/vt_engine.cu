@@ -62,6 +62,10 @@ struct DBuf {
 
 }  // namespace
 
+namespace vt {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace vt
+
 struct vt_result {
     uint64_t num_balls = 0;
     std::vector<uint32_t> a, b;
