@@ -93,6 +93,7 @@ typedef struct vt_stats {
     double total_sas_area, total_volume, total_contact_area;
     uint32_t device_error_bits;
     uint64_t num_kernel_launches; /* kernels this library launched during the call */
+    uint64_t num_cell_redo;       /* FP32 path: cells whose SAS branch needed FP64 inputs */
 } vt_stats;
 int vt_engine_stats(const vt_engine* e, vt_stats* out);
 
@@ -102,6 +103,11 @@ int vt_engine_stats(const vt_engine* e, vt_stats* out);
  * [8] cells  [9] dedup/compaction/totals  [10] whole call (first to last event,
  * including the waits for the three small device->host reads).  Unused stages are 0. */
 #define VT_NUM_STAGES 11
+/* FP32 path: the error budget E assumed for a contour point coordinate, in float ulps of
+ * the pair's length scale R_a + R_b (default 16).  Decisions within an E-derived band of
+ * their threshold, and ill-conditioned constructions, send the pair to FP64.  Larger is
+ * more conservative (more pairs recomputed in FP64). */
+int vt_engine_set_fp32_band(vt_engine* e, double ulps);
 int vt_engine_set_timing(vt_engine* e, int on);
 int vt_engine_stage_times(const vt_engine* e, double* ms);
 

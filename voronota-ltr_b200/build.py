@@ -22,7 +22,9 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relax
 UNITS = {
     "vt_pipeline.cu": ["--fmad=false"],
     "vt_contact64.cu": ["--fmad=false"],
-    "vt_contact32.cu": [],
+    # FP32 bulk kernel: every decision is banded, so approximate division / square root
+    # (a few ulps) are safe; 64 registers per thread for 8 resident blocks per SM
+    "vt_contact32.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false", "-DVT_C32_MINB=8"],
     "vt_engine.cu": ["--fmad=false"],
     "vt_noalloc.cu": ["--fmad=false"],
 }

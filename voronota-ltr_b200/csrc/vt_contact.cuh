@@ -14,17 +14,50 @@
 //   * area, arc angles, solid angles and centrality are warp reductions.
 // Contours that would exceed 32 points set the overflow status; such pairs are
 // recomputed by the serial fallback kernel.
+//
+// FP32 (F = true): contour points are assumed accurate to a budget E (a runtime
+// band, in float ulps of the pair's length scale S).  Every decision whose margin is
+// within its E-derived band is "unsure", and so is every ill-conditioned construction
+// that could exceed the budget (a cut grazing an edge, a segment nearly tangent to the
+// circle); such pairs are recomputed in FP64.  Decisions that cannot change the outcome
+// carry no band: the cuttable pre-filter is skipped (a mark with no outsider is a
+// no-op), and the |cos| >= 1 branch only flags when its two branches would classify the
+// neighbour differently.  The FP64 instantiation (F = false) is the reference's
+// arithmetic operation by operation.
 #pragma once
 #include "vt_geom.cuh"
 
 namespace vt {
 
+// Debug builds (-DVT_DEBUG_SITES) record the first pipeline step at which an FP32
+// decision became unsure; product builds compile the markers away.
+#ifdef VT_DEBUG_SITES
+#define VT_SITE(k)                                             \
+    do {                                                       \
+        if constexpr (F) {                                     \
+            if (res.site < 0 && __any_sync(kFull, d.unsure)) res.site = (k); \
+        }                                                      \
+    } while (0)
+#else
+#define VT_SITE(k) \
+    do {           \
+    } while (0)
+#endif
+
 constexpr unsigned kFull = 0xffffffffu;
+constexpr float kF32Eps = 1.1920929e-7f;
+// FP32: contour edges shorter than kShortEdge * E send the pair to FP64
+constexpr float kShortEdge = 256.f;
 
 template <typename T>
 __device__ __forceinline__ T wsum(T v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+__device__ __forceinline__ float wmax(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(kFull, v, o));
     return v;
 }
 
@@ -77,7 +110,7 @@ __device__ __forceinline__ V3<T> shfl_v3(V3<T> v, int src) {
 // angles k pi/3 accumulate by repeated addition exactly as in the reference, and the
 // rotation needs sin/cos of angle/2.  The angles do not depend on the data, so the host
 // evaluates them once with the C library the CPU oracle uses (set_hex_table) and every
-// FP64 contour starts from bit-identical hexagon points.  Entry 0 holds the count.
+// FP64 contour starts from bit-identical hexagon points.
 static __constant__ double c_hex_sin[8];
 static __constant__ double c_hex_cos[8];
 static __constant__ int c_hex_n[1];
@@ -86,7 +119,7 @@ static __constant__ int c_hex_n[1];
 // accumulated angles give 7 points, the 7th 8.9e-16 rad short of a full turn).  FP32:
 // the same 7 points from a cos/sin table.
 __device__ __forceinline__ int init_contour(Pt<double>& q, int lane, uint32_t a_id, const Sph<double>& ic,
-                                            V3<double> axis) {
+                                            V3<double> axis, float) {
     V3<double> first = any_normal(axis) * ic.r * kHexScale;
     const int npts = c_hex_n[0];
     if (lane < npts) {
@@ -98,7 +131,7 @@ __device__ __forceinline__ int init_contour(Pt<double>& q, int lane, uint32_t a_
     return npts;
 }
 __device__ __forceinline__ int init_contour(Pt<float>& q, int lane, uint32_t a_id, const Sph<float>& ic,
-                                            V3<float> axis) {
+                                            V3<float> axis, float e0) {
     V3<float> first = any_normal(axis) * ic.r * (float)kHexScale;
     V3<float> perp = cross(axis, first);
     const float h = 0.8660254037844386f;
@@ -130,31 +163,118 @@ struct PairGeom {
     Sph<T> A, B, ic;
     V3<T> axis;
     uint32_t a_id, b_id;
-    // FP32 band widths: lengths (k S), squared lengths (k S^2), cubed lengths (k S^3)
-    // and dimensionless quantities (k), with S the pair's length scale.
-    T tol, tolsq, tol3, tola;
+    T e0;  // FP32: error budget E of a contour point coordinate (A); 0 in FP64
+    T S;   // length scale of the pair (R_a + R_b)
 };
+
+// ---- FP32 constructions: decisions banded by the point error budget E ----
+// Ratio of an intersection's sensitivity to its inputs beyond which the construction is
+// treated as ill-conditioned (the point could be off by more than E).
+constexpr float kCondMax = 64.f;
+
+// intersection_of_plane_and_segment (geometry.rs:134-148)
+__device__ __forceinline__ V3<float> plane_segment_e(Dec<float, true>& d, V3<float> pp, V3<float> n, V3<float> a,
+                                                     V3<float> b, float E) {
+    V3<float> nn = normalize(n);
+    float da = sd_plane_unit(pp, nn, a);
+    float db = sd_plane_unit(pp, nn, b);
+    float dd = fabsf(da - db);
+    d.band(dd - (float)kEps, 2.f * E);
+    if (dd < (float)kEps) return a;
+    if (norm(b - a) > kCondMax * dd) d.unsure = true;  // cut grazing the edge
+    float t = da / (da - db);
+    return a + (b - a) * t;
+}
+// intersect_segment_with_circle (geometry.rs:258-280)
+__device__ __forceinline__ bool segment_circle_e(Dec<float, true>& d, const Sph<float>& c, V3<float> p_in,
+                                                 V3<float> p_out, float E, V3<float>* out) {
+    float dist = norm(p_in - p_out);
+    d.band(dist, 2.f * E);
+    if (dist <= 0.f) return false;
+    V3<float> v = (p_in - p_out) / dist;
+    V3<float> u = c.c - p_out;
+    V3<float> s = p_out + v * dot(v, u);
+    V3<float> cs = c.c - s;
+    float ll = fmaf(c.r, c.r, -norm2(cs));
+    d.band(ll, 4.f * E * (c.r + norm(cs)));
+    if (ll >= 0.f) {
+        float sq = sqrtf(ll);
+        if (kCondMax * sq < c.r) d.unsure = true;  // nearly tangent
+        *out = s - v * sq;
+        return true;
+    }
+    return false;
+}
+// project_point_inside_line (geometry.rs:243-255)
+__device__ __forceinline__ bool project_inside_line_e(Dec<float, true>& d, V3<float> o, V3<float> a, V3<float> b,
+                                                      float E, V3<float>* out) {
+    V3<float> ba = b - a;
+    float lb = norm(ba);
+    V3<float> v = ba / lb;
+    float l = dot(v, o - a);
+    Dec<float, true> d1, d2;
+    bool p = d1.greater(l, 0.f, 2.f * E);
+    bool q = d2.less_eq(l * l, lb * lb, 4.f * E * (fabsf(l) + lb));
+    if ((d1.unsure || d2.unsure) && !((!p && !d1.unsure) || (!q && !d2.unsure))) d.unsure = true;
+    if (p && q) {
+        *out = a + v * l;
+        return true;
+    }
+    return false;
+}
 
 // Pre-test classes
 enum { kSkip = 0, kDiscard = 1, kCut = 2 };
 
-template <typename T, bool F>
-__device__ __forceinline__ int pretest(Dec<T, F>& d, const PairGeom<T>& g, const Sph<T>& c, V3<T>& pc, V3<T>& pn) {
-    // contact.rs:236-282
-    if (!sphere_intersects(d, g.ic, c, g.tolsq) || !sphere_intersects(d, g.B, c, g.tolsq)) return kSkip;
-    if (sphere_contains(d, c, g.A, g.tol, g.tolsq) || sphere_contains(d, c, g.B, g.tol, g.tolsq)) return kDiscard;
+// contact.rs:236-282 for neighbour c.
+__device__ __forceinline__ int pretest(Dec<double, false>& d, const PairGeom<double>& g, const Sph<double>& c,
+                                       V3<double>& pc, V3<double>& pn) {
+    if (!sphere_intersects(d, g.ic, c, 0.0) || !sphere_intersects(d, g.B, c, 0.0)) return kSkip;
+    if (sphere_contains(d, c, g.A, 0.0, 0.0) || sphere_contains(d, c, g.B, 0.0, 0.0)) return kDiscard;
     pc = ic_center(g.A, c);
     pn = normalize(c.c - g.A.c);
-    T cos_val = dot(normalize(g.ic.c - g.A.c), normalize(pc - g.A.c));
-    if (d.greater_eq(fabs(cos_val), (T)1, g.tola)) {
-        return halfspace(d, pc, pn, g.ic.c, g.tol) > 0 ? kDiscard : kSkip;
-    }
-    T l = fabs(sd_plane_unit(pc, pn, g.ic.c));
-    T xl = l / sqrt(fma(cos_val, -cos_val, (T)1));
-    if (d.greater_eq(xl, g.ic.r, g.tol)) {
-        return halfspace(d, pc, pn, g.ic.c, g.tol) >= 0 ? kDiscard : kSkip;
-    }
+    double cos_val = dot(normalize(g.ic.c - g.A.c), normalize(pc - g.A.c));
+    if (fabs(cos_val) >= 1.0) return halfspace(d, pc, pn, g.ic.c, 0.0) > 0 ? kDiscard : kSkip;
+    double l = fabs(sd_plane_unit(pc, pn, g.ic.c));
+    double xl = l / sqrt(fma(cos_val, -cos_val, 1.0));
+    if (xl >= g.ic.r) return halfspace(d, pc, pn, g.ic.c, 0.0) >= 0 ? kDiscard : kSkip;
     return kCut;
+}
+__device__ __forceinline__ int pretest(Dec<float, true>& d, const PairGeom<float>& g, const Sph<float>& c,
+                                       V3<float>& pc, V3<float>& pn) {
+    const float e0 = 0.25f * g.e0, S = g.S;
+    if (!sphere_intersects(d, g.ic, c, 2.f * S * e0) || !sphere_intersects(d, g.B, c, 2.f * S * e0)) return kSkip;
+    if (sphere_contains(d, c, g.A, e0, 2.f * S * e0) || sphere_contains(d, c, g.B, e0, 2.f * S * e0))
+        return kDiscard;
+    pc = ic_center(g.A, c);
+    pn = normalize(c.c - g.A.c);
+    // normalize(pc - a) is +-pn (a is the origin): the sign of the plane's offset
+    float h = dot(pc, pn);
+    d.band(h, e0);
+    float cos_val = dot(normalize(g.ic.c - g.A.c), h >= 0.f ? pn : -pn);
+    float sd = sd_plane_unit(pc, pn, g.ic.c);  // shared by both branches
+    Dec<float, true> dh;
+    int hs = halfspace(dh, pc, pn, g.ic.c, 2.f * e0);
+    float one_m = fmaf(cos_val, -cos_val, 1.f);
+    Dec<float, true> dc;
+    bool big = dc.greater_eq(fabsf(cos_val), 1.f, 4.f * kF32Eps);
+    int cls_a = hs > 0 ? kDiscard : kSkip;  // branch |cos| >= 1
+    float xl = fabsf(sd) / sqrtf(fmaxf(one_m, 0.f));
+    Dec<float, true> dx;
+    int cls_b;  // branch |cos| < 1
+    if (dx.greater_eq(xl, g.ic.r, e0 * (2.f + 2.f / fmaxf(one_m, 1e-12f))))
+        cls_b = hs >= 0 ? kDiscard : kSkip;
+    else
+        cls_b = kCut;
+    int cls = big ? cls_a : cls_b;
+    if (dc.unsure) {
+        if (cls_a != cls_b || dh.unsure || dx.unsure) d.unsure = true;
+    } else if (big) {
+        if (dh.unsure) d.unsure = true;
+    } else {
+        if (dx.unsure || (cls_b != kCut && dh.unsure)) d.unsure = true;
+    }
+    return cls;
 }
 
 // Result of the warp computation (uniform across lanes).
@@ -164,48 +284,76 @@ struct WarpContact {
     bool overflow;
     double area, arc, sa_a, sa_b, pv_a, pv_b;
     bool central;
+    int site;  // debug builds: first step with an unsure decision
 };
 
-// Solid angle (contact.rs:797-848) summed over the warp's contour.
+// Solid angle (contact.rs:797-848) summed over the warp's contour.  ea0 / ea1 bound the
+// arc-angle errors of the previous and the own point (FP32).  FP64 follows the reference
+// term by term.  FP32 computes each turn term pi - dihedral as the supplement directly
+// (no float rounding of pi, which would bias every solid angle and so every SAS area)
+// and sums the terms in double.
 template <typename T, bool F>
-__device__ __forceinline__ T solid_angle(Dec<T, F>& d, const Sph<T>& a, const Sph<T>& b, const Sph<T>& ic,
-                                         const Pt<T>& p0, const Pt<T>& p1, const Pt<T>& p2, bool on, int len,
-                                         T tolsq, T tol3, T tola) {
-    T turn = 0;
+__device__ __forceinline__ double solid_angle(Dec<T, F>& d, const Sph<T>& a, const Sph<T>& b, const Sph<T>& ic,
+                                              const Pt<T>& p0, const Pt<T>& p1, const Pt<T>& p2, bool on, int len,
+                                              T e0, T ea0, T ea1) {
+    double sa;
     if (len == 0) {
-        turn = (T)kTau * norm(ic.c - a.c) / a.r;
+        if constexpr (F)
+            sa = kTau - kTau * ((double)norm_rn(ic.c - a.c) / (double)a.r);
+        else
+            sa = kTau - (double)((T)kTau * norm(ic.c - a.c) / a.r);
     } else {
-        T t = 0, t2 = 0;
+        double t = 0;
+        T t2 = 0;
         if (on) {
             const T pi = (T)kPi;
+            // turn term at point p1: pi - dihedral (FP32: the supplement, in double)
+            auto turn_at = [&](V3<T> x1, V3<T> x2) -> double {
+                if constexpr (F)
+                    return dihedral_supplement(a.c, p1.p, x1, x2);
+                else
+                    return pi - min_dihedral(a.c, p1.p, x1, x2);
+            };
             if (p0.ang > (T)0) {
                 V3<T> dd = cross(b.c - a.c, p1.p - ic.c);
-                T dv = dot(dd, p0.p - p1.p);
-                d.band(p0.ang - pi, tola);
-                d.band(dv, tol3);
+                V3<T> w = p0.p - p1.p;
+                T dv = dot(dd, w);
+                if constexpr (F) {
+                    d.band(p0.ang - pi, ea0);
+                    d.band(dv, (T)2 * e0 * (norm(b.c - a.c) * norm(w) + (T)2 * norm(dd)));
+                }
                 bool flip = (p0.ang < pi && dv < (T)0) || (p0.ang > pi && dv > (T)0);
                 if (flip) dd = -dd;
-                t = pi - min_dihedral(a.c, p1.p, p1.p + dd, p2.p);
+                t = turn_at(p1.p + dd, p2.p);
             } else if (p1.ang > (T)0) {
                 V3<T> dd = cross(b.c - a.c, p1.p - ic.c);
-                T dv = dot(dd, p2.p - p1.p);
-                d.band(p1.ang - pi, tola);
-                d.band(dv, tol3);
+                V3<T> w = p2.p - p1.p;
+                T dv = dot(dd, w);
+                if constexpr (F) {
+                    d.band(p1.ang - pi, ea1);
+                    d.band(dv, (T)2 * e0 * (norm(b.c - a.c) * norm(w) + (T)2 * norm(dd)));
+                }
                 bool flip = (p1.ang < pi && dv < (T)0) || (p1.ang > pi && dv > (T)0);
                 if (flip) dd = -dd;
-                t = pi - min_dihedral(a.c, p1.p, p0.p, p1.p + dd);
-                t2 = p1.ang * (norm(ic.c - a.c) / a.r);
+                t = turn_at(p0.p, p1.p + dd);
+                if constexpr (F)
+                    t2 = (T)((double)p1.ang * ((double)norm_rn(ic.c - a.c) / (double)a.r));
+                else
+                    t2 = p1.ang * (norm(ic.c - a.c) / a.r);
             } else {
-                t = pi - min_dihedral(a.c, p1.p, p0.p, p2.p);
+                t = turn_at(p0.p, p2.p);
             }
         }
-        turn = lsum2(t, t2, len);
+        if constexpr (F) {
+            sa = kTau - wsum(t + (double)t2);
+        } else {
+            sa = kTau - lsum2(t, t2, len);
+        }
     }
-    T sa = (T)kTau - turn;
     V3<T> ic_to_a = ic.c - a.c, ic_to_b = ic.c - b.c;
     Dec<T, F> d1, d2;
-    bool c1 = d1.greater(dot(ic_to_a, ic_to_b), (T)0, tolsq);
-    bool c2 = d2.less(norm2(a.c - ic.c), norm2(b.c - ic.c), tolsq);
+    bool c1 = d1.greater(dot(ic_to_a, ic_to_b), (T)0, (T)4 * e0 * (a.r + b.r));
+    bool c2 = d2.less(norm2(a.c - ic.c), norm2(b.c - ic.c), (T)4 * e0 * (a.r + b.r));
     if (F && (d1.unsure || d2.unsure) && !((!c1 && !d1.unsure) || (!c2 && !d2.unsure))) d.unsure = true;
     if (c1 && c2) sa = -sa;
     return sa;
@@ -217,6 +365,7 @@ template <typename T, bool F, bool FULL, typename NbFn>
 __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn nb) {
     const int lane = threadIdx.x & 31;
     PairGeom<T> g = g0;
+    const T e0 = g.e0;
     Dec<T, F> d;
     WarpContact res;
     res.valid = false;
@@ -224,16 +373,18 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
     res.overflow = false;
     res.area = res.arc = res.sa_a = res.sa_b = res.pv_a = res.pv_b = 0.0;
     res.central = false;
+    res.site = -1;
 
     // contact.rs:206-218
-    if (!sphere_intersects(d, g.A, g.B, g.tolsq) || sphere_contains(d, g.A, g.B, g.tol, g.tolsq) ||
-        sphere_contains(d, g.B, g.A, g.tol, g.tolsq)) {
+    if (!sphere_intersects(d, g.A, g.B, (T)2 * g.S * e0) || sphere_contains(d, g.A, g.B, e0, (T)2 * g.S * e0) ||
+        sphere_contains(d, g.B, g.A, e0, (T)2 * g.S * e0)) {
         res.unsure = __any_sync(kFull, d.unsure);
         return res;
     }
     g.ic = intersection_circle(g.A, g.B);
     g.axis = normalize(g.B.c - g.A.c);
-    if (d.less_eq(g.ic.r, (T)0, g.tol)) {
+    if (d.less_eq(g.ic.r, (T)0, e0)) {
+        VT_SITE(0);
         res.unsure = __any_sync(kFull, d.unsure);
         return res;
     }
@@ -256,6 +407,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             cid = c.id;
             cls = pretest(d, g, c.s, pc, pn);
         }
+        VT_SITE(1);
         if (__any_sync(kFull, cls == kDiscard)) {
             discarded = true;
             break;
@@ -267,17 +419,19 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             V3<T> PC = shfl_v3(pc, j), PN = shfl_v3(pn, j);
             uint32_t CID = __shfl_sync(kFull, cid, j);
             if (!init) {
-                len = init_contour(q, lane, g.a_id, g.ic, g.axis);
+                len = init_contour(q, lane, g.a_id, g.ic, g.axis, (float)e0);
                 init = true;
-            } else {
-                // test_contour_cuttable (contact.rs:472-481)
+            } else if constexpr (!F) {
+                // test_contour_cuttable (contact.rs:472-481).  A pure pre-filter: a mark that
+                // finds no outsider changes nothing, so the FP32 path goes straight to the mark.
                 T thr = norm2(PC - g.A.c);
-                bool cut = lane < len && d.greater_eq(norm2(q.p - g.A.c), thr, g.tolsq);
+                bool cut = lane < len && norm2(q.p - g.A.c) >= thr;
                 if (!__any_sync(kFull, cut)) continue;
             }
             // mark_contour (contact.rs:506-521)
-            bool out = lane < len && halfspace(d, PC, PN, q.p, g.tol) >= 0;
+            bool out = lane < len && halfspace(d, PC, PN, q.p, e0) >= 0;
             unsigned om = __ballot_sync(kFull, out);
+            VT_SITE(2);
             if (om == 0) continue;
             int nout = __popc(om);
             if (nout >= len) {  // mark_and_cut_contour clears (contact.rs:496-499)
@@ -324,25 +478,34 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             int il = ns > 0 ? ns - 1 : n2 - 1;
             int ir = ne + 1 < n2 ? ne + 1 : 0;
             Pt<T> nbp = shfl_pt(q, lane == ns ? il : ir);
-            if (lane == ns) {
-                V3<T> ip = plane_segment(d, PC, PN, q.p, nbp.p, g.tol);
-                uint32_t old_l = q.lid;
+            if (lane == ns || lane == ne) {
+                V3<T> ip;
+                if constexpr (F)
+                    ip = plane_segment_e(d, PC, PN, q.p, nbp.p, e0);
+                else
+                    ip = plane_segment(d, PC, PN, q.p, nbp.p, 0.0);
+                if (lane == ns) {
+                    uint32_t old_l = q.lid;
+                    q.lid = nbp.rid;
+                    q.rid = old_l;
+                } else {
+                    uint32_t old_r = q.rid;
+                    q.lid = old_r;
+                    q.rid = nbp.lid;
+                }
                 q.p = ip;
-                q.lid = nbp.rid;
-                q.rid = old_l;
-                q.ang = 0;
-            } else if (lane == ne) {
-                V3<T> ip = plane_segment(d, PC, PN, q.p, nbp.p, g.tol);
-                uint32_t old_r = q.rid;
-                q.p = ip;
-                q.lid = old_r;
-                q.rid = nbp.lid;
                 q.ang = 0;
             }
+            VT_SITE(3);
             // merge very close points (contact.rs:622-626)
             V3<T> ps = shfl_v3(q.p, ns), pe = shfl_v3(q.p, ne);
             uint32_t erid = __shfl_sync(kFull, q.rid, ne);
-            if (!d.gt(norm2(pe - ps), (T)0, g.tolsq)) {
+            T dse = norm2(pe - ps);
+            if constexpr (F) {  // merge threshold: d^2 <= 1e-10, i.e. d <= 1e-5
+                if (fabsf(sqrtf(dse) - 1e-5f) <= 4.f * e0) d.unsure = true;
+            }
+            VT_SITE(4);
+            if (!(dse - (T)kEps > (T)0)) {
                 if (lane == ns) q.rid = erid;
                 int s2 = lane < ne ? lane : lane + 1;
                 s2 = s2 > 31 ? 31 : s2;
@@ -361,6 +524,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
     T sum_arc = 0, area = 0;
     V3<T> bary = mk<T>(0, 0, 0);
     bool on = false;
+    T ang_err = 0;  // FP32: bound on this lane's arc-angle error
     if (!init) {  // contact.rs:311-314
         bary = g.ic.c;
         sum_arc = (T)kTau;
@@ -370,8 +534,14 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
         // restrict_contour_to_circle (contact.rs:631-769)
         const T r2 = g.ic.r * g.ic.r;
         bool in = true;
-        if (lane < len) in = d.less_eq(norm2(q.p - g.ic.c), r2, g.tolsq);
+        if (lane < len) {
+            T dc2 = norm2(q.p - g.ic.c);
+            T tol = 0;
+            if constexpr (F) tol = 4.f * (sqrtf(dc2) + g.ic.r) * e0;
+            in = d.less_eq(dc2, r2, tol);
+        }
         unsigned outm = __ballot_sync(kFull, lane < len && !in);
+        VT_SITE(5);
         if (outm != 0) {
             int nx = lane + 1 < len ? lane + 1 : 0;
             Pt<T> v = shfl_pt(q, nx);
@@ -384,10 +554,24 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             if (lane < len) {
                 if (!in && !v_in) {
                     V3<T> mp, ip1, ip2;
-                    if (project_inside_line(d, g.ic.c, q.p, v.p, &mp, g.tol, g.tolsq) &&
-                        d.less_eq(norm2(mp - g.ic.c), r2, g.tolsq)) {
-                        bool ok1 = segment_circle(d, g.ic, mp, q.p, &ip1, g.tol, g.tolsq);
-                        bool ok2 = segment_circle(d, g.ic, mp, v.p, &ip2, g.tol, g.tolsq);
+                    bool ok1, ok2, proj;
+                    if constexpr (F) {
+                        proj = project_inside_line_e(d, g.ic.c, q.p, v.p, e0, &mp);
+                        if (proj) {
+                            float dm = norm2(mp - g.ic.c);
+                            proj = d.less_eq(dm, r2, 4.f * (sqrtf(dm) + g.ic.r) * e0);
+                        }
+                    } else {
+                        proj = project_inside_line(d, g.ic.c, q.p, v.p, &mp, 0.0, 0.0) && norm2(mp - g.ic.c) <= r2;
+                    }
+                    if (proj) {
+                        if constexpr (F) {
+                            ok1 = segment_circle_e(d, g.ic, mp, q.p, e0, &ip1);
+                            ok2 = segment_circle_e(d, g.ic, mp, v.p, e0, &ip2);
+                        } else {
+                            ok1 = segment_circle(d, g.ic, mp, q.p, &ip1, 0.0, 0.0);
+                            ok2 = segment_circle(d, g.ic, mp, v.p, &ip2, 0.0, 0.0);
+                        }
                         if (ok1 && ok2) {
                             k = 2;
                             i1.p = ip1;
@@ -402,7 +586,12 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                     }
                 } else if (!in) {
                     V3<T> ip;
-                    if (segment_circle(d, g.ic, v.p, q.p, &ip, g.tol, g.tolsq)) {
+                    bool ok;
+                    if constexpr (F)
+                        ok = segment_circle_e(d, g.ic, v.p, q.p, e0, &ip);
+                    else
+                        ok = segment_circle(d, g.ic, v.p, q.p, &ip, 0.0, 0.0);
+                    if (ok) {
                         k = 1;
                         i1.p = ip;
                         i1.lid = g.a_id;
@@ -413,7 +602,12 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                     }
                 } else if (!v_in) {
                     V3<T> ip;
-                    if (segment_circle(d, g.ic, q.p, v.p, &ip, g.tol, g.tolsq)) {
+                    bool ok;
+                    if constexpr (F)
+                        ok = segment_circle_e(d, g.ic, q.p, v.p, e0, &ip);
+                    else
+                        ok = segment_circle(d, g.ic, q.p, v.p, &ip, 0.0, 0.0);
+                    if (ok) {
                         k = 1;
                         i1.p = ip;
                         i1.lid = v.lid;
@@ -424,6 +618,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                     }
                 }
             }
+            VT_SITE(6);
             int insertions = __reduce_add_sync(kFull, (unsigned)k);
             if (insertions == 0) {
                 res.unsure = __any_sync(kFull, d.unsure);
@@ -435,8 +630,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             uint32_t w1_rid = __shfl_sync(kFull, q.rid, pv);
             uint32_t w2_lid = v.lid;
             if (lane < len && in) {
-                bool w1_last = (lane == 0);  // for point 0 the wrap segment writes last
-                if (w1_last) {
+                if (lane == 0) {  // for point 0 the wrap segment writes last
                     if (w1) {
                         q.lid = g.a_id;
                         q.rid = w1_rid;
@@ -455,7 +649,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                 }
             }
             int c = lane < len ? (in ? 1 : 0) + k : 0;
-            // inclusive warp scan of c
             int incl = c;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -494,16 +687,26 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             int nx2 = lane + 1 < len ? lane + 1 : 0;
             Pt<T> v2 = shfl_pt(q, nx2);
             T a = 0;
-            if (lane < len && q.rid == g.a_id && v2.lid == g.a_id)
-                a = directed_angle(d, g.ic.c, q.p, v2.p, g.ic.c + g.axis, g.tola);
+            if (lane < len && q.rid == g.a_id && v2.lid == g.a_id) {
+                T tol_dir = 0;
+                if constexpr (F) {
+                    tol_dir = 4.f * e0 / fmaxf(g.ic.r, 1e-12f) + 8.f * kF32Eps;
+                    ang_err = tol_dir;
+                }
+                a = directed_angle(d, g.ic.c, q.p, v2.p, g.ic.c + g.axis, tol_dir);
+            }
+            VT_SITE(7);
             q.ang = a;
             sum_arc = lsum(a, len);
             // full circle after all (contact.rs:765-768): contour cleared, area stays 0
-            if (d.ge(sum_arc, (T)kTau, g.tola) || (len > 2 && d.eq(sum_arc, (T)kTau, g.tola))) {
+            T sum_err = 0;
+            if constexpr (F) sum_err = wsum(ang_err) + 1e-5f;
+            if (d.ge(sum_arc, (T)kTau, sum_err) || (len > 2 && d.eq(sum_arc, (T)kTau, sum_err))) {
                 res.unsure = __any_sync(kFull, d.unsure);
                 return res;
             }
         }
+        VT_SITE(8);
         int nx = lane + 1 < len ? lane + 1 : 0;
         Pt<T> v = shfl_pt(q, nx);
         // calculate_contour_area (contact.rs:773-793)
@@ -518,7 +721,11 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
         area = lsum2(t, t2, len);
     }
     // area <= 0 -> None (contact.rs:329-331)
-    if (d.less_eq(area, (T)0, g.tolsq)) {
+    T area_tol = 0;
+    if constexpr (F) area_tol = 8.f * (float)kPi * g.ic.r * e0;
+    bool area_none = d.less_eq(area, (T)0, area_tol);
+    VT_SITE(9);
+    if (area_none) {
         res.unsure = __any_sync(kFull, d.unsure);
         return res;
     }
@@ -527,7 +734,8 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
     bool central;
     {
         const T fe = (T)1e-10;
-        bool reflex = on && d.greater(q.ang - fe, (T)kPi, g.tola);
+        bool reflex = on && d.greater(q.ang - fe, (T)kPi, ang_err);
+        VT_SITE(10);
         if (__any_sync(kFull, reflex)) {
             central = true;
         } else {
@@ -537,14 +745,25 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             if (on) {
                 V3<T> edge = pj - q.p;
                 T el = norm(edge);
-                if (!d.less(el, fe, g.tol)) {
+                T eerr = 0;
+                if constexpr (F) {
+                    eerr = 4.f * e0;
+                    // a short edge's FP32 direction (and the turn terms at its ends) is unreliable
+                    if (el < kShortEdge * e0) d.unsure = true;
+                }
+                if (!d.less(el, fe, eerr)) {
                     V3<T> u = edge / el;
                     V3<T> foot = q.p + u * dot(u, bary - q.p);
                     V3<T> nbv = bary - foot;
-                    bad = d.less(dot(nbv, g.ic.c - q.p), (T)0, g.tolsq);
+                    V3<T> cp = g.ic.c - q.p;
+                    T tol = 0;
+                    if constexpr (F)
+                        tol = 4.f * e0 * (norm(nbv) + norm(cp)) * (1.f + 2.f * norm(bary - q.p) / fmaxf(el, 1e-12f));
+                    bad = d.less(dot(nbv, cp), (T)0, tol);
                 }
             }
             central = !__any_sync(kFull, bad);
+            VT_SITE(11);
         }
     }
 
@@ -558,16 +777,23 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
         int nxl = len > 0 ? (lane + 1 < len ? lane + 1 : 0) : 0;
         Pt<T> p0 = shfl_pt(q, pvl);
         Pt<T> p2 = shfl_pt(q, nxl);
-        T sa = solid_angle(d, g.A, g.B, g.ic, p0, q, p2, on, len, g.tolsq, g.tol3, g.tola);
-        T sb = solid_angle(d, g.B, g.A, g.ic, p0, q, p2, on, len, g.tolsq, g.tol3, g.tola);
-        d.band(sa, g.tola);
-        d.band(sb, g.tola);
-        T sign_a = sa < (T)0 ? (T)-1 : (T)1;
-        T sign_b = sb < (T)0 ? (T)-1 : (T)1;
-        res.sa_a = (double)sa;
-        res.sa_b = (double)sb;
-        res.pv_a = (double)(norm(g.ic.c - g.A.c) * area / (T)3 * sign_a);
-        res.pv_b = (double)(norm(g.ic.c - g.B.c) * area / (T)3 * sign_b);
+        T ea0 = 0;
+        if constexpr (F) ea0 = __shfl_sync(kFull, ang_err, pvl);
+        double sa = solid_angle(d, g.A, g.B, g.ic, p0, q, p2, on, len, e0, ea0, ang_err);
+        VT_SITE(12);
+        double sb = solid_angle(d, g.B, g.A, g.ic, p0, q, p2, on, len, e0, ea0, ang_err);
+        VT_SITE(13);
+        T sign_a = sa < 0.0 ? (T)-1 : (T)1;
+        T sign_b = sb < 0.0 ? (T)-1 : (T)1;
+        res.sa_a = sa;
+        res.sa_b = sb;
+        if constexpr (F) {
+            res.pv_a = (double)norm_rn(g.ic.c - g.A.c) * (double)area / 3.0 * (double)sign_a;
+            res.pv_b = (double)norm_rn(g.ic.c - g.B.c) * (double)area / 3.0 * (double)sign_b;
+        } else {
+            res.pv_a = (double)(norm(g.ic.c - g.A.c) * area / (T)3 * sign_a);
+            res.pv_b = (double)(norm(g.ic.c - g.B.c) * area / (T)3 * sign_b);
+        }
     }
     res.unsure = __any_sync(kFull, d.unsure);
     return res;

@@ -13,10 +13,20 @@ namespace vt {
 
 namespace {
 
-constexpr int kWarps = 4;
+#ifndef VT_C32_WARPS
+#define VT_C32_WARPS 4
+#endif
+#ifndef VT_C32_MINB
+#define VT_C32_MINB 1
+#endif
+constexpr int kWarps = VT_C32_WARPS;
+
+#ifdef VT_DEBUG_SITES
+__device__ unsigned long long g_debug_sites[32];
+#endif
 
 template <bool FULL>
-__global__ void __launch_bounds__(kWarps * 32) k_contact32(DevBufs b, uint32_t P) {
+__global__ void __launch_bounds__(kWarps * 32, VT_C32_MINB) k_contact32(DevBufs b, uint32_t P, float band) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (uint32_t p = blockIdx.x * kWarps + w; p < P; p += gridDim.x * kWarps) {
         const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
@@ -28,11 +38,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_contact32(DevBufs b, uint32_t P
         g.B = {{rb.x, rb.y, rb.z}, rb.w};
         g.a_id = a;
         g.b_id = b.nb_id[eb];
-        const float S = Ra + rb.w;
-        g.tol = kTolRel * S;
-        g.tolsq = kTolRel * S * S;
-        g.tol3 = kTolRel * S * S * S;
-        g.tola = kTolRel * 8.f;
+        g.S = Ra + rb.w;
+        g.e0 = band * g.S;
         const float4* rel = b.nb_rel + off;
         const uint32_t* nid = b.nb_id + off;
         auto nbf = [&](int e) {
@@ -43,6 +50,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_contact32(DevBufs b, uint32_t P
             return r;
         };
         WarpContact r = contact_warp<float, true, FULL>(g, (int)cnt, (int)(eb - off), nbf);
+#ifdef VT_DEBUG_SITES
+        if (lane == 0 && r.unsure) atomicAdd(&g_debug_sites[r.site < 0 ? 31 : r.site], 1ull);
+#endif
         if (lane == 0) {
             uint8_t st = (r.valid ? kValid : 0) | (r.unsure ? kUnsure : 0) | (r.overflow ? kOverflow : 0);
             b.p_status[p] = st;
@@ -64,10 +74,20 @@ void launch_contact_f32(const DevBufs& b, uint32_t P, int full, cudaStream_t s) 
     if (g < 1) g = 1;
     if (g > 148 * 64) g = 148 * 64;
     if (full)
-        k_contact32<true><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P);
+        k_contact32<true><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band);
     else
-        k_contact32<false><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P);
+        k_contact32<false><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band);
     count_launch();
 }
 
 }  // namespace vt
+
+#ifdef VT_DEBUG_SITES
+// Debug builds only: histogram of the first unsure step per flagged pair (read and clear).
+extern "C" int vt_debug_flag_sites(unsigned long long* out32) {
+    cudaMemcpyFromSymbol(out32, vt::g_debug_sites, 32 * sizeof(unsigned long long));
+    unsigned long long z[32] = {0};
+    cudaMemcpyToSymbol(vt::g_debug_sites, z, sizeof(z));
+    return 0;
+}
+#endif

@@ -40,7 +40,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_contact64(DevBufs b, uint32_t P
         g.B = sph_of(b.sph[b.nb_slot[eb]]);
         g.a_id = a;
         g.b_id = b.nb_id[eb];
-        g.tol = g.tolsq = g.tol3 = g.tola = 0.0;
+        g.e0 = 0.0;
+        g.S = g.A.r + g.B.r;
         const double4* sph = b.sph;
         const uint32_t* nslot = b.nb_slot + off;
         const uint32_t* nid = b.nb_id + off;

@@ -95,7 +95,8 @@ struct vt_engine {
     DBuf<double> p_area, p_arc, p_sa_a, p_sa_b, p_pv_a, p_pv_b;
     DBuf<uint32_t> redo_list, serial_list, keep, keep_off, cell_off, flags32;
     DBuf<double> serial_scratch;
-    DBuf<uint8_t> cell_flag;
+    DBuf<uint8_t> cell_flag, ball_dirty;
+    DBuf<uint32_t> cell_redo;
     DBuf<double> cell_sas, cell_vol;
     DBuf<uint32_t> out_a, out_b, out_cell_index;
     DBuf<double> out_area, out_arc, out_cell_sas, out_cell_vol;
@@ -130,11 +131,15 @@ struct vt_engine {
             }
         }
     }
+    double fp32_band_ulps = 16.0;  // FP32 point error budget E, in float ulps of the pair scale
     // state of the last call
     vt_stats stats{};
     bool contacts_only = false;
     bool have_result = false;
     DevBufs bufs{};
+    // FP32 path: per-contributing-contact error budget (radians) of a cell's solid-angle
+    // sums; cells within it of a compute_sas branch threshold are recomputed from FP64
+    static constexpr float kCellBand = 4e-6f;
 
     void init(int dev) {
         device = dev;
@@ -176,6 +181,8 @@ struct vt_engine {
         p_status.release();
         p_central.release();
         cell_flag.release();
+        ball_dirty.release();
+        cell_redo.release();
         out_central.release();
         bbox_parts.release();
         bbox.release();
@@ -219,6 +226,7 @@ struct vt_engine {
             for (int k = 0; k < 9; ++k) b.pbox[k] = pbox9[k];
         b.groups = d_groups;
         b.n_groups = d_groups ? n_groups : 0;
+        b.fp32_band = (float)(fp32_band_ulps * 1.1920928955078125e-07);
 
         sph.ensure(max_slots);
         slot_id.ensure(max_slots);
@@ -364,7 +372,7 @@ struct vt_engine {
         p_sa_b.ensure(P);
         p_pv_a.ensure(P);
         p_pv_b.ensure(P);
-        redo_list.ensure(P);
+        redo_list.ensure(2 * (size_t)P);  // the cell fixup may list a pair from both ends
         serial_list.ensure(P);
         const uint32_t serial_slots = 2048;
         serial_scratch.ensure((size_t)serial_slots * kSerialCap * 6);
@@ -436,10 +444,28 @@ struct vt_engine {
         b.totals = totals.p;
         b.partials = partials.p;
         b.zero_word = words.p + 1;
+        cell_redo.ensure(n);
+        ball_dirty.ensure(n);
+        b.cell_redo_list = cell_redo.p;
+        b.d_cell_redo_count = words.p + 5;
+        b.ball_dirty = ball_dirty.p;
         ensure_scan(std::max<size_t>(P, n) + 1);
         if (!contacts_only) {
             t_begin(8);
-            launch_cells(b, stream);
+            if (fp32 && P > 0) {
+                // cells whose compute_sas branch is uncertain on FP32 inputs: recompute all
+                // their pairs in FP64, then the cells of those balls and their neighbours
+                VT_CUDA(cudaMemsetAsync(ball_dirty.p, 0, n, stream));
+                launch_cells(b, kCellBand, 0, stream);
+                VT_CUDA(cudaMemsetAsync(b.d_redo_count, 0, sizeof(uint32_t), stream));
+                launch_mark_ball_pairs(b, stream);
+                launch_contact_f64(b, P, full, 1, stream);
+                launch_cells(b, 0.f, 1, stream);
+                VT_CUDA(cudaMemcpyAsync(h_words + 9, b.d_cell_redo_count, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                        stream));
+            } else {
+                launch_cells(b, 0.f, 0, stream);
+            }
             t_end(8);
         }
         t_begin(9);
@@ -464,6 +490,7 @@ struct vt_engine {
         stats.num_cells = contacts_only ? 0 : h_words[6];
         stats.num_fp64_redo = (P > 0 && fp32) ? h_words[4] : 0;
         stats.num_serial = P > 0 ? h_words[8] : 0;
+        stats.num_cell_redo = (fp32 && P > 0 && !contacts_only) ? h_words[9] : 0;
         stats.device_error_bits = h_words[7];
         stats.total_sas_area = contacts_only ? 0.0 : h_tot[0];
         stats.total_volume = contacts_only ? 0.0 : h_tot[1];
@@ -731,6 +758,11 @@ int vt_engine_download(vt_engine* e, vt_result** out) {
 int vt_engine_stats(const vt_engine* e, vt_stats* out) {
     if (!e || !out) return VT_ERR_INVALID;
     *out = e->stats;
+    return VT_OK;
+}
+int vt_engine_set_fp32_band(vt_engine* e, double ulps) {
+    if (!e || !(ulps > 0.0) || !std::isfinite(ulps)) return VT_ERR_INVALID;
+    e->fp32_band_ulps = ulps;
     return VT_OK;
 }
 int vt_engine_set_timing(vt_engine* e, int on) {

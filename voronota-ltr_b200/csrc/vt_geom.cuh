@@ -129,10 +129,6 @@ struct Dec {
     }
 };
 
-// Tolerances of the FP32 band, relative to a length scale S of the pair (R_a).
-// KTOL is ~2^-14: several hundred float ulps, covering the error accumulated through
-// the contour cuts.  The FP64 path ignores them.
-constexpr float kTolRel = 6.1035e-05f;
 
 // ---- sphere predicates (geometry.rs:66-82) ----
 template <typename T, bool F>
@@ -181,10 +177,12 @@ __device__ __forceinline__ V3<T> plane_segment(Dec<T, F>& d, V3<T> pp, V3<T> n, 
     T t = da / (da - db);
     return a + (b - a) * t;
 }
-// triangle_area (:152-154)
-template <typename T>
-__device__ __forceinline__ T triangle_area(V3<T> a, V3<T> b, V3<T> c) {
-    return norm(cross(b - a, c - a)) / (T)2;
+// triangle_area (:152-154); FP32 with a correctly rounded square root (an output value)
+__device__ __forceinline__ double triangle_area(V3<double> a, V3<double> b, V3<double> c) {
+    return norm(cross(b - a, c - a)) / 2.0;
+}
+__device__ __forceinline__ float triangle_area(V3<float> a, V3<float> b, V3<float> c) {
+    return 0.5f * __fsqrt_rn(norm2(cross(b - a, c - a)));
 }
 
 // angle between two vectors: FP64 follows min_angle (:157-161) exactly (acos of the
@@ -195,18 +193,37 @@ __device__ __forceinline__ double vec_angle(V3<double> u, V3<double> v) {
     c = c < -1.0 ? -1.0 : (c > 1.0 ? 1.0 : c);
     return acos(c);
 }
-__device__ __forceinline__ float vec_angle(V3<float> u, V3<float> v) {
-    return atan2f(norm(cross(u, v)), dot(u, v));
+// FP32 angles are formed in double from the float vectors: products of floats are exact
+// in double, so the only error left is the (unbiased) rounding of the float inputs.  A
+// biased angle would bias every solid angle and, through SAS = (4 pi - sum) R^2 of a
+// buried ball, be amplified in the SAS areas.
+__device__ __forceinline__ V3<double> widen(V3<float> v) { return {(double)v.x, (double)v.y, (double)v.z}; }
+__device__ __forceinline__ double vec_angle_wide(V3<float> u, V3<float> v) {
+    V3<double> a = widen(u), b = widen(v);
+    return atan2(norm(cross(a, b)), dot(a, b));
+}
+__device__ __forceinline__ float vec_angle(V3<float> u, V3<float> v) { return (float)vec_angle_wide(u, v); }
+// pi minus the angle between u and v (FP32 turn terms of the solid angle), in double.
+__device__ __forceinline__ double vec_supplement(V3<float> u, V3<float> v) {
+    V3<double> a = widen(u), b = widen(v);
+    return atan2(norm(cross(a, b)), -dot(a, b));
 }
 
-// directed_angle (:165-176)
+// directed_angle (:165-176).  FP32: the angle and its reflex form 2 pi - angle are
+// evaluated in double and rounded once.
 template <typename T, bool F>
 __device__ __forceinline__ T directed_angle(Dec<T, F>& d, V3<T> o, V3<T> a, V3<T> b, V3<T> c, T tol) {
-    T angle = vec_angle(a - o, b - o);
     V3<T> v1 = normalize(a - o), v2 = normalize(b - o);
     V3<T> n = cross(v1, v2);
-    if (d.greater_eq(dot(c - o, n), (T)0, tol)) return angle;
-    return (T)kTau - angle;
+    bool direct = d.greater_eq(dot(c - o, n), (T)0, tol);
+    if constexpr (sizeof(T) == 4) {
+        double angle = vec_angle_wide(a - o, b - o);
+        return (T)(direct ? angle : kTau - angle);
+    } else {
+        T angle = vec_angle(a - o, b - o);
+        if (direct) return angle;
+        return (T)kTau - angle;
+    }
 }
 
 // any_normal_of_vector (:179-193)
@@ -249,14 +266,18 @@ __device__ __forceinline__ Sph<double> intersection_circle(const Sph<double>& a,
     V3<double> center = a.c + cv * (a.r * cos_g / cm);
     return {center, a.r * sin_g};
 }
+// The FP32 circle feeds every output value (areas, arc lengths, solid angles), so it is
+// formed with correctly rounded square roots and divisions even where the kernel is
+// compiled with approximate ones.
+__device__ __forceinline__ float norm_rn(V3<float> v) { return __fsqrt_rn(norm2(v)); }
 __device__ __forceinline__ Sph<float> intersection_circle(const Sph<float>& a, const Sph<float>& b) {
     V3<float> cv = b.c - a.c;
-    float cm = norm(cv);
+    float cm = norm_rn(cv);
     if (cm < (float)kEps) return {a.c, 0.0f};
-    float h = (a.r * a.r + cm * cm - b.r * b.r) / (2.0f * cm);
+    float h = __fdiv_rn(a.r * a.r + cm * cm - b.r * b.r, 2.0f * cm);
     float s = a.r + b.r, dr = a.r - b.r;
-    float r2 = (s - cm) * (s + cm) * (cm - dr) * (cm + dr) / (4.0f * cm * cm);
-    return {a.c + cv * (h / cm), sqrtf(fmaxf(r2, 0.0f))};
+    float r2 = __fdiv_rn((s - cm) * (s + cm) * (cm - dr) * (cm + dr), 4.0f * cm * cm);
+    return {a.c + cv * __fdiv_rn(h, cm), __fsqrt_rn(fmaxf(r2, 0.0f))};
 }
 // center_of_intersection_circle (:218-226)
 __device__ __forceinline__ V3<double> ic_center(const Sph<double>& a, const Sph<double>& b) {
@@ -322,6 +343,16 @@ __device__ __forceinline__ T min_dihedral(V3<T> o, V3<T> a, V3<T> b1, V3<T> b2) 
     V3<T> d1 = b1 - (o + oa * dot(oa, b1 - o));
     V3<T> d2 = b2 - (o + oa * dot(oa, b2 - o));
     return vec_angle(d1, d2);
+}
+// pi - min_dihedral_angle, computed directly (FP32 turn terms of the solid angle); the
+// unit vector uses correctly rounded square root and division.
+__device__ __forceinline__ double dihedral_supplement(V3<float> o, V3<float> a, V3<float> b1, V3<float> b2) {
+    V3<float> ao = a - o;
+    float l = __fsqrt_rn(norm2(ao));
+    V3<float> oa = {__fdiv_rn(ao.x, l), __fdiv_rn(ao.y, l), __fdiv_rn(ao.z, l)};
+    V3<float> d1 = b1 - (o + oa * dot(oa, b1 - o));
+    V3<float> d2 = b2 - (o + oa * dot(oa, b2 - o));
+    return vec_supplement(d1, d2);
 }
 
 }  // namespace vt

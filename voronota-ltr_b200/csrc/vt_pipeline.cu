@@ -65,16 +65,34 @@ __global__ void k_prepare(const double* __restrict__ xyzr, uint32_t n, double pr
 }
 
 __global__ void k_bbox_final(const BBox* __restrict__ p, int nb, BBox* out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    BBox b = p[0];
-    for (int i = 1; i < nb; ++i) {
+    __shared__ double s[7][kBlock];
+    const int t = threadIdx.x;
+    double v[7] = {DBL_MAX, DBL_MAX, DBL_MAX, -DBL_MAX, -DBL_MAX, -DBL_MAX, 0.0};
+    for (int i = t; i < nb; i += blockDim.x) {
         for (int k = 0; k < 3; ++k) {
-            b.mn[k] = fmin(b.mn[k], p[i].mn[k]);
-            b.mx[k] = fmax(b.mx[k], p[i].mx[k]);
+            v[k] = fmin(v[k], p[i].mn[k]);
+            v[k + 3] = fmax(v[k + 3], p[i].mx[k]);
         }
-        b.max_r = fmax(b.max_r, p[i].max_r);
+        v[6] = fmax(v[6], p[i].max_r);
     }
-    *out = b;
+    for (int k = 0; k < 7; ++k) s[k][t] = v[k];
+    __syncthreads();
+    for (int o = kBlock / 2; o > 0; o >>= 1) {
+        if (t < o) {
+            for (int k = 0; k < 3; ++k) s[k][t] = fmin(s[k][t], s[k][t + o]);
+            for (int k = 3; k < 7; ++k) s[k][t] = fmax(s[k][t], s[k][t + o]);
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        BBox b;
+        for (int k = 0; k < 3; ++k) {
+            b.mn[k] = s[k][0];
+            b.mx[k] = s[k + 3][0];
+        }
+        b.max_r = s[6][0];
+        *out = b;
+    }
 }
 
 // ---- periodic images (types.rs:323-375): only images within `reach` of the balls'
@@ -355,36 +373,43 @@ __device__ __forceinline__ double wsum_d(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
-__global__ void __launch_bounds__(kCellWarps * 32) k_cells(DevBufs b) {
+// Pair index of the pair between ball i and its neighbour entry e (CSR position):
+// pairs (i, j) with j > i or j a periodic image sit in i's own list; pairs (j, i) with
+// j < i are found by locating i in j's sorted list by its (value, id) key.
+__device__ __forceinline__ int32_t incident_pair(const DevBufs& b, uint32_t i, double4 Si, uint32_t e,
+                                                 bool* side_a) {
+    const uint32_t n = b.n;
+    uint32_t j = b.nb_id[e];
+    *side_a = true;
+    if ((b.periodic && j >= n) || j > i) return b.nb_pair[e];
+    double v = dist_to_ic_center(sph_of(b.sph[j]), sph_of(Si));
+    uint32_t lo = b.nb_off[j], hi = lo + b.nb_cnt[j];
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (vless(b.nb_val[mid], b.nb_id[mid], v, i))
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    if (lo < b.nb_off[j] + b.nb_cnt[j] && b.nb_id[lo] == i) {
+        *side_a = false;
+        return b.nb_pair[lo];
+    }
+    return -1;
+}
+
+__global__ void __launch_bounds__(kCellWarps * 32) k_cells(DevBufs b, float cell_band, int only_dirty) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t n = b.n;
     for (uint32_t i = blockIdx.x * kCellWarps + w; i < n; i += gridDim.x * kCellWarps) {
+        if (only_dirty && !b.ball_dirty[i]) continue;
         const uint32_t cnt = b.nb_cnt[i], off = b.nb_off[i];
         const double4 Si = b.sph[i];
         double area = 0, arc = 0, spos = 0, sneg = 0, ppos = 0, pneg = 0;
         uint32_t count = 0;
         for (uint32_t e = lane; e < cnt; e += 32) {
-            uint32_t j = b.nb_id[off + e];
-            int32_t p = -1;
-            bool side_a = true;
-            if ((b.periodic && j >= n) || j > i) {
-                p = b.nb_pair[off + e];
-            } else {
-                // mirror entry: i in j's sorted list, located by its (value, id) key
-                double v = dist_to_ic_center(sph_of(b.sph[j]), sph_of(Si));
-                uint32_t lo = b.nb_off[j], hi = lo + b.nb_cnt[j];
-                while (lo < hi) {
-                    uint32_t mid = (lo + hi) >> 1;
-                    if (vless(b.nb_val[mid], b.nb_id[mid], v, i))
-                        lo = mid + 1;
-                    else
-                        hi = mid;
-                }
-                if (lo < b.nb_off[j] + b.nb_cnt[j] && b.nb_id[lo] == i) {
-                    p = b.nb_pair[lo];
-                    side_a = false;
-                }
-            }
+            bool side_a;
+            int32_t p = incident_pair(b, i, Si, off + e, &side_a);
             if (p >= 0 && (b.p_status[p] & kValid)) {
                 double sa = side_a ? b.p_sa_a[p] : b.p_sa_b[p];
                 double pv = side_a ? b.p_pv_a[p] : b.p_pv_b[p];
@@ -411,6 +436,21 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_cells(DevBufs b) {
             if (count > 0) {  // CellContactSummary::compute_sas (types.rs:623-663)
                 flag = 1;
                 double diff = fabs(spos - sneg);
+                bool unsure = false;
+                if (cell_band > 0.f && arc > 0.0) {
+                    // FP32-derived sums: both branch decisions need a margin
+                    double tol_sa = (double)cell_band * count;
+                    if (fabs(spos - sneg) <= tol_sa + 1e-10) unsure = true;
+                    double sas_g = spos > sneg ? fma(4.0, kPi, -(spos - sneg)) * r * r : (sneg - spos) * r * r;
+                    double vol_g = sas_g * r / 3.0 + ppos - pneg;
+                    double full_g = 4.0 / 3.0 * kPi * r * r * r;
+                    double tol_v = (double)cell_band * count * (ppos + pneg + r * r * r);
+                    if (fabs(vol_g - full_g) <= tol_v) unsure = true;
+                }
+                if (unsure) {
+                    uint32_t at = atomicAdd(b.d_cell_redo_count, 1u);
+                    b.cell_redo_list[at] = i;
+                }
                 if (arc > 0.0 && diff > 1e-10) {
                     if (spos > sneg) {
                         sas = fma(4.0, kPi, -fmax(spos - sneg, 0.0)) * r * r;
@@ -434,6 +474,27 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_cells(DevBufs b) {
             b.cell_flag[i] = flag;
             b.cell_sas[i] = sas;
             b.cell_vol[i] = vol;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kCellWarps * 32) k_mark_ball_pairs(DevBufs b) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t m = *b.d_cell_redo_count;
+    for (uint32_t k = blockIdx.x * kCellWarps + w; k < m; k += gridDim.x * kCellWarps) {
+        const uint32_t i = b.cell_redo_list[k];
+        const uint32_t cnt = b.nb_cnt[i], off = b.nb_off[i];
+        const double4 Si = b.sph[i];
+        if (lane == 0) b.ball_dirty[i] = 1;
+        for (uint32_t e = lane; e < cnt; e += 32) {
+            bool side_a;
+            int32_t p = incident_pair(b, i, Si, off + e, &side_a);
+            uint32_t j = b.nb_id[off + e];
+            if (j < b.n) b.ball_dirty[j] = 1;
+            if (p >= 0) {
+                uint32_t at = atomicAdd(b.d_redo_count, 1u);
+                b.redo_list[at] = (uint32_t)p;
+            }
         }
     }
 }
@@ -674,7 +735,7 @@ void launch_prepare(const DevBufs& b, const double* d_xyzr, double probe, BBox* 
     k_prepare<<<nblocks, kBlock, 0, s>>>(d_xyzr, b.n, probe, b.sph, b.slot_id, d_parts, b.err); count_launch();
 }
 void launch_bbox_final(const BBox* parts, int nblocks, BBox* out, cudaStream_t s) {
-    k_bbox_final<<<1, 32, 0, s>>>(parts, nblocks, out); count_launch();
+    k_bbox_final<<<1, kBlock, 0, s>>>(parts, nblocks, out); count_launch();
 }
 void launch_images(const DevBufs& b, double reach, const BBox* d_bbox, uint32_t* img_cnt, uint32_t* img_off,
                    uint32_t* scan_tmp, size_t, cudaStream_t s) {
@@ -702,9 +763,12 @@ void launch_search_fill(const DevBufs& b, int want_rel, cudaStream_t s) {
     int gb = grid_for(b.n, kSearchWarps, 148 * 64);
     k_search<true><<<gb, kSearchWarps * 32, 0, s>>>(b, want_rel); count_launch();
 }
-void launch_cells(const DevBufs& b, cudaStream_t s) {
+void launch_cells(const DevBufs& b, float cell_band, int only_dirty, cudaStream_t s) {
     int gb = grid_for(b.n, kCellWarps, 148 * 32);
-    k_cells<<<gb, kCellWarps * 32, 0, s>>>(b); count_launch();
+    k_cells<<<gb, kCellWarps * 32, 0, s>>>(b, cell_band, only_dirty); count_launch();
+}
+void launch_mark_ball_pairs(const DevBufs& b, cudaStream_t s) {
+    k_mark_ball_pairs<<<64, kCellWarps * 32, 0, s>>>(b); count_launch();
 }
 void launch_dedup(const DevBufs& b, uint32_t P, int contacts_only, cudaStream_t s) {
     int gb = grid_for(P, kBlock);

@@ -109,6 +109,11 @@ struct DevBufs {
     uint32_t* err;        // device error bits
     uint32_t* zero_word;  // a device word that stays 0 (an empty count)
     uint32_t* params_u;   // n words of scratch (cell flags widened for the scan)
+    float fp32_band;      // FP32 error floor of a computed length, relative to the pair scale
+    // cells whose compute_sas branch is uncertain with FP32 inputs (FP32 path only)
+    uint32_t* cell_redo_list;
+    uint32_t* d_cell_redo_count;
+    uint8_t* ball_dirty;  // balls whose cell is recomputed after the FP64 fixup
 };
 
 // Host-visible bounding-box reduction result.
@@ -130,7 +135,13 @@ void launch_grid(const DevBufs& b, uint32_t ncell, uint32_t max_slots, uint32_t*
                  cudaStream_t s);
 void launch_search_count(const DevBufs& b, cudaStream_t s);
 void launch_search_fill(const DevBufs& b, int want_rel, cudaStream_t s);
-void launch_cells(const DevBufs& b, cudaStream_t s);
+// cell_band > 0 (FP32 inputs): balls whose compute_sas branch decisions lie within
+// cell_band radians per contributing contact of their thresholds go to cell_redo_list.
+// only_dirty: recompute only balls flagged in ball_dirty.
+void launch_cells(const DevBufs& b, float cell_band, int only_dirty, cudaStream_t s);
+// Append every pair incident to a ball of cell_redo_list to redo_list and mark the
+// ball and its neighbours dirty.
+void launch_mark_ball_pairs(const DevBufs& b, cudaStream_t s);
 void launch_dedup(const DevBufs& b, uint32_t P, int contacts_only, cudaStream_t s);
 void launch_compact(const DevBufs& b, uint32_t P, int contacts_only, uint32_t* scan_tmp, size_t scan_tmp_words,
                     cudaStream_t s);

@@ -52,7 +52,7 @@ class VtStats(ctypes.Structure):
         "num_fp64_redo", "num_serial")] + [
         ("total_sas_area", ctypes.c_double), ("total_volume", ctypes.c_double),
         ("total_contact_area", ctypes.c_double), ("device_error_bits", ctypes.c_uint32),
-        ("num_kernel_launches", ctypes.c_uint64)]
+        ("num_kernel_launches", ctypes.c_uint64), ("num_cell_redo", ctypes.c_uint64)]
 
 STAGES = ("prepare", "images", "grid", "neighbor_count", "neighbor_fill", "contact", "fp64_recompute",
           "serial_fallback", "cells", "output", "call")
@@ -101,6 +101,7 @@ def library():
     L.vt_engine_stats.argtypes = [_vp, ctypes.POINTER(VtStats)]
     L.vt_engine_device_outputs.argtypes = [_vp, ctypes.POINTER(VtDeviceOutputs)]
     L.vt_engine_set_timing.argtypes = [_vp, ctypes.c_int]
+    L.vt_engine_set_fp32_band.argtypes = [_vp, ctypes.c_double]
     L.vt_engine_stage_times.argtypes = [_vp, _f64p]
     L.vt_status_string.argtypes = [ctypes.c_int]
     L.vt_status_string.restype = ctypes.c_char_p
@@ -331,6 +332,9 @@ class Engine:
         s = VtStats()
         _check(self._L.vt_engine_stats(self._h, ctypes.byref(s)))
         return s
+
+    def set_fp32_band(self, ulps: float):
+        _check(self._L.vt_engine_set_fp32_band(self._h, float(ulps)))
 
     def set_timing(self, on: bool = True):
         _check(self._L.vt_engine_set_timing(self._h, 1 if on else 0))
