@@ -124,6 +124,58 @@ typedef struct vt_device_outputs {
 } vt_device_outputs;
 int vt_engine_device_outputs(const vt_engine* e, vt_device_outputs* out);
 
+/* ---- updateable tessellation ----
+ * Replaces UpdateableTessellation (src/updateable.rs:154-742) with its state held on the
+ * device: stored balls, exclusion statuses, neighbour lists, the per-ball contact table
+ * and the cells.  An update recomputes only the affected balls (the changed balls and
+ * their old and new neighbours): neighbour search of those balls, the pairs with both
+ * ends affected, their contacts, and the affected cells.  One handle per host thread;
+ * each handle owns a CUDA stream on its device.  Return values of the reference's bool
+ * methods come back through the int* arguments (may be NULL).
+ *
+ * Behaviour follows the reference, with one deviation: the neighbour grid is rebuilt
+ * from the stored balls, so a ball that crossed a grid cell is not left registered in
+ * its old cell (src/spheres_searcher.rs:144-175 removes it from the cell of its new
+ * position).  Summary contact order is the reference's: by owning ball, then in the
+ * order the contacts were added (src/updateable.rs:332-378). */
+typedef struct vt_updateable vt_updateable;
+/* new() / with_backup() (src/updateable.rs:154-182); precision VT_FP64 or VT_FP32_FIXUP. */
+int vt_upd_create(int device, int with_backup, int precision, vt_updateable** out);
+void vt_upd_destroy(vt_updateable* h);
+int vt_upd_set_stream(vt_updateable* h, void* stream);
+/* init(balls, probe, periodic_box) (src/updateable.rs:187-201); *ok = its return value. */
+int vt_upd_init(vt_updateable* h, const double* xyzr, uint64_t n, double probe, const double* periodic_box9,
+                int* ok);
+/* update(balls) (src/updateable.rs:207-209): every ball compared with the stored one. */
+int vt_upd_update(vt_updateable* h, const double* xyzr, uint64_t n, int* changed);
+/* update_with_changed(balls, changed_ids) (src/updateable.rs:215-220): only the listed
+ * balls are read; ids >= n are ignored. */
+int vt_upd_update_with_changed(vt_updateable* h, const double* xyzr, uint64_t n, const uint64_t* ids, uint64_t k,
+                               int* changed);
+/* Device-resident variants: d_xyzr (n x 4 doubles) and d_ids on the handle's device,
+ * ordered on the handle's stream; no host copy of the balls. */
+int vt_upd_init_device(vt_updateable* h, const double* d_xyzr, uint64_t n, double probe,
+                       const double* periodic_box9, int* ok);
+int vt_upd_update_with_changed_device(vt_updateable* h, const double* d_xyzr, uint64_t n, const uint64_t* d_ids,
+                                      uint64_t k, int* changed);
+/* set_exclusion(id, excluded) (src/updateable.rs:226-271). */
+int vt_upd_set_exclusion(vt_updateable* h, uint64_t id, int excluded, int* changed);
+/* restore() (src/updateable.rs:277-322): back to the state before the last operation
+ * (handles created with backup); *ok = its return value. */
+int vt_upd_restore(vt_updateable* h, int* ok);
+/* summary() (src/updateable.rs:332-378) as a result object (free with vt_result_free). */
+int vt_upd_summary(vt_updateable* h, vt_result** out);
+/* total SAS area, volume and contact area of the current summary (3 doubles). */
+int vt_upd_totals(vt_updateable* h, double* totals3);
+/* last_update_was_full_reinit(), changed_ids(), affected_ids() (src/updateable.rs:380-400). */
+int vt_upd_last_full_reinit(const vt_updateable* h);
+uint64_t vt_upd_num_changed(const vt_updateable* h);
+int vt_upd_changed_ids(vt_updateable* h, uint64_t* out);
+uint64_t vt_upd_num_affected(vt_updateable* h);
+int vt_upd_affected_ids(vt_updateable* h, uint64_t* out);
+/* counters of the last operation: list entries, pairs recomputed, FP64 redo, cells */
+int vt_upd_stats(const vt_updateable* h, vt_stats* out);
+
 /* ---- contact descriptors without device allocation ----
  * No counterpart in the reference: an entry point for callers that cannot call
  * cudaMalloc/cudaFree while they run (a custom call inside a framework whose allocator

@@ -27,6 +27,8 @@ UNITS = {
     "vt_contact32.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false", "-DVT_C32_MINB=8"],
     "vt_engine.cu": ["--fmad=false"],
     "vt_noalloc.cu": ["--fmad=false"],
+    "vt_frontier.cu": ["--fmad=false"],
+    "vt_updateable.cu": ["--fmad=false"],
 }
 
 

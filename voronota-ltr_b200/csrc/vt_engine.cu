@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/voronota_b200.h"
+#include "vt_host.cuh"
 #include "vt_pipeline.cuh"
 
 using namespace vt;
@@ -28,53 +29,11 @@ namespace {
 
 thread_local std::string g_last_error;
 
-struct CudaError {
-    int status;
-};
-
-#define VT_CUDA(call)                                                                      \
-    do {                                                                                   \
-        cudaError_t _e = (call);                                                           \
-        if (_e != cudaSuccess) {                                                           \
-            g_last_error = std::string(#call) + ": " + cudaGetErrorString(_e);            \
-            throw CudaError{_e == cudaErrorMemoryAllocation ? VT_ERR_OOM : VT_ERR_CUDA}; \
-        }                                                                                  \
-    } while (0)
-
-template <typename T>
-struct DBuf {
-    T* p = nullptr;
-    size_t cap = 0;
-    void ensure(size_t n) {
-        if (n <= cap && p) return;
-        if (p) cudaFree(p);
-        p = nullptr;
-        size_t c = std::max<size_t>(n + n / 4, 64);
-        VT_CUDA(cudaMalloc(&p, c * sizeof(T)));
-        cap = c;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-    }
-};
-
 }  // namespace
 
 namespace vt {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 }  // namespace vt
-
-struct vt_result {
-    uint64_t num_balls = 0;
-    std::vector<uint32_t> a, b;
-    std::vector<double> area, arc;
-    std::vector<uint8_t> central;
-    std::vector<uint32_t> cell_index;
-    std::vector<double> cell_sas, cell_vol;
-    double totals[3] = {0, 0, 0};
-};
 
 struct vt_engine {
     int device = 0;
@@ -270,31 +229,8 @@ struct vt_engine {
         }
 
         // 3. grid over the extended box (cells of edge >= reach)
-        GridDev g;
-        double ext[3], cell = reach;
-        for (int k = 0; k < 3; ++k) ext[k] = (bb.mx[k] - bb.mn[k]) + 2.0 * reach;
-        double vol_cells = 1.0;
-        auto dims_for = [&](double c, int* d) {
-            for (int k = 0; k < 3; ++k) d[k] = (int)std::floor(ext[k] / c) + 1;
-        };
-        int dd[3];
-        dims_for(cell, dd);
-        vol_cells = (double)dd[0] * dd[1] * dd[2];
-        const double max_cells = 8.0 * (double)max_slots + 4096.0;
-        while (vol_cells > max_cells) {  // sparse inputs: coarser cells keep the grid O(n)
-            cell *= std::cbrt(vol_cells / max_cells) * 1.01;
-            dims_for(cell, dd);
-            vol_cells = (double)dd[0] * dd[1] * dd[2];
-        }
-        g.cell = cell;
-        g.ox = bb.mn[0] - reach;
-        g.oy = bb.mn[1] - reach;
-        g.oz = bb.mn[2] - reach;
-        g.dx = dd[0];
-        g.dy = dd[1];
-        g.dz = dd[2];
-        b.grid = g;
-        const uint32_t ncell = (uint32_t)(dd[0] * (uint64_t)dd[1] * dd[2]);
+        uint32_t ncell = 0;
+        b.grid = plan_grid(bb, reach, max_slots, &ncell);
         cell_count.ensure(ncell);
         cell_start.ensure(ncell + 1);
         cell_cursor.ensure(ncell);
@@ -585,21 +521,6 @@ int validate_host(const double* xyzr, uint64_t n, double probe, const double* pb
 std::mutex g_engines_mu;
 std::vector<std::unique_ptr<vt_engine>> g_engines;
 std::vector<std::unique_ptr<std::mutex>> g_engine_mu;
-
-template <typename F>
-int guarded(F&& f) {
-    try {
-        return f();
-    } catch (const CudaError& e) {
-        return e.status;
-    } catch (const std::bad_alloc&) {
-        g_last_error = "host allocation failed";
-        return VT_ERR_OOM;
-    } catch (...) {
-        g_last_error = "unexpected exception";
-        return VT_ERR_CUDA;
-    }
-}
 
 int host_compute(vt_engine* e, const double* xyzr, uint64_t n, double probe, const double* pbox9,
                  const int32_t* groups, uint64_t n_groups, int precision, int contacts_only) {

@@ -3,6 +3,7 @@
 // operation by operation (compiled with --fmad=false).
 #include <atomic>
 #include <cfloat>
+#include <cmath>
 
 #include "vt_geom.cuh"
 #include "vt_pipeline.cuh"
@@ -97,18 +98,6 @@ __global__ void k_bbox_final(const BBox* __restrict__ p, int nb, BBox* out) {
 
 // ---- periodic images (types.rs:323-375): only images within `reach` of the balls'
 // bounding box can intersect a ball, so only those are materialised.
-__device__ __forceinline__ void neighbor_shift(int g, int& sx, int& sy, int& sz) {
-    int k = g < 13 ? g : g + 1;  // NEIGHBOR_SHIFTS skips the origin (index 13 of 27)
-    sx = k / 9 - 1;
-    sy = (k / 3) % 3 - 1;
-    sz = k % 3 - 1;
-}
-__device__ __forceinline__ double4 shift_sphere(double4 s, const double* pb, double wa, double wb, double wc) {
-    // PeriodicBox::shift_sphere (types.rs:323-347): c.mul_add(wc, b.mul_add(wb, a.mul_add(wa, x)))
-    return make_double4(fma(pb[6], wc, fma(pb[3], wb, fma(pb[0], wa, s.x))),
-                        fma(pb[7], wc, fma(pb[4], wb, fma(pb[1], wa, s.y))),
-                        fma(pb[8], wc, fma(pb[5], wb, fma(pb[2], wa, s.z))), s.w);
-}
 struct PBoxArg {
     double v[9];
 };
@@ -172,14 +161,15 @@ __global__ void k_cell_hist(const double4* __restrict__ sph, const uint32_t* __r
 }
 __global__ void k_cell_scatter(const double4* __restrict__ sph, const uint32_t* __restrict__ slot_id,
                                const uint32_t* __restrict__ d_nslots, GridDev g, uint32_t* __restrict__ cursor,
-                               double4* __restrict__ c_pos, uint32_t* __restrict__ c_id, uint32_t* __restrict__ c_slot) {
+                               double4* __restrict__ c_pos, uint32_t* __restrict__ c_id, uint32_t* __restrict__ c_slot,
+                               int slot_is_id) {
     uint32_t ns = *d_nslots;
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < ns; s += gridDim.x * blockDim.x) {
         double4 p = sph[s];
         uint32_t at = atomicAdd(&cursor[slot_cell(g, p)], 1u);
         c_pos[at] = p;
         c_id[at] = slot_id[s];
-        c_slot[at] = s;
+        c_slot[at] = slot_is_id ? slot_id[s] : s;
     }
 }
 
@@ -204,7 +194,9 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_search(DevBufs b, int wan
     const GridDev g = b.grid;
     const uint32_t n = b.n;
     Dec<double, false> d;
-    for (uint32_t i = blockIdx.x * kSearchWarps + w; i < n; i += gridDim.x * kSearchWarps) {
+    const uint32_t rows = b.frontier ? b.n_frontier : n;
+    for (uint32_t row = blockIdx.x * kSearchWarps + w; row < rows; row += gridDim.x * kSearchWarps) {
+        const uint32_t i = b.frontier ? b.frontier[row] : row;
         const double4 A4 = b.sph[i];
         const Sph<double> A = sph_of(A4);
         int cx = cell_coord(A4.x, g.ox, g.cell, g.dx), cy = cell_coord(A4.y, g.oy, g.cell, g.dy),
@@ -283,7 +275,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_search(DevBufs b, int wan
         __syncwarp();
         if (!FILL) {
             uint32_t np = 0;
-            for (uint32_t e = lane; e < cnt; e += 32) {
+            for (uint32_t e = lane; e < cnt && !b.no_pairs; e += 32) {
                 uint32_t bid = s_id[w][e];
                 uint32_t bc = b.periodic ? bid % n : bid;
                 bool gen = !same_group(b.groups, b.n_groups, i, bc) && ((b.periodic && bid >= n) || i < bid);
@@ -291,8 +283,8 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_search(DevBufs b, int wan
             }
             for (int o = 16; o > 0; o >>= 1) np += __shfl_xor_sync(0xffffffffu, np, o);
             if (lane == 0) {
-                b.nb_cnt[i] = cnt;
-                b.nb_npair[i] = np;
+                b.nb_cnt[row] = cnt;
+                if (!b.no_pairs) b.nb_npair[row] = np;
                 b.excluded[i] = hidden ? 1 : 0;
             }
             __syncwarp();
@@ -332,8 +324,8 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_search(DevBufs b, int wan
                 }
             }
         }
-        const uint32_t off = b.nb_off[i];
-        uint32_t prank = b.pair_off[i];
+        const uint32_t off = b.nb_off[row];
+        uint32_t prank = b.no_pairs ? 0u : b.pair_off[row];
         for (uint32_t e0 = 0; e0 < cnt; e0 += 32) {
             uint32_t e = e0 + lane;
             bool gen = false;
@@ -342,7 +334,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_search(DevBufs b, int wan
                 bid = s_id[w][e];
                 bslot = s_slot[w][e];
                 uint32_t bc = b.periodic ? bid % n : bid;
-                gen = !same_group(b.groups, b.n_groups, i, bc) && ((b.periodic && bid >= n) || i < bid);
+                gen = !b.no_pairs && !same_group(b.groups, b.n_groups, i, bc) && ((b.periodic && bid >= n) || i < bid);
             }
             unsigned m = __ballot_sync(0xffffffffu, gen);
             if (e < cnt) {
@@ -355,7 +347,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_search(DevBufs b, int wan
                     b.pair_a[pidx] = i;
                     b.pair_e[pidx] = off + e;
                 }
-                b.nb_pair[off + e] = pidx;
+                if (!b.no_pairs) b.nb_pair[off + e] = pidx;
                 if (want_rel) {
                     double4 C = b.sph[bslot];
                     b.nb_rel[off + e] = make_float4((float)(C.x - A4.x), (float)(C.y - A4.y), (float)(C.z - A4.z),
@@ -435,38 +427,15 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_cells(DevBufs b, float cell
             double sas = 0.0, vol = 0.0;
             if (count > 0) {  // CellContactSummary::compute_sas (types.rs:623-663)
                 flag = 1;
-                double diff = fabs(spos - sneg);
                 bool unsure = false;
-                if (cell_band > 0.f && arc > 0.0) {
-                    // FP32-derived sums: both branch decisions need a margin
-                    double tol_sa = (double)cell_band * count;
-                    if (fabs(spos - sneg) <= tol_sa + 1e-10) unsure = true;
-                    double sas_g = spos > sneg ? fma(4.0, kPi, -(spos - sneg)) * r * r : (sneg - spos) * r * r;
-                    double vol_g = sas_g * r / 3.0 + ppos - pneg;
-                    double full_g = 4.0 / 3.0 * kPi * r * r * r;
-                    double tol_v = (double)cell_band * count * (ppos + pneg + r * r * r);
-                    if (fabs(vol_g - full_g) <= tol_v) unsure = true;
-                }
+                cell_from_sums(count, arc, spos, sneg, ppos, pneg, r, cell_band, &unsure, &sas, &vol);
                 if (unsure) {
                     uint32_t at = atomicAdd(b.d_cell_redo_count, 1u);
                     b.cell_redo_list[at] = i;
                 }
-                if (arc > 0.0 && diff > 1e-10) {
-                    if (spos > sneg) {
-                        sas = fma(4.0, kPi, -fmax(spos - sneg, 0.0)) * r * r;
-                    } else {
-                        sas = fmax(sneg - spos, 0.0) * r * r;
-                    }
-                    vol = (sas * r / 3.0) + ppos - pneg;
-                    double full = 4.0 / 3.0 * kPi * r * r * r;
-                    if (vol > full) {
-                        sas = 0.0;
-                        vol = ppos - pneg;
-                    }
-                } else {
-                    vol = ppos - pneg;
-                }
-            } else if (cnt == 0) {  // compute_sas_detached (types.rs:666-675)
+            } else if (cnt == 0 && !(b.detached_excl && b.excluded[i])) {
+                // compute_sas_detached (types.rs:666-675); the updateable tessellation also
+                // requires the ball not to be excluded (updateable.rs:680-685)
                 flag = 1;
                 sas = 4.0 * kPi * r * r;
                 vol = sas * r / 3.0;
@@ -753,7 +722,7 @@ void launch_grid(const DevBufs& b, uint32_t ncell, uint32_t max_slots, uint32_t*
     scan_u32(b.cell_count, b.cell_start, ncell, scan_tmp, s);
     cudaMemcpyAsync(b.cell_cursor, b.cell_start, sizeof(uint32_t) * ncell, cudaMemcpyDeviceToDevice, s);
     k_cell_scatter<<<gb, kBlock, 0, s>>>(b.sph, b.slot_id, b.d_nslots, b.grid, b.cell_cursor, b.c_pos, b.c_id,
-                                         b.c_slot); count_launch();
+                                         b.c_slot, b.slot_is_id); count_launch();
 }
 void launch_search_count(const DevBufs& b, cudaStream_t s) {
     int gb = grid_for(b.n, kSearchWarps, 148 * 64);
@@ -800,6 +769,39 @@ void launch_totals(const DevBufs& b, uint32_t P, int contacts_only, cudaStream_t
                                                      b.partials); count_launch();
     }
     k_final_sums<<<1, 32, 0, s>>>(b.partials, b.totals); count_launch();
+}
+void launch_sums3(const double* x0, const uint32_t* cnt0, const double* x1, const double* x2, const uint32_t* cnt1,
+                  double* partials, double* totals, cudaStream_t s) {
+    k_partial_sums<<<kSumBlocks, kBlock, 0, s>>>(x0, cnt0, x1, x2, cnt1, partials); count_launch();
+    k_final_sums<<<1, 32, 0, s>>>(partials, totals); count_launch();
+}
+int grid_blocks(size_t n, int block, int cap) { return grid_for(n, block, cap); }
+
+GridDev plan_grid(const BBox& bb, double reach, size_t max_slots, uint32_t* ncell) {
+    double ext[3], cell = reach;
+    for (int k = 0; k < 3; ++k) ext[k] = (bb.mx[k] - bb.mn[k]) + 2.0 * reach;
+    auto dims_for = [&](double c, int* d) {
+        for (int k = 0; k < 3; ++k) d[k] = (int)std::floor(ext[k] / c) + 1;
+    };
+    int dd[3];
+    dims_for(cell, dd);
+    double vol_cells = (double)dd[0] * dd[1] * dd[2];
+    const double max_cells = 8.0 * (double)max_slots + 4096.0;
+    while (vol_cells > max_cells) {  // sparse inputs: coarser cells keep the grid O(n)
+        cell *= std::cbrt(vol_cells / max_cells) * 1.01;
+        dims_for(cell, dd);
+        vol_cells = (double)dd[0] * dd[1] * dd[2];
+    }
+    GridDev g;
+    g.cell = cell;
+    g.ox = bb.mn[0] - reach;
+    g.oy = bb.mn[1] - reach;
+    g.oz = bb.mn[2] - reach;
+    g.dx = dd[0];
+    g.dy = dd[1];
+    g.dz = dd[2];
+    *ncell = (uint32_t)(dd[0] * (uint64_t)dd[1] * dd[2]);
+    return g;
 }
 void launch_collect_redo(const DevBufs& b, uint32_t P, cudaStream_t s) {
     cudaMemsetAsync(b.d_redo_count, 0, sizeof(uint32_t), s);

@@ -36,6 +36,11 @@ enum PairStatus : uint8_t {
 constexpr int kSortCap = 256;       // neighbour list capacity of the warp sort buffer
 constexpr int kSerialCap = 256;     // contour capacity of the serial fallback
 
+// Host-visible bounding-box reduction result.
+struct BBox {
+    double mn[3], mx[3], max_r;
+};
+
 struct GridDev {
     double ox, oy, oz, cell;
     int dx, dy, dz;
@@ -114,12 +119,68 @@ struct DevBufs {
     uint32_t* cell_redo_list;
     uint32_t* d_cell_redo_count;
     uint8_t* ball_dirty;  // balls whose cell is recomputed after the FP64 fixup
+    // updateable tessellation (all zero for the stateless path)
+    const uint32_t* frontier;  // search only these balls; per-ball CSR arrays are then
+    uint32_t n_frontier;       // indexed by frontier position (excluded stays per ball)
+    int no_pairs;              // fill pass writes the neighbour lists only
+    int slot_is_id;            // grid slots carry reference ids as their sph index
+    int detached_excl;         // cells: an empty list is detached only when not excluded
 };
 
-// Host-visible bounding-box reduction result.
-struct BBox {
-    double mn[3], mx[3], max_r;
-};
+
+#ifdef __CUDACC__
+// NEIGHBOR_SHIFTS (types.rs:292-302) without the origin: image g of ball j has id (g+1) n + j.
+__device__ __forceinline__ void neighbor_shift(int g, int& sx, int& sy, int& sz) {
+    int k = g < 13 ? g : g + 1;
+    sx = k / 9 - 1;
+    sy = (k / 3) % 3 - 1;
+    sz = k % 3 - 1;
+}
+// PeriodicBox::shift_sphere (types.rs:323-347): c.mul_add(wc, b.mul_add(wb, a.mul_add(wa, x)))
+__device__ __forceinline__ double4 shift_sphere(double4 s, const double* pb, double wa, double wb, double wc) {
+    return make_double4(fma(pb[6], wc, fma(pb[3], wb, fma(pb[0], wa, s.x))),
+                        fma(pb[7], wc, fma(pb[4], wb, fma(pb[1], wa, s.y))),
+                        fma(pb[8], wc, fma(pb[5], wb, fma(pb[2], wa, s.z))), s.w);
+}
+// CellContactSummary::compute_sas (types.rs:623-663) from the accumulated sums of a cell
+// with count > 0 contributing contacts.  cell_band > 0 (sums of FP32-derived values):
+// *unsure is set when a branch decision lies within cell_band radians per contact of
+// its threshold.
+__device__ __forceinline__ void cell_from_sums(uint32_t count, double arc, double spos, double sneg, double ppos,
+                                               double pneg, double r, float cell_band, bool* unsure, double* sas_out,
+                                               double* vol_out) {
+    const double kPiD = 3.141592653589793;
+    double sas = 0.0, vol = 0.0;
+    double diff = fabs(spos - sneg);
+    *unsure = false;
+    if (cell_band > 0.f && arc > 0.0) {
+        double tol_sa = (double)cell_band * count;
+        if (fabs(spos - sneg) <= tol_sa + 1e-10) *unsure = true;
+        double sas_g = spos > sneg ? fma(4.0, kPiD, -(spos - sneg)) * r * r : (sneg - spos) * r * r;
+        double vol_g = sas_g * r / 3.0 + ppos - pneg;
+        double full_g = 4.0 / 3.0 * kPiD * r * r * r;
+        double tol_v = (double)cell_band * count * (ppos + pneg + r * r * r);
+        if (fabs(vol_g - full_g) <= tol_v) *unsure = true;
+    }
+    if (arc > 0.0 && diff > 1e-10) {
+        if (spos > sneg) {
+            sas = fma(4.0, kPiD, -fmax(spos - sneg, 0.0)) * r * r;
+        } else {
+            sas = fmax(sneg - spos, 0.0) * r * r;
+        }
+        vol = (sas * r / 3.0) + ppos - pneg;
+        double full = 4.0 / 3.0 * kPiD * r * r * r;
+        if (vol > full) {
+            sas = 0.0;
+            vol = ppos - pneg;
+        }
+    } else {
+        vol = ppos - pneg;
+    }
+    *sas_out = sas;
+    *vol_out = vol;
+}
+#endif
 
 // Host-side count of kernel launches issued by this library (all devices, all engines).
 void count_launch();
@@ -147,6 +208,15 @@ void launch_compact(const DevBufs& b, uint32_t P, int contacts_only, uint32_t* s
                     cudaStream_t s);
 void launch_totals(const DevBufs& b, uint32_t P, int contacts_only, cudaStream_t s);
 void launch_collect_redo(const DevBufs& b, uint32_t P, cudaStream_t s);
+// Deterministic FP64 totals: totals[0] = sum x1[0..*cnt1), totals[1] = sum x2[0..*cnt1),
+// totals[2] = sum x0[0..*cnt0) (fixed grid, fixed tree; partials holds 148 * 3 doubles).
+void launch_sums3(const double* x0, const uint32_t* cnt0, const double* x1, const double* x2, const uint32_t* cnt1,
+                  double* partials, double* totals, cudaStream_t s);
+int grid_blocks(size_t n, int block, int cap);
+// Cell grid over the bounding box extended by `reach` (cell edge >= reach, so that
+// intersecting balls lie in adjacent cells), coarsened for sparse inputs so that the
+// number of cells stays O(max_slots).
+GridDev plan_grid(const BBox& bb, double reach, size_t max_slots, uint32_t* ncell);
 size_t scan_tmp_words_needed(size_t n);
 void scan_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* tmp, cudaStream_t s);
 

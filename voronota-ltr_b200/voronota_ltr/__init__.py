@@ -103,6 +103,30 @@ def library():
     L.vt_engine_set_timing.argtypes = [_vp, ctypes.c_int]
     L.vt_engine_set_fp32_band.argtypes = [_vp, ctypes.c_double]
     L.vt_engine_stage_times.argtypes = [_vp, _f64p]
+    _u64p = ctypes.POINTER(ctypes.c_uint64)
+    _ip = ctypes.POINTER(ctypes.c_int)
+    L.vt_upd_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp)]
+    L.vt_upd_destroy.argtypes = [_vp]
+    L.vt_upd_destroy.restype = None
+    L.vt_upd_set_stream.argtypes = [_vp, _vp]
+    L.vt_upd_init.argtypes = [_vp, _f64p, ctypes.c_uint64, ctypes.c_double, _f64p, _ip]
+    L.vt_upd_init_device.argtypes = [_vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double, _f64p, _ip]
+    L.vt_upd_update.argtypes = [_vp, _f64p, ctypes.c_uint64, _ip]
+    L.vt_upd_update_with_changed.argtypes = [_vp, _f64p, ctypes.c_uint64, _u64p, ctypes.c_uint64, _ip]
+    L.vt_upd_update_with_changed_device.argtypes = [_vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                                    ctypes.c_uint64, _ip]
+    L.vt_upd_set_exclusion.argtypes = [_vp, ctypes.c_uint64, ctypes.c_int, _ip]
+    L.vt_upd_restore.argtypes = [_vp, _ip]
+    L.vt_upd_summary.argtypes = [_vp, ctypes.POINTER(_vp)]
+    L.vt_upd_totals.argtypes = [_vp, _f64p]
+    L.vt_upd_last_full_reinit.argtypes = [_vp]
+    L.vt_upd_num_changed.argtypes = [_vp]
+    L.vt_upd_num_changed.restype = ctypes.c_uint64
+    L.vt_upd_changed_ids.argtypes = [_vp, _u64p]
+    L.vt_upd_num_affected.argtypes = [_vp]
+    L.vt_upd_num_affected.restype = ctypes.c_uint64
+    L.vt_upd_affected_ids.argtypes = [_vp, _u64p]
+    L.vt_upd_stats.argtypes = [_vp, ctypes.POINTER(VtStats)]
     L.vt_status_string.argtypes = [ctypes.c_int]
     L.vt_status_string.restype = ctypes.c_char_p
     L.vt_last_error.restype = ctypes.c_char_p
@@ -358,6 +382,110 @@ class Engine:
             self._L.vt_result_free(h)
 
 
+class UpdateableTessellation:
+    """UpdateableTessellation (src/updateable.rs:154-742) with its state on the GPU.
+
+    Same methods and return values as the reference: ``init``, ``update``,
+    ``update_with_changed``, ``set_exclusion``, ``restore``, ``summary``,
+    ``changed_ids``, ``affected_ids``, ``last_update_was_full_reinit``,
+    ``backup_enabled``.  ``summary()`` returns a :class:`Result` (``to_dict()`` gives the
+    reference's dict layout).  ``update_with_changed_device`` takes device pointers of a
+    float64 (N, 4) ball array and a uint64 id array on the handle's device.
+    """
+
+    def __init__(self, with_backup: bool = False, precision="fp64", device: int = 0):
+        self._L = library()
+        self._h = _vp()
+        self._backup = bool(with_backup)
+        _check(self._L.vt_upd_create(int(device), 1 if with_backup else 0, _precision_code(precision),
+                                     ctypes.byref(self._h)))
+
+    @classmethod
+    def with_backup(cls, precision="fp64", device: int = 0) -> "UpdateableTessellation":
+        return cls(True, precision, device)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.vt_upd_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def backup_enabled(self) -> bool:
+        return self._backup
+
+    def set_stream(self, stream_ptr: int | None):
+        _check(self._L.vt_upd_set_stream(self._h, stream_ptr))
+
+    def _flag(self, fn, *args) -> bool:
+        r = ctypes.c_int(0)
+        _check(fn(self._h, *args, ctypes.byref(r)))
+        return bool(r.value)
+
+    def init(self, balls, probe: float, periodic_box=None) -> bool:
+        x = parse_balls(balls)
+        pb = None if periodic_box is None else parse_periodic_box(periodic_box)
+        return self._flag(self._L.vt_upd_init, x.ctypes.data_as(_f64p), x.shape[0], float(probe),
+                          None if pb is None else pb.ctypes.data_as(_f64p))
+
+    def init_device(self, d_xyzr_ptr: int, n: int, probe: float, periodic_box=None) -> bool:
+        pb = None if periodic_box is None else parse_periodic_box(periodic_box)
+        return self._flag(self._L.vt_upd_init_device, d_xyzr_ptr, int(n), float(probe),
+                          None if pb is None else pb.ctypes.data_as(_f64p))
+
+    def update(self, balls) -> bool:
+        x = parse_balls(balls)
+        return self._flag(self._L.vt_upd_update, x.ctypes.data_as(_f64p), x.shape[0])
+
+    def update_with_changed(self, balls, changed_ids) -> bool:
+        x = parse_balls(balls)
+        ids = np.ascontiguousarray(np.asarray(changed_ids, dtype=np.uint64).reshape(-1))
+        return self._flag(self._L.vt_upd_update_with_changed, x.ctypes.data_as(_f64p), x.shape[0],
+                          ids.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), len(ids))
+
+    def update_with_changed_device(self, d_xyzr_ptr: int, n: int, d_ids_ptr: int, k: int) -> bool:
+        return self._flag(self._L.vt_upd_update_with_changed_device, d_xyzr_ptr, int(n), d_ids_ptr, int(k))
+
+    def set_exclusion(self, idx: int, excluded: bool) -> bool:
+        return self._flag(self._L.vt_upd_set_exclusion, int(idx), 1 if excluded else 0)
+
+    def restore(self) -> bool:
+        return self._flag(self._L.vt_upd_restore)
+
+    def summary(self) -> Result:
+        h = _vp()
+        _check(self._L.vt_upd_summary(self._h, ctypes.byref(h)))
+        try:
+            return Result.from_handle(self._L, h)
+        finally:
+            self._L.vt_result_free(h)
+
+    def totals(self) -> tuple[float, float, float]:
+        """(total SAS area, total volume, total contact area) of the current summary."""
+        t = (ctypes.c_double * 3)()
+        _check(self._L.vt_upd_totals(self._h, t))
+        return t[0], t[1], t[2]
+
+    def last_update_was_full_reinit(self) -> bool:
+        return bool(self._L.vt_upd_last_full_reinit(self._h))
+
+    def changed_ids(self) -> np.ndarray:
+        out = np.zeros(self._L.vt_upd_num_changed(self._h), np.uint64)
+        _check(self._L.vt_upd_changed_ids(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+        return out
+
+    def affected_ids(self) -> np.ndarray:
+        out = np.zeros(self._L.vt_upd_num_affected(self._h), np.uint64)
+        _check(self._L.vt_upd_affected_ids(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+        return out
+
+    def stats(self) -> VtStats:
+        s = VtStats()
+        _check(self._L.vt_upd_stats(self._h, ctypes.byref(s)))
+        return s
+
+
 __all__ = ["compute_tessellation", "compute_tessellation_result", "compute_contacts_only",
-           "compute_contacts_only_result", "Engine", "Result", "VoronotaError", "library", "parse_balls",
-           "parse_periodic_box"]
+           "compute_contacts_only_result", "Engine", "Result", "UpdateableTessellation", "VoronotaError",
+           "library", "parse_balls", "parse_periodic_box"]
