@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--n", type=int, default=N_BALLS)
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison leg")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--upd-n", type=int, default=200_000, help="balls of the periodic updateable trajectory")
+    ap.add_argument("--no-upd", action="store_true", help="skip the updateable trajectory leg")
     return ap.parse_args()
 
 
@@ -154,6 +156,124 @@ def cpu_baseline(balls, seconds=12.0):
     med = statistics.median(times)
     return {"value": len(balls) / med, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{len(times)} full tessellations of the {len(balls)}-ball structure, median time"}
+
+
+def trajectory(n, steps, seed):
+    """Periodic cube at 0.033 balls/A^3, r 1.52; each step moves a seeded random 1% of the
+    balls by N(0, 0.05 A) per axis (the periodic updateable trajectory workload)."""
+    from voronota_ltr import workloads as W
+
+    balls, side = W.periodic_box_balls(n, seed=seed)
+    box = {"corners": [(0.0, 0.0, 0.0), (side, side, side)]}
+    rng = np.random.default_rng(1000 + seed)
+    k = max(1, n // 100)
+    moves = []
+    for _ in range(steps):
+        ids = np.sort(rng.choice(n, k, replace=False)).astype(np.int64)
+        moves.append((ids, rng.normal(0.0, 0.05, (k, 3))))
+    return balls, box, moves
+
+
+def updateable_leg(args, rank, torch, V):
+    """UpdateableTessellation.update_with_changed on the device along the trajectory.
+
+    Per update: CUDA events on the handle's stream around vt_upd_update_with_changed_device
+    (the call returns after its work; inputs already in HBM).  Also: the same steps in
+    FP64, a full FP32 recompute of the final state, and (rank 0) the CPU oracle's
+    updateable tessellation on the first steps, with the GPU replaying those steps from
+    the same start for the accuracy check.
+    """
+    n = args.upd_n
+    warm = max(1, args.warmup)
+    steps = max(5, args.steps)
+    balls, box, moves = trajectory(n, warm + steps, rank)
+    stream = torch.cuda.current_stream()
+
+    def run(precision, nsteps):
+        u = V.UpdateableTessellation(False, precision)
+        u.set_stream(stream.cuda_stream)
+        d = torch.from_numpy(balls).cuda()
+        torch.cuda.synchronize()
+        u.init_device(d.data_ptr(), n, PROBE, box)
+        ms, aff, pairs, redo = [], [], [], []
+        for t, (ids, disp) in enumerate(moves[:warm + nsteps]):
+            ti = torch.from_numpy(ids).cuda()
+            d[ti, :3] += torch.from_numpy(disp).cuda()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            u.update_with_changed_device(d.data_ptr(), n, ti.data_ptr(), len(ids))
+            e1.record(stream)
+            e1.synchronize()
+            if t >= warm:
+                ms.append(e0.elapsed_time(e1))
+                st = u.stats()
+                pairs.append(int(st.num_pairs))
+                redo.append(int(st.num_fp64_redo))
+        aff = len(u.affected_ids())
+        return u, d, ms, aff, pairs, redo
+
+    u32, d32, ms32, aff, pairs, redo = run("fp32", steps)
+    _, _, ms64, _, _, _ = run("fp64", max(3, steps // 2))
+    eng = V.Engine()
+    eng.set_stream(stream.cuda_stream)
+    full = []
+    for _ in range(3):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.compute_device(d32.data_ptr(), n, PROBE, V.parse_periodic_box(box), precision="fp32")
+        e1.record(stream)
+        e1.synchronize()
+        full.append(e0.elapsed_time(e1))
+    eng.close()
+    t32 = statistics.median(ms32)
+    out = {
+        "workload": f"periodic cube {n} balls, 0.033 balls/A^3, r 1.52, probe 1.4; per step 1% of the balls "
+                    "moved by N(0, 0.05 A) per axis, then update_with_changed on the device",
+        "steps": steps, "warmup": warm,
+        "ms_per_update_fp32": t32, "ms_per_update_fp64": statistics.median(ms64),
+        "ms_full_recompute_fp32": statistics.median(full),
+        "speedup_vs_full_recompute": statistics.median(full) / t32,
+        "balls_per_s_fp32": n / (t32 * 1e-3),
+        "affected_per_update": aff, "pairs_per_update": int(statistics.median(pairs)),
+        "fp64_redo_pairs_per_update": int(statistics.median(redo)),
+    }
+    if rank == 0 and not args.no_cpu:
+        out.update(updateable_cpu_check(balls, box, moves[:3], n, torch, V))
+    return out
+
+
+def updateable_cpu_check(balls, box, moves, n, torch, V):
+    """The CPU oracle's UpdateableTessellation on the first steps (timed, all host cores),
+    and the GPU FP32 handle replaying them: contact count and totals compared."""
+    import oracle as O
+
+    O.set_threads(0)
+    O.set_faithful_grid_update(False)
+    o = O.OracleUpdateable(False)
+    b = balls.copy()
+    o.init(b, PROBE, box)
+    u = V.UpdateableTessellation(False, "fp32")
+    u.init(balls, PROBE, box)
+    times = []
+    for ids, disp in moves:
+        b[ids, :3] += disp
+        t0 = time.perf_counter()
+        o.update_with_changed(b, ids)
+        times.append(time.perf_counter() - t0)
+        u.update_with_changed(b, ids)
+    so, sg = o.summary(), u.summary()
+    rel = abs(sg.total_sas_area - so.total_sas_area) / so.total_sas_area
+    relv = abs(sg.total_volume - so.total_volume) / so.total_volume
+    same = (len(sg.id_a) == len(so.contacts_a) and np.array_equal(sg.id_a, so.contacts_a.astype(np.uint32))
+            and np.array_equal(sg.id_b, so.contacts_b.astype(np.uint32)))
+    O.set_faithful_grid_update(True)
+    return {"cpu_oracle_ms_per_update": 1e3 * statistics.median(times), "cpu_cores": O.get_threads(),
+            "cpu_sample": f"{len(times)} updates of the trajectory, median",
+            "fp32_vs_oracle_after_updates": {"steps": len(moves), "contacts_identical": bool(same),
+                                             "rel_err_total_sas": rel, "rel_err_total_volume": relv}}
 
 
 def run_reference(args):
@@ -293,6 +413,8 @@ def run_ours(args):
     if rank == 0 and not args.no_cpu:
         cpu = cpu_baseline(balls)
 
+    upd = None if args.no_upd else updateable_leg(args, rank, torch, V)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -318,6 +440,7 @@ def run_ours(args):
             "stages_ms_fp32": {k: round(v, 4) for k, v in fp32["stages"].items()},
             "stages_ms_fp64": {k: round(v, 4) for k, v in fp64["stages"].items()} if fp64 else None,
             "wall_s_timed_region": fp32["wall_s"],
+            "updateable": upd,
         }
         print(json.dumps(line), flush=True)
     eng.close()

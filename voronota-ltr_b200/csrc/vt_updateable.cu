@@ -440,13 +440,13 @@ struct vt_updateable {
         if (fp32) {
             launch_contact_f32(b, P, 1, stream);
             launch_collect_redo(b, P, stream);
+            VT_CUDA(cudaMemcpyAsync(h_words + 20, w(kWRedo), 4, cudaMemcpyDeviceToHost, stream));
             launch_contact_f64(b, P, 1, 1, stream);
         } else {
             launch_contact_f64(b, P, 1, 0, stream);
         }
         launch_collect_redo(b, P, stream);
         launch_contact_serial(b, P, 1, stream);
-        VT_CUDA(cudaMemcpyAsync(h_words + 20, w(kWRedo), 4, cudaMemcpyDeviceToHost, stream));
         VT_CUDA(cudaMemcpyAsync(h_words + 21, w(kWSerial), 4, cudaMemcpyDeviceToHost, stream));
     }
 
