@@ -124,6 +124,34 @@ typedef struct vt_device_outputs {
 } vt_device_outputs;
 int vt_engine_device_outputs(const vt_engine* e, vt_device_outputs* out);
 
+/* ---- batched structures ----
+ * No counterpart in the reference (which tessellates one structure per call): S
+ * independent structures concatenated in one N x 4 ball array, structure s being balls
+ * [offsets[s], offsets[s+1]) (offsets[0] = 0, non-decreasing, offsets[S] = N).  Each
+ * structure is tessellated exactly as compute_tessellation would tessellate it alone
+ * (non-periodic; its own grid); the work runs as one pass over all structures.  Contacts
+ * and cells of structure s are the ranges [contact_off[s], contact_off[s+1]) and
+ * [cell_off[s], cell_off[s+1]) of the concatenated arrays, with ball ids local to the
+ * structure, in the same order a single call returns them. */
+typedef struct vt_batch_result vt_batch_result;
+int vt_compute_batch(const double* xyzr, const uint64_t* offsets, uint64_t num_structures, double probe,
+                     int precision, vt_batch_result** out);
+/* Device-resident balls (offsets stay in host memory). */
+int vt_engine_compute_batch_device(vt_engine* e, const double* d_xyzr, const uint64_t* offsets,
+                                   uint64_t num_structures, double probe, int precision, int contacts_only);
+int vt_engine_download_batch(vt_engine* e, vt_batch_result** out);
+uint64_t vt_batch_num_structures(const vt_batch_result* r);
+uint64_t vt_batch_num_contacts(const vt_batch_result* r); /* all structures */
+uint64_t vt_batch_num_cells(const vt_batch_result* r);
+/* contact_off and cell_off: S + 1 entries each (either may be NULL). */
+int vt_batch_ranges(const vt_batch_result* r, uint64_t* contact_off, uint64_t* cell_off);
+int vt_batch_contacts(const vt_batch_result* r, uint32_t* id_a, uint32_t* id_b, double* area, double* arc_length,
+                      uint8_t* central);
+int vt_batch_cells(const vt_batch_result* r, uint32_t* index, double* sas_area, double* volume);
+/* 3 doubles per structure: total SAS area, total volume, total contact area. */
+int vt_batch_totals(const vt_batch_result* r, double* totals3);
+void vt_batch_free(vt_batch_result* r);
+
 /* ---- updateable tessellation ----
  * Replaces UpdateableTessellation (src/updateable.rs:154-742) with its state held on the
  * device: stored balls, exclusion statuses, neighbour lists, the per-ball contact table

@@ -28,6 +28,7 @@ UNITS = {
     "vt_engine.cu": ["--fmad=false"],
     "vt_noalloc.cu": ["--fmad=false"],
     "vt_frontier.cu": ["--fmad=false"],
+    "vt_batch.cu": ["--fmad=false"],
     "vt_updateable.cu": ["--fmad=false"],
 }
 

@@ -22,6 +22,7 @@
 #include "../../include/voronota_b200.h"
 #include "vt_host.cuh"
 #include "vt_pipeline.cuh"
+#include "vt_batch.cuh"
 
 using namespace vt;
 
@@ -34,6 +35,15 @@ thread_local std::string g_last_error;
 namespace vt {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 }  // namespace vt
+
+// Host copy of a batched result: all structures' contacts and cells concatenated (ids
+// local to their structure) and the per-structure ranges and totals.
+struct vt_batch_result {
+    uint64_t S = 0;
+    std::unique_ptr<vt_result> all;
+    std::vector<uint64_t> contact_off, cell_off;  // S + 1
+    std::vector<double> totals;                   // 3 per structure
+};
 
 struct vt_engine {
     int device = 0;
@@ -90,6 +100,15 @@ struct vt_engine {
             }
         }
     }
+    // batched call state
+    bool batch = false;
+    uint64_t batch_S = 0;
+    DBuf<uint32_t> boff, ball_struct, sncell, cell_base, crange, mrange;
+    DBuf<BBox> sbbox;
+    DBuf<GridDev> sgrid;
+    DBuf<double> btotals;
+    std::vector<uint32_t> h_crange, h_mrange;
+    std::vector<double> h_btot;
     double fp32_band_ulps = 16.0;  // FP32 point error budget E, in float ulps of the pair scale
     // state of the last call
     vt_stats stats{};
@@ -158,11 +177,16 @@ struct vt_engine {
 
     void ensure_scan(size_t n) { scan_tmp.ensure(scan_tmp_words_needed(n) + 8); }
 
+    // batch_off (host, S+1 ball offsets): S independent structures concatenated in d_in,
+    // tessellated together (non-periodic); outputs are per-structure ranges with local ids.
     int run(const double* d_in, uint64_t n64, double probe, const double* pbox9, const int32_t* d_groups,
-            uint64_t n_groups, int precision, int contacts_only_) {
+            uint64_t n_groups, int precision, int contacts_only_, const uint64_t* batch_off = nullptr,
+            uint64_t S = 0) {
         VT_CUDA(cudaSetDevice(device));
         contacts_only = contacts_only_ != 0;
         have_result = false;
+        batch = batch_off != nullptr;
+        batch_S = batch ? S : 0;
         stats = vt_stats{};
         stats.num_balls = n64;
         const uint64_t launches0 = launch_count();
@@ -171,6 +195,11 @@ struct vt_engine {
             stage_ms[k] = 0.0;
         }
         if (n64 == 0) {  // tessellation.rs:131-133, 205-207
+            if (batch) {
+                h_crange.assign(S + 1, 0);
+                h_mrange.assign(S + 1, 0);
+                h_btot.assign(3 * S, 0.0);
+            }
             have_result = true;
             return VT_OK;
         }
@@ -228,12 +257,34 @@ struct vt_engine {
             VT_CUDA(cudaMemcpyAsync(b.d_nslots, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
         }
 
-        // 3. grid over the extended box (cells of edge >= reach)
+        // 3. grid over the extended box (cells of edge >= reach); batched: one grid per
+        // structure, concatenated
         uint32_t ncell = 0;
-        b.grid = plan_grid(bb, reach, max_slots, &ncell);
-        cell_count.ensure(ncell);
+        if (batch) {
+            std::vector<uint32_t> h_off(S + 1);
+            for (uint64_t k = 0; k <= S; ++k) h_off[k] = (uint32_t)batch_off[k];
+            boff.ensure(S + 1);
+            VT_CUDA(cudaMemcpyAsync(boff.p, h_off.data(), 4 * (S + 1), cudaMemcpyHostToDevice, stream));
+            ball_struct.ensure(n);
+            sbbox.ensure(S);
+            sgrid.ensure(S);
+            sncell.ensure(S + 1);
+            cell_base.ensure(S + 1);
+            launch_batch_grid_setup(boff.p, (uint32_t)S, n, sph.p, ball_struct.p, sbbox.p, sgrid.p, sncell.p, stream);
+            ensure_scan(S + 1);
+            scan_u32(sncell.p, cell_base.p, S, scan_tmp.p, stream);
+            VT_CUDA(cudaMemcpyAsync(h_words + 12, cell_base.p + S, 4, cudaMemcpyDeviceToHost, stream));
+            sync();  // h_off is pageable
+            ncell = h_words[12];
+            b.ball_struct = ball_struct.p;
+            b.grids = sgrid.p;
+            b.cell_base = cell_base.p;
+        } else {
+            b.grid = plan_grid(bb, reach, max_slots, &ncell);
+        }
+        cell_count.ensure(ncell + 1);
         cell_start.ensure(ncell + 1);
-        cell_cursor.ensure(ncell);
+        cell_cursor.ensure(ncell + 1);
         c_pos.ensure(max_slots);
         c_id.ensure(max_slots);
         c_slot.ensure(max_slots);
@@ -245,7 +296,10 @@ struct vt_engine {
         b.c_slot = c_slot.p;
         ensure_scan(std::max<size_t>(ncell, n) + 1);
         t_begin(2);
-        launch_grid(b, ncell, (uint32_t)max_slots, scan_tmp.p, scan_tmp.cap, stream);
+        if (batch)
+            launch_batch_grid(b, n, ncell, scan_tmp.p, stream);
+        else
+            launch_grid(b, ncell, (uint32_t)max_slots, scan_tmp.p, scan_tmp.cap, stream);
         t_end(2);
 
         // 4. neighbour counts
@@ -408,6 +462,16 @@ struct vt_engine {
         launch_dedup(b, P, contacts_only ? 1 : 0, stream);
         launch_compact(b, P, contacts_only ? 1 : 0, scan_tmp.p, scan_tmp.cap, stream);
         launch_totals(b, P, contacts_only ? 1 : 0, stream);
+        if (batch) {
+            crange.ensure(S + 1);
+            mrange.ensure(S + 1);
+            btotals.ensure(3 * S + 1);
+            launch_batch_outputs(b, boff.p, (uint32_t)S, P, contacts_only ? 1 : 0, crange.p, mrange.p, btotals.p,
+                                 stream);
+            h_crange.resize(S + 1);
+            h_mrange.resize(S + 1);
+            h_btot.resize(3 * S);
+        }
         t_end(9);
         t_end(10);
 
@@ -418,6 +482,11 @@ struct vt_engine {
         VT_CUDA(cudaMemcpyAsync(h_words + 8, b.d_serial_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         double h_tot[3];
         VT_CUDA(cudaMemcpyAsync(h_tot, totals.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        if (batch) {
+            VT_CUDA(cudaMemcpyAsync(h_crange.data(), crange.p, 4 * (S + 1), cudaMemcpyDeviceToHost, stream));
+            VT_CUDA(cudaMemcpyAsync(h_mrange.data(), mrange.p, 4 * (S + 1), cudaMemcpyDeviceToHost, stream));
+            if (S) VT_CUDA(cudaMemcpyAsync(h_btot.data(), btotals.p, 8 * 3 * S, cudaMemcpyDeviceToHost, stream));
+        }
         sync();
         VT_CUDA(cudaGetLastError());
         t_collect();
@@ -479,7 +548,26 @@ struct vt_engine {
         *out = r.release();
         return VT_OK;
     }
+
+    int download_batch(vt_batch_result** out) {
+        if (!have_result || !batch) {
+            g_last_error = "no batched result";
+            return VT_ERR_INVALID;
+        }
+        vt_result* all = nullptr;
+        int st = download(&all);
+        if (st != VT_OK) return st;
+        std::unique_ptr<vt_batch_result> r(new vt_batch_result());
+        r->all.reset(all);
+        r->S = batch_S;
+        r->contact_off.assign(h_crange.begin(), h_crange.end());
+        r->cell_off.assign(h_mrange.begin(), h_mrange.end());
+        r->totals = h_btot;
+        *out = r.release();
+        return VT_OK;
+    }
 };
+
 
 namespace {
 
@@ -522,8 +610,26 @@ std::mutex g_engines_mu;
 std::vector<std::unique_ptr<vt_engine>> g_engines;
 std::vector<std::unique_ptr<std::mutex>> g_engine_mu;
 
+int validate_batch_offsets(const uint64_t* off, uint64_t S) {
+    if (S == 0 || S >= 0xffffffffu) {
+        g_last_error = "number of structures must be in [1, 2^32)";
+        return VT_ERR_INVALID;
+    }
+    if (off[0] != 0) {
+        g_last_error = "offsets[0] must be 0";
+        return VT_ERR_INVALID;
+    }
+    for (uint64_t s = 0; s < S; ++s)
+        if (off[s + 1] < off[s]) {
+            g_last_error = "offsets must be non-decreasing";
+            return VT_ERR_INVALID;
+        }
+    return VT_OK;
+}
+
 int host_compute(vt_engine* e, const double* xyzr, uint64_t n, double probe, const double* pbox9,
-                 const int32_t* groups, uint64_t n_groups, int precision, int contacts_only) {
+                 const int32_t* groups, uint64_t n_groups, int precision, int contacts_only,
+                 const uint64_t* batch_off = nullptr, uint64_t S = 0) {
     int st = validate_host(xyzr, n, probe, pbox9, groups, n_groups);
     if (st != VT_OK) return st;
     if (precision != VT_FP64 && precision != VT_FP32_FIXUP) {
@@ -544,16 +650,11 @@ int host_compute(vt_engine* e, const double* xyzr, uint64_t n, double probe, con
                                 e->stream));
         d_g = e->groups.p;
     }
-    return e->run(d_in, n, probe, pbox9, d_g, n_groups, precision, contacts_only);
+    return e->run(d_in, n, probe, pbox9, d_g, n_groups, precision, contacts_only, batch_off, S);
 }
 
-int stateless(const double* xyzr, uint64_t n, double probe, const double* pbox9, const int32_t* groups,
-              uint64_t n_groups, int precision, int contacts_only, vt_result** out) {
-    if (!out) {
-        g_last_error = "null result pointer";
-        return VT_ERR_INVALID;
-    }
-    *out = nullptr;
+template <typename F>
+int with_default_engine(F&& f) {
     return guarded([&]() -> int {
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -580,6 +681,18 @@ int stateless(const double* xyzr, uint64_t n, double probe, const double* pbox9,
             mu = g_engine_mu[dev].get();
         }
         std::lock_guard<std::mutex> lk(*mu);
+        return f(e);
+    });
+}
+
+int stateless(const double* xyzr, uint64_t n, double probe, const double* pbox9, const int32_t* groups,
+              uint64_t n_groups, int precision, int contacts_only, vt_result** out) {
+    if (!out) {
+        g_last_error = "null result pointer";
+        return VT_ERR_INVALID;
+    }
+    *out = nullptr;
+    return with_default_engine([&](vt_engine* e) -> int {
         int st = host_compute(e, xyzr, n, probe, pbox9, groups, n_groups, precision, contacts_only);
         if (st != VT_OK) return st;
         return e->download(out);
@@ -597,6 +710,65 @@ int vt_compute_tessellation(const double* xyzr, uint64_t n, double probe, const 
 int vt_compute_contacts_only(const double* xyzr, uint64_t n, double probe, const double* periodic_box9,
                              const int32_t* groups, uint64_t n_groups, int precision, vt_result** out) {
     return stateless(xyzr, n, probe, periodic_box9, groups, n_groups, precision, 1, out);
+}
+
+int vt_compute_batch(const double* xyzr, const uint64_t* offsets, uint64_t num_structures, double probe,
+                     int precision, vt_batch_result** out) {
+    if (!out) return VT_ERR_INVALID;
+    *out = nullptr;
+    if (!offsets) {
+        g_last_error = "null offsets";
+        return VT_ERR_INVALID;
+    }
+    int st = validate_batch_offsets(offsets, num_structures);
+    if (st != VT_OK) return st;
+    const uint64_t n = offsets[num_structures];
+    return with_default_engine([&](vt_engine* e) -> int {
+        int s2 = host_compute(e, xyzr, n, probe, nullptr, nullptr, 0, precision, 0, offsets, num_structures);
+        if (s2 != VT_OK) return s2;
+        return e->download_batch(out);
+    });
+}
+uint64_t vt_batch_num_structures(const vt_batch_result* r) { return r ? r->S : 0; }
+uint64_t vt_batch_num_contacts(const vt_batch_result* r) { return r ? r->all->a.size() : 0; }
+uint64_t vt_batch_num_cells(const vt_batch_result* r) { return r ? r->all->cell_index.size() : 0; }
+int vt_batch_ranges(const vt_batch_result* r, uint64_t* contact_off, uint64_t* cell_off) {
+    if (!r) return VT_ERR_INVALID;
+    if (contact_off) std::memcpy(contact_off, r->contact_off.data(), 8 * (r->S + 1));
+    if (cell_off) std::memcpy(cell_off, r->cell_off.data(), 8 * (r->S + 1));
+    return VT_OK;
+}
+int vt_batch_contacts(const vt_batch_result* r, uint32_t* id_a, uint32_t* id_b, double* area, double* arc_length,
+                      uint8_t* central) {
+    if (!r) return VT_ERR_INVALID;
+    return vt_result_contacts(r->all.get(), id_a, id_b, area, arc_length, central);
+}
+int vt_batch_cells(const vt_batch_result* r, uint32_t* index, double* sas_area, double* volume) {
+    if (!r) return VT_ERR_INVALID;
+    return vt_result_cells(r->all.get(), index, sas_area, volume);
+}
+int vt_batch_totals(const vt_batch_result* r, double* totals3) {
+    if (!r || (!totals3 && r->S)) return VT_ERR_INVALID;
+    if (r->S) std::memcpy(totals3, r->totals.data(), 8 * 3 * r->S);
+    return VT_OK;
+}
+void vt_batch_free(vt_batch_result* r) { delete r; }
+int vt_engine_compute_batch_device(vt_engine* e, const double* d_xyzr, const uint64_t* offsets,
+                                   uint64_t num_structures, double probe, int precision, int contacts_only) {
+    if (!e || !offsets) return VT_ERR_INVALID;
+    int st = validate_batch_offsets(offsets, num_structures);
+    if (st != VT_OK) return st;
+    const uint64_t n = offsets[num_structures];
+    if (n && !d_xyzr) return VT_ERR_INVALID;
+    if (precision != VT_FP64 && precision != VT_FP32_FIXUP) return VT_ERR_INVALID;
+    return guarded([&]() {
+        return e->run(d_xyzr, n, probe, nullptr, nullptr, 0, precision, contacts_only, offsets, num_structures);
+    });
+}
+int vt_engine_download_batch(vt_engine* e, vt_batch_result** out) {
+    if (!e || !out) return VT_ERR_INVALID;
+    *out = nullptr;
+    return guarded([&]() { return e->download_batch(out); });
 }
 
 uint64_t vt_result_num_balls(const vt_result* r) { return r ? r->num_balls : 0; }

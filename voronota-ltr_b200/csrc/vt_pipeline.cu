@@ -141,18 +141,6 @@ __global__ void k_image_fill(double4* __restrict__ sph, uint32_t* __restrict__ s
 }
 
 // ---- uniform grid: counting sort of the slots by cell ----
-__device__ __forceinline__ int cell_coord(double x, double o, double cell, int d) {
-    double f = floor((x - o) / cell);
-    int c = f < 0.0 ? 0 : (f > (double)(d - 1) ? d - 1 : (int)f);
-    return c;
-}
-__device__ __forceinline__ uint32_t cell_key(const GridDev& g, int x, int y, int z) {
-    return (uint32_t)x + (uint32_t)g.dx * ((uint32_t)y + (uint32_t)g.dy * (uint32_t)z);
-}
-__device__ __forceinline__ uint32_t slot_cell(const GridDev& g, double4 p) {
-    return cell_key(g, cell_coord(p.x, g.ox, g.cell, g.dx), cell_coord(p.y, g.oy, g.cell, g.dy),
-                    cell_coord(p.z, g.oz, g.cell, g.dz));
-}
 __global__ void k_cell_hist(const double4* __restrict__ sph, const uint32_t* __restrict__ d_nslots, GridDev g,
                             uint32_t* __restrict__ cnt) {
     uint32_t ns = *d_nslots;
@@ -191,12 +179,18 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_search(DevBufs b, int wan
     __shared__ uint32_t s_id[kSearchWarps][kSortCap];
     __shared__ uint32_t s_slot[kSearchWarps][kSortCap];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const GridDev g = b.grid;
+    GridDev g = b.grid;
+    uint32_t cbase = 0;  // first cell of the ball's structure (batched grids)
     const uint32_t n = b.n;
     Dec<double, false> d;
     const uint32_t rows = b.frontier ? b.n_frontier : n;
     for (uint32_t row = blockIdx.x * kSearchWarps + w; row < rows; row += gridDim.x * kSearchWarps) {
         const uint32_t i = b.frontier ? b.frontier[row] : row;
+        if (b.grids) {
+            const uint32_t st = b.ball_struct[i];
+            g = b.grids[st];
+            cbase = b.cell_base[st];
+        }
         const double4 A4 = b.sph[i];
         const Sph<double> A = sph_of(A4);
         int cx = cell_coord(A4.x, g.ox, g.cell, g.dx), cy = cell_coord(A4.y, g.oy, g.cell, g.dy),
@@ -206,8 +200,8 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_search(DevBufs b, int wan
             int y = cy + lane / 3 - 1, z = cz + lane % 3 - 1;
             if (y >= 0 && y < g.dy && z >= 0 && z < g.dz) {
                 int x0 = cx > 0 ? cx - 1 : 0, x1 = cx + 1 < g.dx ? cx + 1 : g.dx - 1;
-                rbeg = b.cell_start[cell_key(g, x0, y, z)];
-                rcnt = b.cell_start[cell_key(g, x1, y, z) + 1] - rbeg;
+                rbeg = b.cell_start[cbase + cell_key(g, x0, y, z)];
+                rcnt = b.cell_start[cbase + cell_key(g, x1, y, z) + 1] - rbeg;
             }
         }
         uint32_t incl = rcnt;

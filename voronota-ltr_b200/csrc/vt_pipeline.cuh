@@ -125,6 +125,11 @@ struct DevBufs {
     int no_pairs;              // fill pass writes the neighbour lists only
     int slot_is_id;            // grid slots carry reference ids as their sph index
     int detached_excl;         // cells: an empty list is detached only when not excluded
+    // batched structures (null for one structure): ball -> structure, the structure's
+    // grid and the index of its first cell in the concatenated cell arrays
+    const uint32_t* ball_struct;
+    const GridDev* grids;
+    const uint32_t* cell_base;
 };
 
 
@@ -142,6 +147,20 @@ __device__ __forceinline__ double4 shift_sphere(double4 s, const double* pb, dou
                         fma(pb[7], wc, fma(pb[4], wb, fma(pb[1], wa, s.y))),
                         fma(pb[8], wc, fma(pb[5], wb, fma(pb[2], wa, s.z))), s.w);
 }
+// ---- uniform grid cells ----
+__device__ __forceinline__ int cell_coord(double x, double o, double cell, int d) {
+    double f = floor((x - o) / cell);
+    int c = f < 0.0 ? 0 : (f > (double)(d - 1) ? d - 1 : (int)f);
+    return c;
+}
+__device__ __forceinline__ uint32_t cell_key(const GridDev& g, int x, int y, int z) {
+    return (uint32_t)x + (uint32_t)g.dx * ((uint32_t)y + (uint32_t)g.dy * (uint32_t)z);
+}
+__device__ __forceinline__ uint32_t slot_cell(const GridDev& g, double4 p) {
+    return cell_key(g, cell_coord(p.x, g.ox, g.cell, g.dx), cell_coord(p.y, g.oy, g.cell, g.dy),
+                    cell_coord(p.z, g.oz, g.cell, g.dz));
+}
+
 // CellContactSummary::compute_sas (types.rs:623-663) from the accumulated sums of a cell
 // with count > 0 contributing contacts.  cell_band > 0 (sums of FP32-derived values):
 // *unsure is set when a branch decision lies within cell_band radians per contact of

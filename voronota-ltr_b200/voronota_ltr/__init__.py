@@ -34,6 +34,7 @@ VT_FP64 = 0
 VT_FP32_FIXUP = 1
 
 _u32p = ctypes.POINTER(ctypes.c_uint32)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
 _f64p = ctypes.POINTER(ctypes.c_double)
 _u8p = ctypes.POINTER(ctypes.c_uint8)
 _i32p = ctypes.POINTER(ctypes.c_int32)
@@ -103,7 +104,6 @@ def library():
     L.vt_engine_set_timing.argtypes = [_vp, ctypes.c_int]
     L.vt_engine_set_fp32_band.argtypes = [_vp, ctypes.c_double]
     L.vt_engine_stage_times.argtypes = [_vp, _f64p]
-    _u64p = ctypes.POINTER(ctypes.c_uint64)
     _ip = ctypes.POINTER(ctypes.c_int)
     L.vt_upd_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp)]
     L.vt_upd_destroy.argtypes = [_vp]
@@ -127,6 +127,20 @@ def library():
     L.vt_upd_num_affected.restype = ctypes.c_uint64
     L.vt_upd_affected_ids.argtypes = [_vp, _u64p]
     L.vt_upd_stats.argtypes = [_vp, ctypes.POINTER(VtStats)]
+    L.vt_compute_batch.argtypes = [_f64p, _u64p, ctypes.c_uint64, ctypes.c_double, ctypes.c_int,
+                                   ctypes.POINTER(_vp)]
+    L.vt_engine_compute_batch_device.argtypes = [_vp, ctypes.c_void_p, _u64p, ctypes.c_uint64, ctypes.c_double,
+                                                 ctypes.c_int, ctypes.c_int]
+    L.vt_engine_download_batch.argtypes = [_vp, ctypes.POINTER(_vp)]
+    for name in ("vt_batch_num_structures", "vt_batch_num_contacts", "vt_batch_num_cells"):
+        getattr(L, name).argtypes = [_vp]
+        getattr(L, name).restype = ctypes.c_uint64
+    L.vt_batch_ranges.argtypes = [_vp, _u64p, _u64p]
+    L.vt_batch_contacts.argtypes = [_vp, _u32p, _u32p, _f64p, _f64p, _u8p]
+    L.vt_batch_cells.argtypes = [_vp, _u32p, _f64p, _f64p]
+    L.vt_batch_totals.argtypes = [_vp, _f64p]
+    L.vt_batch_free.argtypes = [_vp]
+    L.vt_batch_free.restype = None
     L.vt_status_string.argtypes = [ctypes.c_int]
     L.vt_status_string.restype = ctypes.c_char_p
     L.vt_last_error.restype = ctypes.c_char_p
@@ -305,6 +319,71 @@ def compute_contacts_only_result(balls, probe, periodic_box=None, groups=None, p
     return _run("vt_compute_contacts_only", balls, probe, periodic_box, groups, precision)
 
 
+class BatchResult:
+    """Results of a batched call: per-structure contacts and cells (ids local to the
+    structure), concatenated, with the ranges of each structure and its totals."""
+
+    def __init__(self, contact_off, cell_off, totals, all_result: Result):
+        self.contact_off, self.cell_off = contact_off, cell_off
+        self.totals = totals  # (S, 3): SAS area, volume, contact area
+        self.all = all_result
+
+    @classmethod
+    def from_handle(cls, L, h):
+        S = L.vt_batch_num_structures(h)
+        nc, nm = L.vt_batch_num_contacts(h), L.vt_batch_num_cells(h)
+        co = np.empty(S + 1, np.uint64)
+        mo = np.empty(S + 1, np.uint64)
+        _check(L.vt_batch_ranges(h, co.ctypes.data_as(_u64p), mo.ctypes.data_as(_u64p)))
+        a, b = np.empty(nc, np.uint32), np.empty(nc, np.uint32)
+        ar, arc, ce = np.empty(nc), np.empty(nc), np.empty(nc, np.uint8)
+        _check(L.vt_batch_contacts(h, a.ctypes.data_as(_u32p), b.ctypes.data_as(_u32p), ar.ctypes.data_as(_f64p),
+                                   arc.ctypes.data_as(_f64p), ce.ctypes.data_as(_u8p)))
+        ci, cs, cv = np.empty(nm, np.uint32), np.empty(nm), np.empty(nm)
+        _check(L.vt_batch_cells(h, ci.ctypes.data_as(_u32p), cs.ctypes.data_as(_f64p), cv.ctypes.data_as(_f64p)))
+        tot = np.empty((S, 3))
+        _check(L.vt_batch_totals(h, tot.ctypes.data_as(_f64p)))
+        return cls(co, mo, tot, Result(0, a, b, ar, arc, ce.astype(bool), ci, cs, cv, (0.0, 0.0, 0.0)))
+
+    def __len__(self):
+        return len(self.totals)
+
+    def structure(self, s: int, num_balls: int = 0) -> Result:
+        c0, c1 = int(self.contact_off[s]), int(self.contact_off[s + 1])
+        m0, m1 = int(self.cell_off[s]), int(self.cell_off[s + 1])
+        A = self.all
+        return Result(num_balls, A.id_a[c0:c1], A.id_b[c0:c1], A.area[c0:c1], A.arc_length[c0:c1],
+                      A.central[c0:c1], A.cell_index[m0:m1], A.cell_sas_area[m0:m1], A.cell_volume[m0:m1],
+                      tuple(float(x) for x in self.totals[s]))
+
+
+def _batch_input(structures):
+    if isinstance(structures, tuple) and len(structures) == 2:
+        balls = np.ascontiguousarray(np.asarray(structures[0], dtype=np.float64).reshape(-1, 4))
+        off = np.ascontiguousarray(np.asarray(structures[1], dtype=np.uint64))
+        return balls, off
+    parts = [parse_balls(x) for x in structures]
+    off = np.zeros(len(parts) + 1, np.uint64)
+    off[1:] = np.cumsum([len(x) for x in parts])
+    balls = np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros((0, 4)))
+    return balls, off
+
+
+def compute_batch(structures, probe, precision="fp32") -> BatchResult:
+    """Tessellate many independent structures in one pass (no counterpart in the
+    reference).  ``structures``: a list of ball arrays, or ``(balls (N, 4), offsets
+    (S+1))``.  Each structure's result equals compute_tessellation on it alone."""
+    L = library()
+    balls, off = _batch_input(structures)
+    h = _vp()
+    _check(L.vt_compute_batch(balls.ctypes.data_as(_f64p), off.ctypes.data_as(_u64p), len(off) - 1, float(probe),
+                              _precision_code(precision), ctypes.byref(h)))
+    try:
+        return BatchResult.from_handle(L, h)
+    finally:
+        L.vt_batch_free(h)
+
+
 class Engine:
     """Explicit engine: a device, a stream and a reusable device workspace.
 
@@ -372,6 +451,21 @@ class Engine:
         o = VtDeviceOutputs()
         _check(self._L.vt_engine_device_outputs(self._h, ctypes.byref(o)))
         return o
+
+    def compute_batch_device(self, d_xyzr_ptr: int, offsets, probe: float, precision="fp32",
+                             contacts_only: bool = False):
+        off = np.ascontiguousarray(np.asarray(offsets, dtype=np.uint64))
+        _check(self._L.vt_engine_compute_batch_device(self._h, d_xyzr_ptr, off.ctypes.data_as(_u64p), len(off) - 1,
+                                                      float(probe), _precision_code(precision),
+                                                      1 if contacts_only else 0))
+
+    def download_batch(self) -> BatchResult:
+        h = _vp()
+        _check(self._L.vt_engine_download_batch(self._h, ctypes.byref(h)))
+        try:
+            return BatchResult.from_handle(self._L, h)
+        finally:
+            self._L.vt_batch_free(h)
 
     def download(self) -> Result:
         h = _vp()
@@ -487,5 +581,5 @@ class UpdateableTessellation:
 
 
 __all__ = ["compute_tessellation", "compute_tessellation_result", "compute_contacts_only",
-           "compute_contacts_only_result", "Engine", "Result", "UpdateableTessellation", "VoronotaError",
+           "compute_contacts_only_result", "compute_batch", "BatchResult", "Engine", "Result", "UpdateableTessellation", "VoronotaError",
            "library", "parse_balls", "parse_periodic_box"]
