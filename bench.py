@@ -56,6 +56,8 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--upd-n", type=int, default=200_000, help="balls of the periodic updateable trajectory")
     ap.add_argument("--no-upd", action="store_true", help="skip the updateable trajectory leg")
+    ap.add_argument("--batch-count", type=int, default=4096, help="structures of the batched leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched leg")
     return ap.parse_args()
 
 
@@ -276,6 +278,64 @@ def updateable_cpu_check(balls, box, moves, n, torch, V):
                                              "rel_err_total_sas": rel, "rel_err_total_volume": relv}}
 
 
+def batched_leg(args, rank, torch, V):
+    """Batched structures: sizes log-uniform in [300, 20000], structure i from the lattice
+    generator with seed 1000 + i, FP32+fixup (and FP64) in one batched call per step;
+    per-structure SAS / volume error against the CPU oracle on a sample (rank 0)."""
+    from voronota_ltr import workloads as W
+
+    sizes = W.batch_sizes(args.batch_count)
+    structs = [W.lattice_balls(int(n), 1000 + i + 100000 * rank) for i, n in enumerate(sizes)]
+    balls = np.concatenate(structs)
+    off = np.zeros(len(sizes) + 1, np.uint64)
+    off[1:] = np.cumsum(sizes)
+    d = torch.from_numpy(balls).cuda()
+    stream = torch.cuda.current_stream()
+    eng = V.Engine()
+    eng.set_stream(stream.cuda_stream)
+
+    def timed(precision, reps, warm):
+        for _ in range(warm):
+            eng.compute_batch_device(d.data_ptr(), off, PROBE, precision)
+        ms = []
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            eng.compute_batch_device(d.data_ptr(), off, PROBE, precision)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms)
+
+    t64 = timed("fp64", 1, 0)
+    t32 = timed("fp32", 3, 1)
+    st = eng.stats()
+    out = {"workload": f"{len(sizes)} structures, sizes log-uniform in [300, 20000] ({len(balls)} balls), "
+                       "lattice generator seed 1000+i, probe 1.4, one batched call",
+           "balls": int(len(balls)), "ms_fp32": t32, "balls_per_s_fp32": len(balls) / (t32 * 1e-3),
+           "ms_fp64": t64, "balls_per_s_fp64": len(balls) / (t64 * 1e-3), "speedup_vs_fp64": t64 / t32,
+           "pairs": int(st.num_pairs), "fp64_redo_pairs": int(st.num_fp64_redo)}
+    if rank == 0 and not args.no_cpu:
+        import oracle as O
+
+        O.set_threads(0)
+        r = eng.download_batch()
+        rng = np.random.default_rng(0)
+        errs = []
+        for s in rng.choice(len(sizes), 16, replace=False):
+            o = O.compute(structs[s], PROBE)
+            g = r.structure(int(s))
+            errs.append((abs(g.total_sas_area - o.total_sas_area) / o.total_sas_area,
+                         abs(g.total_volume - o.total_volume) / o.total_volume))
+        errs = np.array(errs)
+        out["fp32_vs_oracle_sample"] = {"structures": 16, "max_rel_err_sas": float(errs[:, 0].max()),
+                                        "max_rel_err_volume": float(errs[:, 1].max()),
+                                        "median_rel_err_sas": float(np.median(errs[:, 0]))}
+    eng.close()
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -414,6 +474,7 @@ def run_ours(args):
         cpu = cpu_baseline(balls)
 
     upd = None if args.no_upd else updateable_leg(args, rank, torch, V)
+    bat = None if args.no_batch else batched_leg(args, rank, torch, V)
 
     if rank == 0:
         line = {
@@ -441,6 +502,7 @@ def run_ours(args):
             "stages_ms_fp64": {k: round(v, 4) for k, v in fp64["stages"].items()} if fp64 else None,
             "wall_s_timed_region": fp32["wall_s"],
             "updateable": upd,
+            "batched": bat,
         }
         print(json.dumps(line), flush=True)
     eng.close()
