@@ -124,6 +124,25 @@ typedef struct vt_device_outputs {
 } vt_device_outputs;
 int vt_engine_device_outputs(const vt_engine* e, vt_device_outputs* out);
 
+/* ---- gradient ----
+ * No counterpart in the reference: the adjoint of
+ *     L = sum_i w_sas[i] SAS_i + sum_k u_contact[k] area_k
+ * with respect to every ball's x, y, z and r (SAS_i of a ball without a cell counts as 0;
+ * contact k is the k-th contact of the tessellation's output).  The backward pass
+ * recomputes each contact's contour in FP64 and differentiates the final region
+ * analytically (boundary velocities of its edges and arcs); it does not store contours.
+ * Balls of periodic images accumulate into the ball they image; the box is fixed.
+ * A contact whose contour needed more than 32 points is not differentiated
+ * (VT_ERR_CAPACITY). */
+/* After vt_engine_compute_device/_host (full tessellation, one structure): device arrays
+ * d_w_sas (n doubles) and d_u_contact (one per contact) may be NULL; d_grad: n x 4
+ * doubles, overwritten. */
+int vt_engine_grad_device(vt_engine* e, const double* d_w_sas, const double* d_u_contact, double* d_grad);
+/* Forward (as vt_compute_tessellation, no groups) + adjoint on host arrays; u_contact
+ * must have num_contacts = the tessellation's contact count entries. */
+int vt_grad(const double* xyzr, uint64_t n, double probe, const double* periodic_box9, int precision,
+            const double* w_sas, const double* u_contact, uint64_t num_contacts, double* grad_out);
+
 /* ---- batched structures ----
  * No counterpart in the reference (which tessellates one structure per call): S
  * independent structures concatenated in one N x 4 ball array, structure s being balls

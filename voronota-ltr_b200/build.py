@@ -29,6 +29,7 @@ UNITS = {
     "vt_noalloc.cu": ["--fmad=false"],
     "vt_frontier.cu": ["--fmad=false"],
     "vt_batch.cu": ["--fmad=false"],
+    "vt_adjoint.cu": ["--fmad=false"],
     "vt_updateable.cu": ["--fmad=false"],
 }
 

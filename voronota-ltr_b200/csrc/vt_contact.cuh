@@ -361,8 +361,21 @@ __device__ __forceinline__ double solid_angle(Dec<T, F>& d, const Sph<T>& a, con
 
 // The warp-wide contact computation.  `nb(e)` returns neighbour record e of a's sorted
 // list (0 <= e < cnt); entry `kb` is b itself.
+// The final contour of a valid contact, for the adjoint: this lane's point (its segment to
+// the next point is an arc of angle q.ang when q.rid and the next point's lid are a's id,
+// otherwise a straight edge on the radical plane of a and neighbour q.rid), the point
+// count (0 with full = true: the whole circle), the circle and the axis a -> b.
+template <typename T>
+struct ContourOut {
+    Pt<T> q;
+    int len;
+    bool full;
+    Sph<T> ic;
+    V3<T> axis;
+};
+
 template <typename T, bool F, bool FULL, typename NbFn>
-__device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn nb) {
+__device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn nb, ContourOut<T>* co = nullptr) {
     const int lane = threadIdx.x & 31;
     PairGeom<T> g = g0;
     const T e0 = g.e0;
@@ -771,6 +784,13 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
     res.area = (double)area;
     res.arc = (double)(sum_arc * g.ic.r);
     res.central = central;
+    if (co) {
+        co->q = q;
+        co->len = len;
+        co->full = !init;
+        co->ic = g.ic;
+        co->axis = g.axis;
+    }
     if (FULL) {
         // construct_contact_descriptor (contact.rs:357-381)
         int pvl = lane > 0 ? lane - 1 : (len > 0 ? len - 1 : 0);

@@ -391,19 +391,26 @@ __global__ void k_contact_serial(DevBufs b, int full) {
 
 }  // namespace
 
-void set_hex_table() {
+void hex_table_values(double* hs, double* hc, int* n) {
     // the reference's accumulation: rotation_angle = pi/3, += pi/3 while < 2 pi
-    double hs[8] = {0}, hc[8] = {0};
+    for (int j = 0; j < 8; ++j) hs[j] = hc[j] = 0.0;
     int k = 1;
     for (double ang = kFracPi3; ang < kTau && k < 8; ang += kFracPi3, ++k) {
         double half = ang / 2.0;
         hs[k] = std::sin(half);
         hc[k] = std::cos(half);
     }
-    int n = k;
+    *n = k;
+}
+
+void set_hex_table() {
+    double hs[8], hc[8];
+    int n = 0;
+    hex_table_values(hs, hc, &n);
     cudaMemcpyToSymbol(c_hex_sin, hs, sizeof(hs));
     cudaMemcpyToSymbol(c_hex_cos, hc, sizeof(hc));
     cudaMemcpyToSymbol(c_hex_n, &n, sizeof(int));
+    set_hex_table_adjoint();  // the adjoint's translation unit holds its own copy
 }
 
 void launch_contact_f64(const DevBufs& b, uint32_t P, int full, int from_list, cudaStream_t s) {

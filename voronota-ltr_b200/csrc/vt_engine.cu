@@ -549,6 +549,29 @@ struct vt_engine {
         return VT_OK;
     }
 
+    // adjoint of the last full tessellation (device arrays)
+    DBuf<double> w_eff, grad_w, grad_u, grad_out;
+    int grad_device(const double* d_w, const double* d_u, double* d_grad) {
+        if (!have_result || contacts_only || batch) {
+            g_last_error = "the gradient needs the result of a full single-structure tessellation";
+            return VT_ERR_INVALID;
+        }
+        VT_CUDA(cudaSetDevice(device));
+        const uint32_t n = (uint32_t)stats.num_balls;
+        if (n == 0) return VT_OK;
+        w_eff.ensure(n);
+        VT_CUDA(cudaMemsetAsync(words.p, 0, sizeof(uint32_t), stream));
+        launch_adjoint(bufs, (uint32_t)stats.num_pairs, d_w, d_u, w_eff.p, d_grad, stream);
+        VT_CUDA(cudaMemcpyAsync(h_words + 13, words.p, 4, cudaMemcpyDeviceToHost, stream));
+        sync();
+        VT_CUDA(cudaGetLastError());
+        if (h_words[13] & 32u) {
+            g_last_error = "a contact whose contour has more than 32 points is not differentiated";
+            return VT_ERR_CAPACITY;
+        }
+        return VT_OK;
+    }
+
     int download_batch(vt_batch_result** out) {
         if (!have_result || !batch) {
             g_last_error = "no batched result";
@@ -729,6 +752,37 @@ int vt_compute_batch(const double* xyzr, const uint64_t* offsets, uint64_t num_s
         return e->download_batch(out);
     });
 }
+int vt_engine_grad_device(vt_engine* e, const double* d_w_sas, const double* d_u_contact, double* d_grad) {
+    if (!e || !d_grad) return VT_ERR_INVALID;
+    return guarded([&]() { return e->grad_device(d_w_sas, d_u_contact, d_grad); });
+}
+int vt_grad(const double* xyzr, uint64_t n, double probe, const double* periodic_box9, int precision,
+            const double* w_sas, const double* u_contact, uint64_t num_contacts, double* grad_out) {
+    if (n && !grad_out) return VT_ERR_INVALID;
+    return with_default_engine([&](vt_engine* e) -> int {
+        int st = host_compute(e, xyzr, n, probe, periodic_box9, nullptr, 0, precision, 0);
+        if (st != VT_OK) return st;
+        if (n == 0) return VT_OK;
+        if (u_contact && num_contacts != e->stats.num_contacts) {
+            g_last_error = "u_contact must have one weight per contact of the tessellation (" +
+                           std::to_string(e->stats.num_contacts) + ")";
+            return VT_ERR_INVALID;
+        }
+        e->grad_w.ensure(n);
+        e->grad_u.ensure(num_contacts + 1);
+        e->grad_out.ensure(4 * n);
+        if (w_sas)
+            VT_CUDA(cudaMemcpyAsync(e->grad_w.p, w_sas, 8 * n, cudaMemcpyHostToDevice, e->stream));
+        if (u_contact && num_contacts)
+            VT_CUDA(cudaMemcpyAsync(e->grad_u.p, u_contact, 8 * num_contacts, cudaMemcpyHostToDevice, e->stream));
+        st = e->grad_device(w_sas ? e->grad_w.p : nullptr, u_contact ? e->grad_u.p : nullptr, e->grad_out.p);
+        if (st != VT_OK) return st;
+        VT_CUDA(cudaMemcpyAsync(grad_out, e->grad_out.p, 32 * n, cudaMemcpyDeviceToHost, e->stream));
+        e->sync();
+        return VT_OK;
+    });
+}
+
 uint64_t vt_batch_num_structures(const vt_batch_result* r) { return r ? r->S : 0; }
 uint64_t vt_batch_num_contacts(const vt_batch_result* r) { return r ? r->all->a.size() : 0; }
 uint64_t vt_batch_num_cells(const vt_batch_result* r) { return r ? r->all->cell_index.size() : 0; }

@@ -239,6 +239,12 @@ GridDev plan_grid(const BBox& bb, double reach, size_t max_slots, uint32_t* ncel
 size_t scan_tmp_words_needed(size_t n);
 void scan_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* tmp, cudaStream_t s);
 
+// ---- adjoint (vt_adjoint.cu): grad (n x 4, overwritten) = dL/d(x, y, z, r) for
+// L = sum_i w_sas[i] SAS_i + sum_k u_contact[k] area_k over the last full tessellation in
+// b (w_sas, u_contact: device arrays or null; w_eff: n doubles of scratch).
+void launch_adjoint(const DevBufs& b, uint32_t P, const double* w_sas, const double* u_contact, double* w_eff,
+                    double* grad, cudaStream_t s);
+
 // ---- contact kernels (vt_contact64.cu / vt_contact32.cu) ----
 // mode: 0 = all pairs; 1 = pairs listed in redo_list (count on device)
 void launch_contact_f64(const DevBufs& b, uint32_t P, int full, int from_list, cudaStream_t s);
@@ -247,5 +253,8 @@ void launch_contact_serial(const DevBufs& b, uint32_t P, int full, cudaStream_t 
 // Upload the FP64 hexagon rotation table (sin/cos from the host C library) to the
 // current device; call once per device before the first FP64 contact launch.
 void set_hex_table();
+// The hexagon table's values (host C library) and the upload into the adjoint's unit.
+void hex_table_values(double* hs, double* hc, int* n);
+void set_hex_table_adjoint();
 
 }  // namespace vt
