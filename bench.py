@@ -58,6 +58,8 @@ def parse_args():
     ap.add_argument("--no-upd", action="store_true", help="skip the updateable trajectory leg")
     ap.add_argument("--batch-count", type=int, default=4096, help="structures of the batched leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched leg")
+    ap.add_argument("--grad-n", type=int, default=20_000, help="balls of the differentiation leg")
+    ap.add_argument("--no-grad", action="store_true", help="skip the differentiation leg")
     return ap.parse_args()
 
 
@@ -336,6 +338,106 @@ def batched_leg(args, rank, torch, V):
     return out
 
 
+def _pair_keys(a, b, n):
+    return np.asarray(a, np.int64) * n + np.asarray(b, np.int64)
+
+
+def _loss_fn(n, w, key_sorted, u_sorted):
+    """L = sum w SAS + sum u area, u attached to the contact's ball pair (contacts absent
+    from the reference list weigh 0)."""
+    def loss(cell_index, cell_sas, ida, idb, area):
+        k = _pair_keys(ida, idb, n)
+        pos = np.clip(np.searchsorted(key_sorted, k), 0, len(key_sorted) - 1)
+        uu = np.where(key_sorted[pos] == k, u_sorted[pos], 0.0)
+        return float(np.dot(w[cell_index.astype(np.int64)], cell_sas)) + float(np.dot(uu, area))
+    return loss
+
+
+def grad_leg(args, rank, torch, V):
+    """L = sum_i w_i SAS_i + sum_ab u_ab area_ab on a lattice structure, w ~ U(0,1),
+    u ~ N(0,1) (seeded): forward + hand-written adjoint timed on the device; the gradient
+    checked at 256 random coordinates against central differences (h = 1e-4 A, f64) of
+    the GPU FP64 forward, and at 24 of them against the CPU oracle (rank 0)."""
+    n = args.grad_n
+    balls = workload(n, 7 + rank)
+    rng = np.random.default_rng(20 + rank)
+    w = rng.uniform(0.0, 1.0, n)
+    ref = V.compute_tessellation_result(balls, PROBE, precision="fp64")
+    u = rng.normal(0.0, 1.0, len(ref.id_a))
+    stream = torch.cuda.current_stream()
+    eng = V.Engine()
+    eng.set_stream(stream.cuda_stream)
+    d = torch.from_numpy(balls).cuda()
+    dw = torch.from_numpy(w).cuda()
+    du = torch.from_numpy(u).cuda()
+    dg = torch.empty((n, 4), dtype=torch.float64, device="cuda")
+
+    def timed(precision, reps=7):
+        fwd, bwd = [], []
+        for k in range(reps + 2):
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            eng.compute_device(d.data_ptr(), n, PROBE, precision=precision)
+            e1.record(stream)
+            eng.grad_device(dw.data_ptr(), du.data_ptr(), dg.data_ptr())
+            e2.record(stream)
+            e2.synchronize()
+            if k >= 2:
+                fwd.append(e0.elapsed_time(e1))
+                bwd.append(e1.elapsed_time(e2))
+        return statistics.median(fwd), statistics.median(bwd)
+
+    f64, b64 = timed("fp64")
+    g64 = dg.cpu().numpy().copy()
+    f32, b32 = timed("fp32")
+    g = dg.cpu().numpy().copy()
+    eng.close()
+    key = _pair_keys(ref.id_a, ref.id_b, n)
+    order = np.argsort(key)
+    loss = _loss_fn(n, w, key[order], u[order])
+
+    def l_gpu(b):
+        r = V.compute_tessellation_result(b, PROBE, precision="fp64")
+        return loss(r.cell_index, r.cell_sas_area, r.id_a, r.id_b, r.area)
+
+    def fd(lf, i, c, h):
+        bp, bm = balls.copy(), balls.copy()
+        bp[i, c] += h
+        bm[i, c] -= h
+        return (lf(bp) - lf(bm)) / (2 * h)
+
+    crng = np.random.default_rng(30 + rank)
+    coords = list(zip(crng.choice(n, 256, replace=False).tolist(), crng.integers(0, 4, 256).tolist()))
+    errs = []
+    for i, c in coords:
+        f = fd(l_gpu, i, c, 1e-4)
+        errs.append(abs(g64[i, c] - f) / (1 + abs(f)))
+    errs = np.array(errs)
+    out = {"workload": f"lattice {n} balls, probe 1.4; L = sum w SAS + sum u area, w ~ U(0,1), u ~ N(0,1)",
+           "forward_ms_fp32": f32, "adjoint_ms_after_fp32": b32, "forward_plus_adjoint_over_forward_fp32": (f32 + b32) / f32,
+           "forward_ms_fp64": f64, "adjoint_ms_after_fp64": b64,
+           "fd_check_gpu_fp64": {"coordinates": len(coords), "h": 1e-4, "max_rel_err": float(errs.max()),
+                                 "median_rel_err": float(np.median(errs)),
+                                 "within_1e-5": int((errs <= 1e-5).sum())},
+           "fp32_vs_fp64_forward_grad_max_abs_diff_xyz": float(np.abs(g[:, :3] - g64[:, :3]).max())}
+    if rank == 0 and not args.no_cpu:
+        import oracle as O
+
+        O.set_threads(0)
+
+        def l_or(b):
+            o = O.compute(b, PROBE)
+            return loss(o.cells_index, o.cells_sas, o.contacts_a, o.contacts_b, o.contacts_area)
+
+        oe = []
+        for i, c in coords[:24]:
+            f = fd(l_or, i, c, 1e-4)
+            oe.append(abs(g64[i, c] - f) / (1 + abs(f)))
+        out["fd_check_oracle"] = {"coordinates": 24, "h": 1e-4, "max_rel_err": float(max(oe)),
+                                  "median_rel_err": float(np.median(oe))}
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -475,6 +577,7 @@ def run_ours(args):
 
     upd = None if args.no_upd else updateable_leg(args, rank, torch, V)
     bat = None if args.no_batch else batched_leg(args, rank, torch, V)
+    grd = None if args.no_grad else grad_leg(args, rank, torch, V)
 
     if rank == 0:
         line = {
@@ -503,6 +606,7 @@ def run_ours(args):
             "wall_s_timed_region": fp32["wall_s"],
             "updateable": upd,
             "batched": bat,
+            "differentiation": grd,
         }
         print(json.dumps(line), flush=True)
     eng.close()

@@ -93,9 +93,10 @@ def test_separate_terms_and_fp32_forward():
     g_a = V.grad(balls, 1.4, None, u, precision="fp64")
     g = V.grad(balls, 1.4, w, u, precision="fp64")
     assert np.allclose(g, g_s + g_a, rtol=1e-12, atol=1e-9)
-    # FP32 forward: same pair set, contours recomputed in FP64, so x, y, z agree to
-    # rounding; r carries the SAS scaling term 2 w SAS / R with the forward's FP32 cell
-    # SAS (per-cell relative error up to ~1e-4)
+    # FP32 forward: same pair set; the adjoint takes each contour's topology from an FP32
+    # recomputation (FP64 for pairs in the band) and its vertices and arc angles in FP64,
+    # so x, y, z agree to rounding; r also carries the SAS scaling term 2 w SAS / R with the
+    # forward's FP32 cell SAS (per-cell relative error up to ~1e-4)
     g32 = V.grad(balls, 1.4, w, u, precision="fp32")
     assert np.allclose(g32[:, :3], g[:, :3], rtol=1e-9, atol=1e-9)
     assert np.allclose(g32[:, 3], g[:, 3], rtol=1e-4, atol=1e-4)

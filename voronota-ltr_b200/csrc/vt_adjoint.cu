@@ -28,31 +28,15 @@
 // whose SAS is positive receive SAS terms.  Accumulation uses double atomics.
 #include <cmath>
 
-#include "vt_contact.cuh"
-#include "vt_pipeline.cuh"
+#include "vt_adjoint.cuh"
 
 namespace vt {
 
 namespace {
 
 constexpr int kWarps = 4;
-constexpr uint32_t kErrAdjoint = 32u;  // a contour needed the serial kernel: not differentiated
 
 __device__ __forceinline__ Sph<double> sph_of(double4 v) { return {{v.x, v.y, v.z}, v.w}; }
-
-__device__ __forceinline__ double wsum(double v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-    return v;
-}
-__device__ __forceinline__ V3<double> wsum3(V3<double> v) { return {wsum(v.x), wsum(v.y), wsum(v.z)}; }
-
-__device__ __forceinline__ void add_grad(double* grad, uint32_t id, uint32_t n, V3<double> gp, double gr) {
-    const size_t i = 4 * (size_t)(id % n);
-    atomicAdd(grad + i, gp.x);
-    atomicAdd(grad + i + 1, gp.y);
-    atomicAdd(grad + i + 2, gp.z);
-    atomicAdd(grad + i + 3, gr);
-}
 
 __global__ void k_w_eff(uint32_t n, const double* __restrict__ w, const uint8_t* __restrict__ cell_flag,
                         const double* __restrict__ cell_sas, double* __restrict__ w_eff) {
@@ -66,20 +50,20 @@ __global__ void k_sas_scale(uint32_t n, const double* __restrict__ w_eff, const 
         if (w_eff[i] != 0.0) grad[4 * (size_t)i + 3] += w_eff[i] * 2.0 * cell_sas[i] / sph[i].w;
 }
 
+// FP64 adjoint: all valid pairs, or (from_list) the pairs the FP32 adjoint listed.
 __global__ void __launch_bounds__(kWarps * 32)
-    k_adjoint64(DevBufs b, uint32_t P, const double* __restrict__ u_contact, const double* __restrict__ w_eff,
-                double* __restrict__ grad) {
+    k_adjoint64(DevBufs b, uint32_t P, int from_list, const double* __restrict__ u_contact,
+                const double* __restrict__ w_eff, double* __restrict__ grad) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t n = b.n;
-    for (uint32_t p = blockIdx.x * kWarps + w; p < P; p += gridDim.x * kWarps) {
+    const uint32_t count = from_list ? *b.d_redo_count : P;
+    for (uint32_t it = blockIdx.x * kWarps + w; it < count; it += gridDim.x * kWarps) {
+        const uint32_t p = from_list ? b.redo_list[it] : it;
         if (!(b.p_status[p] & kValid)) continue;
         const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
         const uint32_t bid = b.nb_id[eb];
-        const bool kept = b.keep_off[p + 1] != b.keep_off[p];
-        const double u = (u_contact && kept) ? u_contact[b.keep_off[p]] : 0.0;
-        const double wa = w_eff[a];
-        const double wb = bid < n ? w_eff[bid] : 0.0;
-        if (u == 0.0 && wa == 0.0 && wb == 0.0) continue;
+        AdjPair G;
+        if (!adjoint_weights(b, p, a, bid, u_contact, w_eff, G)) continue;
         const uint32_t off = b.nb_off[a], cnt = b.nb_cnt[a];
         PairGeom<double> g;
         g.A = sph_of(b.sph[a]);
@@ -103,86 +87,24 @@ __global__ void __launch_bounds__(kWarps * 32)
             if (lane == 0 && r.overflow) atomicOr(b.err, kErrAdjoint);
             continue;
         }
-        const V3<double> pa = g.A.c, pb = g.B.c;
-        const double Ra = g.A.r, Rb = g.B.r;
-        const V3<double> q = co.ic.c;
-        const double rho = co.ic.r;
-        const V3<double> dab = pb - pa;
-        const double D2 = dot(dab, dab), D = sqrt(D2);
+        G.pa = g.A.c;
+        G.pb = g.B.c;
+        G.Ra = g.A.r;
+        G.Rb = g.B.r;
+        G.q = co.ic.c;
+        G.rho = co.ic.r;
+        G.axis = co.axis;
+        G.a = a;
+        G.bid = bid;
         const int len = co.len;
-        // this lane's boundary piece
-        V3<double> ga = mk<double>(0, 0, 0), gb = mk<double>(0, 0, 0);
-        double gra = 0.0, grb = 0.0, Lk = 0.0;
-        V3<double> Xk = mk<double>(0, 0, 0);
         const int nx = len > 0 ? (lane + 1 < len ? lane + 1 : 0) : 0;
         const Pt<double> nxt = shfl_pt(co.q, nx);
-        if (!co.full && lane < len) {
-            const Pt<double>& pt = co.q;
-            if (pt.rid == a && nxt.lid == a) {
-                const double al = pt.ang;
-                if (al > 0.0) {
-                    const V3<double> e1 = normalize(pt.p - q);
-                    const double h = 0.5 * al;
-                    const V3<double> mm = e1 * cos(h) + cross(co.axis, e1) * sin(h);
-                    Lk = rho * al;
-                    Xk = q * Lk + mm * (2.0 * rho * rho * sin(h));
-                }
-            } else if (u != 0.0) {
-                // straight edge on the radical plane of a and c = pt.rid
-                const uint32_t c = pt.rid;
-                uint32_t slot = 0xffffffffu;
-                for (uint32_t e = 0; e < cnt; ++e)
-                    if (nid[e] == c) {
-                        slot = nslot[e];
-                        break;
-                    }
-                if (slot != 0xffffffffu) {
-                    const Sph<double> C = sph_of(sph[slot]);
-                    const V3<double> dac = C.c - pa;
-                    const double kap = dot(dac, dab) / D2;
-                    const V3<double> perp = (dac - dab * kap) * 2.0;
-                    const double lam = 1.0 / norm(perp);
-                    const V3<double> xm = (pt.p + nxt.p) * 0.5;
-                    const double coef = u * norm(nxt.p - pt.p) * lam;
-                    add_grad(grad, c, n, (xm - C.c) * (-2.0 * coef), -2.0 * C.r * coef);
-                    ga = (xm - pa) * (2.0 * coef * (1.0 - kap));
-                    gra = 2.0 * Ra * coef * (1.0 - kap);
-                    gb = (xm - pb) * (2.0 * coef * kap);
-                    grb = 2.0 * Rb * coef * kap;
-                }
-            }
-        }
-        double L = wsum(Lk);
-        V3<double> X = wsum3(Xk);
-        ga = wsum3(ga);
-        gb = wsum3(gb);
-        gra = wsum(gra);
-        grb = wsum(grb);
-        if (co.full) {
-            L = 2.0 * kPi * rho;
-            X = q * L;
-        }
-        if (lane == 0) {
-            if (L > 0.0 && rho > 0.0) {
-                const double da = dot(q - pa, dab) / D;
-                const double kG = da / D;
-                const V3<double> Xa = X - pa * L, Xb = X - pb * L;
-                // area through the arcs
-                ga = ga + Xa * (u * (1.0 - kG) / rho);
-                gra += u * (1.0 - kG) * Ra * L / rho;
-                gb = gb + Xb * (u * kG / rho);
-                grb += u * kG * Rb * L / rho;
-                // SAS of a and of b through the same arcs
-                const double s = 1.0 / (D * rho);
-                const double cmix = (Ra * Ra + Rb * Rb - D2) * 0.5;
-                ga = ga + Xb * (wa * Ra * s) - Xa * (wb * Rb * s);
-                gb = gb - Xb * (wa * Ra * s) + Xa * (wb * Rb * s);
-                gra += wa * L * cmix * s - wb * Rb * Ra * L * s;
-                grb += wb * L * cmix * s - wa * Ra * Rb * L * s;
-            }
-            add_grad(grad, a, n, ga, gra);
-            add_grad(grad, bid, n, gb, grb);
-        }
+        auto sphere_of = [&](uint32_t c) {
+            for (uint32_t e = 0; e < cnt; ++e)
+                if (nid[e] == c) return sph[nslot[e]];
+            return make_double4(0.0, 0.0, 0.0, 0.0);
+        };
+        adjoint_pair(G, co.full, len, co.q.p, nxt.p, co.q.ang, co.q.rid, nxt.lid, sphere_of, grad, n);
     }
 }
 
@@ -205,7 +127,14 @@ void launch_adjoint(const DevBufs& b, uint32_t P, const double* w_sas, const dou
     cudaMemsetAsync(grad, 0, 4 * sizeof(double) * n, s);
     k_w_eff<<<gb(n), 256, 0, s>>>(n, w_sas, b.cell_flag, b.cell_sas, w_eff); count_launch();
     if (P) {
-        k_adjoint64<<<grid_blocks(P, kWarps, 148 * 64), kWarps * 32, 0, s>>>(b, P, u_contact, w_eff, grad);
+        if (b.nb_rel) {
+            // FP32 contours; pairs with a decision in the band are redone in FP64
+            cudaMemsetAsync(b.d_redo_count, 0, sizeof(uint32_t), s);
+            launch_adjoint_f32(b, P, u_contact, w_eff, grad, s);
+            k_adjoint64<<<grid_blocks(P, kWarps, 148 * 64), kWarps * 32, 0, s>>>(b, P, 1, u_contact, w_eff, grad);
+        } else {
+            k_adjoint64<<<grid_blocks(P, kWarps, 148 * 64), kWarps * 32, 0, s>>>(b, P, 0, u_contact, w_eff, grad);
+        }
         count_launch();
     }
     k_sas_scale<<<gb(n), 256, 0, s>>>(n, w_eff, b.cell_sas, b.sph, grad); count_launch();

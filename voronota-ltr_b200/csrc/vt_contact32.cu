@@ -6,6 +6,7 @@
 // Every fuzzy decision is evaluated with an uncertainty band (vt_geom.cuh, Dec<float,
 // true>); a pair with any decision inside its band is marked unsure and recomputed by
 // the FP64 kernel, as is a pair whose contour outgrew the warp.
+#include "vt_adjoint.cuh"
 #include "vt_contact.cuh"
 #include "vt_pipeline.cuh"
 
@@ -67,7 +68,95 @@ __global__ void __launch_bounds__(kWarps * 32, VT_C32_MINB) k_contact32(DevBufs 
     }
 }
 
+// FP32 adjoint: the contour recomputed in FP32 (relative to a), the gradient formed in
+// double from its points; pairs whose recomputation is unsure or overflows are listed for
+// the FP64 adjoint.
+__global__ void __launch_bounds__(kWarps * 32, 4)
+    k_adjoint32(DevBufs b, uint32_t P, float band, const double* __restrict__ u_contact,
+                const double* __restrict__ w_eff, double* __restrict__ grad) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t n = b.n;
+    for (uint32_t p = blockIdx.x * kWarps + w; p < P; p += gridDim.x * kWarps) {
+        if (!(b.p_status[p] & kValid)) continue;
+        const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
+        const uint32_t bid = b.nb_id[eb];
+        AdjPair G;
+        if (!adjoint_weights(b, p, a, bid, u_contact, w_eff, G)) continue;
+        const uint32_t off = b.nb_off[a], cnt = b.nb_cnt[a];
+        const double4 A4 = b.sph[a], B4 = b.sph[b.nb_slot[eb]];
+        PairGeom<float> g;
+        const float Ra = (float)A4.w;
+        const float4 rb = b.nb_rel[eb];
+        g.A = {{0.f, 0.f, 0.f}, Ra};
+        g.B = {{rb.x, rb.y, rb.z}, rb.w};
+        g.a_id = a;
+        g.b_id = bid;
+        g.S = Ra + rb.w;
+        g.e0 = band * g.S;
+        const float4* rel = b.nb_rel + off;
+        const uint32_t* nid = b.nb_id + off;
+        const uint32_t* nslot = b.nb_slot + off;
+        auto nbf = [&](int e) {
+            Nb<float> r;
+            float4 v = rel[e];
+            r.s = {{v.x, v.y, v.z}, v.w};
+            r.id = nid[e];
+            return r;
+        };
+        ContourOut<float> co;
+        WarpContact r = contact_warp<float, true, false>(g, (int)cnt, (int)(eb - off), nbf, &co);
+        if (!r.valid || r.unsure || r.overflow) {
+            if (lane == 0) b.redo_list[atomicAdd(b.d_redo_count, 1u)] = p;
+            continue;
+        }
+        const Sph<double> A = {{A4.x, A4.y, A4.z}, A4.w}, B = {{B4.x, B4.y, B4.z}, B4.w};
+        const Sph<double> ic = intersection_circle(A, B);
+        G.pa = A.c;
+        G.pb = B.c;
+        G.Ra = A.r;
+        G.Rb = B.r;
+        G.q = ic.c;
+        G.rho = ic.r;
+        G.axis = normalize(B.c - A.c);
+        G.a = a;
+        G.bid = bid;
+        const int len = co.len;
+        const int nx = len > 0 ? (lane + 1 < len ? lane + 1 : 0) : 0;
+        const double4* sph = b.sph;
+        auto sphere_of = [&](uint32_t c) {
+            for (uint32_t e = 0; e < cnt; ++e)
+                if (nid[e] == c) return sph[nslot[e]];
+            return make_double4(0.0, 0.0, 0.0, 0.0);
+        };
+        // the FP32 topology with FP64 vertices and arc angles
+        V3<double> y = widen(co.q.p);
+        if (!co.full && lane < len) y = snap_vertex(G, y, co.q.lid, co.q.rid, sphere_of);
+        const V3<double> P0 = A.c + y;
+        const V3<double> P1 = mk<double>(__shfl_sync(kFull, P0.x, nx), __shfl_sync(kFull, P0.y, nx),
+                                         __shfl_sync(kFull, P0.z, nx));
+        const uint32_t nlid = __shfl_sync(kFull, co.q.lid, nx);
+        double ang = 0.0;
+        if (!co.full && lane < len && co.q.rid == a && nlid == a && co.q.ang > 0.f) {
+            const V3<double> v1 = P0 - G.q, v2 = P1 - G.q;
+            ang = atan2(dot(cross(v1, v2), G.axis), dot(v1, v2));
+            if (ang < 0.0) ang += kTau;
+            // a nearly full or nearly empty arc keeps the FP32 branch of the angle
+            if (fabs((double)co.q.ang - ang) > 1.0) ang = (double)co.q.ang;
+        }
+        adjoint_pair(G, co.full, len, P0, P1, ang, co.q.rid, nlid, sphere_of, grad, n);
+    }
+}
+
 }  // namespace
+
+void launch_adjoint_f32(const DevBufs& b, uint32_t P, const double* u_contact, const double* w_eff, double* grad,
+                        cudaStream_t s) {
+    size_t g = (P + kWarps - 1) / kWarps;
+    if (g < 1) g = 1;
+    if (g > 148 * 64) g = 148 * 64;
+    k_adjoint32<<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band, u_contact, w_eff, grad);
+    count_launch();
+}
 
 void launch_contact_f32(const DevBufs& b, uint32_t P, int full, cudaStream_t s) {
     size_t g = (P + kWarps - 1) / kWarps;

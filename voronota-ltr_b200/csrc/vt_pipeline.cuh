@@ -244,6 +244,10 @@ void scan_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* tmp, cudaSt
 // b (w_sas, u_contact: device arrays or null; w_eff: n doubles of scratch).
 void launch_adjoint(const DevBufs& b, uint32_t P, const double* w_sas, const double* u_contact, double* w_eff,
                     double* grad, cudaStream_t s);
+// FP32 adjoint over all valid pairs (vt_contact32.cu); lists the pairs it cannot decide
+// in redo_list for the FP64 adjoint.
+void launch_adjoint_f32(const DevBufs& b, uint32_t P, const double* u_contact, const double* w_eff, double* grad,
+                        cudaStream_t s);
 
 // ---- contact kernels (vt_contact64.cu / vt_contact32.cu) ----
 // mode: 0 = all pairs; 1 = pairs listed in redo_list (count on device)
