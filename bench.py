@@ -17,7 +17,9 @@ geometry with FP64 recomputation of band pairs.  One step = one full tessellatio
          in this image) on the host cores
 
 With torchrun (N > 1) each rank tessellates its own structure (seed = rank): independent
-replicas, no collective on the data path; value = all ranks' balls / max-over-ranks time.
+replicas, no collective on the data path; value = all ranks' balls / max-over-ranks time
+(voronota_ltr.replicas).  The updateable, batched and differentiation legs run on every
+rank on its own inputs and report max-over-ranks times.
 
 ``--impl reference`` times the reference's algorithm on the host cores instead (the CPU
 oracle port: the Rust reference cannot be built here) on the same workload.
@@ -178,7 +180,7 @@ def trajectory(n, steps, seed):
     return balls, box, moves
 
 
-def updateable_leg(args, rank, torch, V):
+def updateable_leg(args, rank, torch, V, R):
     """UpdateableTessellation.update_with_changed on the device along the trajectory.
 
     Per update: CUDA events on the handle's stream around vt_upd_update_with_changed_device
@@ -199,27 +201,30 @@ def updateable_leg(args, rank, torch, V):
         d = torch.from_numpy(balls).cuda()
         torch.cuda.synchronize()
         u.init_device(d.data_ptr(), n, PROBE, box)
-        ms, aff, pairs, redo = [], [], [], []
+        ms, adj, pairs, redo = [], [], [], []
+        dg = torch.empty((n, 4), dtype=torch.float64, device="cuda")
         for t, (ids, disp) in enumerate(moves[:warm + nsteps]):
             ti = torch.from_numpy(ids).cuda()
             d[ti, :3] += torch.from_numpy(disp).cuda()
             torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
             e0.record(stream)
             u.update_with_changed_device(d.data_ptr(), n, ti.data_ptr(), len(ids))
             e1.record(stream)
-            e1.synchronize()
+            st = u.stats()
+            u.grad_sas_device(0, dg.data_ptr())  # adjoint of the total SAS
+            e2.record(stream)
+            e2.synchronize()
             if t >= warm:
                 ms.append(e0.elapsed_time(e1))
-                st = u.stats()
+                adj.append(e1.elapsed_time(e2))
                 pairs.append(int(st.num_pairs))
                 redo.append(int(st.num_fp64_redo))
         aff = len(u.affected_ids())
-        return u, d, ms, aff, pairs, redo
+        return u, d, ms, aff, pairs, redo, adj
 
-    u32, d32, ms32, aff, pairs, redo = run("fp32", steps)
-    _, _, ms64, _, _, _ = run("fp64", max(3, steps // 2))
+    u32, d32, ms32, aff, pairs, redo, adj32 = run("fp32", steps)
+    _, _, ms64, _, _, _, adj64 = run("fp64", max(3, steps // 2))
     eng = V.Engine()
     eng.set_stream(stream.cuda_stream)
     full = []
@@ -232,15 +237,20 @@ def updateable_leg(args, rank, torch, V):
         e1.synchronize()
         full.append(e0.elapsed_time(e1))
     eng.close()
-    t32 = statistics.median(ms32)
+    t32 = R.max(statistics.median(ms32))
+    t64 = R.max(statistics.median(ms64))
+    a32 = R.max(statistics.median(adj32))
+    a64 = R.max(statistics.median(adj64))
+    tfull = R.max(statistics.median(full))
     out = {
         "workload": f"periodic cube {n} balls, 0.033 balls/A^3, r 1.52, probe 1.4; per step 1% of the balls "
                     "moved by N(0, 0.05 A) per axis, then update_with_changed on the device",
         "steps": steps, "warmup": warm,
-        "ms_per_update_fp32": t32, "ms_per_update_fp64": statistics.median(ms64),
-        "ms_full_recompute_fp32": statistics.median(full),
-        "speedup_vs_full_recompute": statistics.median(full) / t32,
-        "balls_per_s_fp32": n / (t32 * 1e-3),
+        "ms_per_update_fp32": t32, "ms_per_update_fp64": t64,
+        "ms_adjoint_total_sas_fp32": a32, "ms_adjoint_total_sas_fp64": a64,
+        "ms_per_step_update_plus_adjoint_fp32": t32 + a32,
+        "ms_full_recompute_fp32": tfull, "speedup_vs_full_recompute": tfull / t32,
+        "balls_per_s_fp32": replica_throughput(n, R.world, t32), "max_over_ranks": R.world,
         "affected_per_update": aff, "pairs_per_update": int(statistics.median(pairs)),
         "fp64_redo_pairs_per_update": int(statistics.median(redo)),
     }
@@ -280,7 +290,7 @@ def updateable_cpu_check(balls, box, moves, n, torch, V):
                                              "rel_err_total_sas": rel, "rel_err_total_volume": relv}}
 
 
-def batched_leg(args, rank, torch, V):
+def batched_leg(args, rank, torch, V, R):
     """Batched structures: sizes log-uniform in [300, 20000], structure i from the lattice
     generator with seed 1000 + i, FP32+fixup (and FP64) in one batched call per step;
     per-structure SAS / volume error against the CPU oracle on a sample (rank 0)."""
@@ -310,13 +320,15 @@ def batched_leg(args, rank, torch, V):
             ms.append(e0.elapsed_time(e1))
         return statistics.median(ms)
 
-    t64 = timed("fp64", 1, 0)
-    t32 = timed("fp32", 3, 1)
+    t64 = R.max(timed("fp64", 1, 0))
+    t32 = R.max(timed("fp32", 3, 1))
     st = eng.stats()
     out = {"workload": f"{len(sizes)} structures, sizes log-uniform in [300, 20000] ({len(balls)} balls), "
                        "lattice generator seed 1000+i, probe 1.4, one batched call",
-           "balls": int(len(balls)), "ms_fp32": t32, "balls_per_s_fp32": len(balls) / (t32 * 1e-3),
-           "ms_fp64": t64, "balls_per_s_fp64": len(balls) / (t64 * 1e-3), "speedup_vs_fp64": t64 / t32,
+           "balls": int(len(balls)), "ms_fp32": t32,
+           "balls_per_s_fp32": replica_throughput(len(balls), R.world, t32),
+           "ms_fp64": t64, "balls_per_s_fp64": replica_throughput(len(balls), R.world, t64),
+           "speedup_vs_fp64": t64 / t32, "max_over_ranks": R.world,
            "pairs": int(st.num_pairs), "fp64_redo_pairs": int(st.num_fp64_redo)}
     if rank == 0 and not args.no_cpu:
         import oracle as O
@@ -353,7 +365,7 @@ def _loss_fn(n, w, key_sorted, u_sorted):
     return loss
 
 
-def grad_leg(args, rank, torch, V):
+def grad_leg(args, rank, torch, V, R):
     """L = sum_i w_i SAS_i + sum_ab u_ab area_ab on a lattice structure, w ~ U(0,1),
     u ~ N(0,1) (seeded): forward + hand-written adjoint timed on the device; the gradient
     checked at 256 random coordinates against central differences (h = 1e-4 A, f64) of
@@ -390,6 +402,7 @@ def grad_leg(args, rank, torch, V):
     f64, b64 = timed("fp64")
     g64 = dg.cpu().numpy().copy()
     f32, b32 = timed("fp32")
+    f64, b64, f32, b32 = (R.max(x) for x in (f64, b64, f32, b32))
     g = dg.cpu().numpy().copy()
     eng.close()
     key = _pair_keys(ref.id_a, ref.id_b, n)
@@ -475,29 +488,13 @@ def run_reference(args):
 def run_ours(args):
     import torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    from voronota_ltr.replicas import Ranks, replica_throughput
+
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    R = Ranks("nccl")
+    world, rank = R.world, R.rank
+    barrier, max_over_ranks = R.barrier, R.max
 
     import voronota_ltr as V
 
@@ -539,7 +536,7 @@ def run_ours(args):
 
     fp32 = device_leg("fp32", args.steps, args.warmup, True)
     mean_ms = max_over_ranks(fp32["mean_ms"])
-    value = world * args.n / (mean_ms * 1e-3)
+    value = replica_throughput(args.n, world, mean_ms)
 
     fp64 = None
     if not args.no_fp64:
@@ -575,9 +572,9 @@ def run_ours(args):
     if rank == 0 and not args.no_cpu:
         cpu = cpu_baseline(balls)
 
-    upd = None if args.no_upd else updateable_leg(args, rank, torch, V)
-    bat = None if args.no_batch else batched_leg(args, rank, torch, V)
-    grd = None if args.no_grad else grad_leg(args, rank, torch, V)
+    upd = None if args.no_upd else updateable_leg(args, rank, torch, V, R)
+    bat = None if args.no_batch else batched_leg(args, rank, torch, V, R)
+    grd = None if args.no_grad else grad_leg(args, rank, torch, V, R)
 
     if rank == 0:
         line = {
@@ -610,9 +607,7 @@ def run_ours(args):
         }
         print(json.dumps(line), flush=True)
     eng.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    R.close()
     return 0
 
 

@@ -220,6 +220,11 @@ uint64_t vt_upd_num_changed(const vt_updateable* h);
 int vt_upd_changed_ids(vt_updateable* h, uint64_t* out);
 uint64_t vt_upd_num_affected(vt_updateable* h);
 int vt_upd_affected_ids(vt_updateable* h, uint64_t* out);
+/* Adjoint of sum_i w_sas[i] SAS_i over the current state (no counterpart in the
+ * reference; the gradient of vt_engine_grad_device restricted to SAS terms): d_w_sas (n
+ * doubles on the device, NULL: all 1, the total SAS) and d_grad (n x 4 doubles on the
+ * device, overwritten with dL/d(x, y, z, r)). */
+int vt_upd_grad_sas(vt_updateable* h, const double* d_w_sas, double* d_grad);
 /* counters of the last operation: list entries, pairs recomputed, FP64 redo, cells */
 int vt_upd_stats(const vt_updateable* h, vt_stats* out);
 

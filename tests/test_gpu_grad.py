@@ -128,3 +128,32 @@ def test_torch_autograd_matches_c_abi():
     loss.backward()
     g = V.grad(balls, 1.4, w, u, precision="fp64")
     assert np.allclose(x.grad.cpu().numpy(), g, rtol=1e-12, atol=1e-10)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_updateable_sas_adjoint_matches_stateless(precision):
+    import torch
+
+    balls = W.lattice_balls(2000, 25)
+    t = V.UpdateableTessellation(precision=precision)
+    assert t.init(balls, 1.4)
+    rng = np.random.default_rng(3)
+    for _ in range(3):
+        ids = np.sort(rng.choice(len(balls), 20, replace=False))
+        balls[ids, :3] += rng.normal(0.0, 0.05, (20, 3))
+        assert t.update_with_changed(balls, ids)
+    w = rng.uniform(0.0, 1.0, len(balls))
+    dw = torch.from_numpy(w).cuda()
+    dg = torch.empty((len(balls), 4), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    t.grad_sas_device(dw.data_ptr(), dg.data_ptr())
+    g = V.grad(balls, 1.4, w, None, precision=precision)
+    gu = dg.cpu().numpy()
+    assert np.allclose(gu[:, :3], g[:, :3], rtol=1e-9, atol=1e-9)
+    # r carries 2 w SAS / R with each path's own cell SAS (FP32: per-cell error ~1e-4)
+    tol = 1e-9 if precision == "fp64" else 1e-4
+    assert np.allclose(gu[:, 3], g[:, 3], rtol=tol, atol=tol)
+    # the total SAS (w = 1)
+    t.grad_sas_device(0, dg.data_ptr())
+    g1 = V.grad(balls, 1.4, np.ones(len(balls)), None, precision=precision)
+    assert np.allclose(dg.cpu().numpy()[:, :3], g1[:, :3], rtol=1e-9, atol=1e-9)

@@ -105,10 +105,11 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
         };
         ContourOut<float> co;
         WarpContact r = contact_warp<float, true, false>(g, (int)cnt, (int)(eb - off), nbf, &co);
-        if (!r.valid || r.unsure || r.overflow) {
+        if (r.unsure || r.overflow) {
             if (lane == 0) b.redo_list[atomicAdd(b.d_redo_count, 1u)] = p;
             continue;
         }
+        if (!r.valid) continue;  // no contact, decided outside the band
         const Sph<double> A = {{A4.x, A4.y, A4.z}, A4.w}, B = {{B4.x, B4.y, B4.z}, B4.w};
         const Sph<double> ic = intersection_circle(A, B);
         G.pa = A.c;

@@ -861,6 +861,44 @@ struct vt_updateable {
         return VT_OK;
     }
 
+    // adjoint of sum_i w_i SAS_i over the current state (w == null: every w_i = 1)
+    DBuf<double> ones, w_eff;
+    int grad_sas(const double* d_w, double* d_grad) {
+        UState& S = *cur;
+        const uint32_t n = S.n;
+        if (n == 0) return VT_OK;
+        if (!sph_fresh) {
+            int st = build_spheres(S);
+            if (st != VT_OK) return st;
+        }
+        const uint32_t P = gen_pairs(S, nullptr, nullptr, n, nullptr);
+        DevBufs b = pair_bufs(S, P);
+        keep_off.ensure(P + 2);
+        zero(keep_off.p, 4 * ((size_t)P + 2));
+        b.keep_off = keep_off.p;
+        // validity is decided by the adjoint's own recomputation
+        VT_CUDA(cudaMemsetAsync(p_status.p, kValid, P, stream));
+        if (!d_w) {
+            if (ones.cap < n) {
+                ones.ensure(n);
+                std::vector<double> h1(ones.cap, 1.0);
+                VT_CUDA(cudaMemcpy(ones.p, h1.data(), 8 * ones.cap, cudaMemcpyHostToDevice));
+            }
+            d_w = ones.p;
+        }
+        w_eff.ensure(n);
+        zero(w(kWErr), 4);
+        launch_adjoint(b, P, d_w, nullptr, w_eff.p, d_grad, stream);
+        const uint32_t err = read_word(w(kWErr));
+        VT_CUDA(cudaGetLastError());
+        stats.num_pairs = P;
+        if (err & 32u) {
+            set_last_error("a contact whose contour has more than 32 points is not differentiated");
+            return VT_ERR_CAPACITY;
+        }
+        return VT_OK;
+    }
+
     // totals of the current summary without downloading it: sas, volume, contact area
     int totals3(double* out3) {
         vt_result* r = nullptr;
@@ -1114,6 +1152,13 @@ int vt_upd_totals(vt_updateable* h, double* totals3) {
     return guarded([&]() -> int {
         VT_CUDA(cudaSetDevice(h->device));
         return h->totals3(totals3);
+    });
+}
+int vt_upd_grad_sas(vt_updateable* h, const double* d_w_sas, double* d_grad) {
+    if (check_handle(h) || !d_grad) return VT_ERR_INVALID;
+    return guarded([&]() -> int {
+        h->begin_op();
+        return h->grad_sas(d_w_sas, d_grad);
     });
 }
 int vt_upd_last_full_reinit(const vt_updateable* h) { return h && h->cur->full ? 1 : 0; }

@@ -127,6 +127,7 @@ def library():
     L.vt_upd_num_affected.restype = ctypes.c_uint64
     L.vt_upd_affected_ids.argtypes = [_vp, _u64p]
     L.vt_upd_stats.argtypes = [_vp, ctypes.POINTER(VtStats)]
+    L.vt_upd_grad_sas.argtypes = [_vp, ctypes.c_void_p, ctypes.c_void_p]
     L.vt_compute_batch.argtypes = [_f64p, _u64p, ctypes.c_uint64, ctypes.c_double, ctypes.c_int,
                                    ctypes.POINTER(_vp)]
     L.vt_engine_compute_batch_device.argtypes = [_vp, ctypes.c_void_p, _u64p, ctypes.c_uint64, ctypes.c_double,
@@ -606,6 +607,11 @@ class UpdateableTessellation:
         s = VtStats()
         _check(self._L.vt_upd_stats(self._h, ctypes.byref(s)))
         return s
+
+    def grad_sas_device(self, d_w_ptr, d_grad_ptr: int):
+        """d_grad (N x 4 doubles on the device) = d(sum w SAS)/d(x, y, z, r) of the current
+        state; d_w_ptr 0/None: the total SAS."""
+        _check(self._L.vt_upd_grad_sas(self._h, d_w_ptr or None, d_grad_ptr))
 
 
 __all__ = ["compute_tessellation", "compute_tessellation_result", "compute_contacts_only",
