@@ -68,6 +68,20 @@ int vt_result_cells(const vt_result* r, uint32_t* index, double* sas_area, doubl
 void vt_result_totals(const vt_result* r, double* total_sas_area, double* total_volume,
                       double* total_contact_area);
 void vt_result_free(vt_result* r);
+/* Read-only views of a result's arrays, valid until vt_result_free (no copy; the arrays
+ * live in page-locked host memory the device wrote directly). */
+typedef struct vt_result_view {
+    uint64_t num_contacts, num_cells;
+    const uint32_t* id_a;
+    const uint32_t* id_b;
+    const double* area;
+    const double* arc_length;
+    const uint8_t* central;
+    const uint32_t* cell_index;
+    const double* cell_sas_area;
+    const double* cell_volume;
+} vt_result_view;
+int vt_result_view_get(const vt_result* r, vt_result_view* view);
 
 /* ---- engine: explicit device, stream and device-resident inputs ---- */
 int vt_engine_create(int device, vt_engine** out);

@@ -34,6 +34,58 @@ thread_local std::string g_last_error;
 
 namespace vt {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+namespace {
+std::mutex g_pool_mu;
+std::vector<std::pair<size_t, void*>> g_pool;  // free page-locked blocks (capacity, pointer)
+size_t g_pool_bytes = 0;
+constexpr size_t kPoolMaxBytes = size_t(4) << 30;  // cached page-locked memory kept for reuse
+}  // namespace
+
+void* host_block_acquire(size_t bytes, size_t* cap, bool* pinned) {
+    size_t c = 64 * 1024;
+    while (c < bytes) c <<= 1;
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        for (size_t k = 0; k < g_pool.size(); ++k)
+            if (g_pool[k].first == c) {
+                void* p = g_pool[k].second;
+                g_pool[k] = g_pool.back();
+                g_pool.pop_back();
+                g_pool_bytes -= c;
+                *cap = c;
+                *pinned = true;
+                return p;
+            }
+    }
+    void* p = nullptr;
+    if (cudaMallocHost(&p, c) == cudaSuccess) {
+        *cap = c;
+        *pinned = true;
+        return p;
+    }
+    cudaGetLastError();
+    p = std::malloc(c);
+    *cap = c;
+    *pinned = false;
+    return p;
+}
+
+void host_block_release(void* p, size_t cap, bool pinned) {
+    if (!pinned) {
+        std::free(p);
+        return;
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        if (g_pool_bytes + cap <= kPoolMaxBytes) {
+            g_pool.emplace_back(cap, p);
+            g_pool_bytes += cap;
+            return;
+        }
+    }
+    cudaFreeHost(p);
+}
 }  // namespace vt
 
 // Host copy of a batched result: all structures' contacts and cells concatenated (ids
@@ -855,6 +907,20 @@ void vt_result_totals(const vt_result* r, double* s, double* v, double* c) {
     if (c) *c = r->totals[2];
 }
 void vt_result_free(vt_result* r) { delete r; }
+int vt_result_view_get(const vt_result* r, vt_result_view* v) {
+    if (!r || !v) return VT_ERR_INVALID;
+    v->num_contacts = r->a.size();
+    v->num_cells = r->cell_index.size();
+    v->id_a = r->a.data();
+    v->id_b = r->b.data();
+    v->area = r->area.data();
+    v->arc_length = r->arc.data();
+    v->central = r->central.data();
+    v->cell_index = r->cell_index.data();
+    v->cell_sas_area = r->cell_sas.data();
+    v->cell_volume = r->cell_vol.data();
+    return VT_OK;
+}
 
 int vt_engine_create(int device, vt_engine** out) {
     if (!out) return VT_ERR_INVALID;

@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <new>
 #include <string>
 #include <vector>
@@ -81,15 +82,49 @@ int guarded(F&& f) {
     }
 }
 
+// Page-locked host blocks for results, recycled through a process-wide pool so that a
+// result is copied from the device by DMA without a bounce buffer or a zero-fill.
+// Falls back to malloc when page-locked memory is not available.
+void* host_block_acquire(size_t bytes, size_t* cap, bool* pinned);
+void host_block_release(void* p, size_t cap, bool pinned);
+
+// Uninitialised host array in a pooled block (resize discards the contents).
+template <typename T>
+struct HostArr {
+    T* p = nullptr;
+    size_t n = 0, capb = 0;
+    bool pinned = false;
+    HostArr() = default;
+    HostArr(const HostArr&) = delete;
+    HostArr& operator=(const HostArr&) = delete;
+    ~HostArr() { release(); }
+    void release() {
+        if (p) host_block_release(p, capb, pinned);
+        p = nullptr;
+        n = capb = 0;
+    }
+    void resize(size_t m) {
+        if (m * sizeof(T) > capb || !p) {
+            release();
+            p = (T*)host_block_acquire(std::max<size_t>(m, 1) * sizeof(T), &capb, &pinned);
+            if (!p) throw std::bad_alloc();
+        }
+        n = m;
+    }
+    T* data() { return p; }
+    const T* data() const { return p; }
+    size_t size() const { return n; }
+};
+
 }  // namespace vt
 
 // Host copy of a tessellation result (TessellationResult, types.rs:69-95).
 struct vt_result {
     uint64_t num_balls = 0;
-    std::vector<uint32_t> a, b;
-    std::vector<double> area, arc;
-    std::vector<uint8_t> central;
-    std::vector<uint32_t> cell_index;
-    std::vector<double> cell_sas, cell_vol;
+    vt::HostArr<uint32_t> a, b;
+    vt::HostArr<double> area, arc;
+    vt::HostArr<uint8_t> central;
+    vt::HostArr<uint32_t> cell_index;
+    vt::HostArr<double> cell_sas, cell_vol;
     double totals[3] = {0, 0, 0};
 };

@@ -90,6 +90,7 @@ def library():
     L.vt_result_totals.restype = None
     L.vt_result_free.argtypes = [_vp]
     L.vt_result_free.restype = None
+    L.vt_result_view_get.argtypes = [_vp, ctypes.POINTER(VtResultView)]
     L.vt_engine_create.argtypes = [ctypes.c_int, ctypes.POINTER(_vp)]
     L.vt_engine_destroy.argtypes = [_vp]
     L.vt_engine_destroy.restype = None
@@ -225,8 +226,34 @@ def _groups_array(groups):
     return np.ascontiguousarray(np.asarray(groups, dtype=np.int32).reshape(-1))
 
 
+class VtResultView(ctypes.Structure):
+    _fields_ = [("num_contacts", ctypes.c_uint64), ("num_cells", ctypes.c_uint64)] + [
+        (k, ctypes.c_void_p) for k in ("id_a", "id_b", "area", "arc_length", "central", "cell_index",
+                                       "cell_sas_area", "cell_volume")]
+
+
+class _ResultOwner:
+    """Frees a library result when the last numpy view of its arrays is gone."""
+
+    def __init__(self, L, h):
+        self.L, self.h = L, h
+
+    def __del__(self):
+        if self.h:
+            self.L.vt_result_free(self.h)
+            self.h = None
+
+
+def _view(ptr, count, ctype, dtype, owner):
+    if count == 0 or not ptr:
+        return np.empty(0, dtype)
+    buf = (ctype * count).from_address(ptr)
+    buf._owner = owner  # the view keeps the result alive
+    return np.frombuffer(buf, dtype=dtype)
+
+
 class Result:
-    """Host copy of a tessellation result (numpy arrays)."""
+    """A tessellation result as numpy arrays (zero-copy views of the library's result)."""
 
     def __init__(self, num_balls, id_a, id_b, area, arc_length, central, cell_index, cell_sas, cell_volume,
                  totals):
@@ -238,23 +265,24 @@ class Result:
 
     @classmethod
     def from_handle(cls, L, h):
-        nc = L.vt_result_num_contacts(h)
-        a = np.empty(nc, np.uint32)
-        b = np.empty(nc, np.uint32)
-        ar = np.empty(nc, np.float64)
-        arc = np.empty(nc, np.float64)
-        ce = np.empty(nc, np.uint8)
-        _check(L.vt_result_contacts(h, a.ctypes.data_as(_u32p), b.ctypes.data_as(_u32p), ar.ctypes.data_as(_f64p),
-                                    arc.ctypes.data_as(_f64p), ce.ctypes.data_as(_u8p)))
-        m = L.vt_result_num_cells(h)
-        ci = np.empty(m, np.uint32)
-        cs = np.empty(m, np.float64)
-        cv = np.empty(m, np.float64)
-        _check(L.vt_result_cells(h, ci.ctypes.data_as(_u32p), cs.ctypes.data_as(_f64p), cv.ctypes.data_as(_f64p)))
+        """Wrap a library result without copying: the arrays are views of the result's
+        page-locked host memory, and the result is freed when the last of them is gone.
+        Takes ownership of `h`."""
+        owner = _ResultOwner(L, h)
+        v = VtResultView()
+        _check(L.vt_result_view_get(h, ctypes.byref(v)))
+        C, M = int(v.num_contacts), int(v.num_cells)
+        a = _view(v.id_a, C, ctypes.c_uint32, np.uint32, owner)
+        b = _view(v.id_b, C, ctypes.c_uint32, np.uint32, owner)
+        ar = _view(v.area, C, ctypes.c_double, np.float64, owner)
+        arc = _view(v.arc_length, C, ctypes.c_double, np.float64, owner)
+        ce = _view(v.central, C, ctypes.c_uint8, np.bool_, owner)
+        ci = _view(v.cell_index, M, ctypes.c_uint32, np.uint32, owner)
+        cs = _view(v.cell_sas_area, M, ctypes.c_double, np.float64, owner)
+        cv = _view(v.cell_volume, M, ctypes.c_double, np.float64, owner)
         t = (ctypes.c_double(), ctypes.c_double(), ctypes.c_double())
         L.vt_result_totals(h, ctypes.byref(t[0]), ctypes.byref(t[1]), ctypes.byref(t[2]))
-        return cls(L.vt_result_num_balls(h), a, b, ar, arc, ce.astype(bool), ci, cs, cv,
-                   (t[0].value, t[1].value, t[2].value))
+        return cls(L.vt_result_num_balls(h), a, b, ar, arc, ce, ci, cs, cv, (t[0].value, t[1].value, t[2].value))
 
     def sas_areas(self):
         """Per-ball SAS area or None (Results::sas_areas, types.rs:207-213)."""
@@ -294,10 +322,7 @@ def _run(fn_name, balls, probe, periodic_box, groups, precision) -> Result:
                              None if g is None else g.ctypes.data_as(_i32p), 0 if g is None else len(g),
                              _precision_code(precision), ctypes.byref(h))
     _check(st)
-    try:
-        return Result.from_handle(L, h)
-    finally:
-        L.vt_result_free(h)
+    return Result.from_handle(L, h)
 
 
 def compute_tessellation_result(balls, probe, periodic_box=None, groups=None, precision="fp32") -> Result:
@@ -499,10 +524,7 @@ class Engine:
     def download(self) -> Result:
         h = _vp()
         _check(self._L.vt_engine_download(self._h, ctypes.byref(h)))
-        try:
-            return Result.from_handle(self._L, h)
-        finally:
-            self._L.vt_result_free(h)
+        return Result.from_handle(self._L, h)
 
 
 class UpdateableTessellation:
@@ -579,10 +601,7 @@ class UpdateableTessellation:
     def summary(self) -> Result:
         h = _vp()
         _check(self._L.vt_upd_summary(self._h, ctypes.byref(h)))
-        try:
-            return Result.from_handle(self._L, h)
-        finally:
-            self._L.vt_result_free(h)
+        return Result.from_handle(self._L, h)
 
     def totals(self) -> tuple[float, float, float]:
         """(total SAS area, total volume, total contact area) of the current summary."""
