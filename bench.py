@@ -189,6 +189,8 @@ def updateable_leg(args, rank, torch, V, R):
     updateable tessellation on the first steps, with the GPU replaying those steps from
     the same start for the accuracy check.
     """
+    from voronota_ltr.replicas import replica_throughput
+
     n = args.upd_n
     warm = max(1, args.warmup)
     steps = max(5, args.steps)
@@ -294,6 +296,8 @@ def batched_leg(args, rank, torch, V, R):
     """Batched structures: sizes log-uniform in [300, 20000], structure i from the lattice
     generator with seed 1000 + i, FP32+fixup (and FP64) in one batched call per step;
     per-structure SAS / volume error against the CPU oracle on a sample (rank 0)."""
+    from voronota_ltr.replicas import replica_throughput
+
     from voronota_ltr import workloads as W
 
     sizes = W.batch_sizes(args.batch_count)

@@ -90,6 +90,9 @@ struct Pt {  // one contour point (contact.rs:36-47), held by one lane
     T ang;
 };
 
+__device__ __forceinline__ V3<double> wide3(V3<double> v) { return v; }
+__device__ __forceinline__ V3<double> wide3(V3<float> v) { return {(double)v.x, (double)v.y, (double)v.z}; }
+
 template <typename T>
 __device__ __forceinline__ Pt<T> shfl_pt(const Pt<T>& q, int src) {
     Pt<T> r;
@@ -165,6 +168,7 @@ struct PairGeom {
     uint32_t a_id, b_id;
     T e0;  // FP32: error budget E of a contour point coordinate (A); 0 in FP64
     T S;   // length scale of the pair (R_a + R_b)
+    bool want_xm = false;  // FULL: also the first moment of the arcs (the SAS adjoint)
 };
 
 // ---- FP32 constructions: decisions banded by the point error budget E ----
@@ -283,6 +287,7 @@ struct WarpContact {
     bool unsure;
     bool overflow;
     double area, arc, sa_a, sa_b, pv_a, pv_b;
+    double xm[3];  // first moment of the contact's arcs about a's centre (want_xm)
     bool central;
     int site;  // debug builds: first step with an unsure decision
 };
@@ -374,7 +379,8 @@ struct ContourOut {
     V3<T> axis;
 };
 
-template <typename T, bool F, bool FULL, typename NbFn>
+// XM: compile in the arc first moment (computed when g.want_xm).
+template <typename T, bool F, bool FULL, bool XM = false, typename NbFn>
 __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn nb, ContourOut<T>* co = nullptr) {
     const int lane = threadIdx.x & 31;
     PairGeom<T> g = g0;
@@ -385,6 +391,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
     res.unsure = false;
     res.overflow = false;
     res.area = res.arc = res.sa_a = res.sa_b = res.pv_a = res.pv_b = 0.0;
+    res.xm[0] = res.xm[1] = res.xm[2] = 0.0;
     res.central = false;
     res.site = -1;
 
@@ -813,6 +820,25 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
         } else {
             res.pv_a = (double)(norm(g.ic.c - g.A.c) * area / (T)3 * sign_a);
             res.pv_b = (double)(norm(g.ic.c - g.B.c) * area / (T)3 * sign_b);
+        }
+        if (XM && g.want_xm) {
+            // integral of (x - a) over the arcs: an arc of angle t from e1 (unit, from the
+            // circle centre) around the axis contributes (q - a) rho t + rho^2 (sin t e1 +
+            // (1 - cos t) axis x e1), with cos t = e1.e2, sin t = e2.(axis x e1)
+            const double rho = (double)g.ic.r;
+            const V3<double> qa = wide3(g.ic.c - g.A.c);
+            V3<double> xk = mk<double>(0, 0, 0);
+            if (!init) {
+                if (lane == 0) xk = qa * (kTau * rho);
+            } else if (on && q.ang > (T)0 && rho > 0.0) {
+                const V3<double> qc = wide3(g.ic.c);
+                const V3<double> e1 = (wide3(q.p) - qc) / rho, e2 = (wide3(p2.p) - qc) / rho;
+                const V3<double> f = cross(wide3(g.axis), e1);
+                xk = qa * (rho * (double)q.ang) + (e1 * dot(e2, f) + f * (1.0 - dot(e2, e1))) * (rho * rho);
+            }
+            res.xm[0] = wsum(xk.x);
+            res.xm[1] = wsum(xk.y);
+            res.xm[2] = wsum(xk.z);
         }
     }
     res.unsure = __any_sync(kFull, d.unsure);

@@ -26,8 +26,8 @@ constexpr int kWarps = VT_C32_WARPS;
 __device__ unsigned long long g_debug_sites[32];
 #endif
 
-template <bool FULL>
-__global__ void __launch_bounds__(kWarps * 32, VT_C32_MINB) k_contact32(DevBufs b, uint32_t P, float band) {
+template <bool FULL, bool XM>
+__global__ void __launch_bounds__(kWarps * 32, XM ? 6 : VT_C32_MINB) k_contact32(DevBufs b, uint32_t P, float band) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (uint32_t p = blockIdx.x * kWarps + w; p < P; p += gridDim.x * kWarps) {
         const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
@@ -41,6 +41,7 @@ __global__ void __launch_bounds__(kWarps * 32, VT_C32_MINB) k_contact32(DevBufs 
         g.b_id = b.nb_id[eb];
         g.S = Ra + rb.w;
         g.e0 = band * g.S;
+        g.want_xm = b.p_arcm != nullptr;
         const float4* rel = b.nb_rel + off;
         const uint32_t* nid = b.nb_id + off;
         auto nbf = [&](int e) {
@@ -50,7 +51,7 @@ __global__ void __launch_bounds__(kWarps * 32, VT_C32_MINB) k_contact32(DevBufs 
             r.id = nid[e];
             return r;
         };
-        WarpContact r = contact_warp<float, true, FULL>(g, (int)cnt, (int)(eb - off), nbf);
+        WarpContact r = contact_warp<float, true, FULL, XM>(g, (int)cnt, (int)(eb - off), nbf);
 #ifdef VT_DEBUG_SITES
         if (lane == 0 && r.unsure) atomicAdd(&g_debug_sites[r.site < 0 ? 31 : r.site], 1ull);
 #endif
@@ -64,6 +65,8 @@ __global__ void __launch_bounds__(kWarps * 32, VT_C32_MINB) k_contact32(DevBufs 
             b.p_sa_b[p] = r.valid ? r.sa_b : 0.0;
             b.p_pv_a[p] = r.valid ? r.pv_a : 0.0;
             b.p_pv_b[p] = r.valid ? r.pv_b : 0.0;
+            if (XM && b.p_arcm)
+                for (int k = 0; k < 3; ++k) b.p_arcm[3 * (size_t)p + k] = r.valid ? r.xm[k] : 0.0;
         }
     }
 }
@@ -163,10 +166,12 @@ void launch_contact_f32(const DevBufs& b, uint32_t P, int full, cudaStream_t s) 
     size_t g = (P + kWarps - 1) / kWarps;
     if (g < 1) g = 1;
     if (g > 148 * 64) g = 148 * 64;
-    if (full)
-        k_contact32<true><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band);
+    if (full && b.p_arcm)  // the updateable tessellation records arc moments
+        k_contact32<true, true><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band);
+    else if (full)
+        k_contact32<true, false><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band);
     else
-        k_contact32<false><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band);
+        k_contact32<false, false><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band);
     count_launch();
 }
 

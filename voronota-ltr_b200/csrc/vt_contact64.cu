@@ -25,6 +25,8 @@ __device__ __forceinline__ void write_pair(const DevBufs& b, uint32_t p, const W
     b.p_sa_b[p] = r.valid ? r.sa_b : 0.0;
     b.p_pv_a[p] = r.valid ? r.pv_a : 0.0;
     b.p_pv_b[p] = r.valid ? r.pv_b : 0.0;
+    if (b.p_arcm)
+        for (int k = 0; k < 3; ++k) b.p_arcm[3 * (size_t)p + k] = r.valid ? r.xm[k] : 0.0;
 }
 
 template <bool FULL>
@@ -42,6 +44,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_contact64(DevBufs b, uint32_t P
         g.b_id = b.nb_id[eb];
         g.e0 = 0.0;
         g.S = g.A.r + g.B.r;
+        g.want_xm = b.p_arcm != nullptr;
         const double4* sph = b.sph;
         const uint32_t* nslot = b.nb_slot + off;
         const uint32_t* nid = b.nb_id + off;
@@ -51,7 +54,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_contact64(DevBufs b, uint32_t P
             r.id = nid[e];
             return r;
         };
-        WarpContact r = contact_warp<double, false, FULL>(g, (int)cnt, (int)(eb - off), nbf);
+        WarpContact r = contact_warp<double, false, FULL, true>(g, (int)cnt, (int)(eb - off), nbf);
         if (lane == 0) write_pair(b, p, r, r.overflow ? kOverflow : 0);
     }
 }
@@ -374,6 +377,24 @@ __global__ void k_contact_serial(DevBufs b, int full) {
         r.arc = sum_arc * ic.r;
         r.central = r.valid ? serial_central(ic.c, c, bary) : false;
         r.sa_a = r.sa_b = r.pv_a = r.pv_b = 0.0;
+        r.xm[0] = r.xm[1] = r.xm[2] = 0.0;
+        if (r.valid && full && b.p_arcm) {  // first moment of the arcs about a
+            const V3<double> pa = sph_of(b.sph[b.pair_a[p]]).c;
+            V3<double> X = mk<double>(0, 0, 0);
+            if (c.n == 0) {
+                X = (ic.c - pa) * (kTau * ic.r);
+            } else {
+                for (int k = 0; k < c.n; ++k) {
+                    if (!(c.v[k].ang > 0.0)) continue;
+                    const V3<double> e1 = (P3(c.v[k]) - ic.c) / ic.r, e2 = (P3(c.v[(k + 1) % c.n]) - ic.c) / ic.r;
+                    const V3<double> f = cross(axis, e1);
+                    X = X + (ic.c - pa) * (ic.r * c.v[k].ang) + (e1 * dot(e2, f) + f * (1.0 - dot(e2, e1))) * (ic.r * ic.r);
+                }
+            }
+            r.xm[0] = X.x;
+            r.xm[1] = X.y;
+            r.xm[2] = X.z;
+        }
         if (r.valid && full) {
             const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
             const Sph<double> A = sph_of(b.sph[a]);

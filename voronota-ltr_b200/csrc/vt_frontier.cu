@@ -200,8 +200,9 @@ __global__ void k_new_contacts(uint32_t P, const uint32_t* __restrict__ keep_off
         // ensure_ids_ordered on the raw ids is a no-op (a < b or b an image); then ids % n
         // and ensure_ids_ordered again (types.rs:408-414)
         uint32_t ia = b.pair_a[p] % n, ib = b.nb_id[b.pair_e[p]] % n;
+        const bool swap = ia > ib;
         double sa = b.p_sa_a[p], sb = b.p_sa_b[p], pa = b.p_pv_a[p], pb = b.p_pv_b[p];
-        if (ia > ib) {
+        if (swap) {
             uint32_t t = ia;
             ia = ib;
             ib = t;
@@ -222,6 +223,34 @@ __global__ void k_new_contacts(uint32_t P, const uint32_t* __restrict__ keep_off
         nc.pv_b[k] = pb;
         nc.central[k] = b.p_central[p];
         nc.pair[k] = p;
+        if (nc.gaa && b.p_arcm) {
+            // the SAS adjoint through this contact's arcs: with X the arcs' first moment
+            // about a, L their length, s = 1 / (D rho) and c = (Ra^2 + Rb^2 - D^2) / 2,
+            //   dSAS_a/dp_a = Ra s (X - (b-a) L),  dSAS_a/dR_a = L c s,  dSAS_a/dR_b = -Ra Rb L s
+            // (and a <-> b), dSAS_a/dp_b = -dSAS_a/dp_a
+            const double4 A4 = b.sph[b.pair_a[p]], B4 = b.sph[b.nb_slot[b.pair_e[p]]];
+            const V3<double> dab = mk<double>(B4.x - A4.x, B4.y - A4.y, B4.z - A4.z);
+            const double Ra = A4.w, Rb = B4.w, D2 = dot(dab, dab), D = sqrt(D2);
+            const double L = b.p_arc[p];
+            const V3<double> Xa = mk<double>(b.p_arcm[3 * (size_t)p], b.p_arcm[3 * (size_t)p + 1],
+                                             b.p_arcm[3 * (size_t)p + 2]);
+            double4 aa = make_double4(0, 0, 0, 0), ab = aa, ba = aa, bb = aa;
+            const double da = D > 0.0 ? (D2 + Ra * Ra - Rb * Rb) / (2.0 * D) : 0.0;
+            const double rho = sqrt(fmax(Ra * Ra - da * da, 0.0));
+            if (L > 0.0 && rho > 0.0 && D > 0.0) {
+                const double s = 1.0 / (D * rho), c = 0.5 * (Ra * Ra + Rb * Rb - D2);
+                const V3<double> Xb = Xa - dab * L;
+                const V3<double> ga = Xb * (Ra * s), gb = Xa * (Rb * s);
+                aa = make_double4(ga.x, ga.y, ga.z, L * c * s);
+                ab = make_double4(-ga.x, -ga.y, -ga.z, -Ra * Rb * L * s);
+                bb = make_double4(gb.x, gb.y, gb.z, L * c * s);
+                ba = make_double4(-gb.x, -gb.y, -gb.z, -Rb * Ra * L * s);
+            }
+            nc.gaa[k] = swap ? bb : aa;
+            nc.gab[k] = swap ? ba : ab;
+            nc.gba[k] = swap ? ab : ba;
+            nc.gbb[k] = swap ? aa : bb;
+        }
     }
 }
 
@@ -264,6 +293,10 @@ __device__ __forceinline__ void copy_entry(const TableRef& o, uint32_t q, const 
     w.sa[d] = o.sa[q];
     w.pv[d] = o.pv[q];
     w.flags[d] = o.flags[q];
+    if (w.gA) {
+        w.gA[d] = o.gA[q];
+        w.gB[d] = o.gB[q];
+    }
 }
 __global__ void __launch_bounds__(kWarps * 32)
     k_table_copy_kept(uint32_t n, const uint32_t* __restrict__ mark, TableRef o, TableRef w) {
@@ -330,6 +363,10 @@ __global__ void __launch_bounds__(kWarps * 32)
             w.sa[d] = own_a ? nc.sa_a[k] : nc.sa_b[k];
             w.pv[d] = own_a ? nc.pv_a[k] : nc.pv_b[k];
             w.flags[d] = (uint8_t)((nc.central[k] ? 1u : 0u) | (own_a ? 2u : 0u));
+            if (w.gA) {
+                w.gA[d] = own_a ? nc.gaa[k] : nc.gbb[k];
+                w.gB[d] = own_a ? nc.gba[k] : nc.gab[k];
+            }
         }
         __syncwarp();
     }
@@ -384,6 +421,40 @@ __global__ void k_redo_unsure(NewContacts nc, const uint32_t* __restrict__ nc_co
     const uint32_t m = *nc_count;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
         if (unsure[nc.a[k]] || unsure[nc.b[k]]) redo_list[atomicAdd(d_redo_count, 1u)] = nc.pair[k];
+}
+__device__ __forceinline__ double sas_weight(const double* w, const uint8_t* cell_flag, const double* cell_sas,
+                                             uint32_t i) {
+    return (cell_flag[i] && cell_sas[i] > 0.0) ? (w ? w[i] : 1.0) : 0.0;
+}
+__global__ void __launch_bounds__(kWarps * 32)
+    k_table_grad(uint32_t n, TableRef T, const double* __restrict__ w, const uint8_t* __restrict__ cell_flag,
+                 const double* __restrict__ cell_sas, const double4* __restrict__ sph, double* __restrict__ grad) {
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    for (uint32_t i = blockIdx.x * kWarps + wp; i < n; i += gridDim.x * kWarps) {
+        const double wi = sas_weight(w, cell_flag, cell_sas, i);
+        double gx = 0, gy = 0, gz = 0, gr = 0;
+        for (uint32_t q = T.off[i] + lane; q < T.off[i + 1]; q += 32) {
+            const uint32_t other = T.a[q] == i ? T.b[q] : T.a[q];
+            const double wo = sas_weight(w, cell_flag, cell_sas, other);
+            const double4 A = T.gA[q], B = T.gB[q];
+            gx += wi * A.x + wo * B.x;
+            gy += wi * A.y + wo * B.y;
+            gz += wi * A.z + wo * B.z;
+            gr += wi * A.w + wo * B.w;
+        }
+        gx = wsum(gx);
+        gy = wsum(gy);
+        gz = wsum(gz);
+        gr = wsum(gr);
+        if (lane == 0) {
+            // radius scaling of the exposed area: dSAS/dR = 2 SAS / R at fixed directions
+            if (wi != 0.0) gr += wi * 2.0 * cell_sas[i] / sph[i].w;
+            grad[4 * (size_t)i] = gx;
+            grad[4 * (size_t)i + 1] = gy;
+            grad[4 * (size_t)i + 2] = gz;
+            grad[4 * (size_t)i + 3] = gr;
+        }
+    }
 }
 __global__ void k_owner_flags(const uint8_t* __restrict__ flags, uint32_t M, uint32_t* __restrict__ out) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x)
@@ -522,6 +593,10 @@ void launch_table_cells(const uint32_t* list, const uint32_t* count, uint32_t ma
 void launch_redo_unsure(const NewContacts& nc, const uint32_t* nc_count, uint32_t max_nc, const uint8_t* unsure,
                         uint32_t* redo_list, uint32_t* d_redo_count, cudaStream_t s) {
     k_redo_unsure<<<gb(max_nc), kBlock, 0, s>>>(nc, nc_count, unsure, redo_list, d_redo_count); count_launch();
+}
+void launch_table_grad(uint32_t n, TableRef tab, const double* w, const uint8_t* cell_flag, const double* cell_sas,
+                       const double4* sph, double* grad, cudaStream_t s) {
+    k_table_grad<<<gw(n), kWarps * 32, 0, s>>>(n, tab, w, cell_flag, cell_sas, sph, grad); count_launch();
 }
 void launch_owner_flags(const uint8_t* flags, uint32_t M, uint32_t* out, cudaStream_t s) {
     k_owner_flags<<<gb(M), kBlock, 0, s>>>(flags, M, out); count_launch();

@@ -38,6 +38,10 @@ struct TableRef {
     double* sa;
     double* pv;
     uint8_t* flags;
+    // optional: SAS adjoint coefficients of the entry (x, y, z, r): gA = dSAS_owner /
+    // d(owner), gB = dSAS_other / d(owner)
+    double4* gA;
+    double4* gB;
 };
 
 // Contacts computed by one pass, deduplicated and canonicalised, in the reference's
@@ -53,6 +57,11 @@ struct NewContacts {
     double* pv_b;
     uint8_t* central;
     uint32_t* pair;
+    // optional: SAS adjoint coefficients, dSAS_x / d(y) for x, y in {a, b}
+    double4* gaa;
+    double4* gab;
+    double4* gba;
+    double4* gbb;
 };
 
 // Every periodic image at id (g+1) n + j (populate_periodic_spheres, types.rs:351-375).
@@ -130,6 +139,10 @@ void launch_table_cells(const uint32_t* list, const uint32_t* count, uint32_t ma
 // Appends to redo_list the pair of every new contact with an unsure end.
 void launch_redo_unsure(const NewContacts& nc, const uint32_t* nc_count, uint32_t max_nc, const uint8_t* unsure,
                         uint32_t* redo_list, uint32_t* d_redo_count, cudaStream_t s);
+// grad (n x 4, overwritten) = d(sum_i w_i SAS_i)/d(x, y, z, r) from the table's adjoint
+// coefficients (w == null: all 1; balls without a cell or with zero SAS weigh 0).
+void launch_table_grad(uint32_t n, TableRef tab, const double* w, const uint8_t* cell_flag, const double* cell_sas,
+                       const double4* sph, double* grad, cudaStream_t s);
 // Summary (updateable.rs:332-378): entries owned by their id a, in table order.
 void launch_owner_flags(const uint8_t* flags, uint32_t M, uint32_t* out, cudaStream_t s);
 void launch_summary_contacts(TableRef tab, uint32_t M, const uint32_t* off, uint32_t* a, uint32_t* b, double* area,

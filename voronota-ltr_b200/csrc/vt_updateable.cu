@@ -66,9 +66,12 @@ struct Table {
     DBuf<uint32_t> off, a, b;
     DBuf<double> area, arc, sa, pv;
     DBuf<uint8_t> flags;
+    DBuf<double4> gA, gB;  // SAS adjoint coefficients per entry
     uint64_t M = 0;
-    TableRef ref() const { return {off.p, a.p, b.p, area.p, arc.p, sa.p, pv.p, flags.p}; }
+    TableRef ref() const { return {off.p, a.p, b.p, area.p, arc.p, sa.p, pv.p, flags.p, gA.p, gB.p}; }
     void ensure(size_t n, size_t m) {
+        gA.ensure(m);
+        gB.ensure(m);
         off.ensure(n + 1);
         a.ensure(m);
         b.ensure(m);
@@ -87,6 +90,8 @@ struct Table {
         sa.swap(o.sa);
         pv.swap(o.pv);
         flags.swap(o.flags);
+        gA.swap(o.gA);
+        gB.swap(o.gB);
         std::swap(M, o.M);
     }
 };
@@ -134,6 +139,8 @@ void copy_state(UState& d, const UState& s, bool fp32, cudaStream_t st) {
     d.tab.sa.copy_from(s.tab.sa, s.tab.M, st);
     d.tab.pv.copy_from(s.tab.pv, s.tab.M, st);
     d.tab.flags.copy_from(s.tab.flags, s.tab.M, st);
+    d.tab.gA.copy_from(s.tab.gA, s.tab.M, st);
+    d.tab.gB.copy_from(s.tab.gB, s.tab.M, st);
     d.tab.M = s.tab.M;
     d.cell_flag.copy_from(s.cell_flag, n, st);
     d.cell_sas.copy_from(s.cell_sas, n, st);
@@ -190,6 +197,8 @@ struct vt_updateable {
     DBuf<uint32_t> nc_a, nc_b, nc_pair;
     DBuf<double> nc_area, nc_arc, nc_sa_a, nc_sa_b, nc_pv_a, nc_pv_b;
     DBuf<uint8_t> nc_central;
+    DBuf<double4> nc_gaa, nc_gab, nc_gba, nc_gbb;
+    DBuf<double> p_arcm;
     Table next_tab;
     DBuf<uint32_t> keep_cnt, new_cnt, tot_cnt, cursor, tmp_k;
     DBuf<uint32_t> cell_redo;
@@ -422,6 +431,8 @@ struct vt_updateable {
         b.p_sa_b = p_sa_b.p;
         b.p_pv_a = p_pv_a.p;
         b.p_pv_b = p_pv_b.p;
+        p_arcm.ensure(3 * (size_t)P + 3);
+        b.p_arcm = p_arcm.p;
         b.redo_list = redo_list.p;
         b.serial_list = serial_list.p;
         b.serial_scratch = serial_scratch.p;
@@ -451,8 +462,8 @@ struct vt_updateable {
     }
 
     NewContacts nc_ref() {
-        return {nc_a.p, nc_b.p, nc_area.p, nc_arc.p, nc_sa_a.p, nc_sa_b.p, nc_pv_a.p, nc_pv_b.p, nc_central.p,
-                nc_pair.p};
+        return {nc_a.p,    nc_b.p,      nc_area.p,  nc_arc.p,   nc_sa_a.p,  nc_sa_b.p, nc_pv_a.p,
+                nc_pv_b.p, nc_central.p, nc_pair.p, nc_gaa.p, nc_gab.p, nc_gba.p, nc_gbb.p};
     }
 
     // kept contacts of this pass (periodic dedup) as canonical new contacts; the count is
@@ -470,6 +481,10 @@ struct vt_updateable {
         nc_pv_a.ensure(P + 1);
         nc_pv_b.ensure(P + 1);
         nc_central.ensure(P + 1);
+        nc_gaa.ensure(P + 1);
+        nc_gab.ensure(P + 1);
+        nc_gba.ensure(P + 1);
+        nc_gbb.ensure(P + 1);
         if (P == 0) {
             zero(keep_off.p, 4);
             return;
@@ -861,8 +876,8 @@ struct vt_updateable {
         return VT_OK;
     }
 
-    // adjoint of sum_i w_i SAS_i over the current state (w == null: every w_i = 1)
-    DBuf<double> ones, w_eff;
+    // adjoint of sum_i w_i SAS_i over the current state (w == null: every w_i = 1), a
+    // gather over the table's per-entry coefficients (no contour is recomputed)
     int grad_sas(const double* d_w, double* d_grad) {
         UState& S = *cur;
         const uint32_t n = S.n;
@@ -871,31 +886,9 @@ struct vt_updateable {
             int st = build_spheres(S);
             if (st != VT_OK) return st;
         }
-        const uint32_t P = gen_pairs(S, nullptr, nullptr, n, nullptr);
-        DevBufs b = pair_bufs(S, P);
-        keep_off.ensure(P + 2);
-        zero(keep_off.p, 4 * ((size_t)P + 2));
-        b.keep_off = keep_off.p;
-        // validity is decided by the adjoint's own recomputation
-        VT_CUDA(cudaMemsetAsync(p_status.p, kValid, P, stream));
-        if (!d_w) {
-            if (ones.cap < n) {
-                ones.ensure(n);
-                std::vector<double> h1(ones.cap, 1.0);
-                VT_CUDA(cudaMemcpy(ones.p, h1.data(), 8 * ones.cap, cudaMemcpyHostToDevice));
-            }
-            d_w = ones.p;
-        }
-        w_eff.ensure(n);
-        zero(w(kWErr), 4);
-        launch_adjoint(b, P, d_w, nullptr, w_eff.p, d_grad, stream);
-        const uint32_t err = read_word(w(kWErr));
+        launch_table_grad(n, S.tab.ref(), d_w, S.cell_flag.p, S.cell_sas.p, sph.p, d_grad, stream);
+        sync();
         VT_CUDA(cudaGetLastError());
-        stats.num_pairs = P;
-        if (err & 32u) {
-            set_last_error("a contact whose contour has more than 32 points is not differentiated");
-            return VT_ERR_CAPACITY;
-        }
         return VT_OK;
     }
 
