@@ -310,6 +310,8 @@ def batched_leg(args, rank, torch, V, R):
     eng = V.Engine()
     eng.set_stream(stream.cuda_stream)
 
+    tuning = eng.autotune_device(d.data_ptr(), len(balls), PROBE, precision="fp32", offsets=off)
+
     def timed(precision, reps, warm):
         for _ in range(warm):
             eng.compute_batch_device(d.data_ptr(), off, PROBE, precision)
@@ -332,7 +334,7 @@ def batched_leg(args, rank, torch, V, R):
            "balls": int(len(balls)), "ms_fp32": t32,
            "balls_per_s_fp32": replica_throughput(len(balls), R.world, t32),
            "ms_fp64": t64, "balls_per_s_fp64": replica_throughput(len(balls), R.world, t64),
-           "speedup_vs_fp64": t64 / t32, "max_over_ranks": R.world,
+           "speedup_vs_fp64": t64 / t32, "max_over_ranks": R.world, "autotuned": tuning,
            "pairs": int(st.num_pairs), "fp64_redo_pairs": int(st.num_fp64_redo)}
     if rank == 0 and not args.no_cpu:
         import oracle as O
@@ -508,6 +510,7 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
     eng = V.Engine(local)
     eng.set_stream(stream.cuda_stream)
+    tuning = eng.autotune_device(d_xyzr.data_ptr(), args.n, PROBE, precision="fp32")  # untimed set-up
     eng.set_timing(True)
 
     def device_leg(precision, steps, warmup, sample_clocks):
@@ -605,6 +608,7 @@ def run_ours(args):
             "stages_ms_fp32": {k: round(v, 4) for k, v in fp32["stages"].items()},
             "stages_ms_fp64": {k: round(v, 4) for k, v in fp64["stages"].items()} if fp64 else None,
             "wall_s_timed_region": fp32["wall_s"],
+            "autotuned": tuning,
             "updateable": upd,
             "batched": bat,
             "differentiation": grd,

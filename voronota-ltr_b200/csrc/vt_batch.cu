@@ -63,7 +63,7 @@ __global__ void k_struct_bbox(const double4* __restrict__ sph, const uint32_t* _
 // plan_grid per structure: cell edge = max(2 max R + 0.25, 1), coarsened so that the
 // structure's grid has at most 8 n_s + 4096 cells
 __global__ void k_struct_grid(const BBox* __restrict__ bb, const uint32_t* __restrict__ off, uint32_t S,
-                              GridDev* __restrict__ grids, uint32_t* __restrict__ ncell) {
+                              double cell_scale, GridDev* __restrict__ grids, uint32_t* __restrict__ ncell) {
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
         const uint32_t ns = off[s + 1] - off[s];
         GridDev g{};
@@ -78,7 +78,7 @@ __global__ void k_struct_grid(const BBox* __restrict__ bb, const uint32_t* __res
         const double reach = fmax(2.0 * b.max_r + 0.25, 1.0);
         double ext[3];
         for (int k = 0; k < 3; ++k) ext[k] = (b.mx[k] - b.mn[k]) + 2.0 * reach;
-        double cell = reach;
+        double cell = reach * cell_scale;
         int d[3];
         for (int k = 0; k < 3; ++k) d[k] = (int)floor(ext[k] / cell) + 1;
         double vol = (double)d[0] * d[1] * d[2];
@@ -191,11 +191,12 @@ int gb(size_t n) { return grid_blocks(n, kBlock, 148 * 16); }
 }  // namespace
 
 void launch_batch_grid_setup(const uint32_t* off, uint32_t S, uint32_t N, const double4* sph, uint32_t* ball_struct,
-                             BBox* bboxes, GridDev* grids, uint32_t* ncell, cudaStream_t s) {
+                             BBox* bboxes, GridDev* grids, uint32_t* ncell, double cell_scale, cudaStream_t s) {
     const int sb = (int)(S < 148u * 8u ? S : 148u * 8u);
     k_ball_struct<<<sb > 0 ? sb : 1, kBlock, 0, s>>>(off, S, ball_struct); count_launch();
     k_struct_bbox<<<sb > 0 ? sb : 1, kBlock, 0, s>>>(sph, off, S, bboxes); count_launch();
-    k_struct_grid<<<gb(S), kBlock, 0, s>>>(bboxes, off, S, grids, ncell); count_launch();
+    k_struct_grid<<<gb(S), kBlock, 0, s>>>(bboxes, off, S, cell_scale > 1.0 ? cell_scale : 1.0, grids, ncell);
+    count_launch();
     (void)N;
 }
 void launch_batch_grid(const DevBufs& b, uint32_t N, uint32_t total_cells, uint32_t* scan_tmp, cudaStream_t s) {

@@ -17,7 +17,7 @@ namespace vt {
 
 // ball_struct, per-structure bounding boxes, grids and cell counts (ncell u32[S]).
 void launch_batch_grid_setup(const uint32_t* off, uint32_t S, uint32_t N, const double4* sph, uint32_t* ball_struct,
-                             BBox* bboxes, GridDev* grids, uint32_t* ncell, cudaStream_t s);
+                             BBox* bboxes, GridDev* grids, uint32_t* ncell, double cell_scale, cudaStream_t s);
 // Counting sort of the balls into the concatenated grid (b.cell_base filled).
 void launch_batch_grid(const DevBufs& b, uint32_t N, uint32_t total_cells, uint32_t* scan_tmp, cudaStream_t s);
 // Per-structure contact / cell ranges, local ids, per-structure totals (3 doubles per

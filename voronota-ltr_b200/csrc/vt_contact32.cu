@@ -26,10 +26,13 @@ constexpr int kWarps = VT_C32_WARPS;
 __device__ unsigned long long g_debug_sites[32];
 #endif
 
-template <bool FULL, bool XM>
-__global__ void __launch_bounds__(kWarps * 32, XM ? 6 : VT_C32_MINB) k_contact32(DevBufs b, uint32_t P, float band) {
+// W warps per block (chosen by the engine's autotuner); the minimum resident blocks keep
+// the register budget of a thread at 64 (80 with the arc moments) for every W.
+template <bool FULL, bool XM, int W>
+__global__ void __launch_bounds__(W * 32, (XM ? 6 : VT_C32_MINB) * 4 / W)
+    k_contact32(DevBufs b, uint32_t P, float band) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (uint32_t p = blockIdx.x * kWarps + w; p < P; p += gridDim.x * kWarps) {
+    for (uint32_t p = blockIdx.x * W + w; p < P; p += gridDim.x * W) {
         const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
         const uint32_t off = b.nb_off[a], cnt = b.nb_cnt[a];
         PairGeom<float> g;
@@ -162,17 +165,27 @@ void launch_adjoint_f32(const DevBufs& b, uint32_t P, const double* u_contact, c
     count_launch();
 }
 
-void launch_contact_f32(const DevBufs& b, uint32_t P, int full, cudaStream_t s) {
-    size_t g = (P + kWarps - 1) / kWarps;
+template <int W>
+void launch_c32(const DevBufs& b, uint32_t P, int full, cudaStream_t s) {
+    size_t g = (P + W - 1) / W;
     if (g < 1) g = 1;
-    if (g > 148 * 64) g = 148 * 64;
+    if (g > (size_t)148 * 16 * 32 / W) g = (size_t)148 * 16 * 32 / W;
     if (full && b.p_arcm)  // the updateable tessellation records arc moments
-        k_contact32<true, true><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band);
+        k_contact32<true, true, W><<<(unsigned)g, W * 32, 0, s>>>(b, P, b.fp32_band);
     else if (full)
-        k_contact32<true, false><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band);
+        k_contact32<true, false, W><<<(unsigned)g, W * 32, 0, s>>>(b, P, b.fp32_band);
     else
-        k_contact32<false, false><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band);
+        k_contact32<false, false, W><<<(unsigned)g, W * 32, 0, s>>>(b, P, b.fp32_band);
     count_launch();
+}
+
+void launch_contact_f32(const DevBufs& b, uint32_t P, int full, cudaStream_t s) {
+    if (b.c32_warps == 2)
+        launch_c32<2>(b, P, full, s);
+    else if (b.c32_warps == 8)
+        launch_c32<8>(b, P, full, s);
+    else
+        launch_c32<4>(b, P, full, s);
 }
 
 }  // namespace vt

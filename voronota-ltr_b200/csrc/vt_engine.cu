@@ -162,6 +162,9 @@ struct vt_engine {
     std::vector<uint32_t> h_crange, h_mrange;
     std::vector<double> h_btot;
     double fp32_band_ulps = 16.0;  // FP32 point error budget E, in float ulps of the pair scale
+    // launch configuration, set by the autotuner or by hand
+    int c32_warps = 4;        // warps per block of the FP32 contact kernel
+    double cell_scale = 1.0;  // grid cell edge / the minimum edge (2 max R + 0.25)
     // state of the last call
     vt_stats stats{};
     bool contacts_only = false;
@@ -267,6 +270,7 @@ struct vt_engine {
         b.groups = d_groups;
         b.n_groups = d_groups ? n_groups : 0;
         b.fp32_band = (float)(fp32_band_ulps * 1.1920928955078125e-07);
+        b.c32_warps = c32_warps;
 
         sph.ensure(max_slots);
         slot_id.ensure(max_slots);
@@ -322,7 +326,8 @@ struct vt_engine {
             sgrid.ensure(S);
             sncell.ensure(S + 1);
             cell_base.ensure(S + 1);
-            launch_batch_grid_setup(boff.p, (uint32_t)S, n, sph.p, ball_struct.p, sbbox.p, sgrid.p, sncell.p, stream);
+            launch_batch_grid_setup(boff.p, (uint32_t)S, n, sph.p, ball_struct.p, sbbox.p, sgrid.p, sncell.p, cell_scale,
+                                    stream);
             ensure_scan(S + 1);
             scan_u32(sncell.p, cell_base.p, S, scan_tmp.p, stream);
             VT_CUDA(cudaMemcpyAsync(h_words + 12, cell_base.p + S, 4, cudaMemcpyDeviceToHost, stream));
@@ -332,7 +337,7 @@ struct vt_engine {
             b.grids = sgrid.p;
             b.cell_base = cell_base.p;
         } else {
-            b.grid = plan_grid(bb, reach, max_slots, &ncell);
+            b.grid = plan_grid(bb, reach, max_slots, &ncell, cell_scale);
         }
         cell_count.ensure(ncell + 1);
         cell_start.ensure(ncell + 1);
@@ -601,6 +606,59 @@ struct vt_engine {
         return VT_OK;
     }
 
+    // Autotuner: times the candidate launch configurations on this input (CUDA events per
+    // stage) and keeps the fastest -- warps per block of the FP32 contact kernel by its
+    // stage time, then the grid cell scale by the grid + neighbour-search stage times.
+    int autotune(const double* d_in, uint64_t n, double probe, const double* pbox9, int precision,
+                 const uint64_t* batch_off, uint64_t S) {
+        const bool old_timing = timing;
+        timing = true;
+        auto stage_sum = [&](std::initializer_list<int> ks, double* out) -> int {
+            double best = 1e300;
+            for (int rep = 0; rep < 3; ++rep) {
+                int st = run(d_in, n, probe, pbox9, nullptr, 0, precision, 0, batch_off, S);
+                if (st != VT_OK) return st;
+                double t = 0.0;
+                for (int k : ks) t += stage_ms[k];
+                if (rep > 0) best = std::min(best, t);  // the first run warms up
+            }
+            *out = best;
+            return VT_OK;
+        };
+        int st = VT_OK;
+        if (precision == VT_FP32_FIXUP) {
+            int best_w = c32_warps;
+            double best_t = 1e300;
+            for (int wv : {2, 4, 8}) {
+                c32_warps = wv;
+                double t = 0.0;
+                st = stage_sum({5}, &t);
+                if (st != VT_OK) break;
+                if (t < best_t) {
+                    best_t = t;
+                    best_w = wv;
+                }
+            }
+            c32_warps = best_w;
+        }
+        if (st == VT_OK) {
+            double best_s = cell_scale, best_t = 1e300;
+            for (double sc : {1.0, 1.25, 1.5}) {
+                cell_scale = sc;
+                double t = 0.0;
+                st = stage_sum({2, 3, 4}, &t);
+                if (st != VT_OK) break;
+                if (t < best_t) {
+                    best_t = t;
+                    best_s = sc;
+                }
+            }
+            cell_scale = best_s;
+        }
+        timing = old_timing;
+        return st;
+    }
+
     // adjoint of the last full tessellation (device arrays)
     DBuf<double> w_eff, grad_w, grad_u, grad_out;
     int grad_device(const double* d_w, const double* d_u, double* d_grad) {
@@ -803,6 +861,37 @@ int vt_compute_batch(const double* xyzr, const uint64_t* offsets, uint64_t num_s
         if (s2 != VT_OK) return s2;
         return e->download_batch(out);
     });
+}
+int vt_engine_autotune_device(vt_engine* e, const double* d_xyzr, uint64_t n, double probe,
+                              const double* periodic_box9, int precision, const uint64_t* batch_offsets,
+                              uint64_t num_structures) {
+    if (!e || (n && !d_xyzr)) return VT_ERR_INVALID;
+    if (precision != VT_FP64 && precision != VT_FP32_FIXUP) return VT_ERR_INVALID;
+    if (batch_offsets) {
+        int st = validate_batch_offsets(batch_offsets, num_structures);
+        if (st != VT_OK) return st;
+        if (periodic_box9 || batch_offsets[num_structures] != n) {
+            g_last_error = "batched autotuning: no periodic box, offsets[S] must equal n";
+            return VT_ERR_INVALID;
+        }
+    }
+    return guarded([&]() {
+        return e->autotune(d_xyzr, n, probe, periodic_box9, precision, batch_offsets,
+                           batch_offsets ? num_structures : 0);
+    });
+}
+int vt_engine_get_tuning(const vt_engine* e, int* warps, double* cell_scale) {
+    if (!e) return VT_ERR_INVALID;
+    if (warps) *warps = e->c32_warps;
+    if (cell_scale) *cell_scale = e->cell_scale;
+    return VT_OK;
+}
+int vt_engine_set_tuning(vt_engine* e, int warps, double cell_scale) {
+    if (!e || (warps != 2 && warps != 4 && warps != 8) || !(cell_scale >= 1.0) || !(cell_scale <= 4.0))
+        return VT_ERR_INVALID;
+    e->c32_warps = warps;
+    e->cell_scale = cell_scale;
+    return VT_OK;
 }
 int vt_engine_grad_device(vt_engine* e, const double* d_w_sas, const double* d_u_contact, double* d_grad) {
     if (!e || !d_grad) return VT_ERR_INVALID;

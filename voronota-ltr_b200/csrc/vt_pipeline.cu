@@ -771,8 +771,8 @@ void launch_sums3(const double* x0, const uint32_t* cnt0, const double* x1, cons
 }
 int grid_blocks(size_t n, int block, int cap) { return grid_for(n, block, cap); }
 
-GridDev plan_grid(const BBox& bb, double reach, size_t max_slots, uint32_t* ncell) {
-    double ext[3], cell = reach;
+GridDev plan_grid(const BBox& bb, double reach, size_t max_slots, uint32_t* ncell, double cell_scale) {
+    double ext[3], cell = reach * (cell_scale > 1.0 ? cell_scale : 1.0);
     for (int k = 0; k < 3; ++k) ext[k] = (bb.mx[k] - bb.mn[k]) + 2.0 * reach;
     auto dims_for = [&](double c, int* d) {
         for (int k = 0; k < 3; ++k) d[k] = (int)std::floor(ext[k] / c) + 1;

@@ -131,6 +131,7 @@ struct DevBufs {
     const uint32_t* ball_struct;
     const GridDev* grids;
     const uint32_t* cell_base;
+    int c32_warps;  // warps per block of the FP32 contact kernel (2, 4 or 8; 0: 4)
 };
 
 
@@ -236,7 +237,8 @@ int grid_blocks(size_t n, int block, int cap);
 // Cell grid over the bounding box extended by `reach` (cell edge >= reach, so that
 // intersecting balls lie in adjacent cells), coarsened for sparse inputs so that the
 // number of cells stays O(max_slots).
-GridDev plan_grid(const BBox& bb, double reach, size_t max_slots, uint32_t* ncell);
+// cell_scale >= 1 widens the cells (fewer cells, more candidates per ball).
+GridDev plan_grid(const BBox& bb, double reach, size_t max_slots, uint32_t* ncell, double cell_scale = 1.0);
 size_t scan_tmp_words_needed(size_t n);
 void scan_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* tmp, cudaStream_t s);
 

@@ -144,6 +144,10 @@ def library():
     L.vt_batch_free.argtypes = [_vp]
     L.vt_batch_free.restype = None
     L.vt_engine_grad_device.argtypes = [_vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.vt_engine_autotune_device.argtypes = [_vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double, _f64p,
+                                            ctypes.c_int, _u64p, ctypes.c_uint64]
+    L.vt_engine_get_tuning.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
+    L.vt_engine_set_tuning.argtypes = [_vp, ctypes.c_int, ctypes.c_double]
     L.vt_grad.argtypes = [_f64p, ctypes.c_uint64, ctypes.c_double, _f64p, ctypes.c_int, _f64p, _f64p,
                           ctypes.c_uint64, _f64p]
     L.vt_status_string.argtypes = [ctypes.c_int]
@@ -500,6 +504,26 @@ class Engine:
         o = VtDeviceOutputs()
         _check(self._L.vt_engine_device_outputs(self._h, ctypes.byref(o)))
         return o
+
+    def autotune_device(self, d_xyzr_ptr: int, n: int, probe: float, periodic_box=None, precision="fp32",
+                        offsets=None) -> dict:
+        """Time candidate launch configurations on this input and keep the fastest."""
+        pb = None if periodic_box is None else parse_periodic_box(periodic_box)
+        off = None if offsets is None else np.ascontiguousarray(np.asarray(offsets, dtype=np.uint64))
+        _check(self._L.vt_engine_autotune_device(self._h, d_xyzr_ptr, int(n), float(probe),
+                                                 None if pb is None else pb.ctypes.data_as(_f64p),
+                                                 _precision_code(precision),
+                                                 None if off is None else off.ctypes.data_as(_u64p),
+                                                 0 if off is None else len(off) - 1))
+        return self.tuning()
+
+    def tuning(self) -> dict:
+        w, c = ctypes.c_int(), ctypes.c_double()
+        _check(self._L.vt_engine_get_tuning(self._h, ctypes.byref(w), ctypes.byref(c)))
+        return {"warps_per_block": w.value, "cell_scale": c.value}
+
+    def set_tuning(self, warps_per_block: int = 4, cell_scale: float = 1.0):
+        _check(self._L.vt_engine_set_tuning(self._h, int(warps_per_block), float(cell_scale)))
 
     def grad_device(self, d_w_ptr, d_u_ptr, d_grad_ptr: int):
         """Adjoint of the last full tessellation: d_grad (N x 4 doubles on the device) =
