@@ -127,14 +127,16 @@ int vt_engine_stage_times(const vt_engine* e, double* ms);
 
 /* Autotuner (no counterpart in the reference): times candidate launch configurations on
  * this input and keeps the fastest for later calls of the engine -- warps per block of the
- * FP32 contact kernel (2, 4 or 8; one warp per pair) and the grid cell edge as a multiple
- * of the minimum edge 2 max R + 0.25 (1, 1.25 or 1.5; results do not depend on it).
+ * FP32 contact kernel (2, 4 or 8; one warp per pair), its launch form (grid-stride, or
+ * persistent with warps taking chunks of 4 or 16 pairs from a work counter; chunk 0 is
+ * grid-stride) and the grid cell edge as a multiple of the minimum edge 2 max R + 0.25
+ * (1, 1.25 or 1.5).  Results do not depend on any of them.
  * batch_offsets: NULL for one structure, else as vt_engine_compute_batch_device. */
 int vt_engine_autotune_device(vt_engine* e, const double* d_xyzr, uint64_t n, double probe,
                               const double* periodic_box9, int precision, const uint64_t* batch_offsets,
                               uint64_t num_structures);
-int vt_engine_get_tuning(const vt_engine* e, int* warps, double* cell_scale);
-int vt_engine_set_tuning(vt_engine* e, int warps, double cell_scale);
+int vt_engine_get_tuning(const vt_engine* e, int* warps, double* cell_scale, int* chunk);
+int vt_engine_set_tuning(vt_engine* e, int warps, double cell_scale, int chunk);
 
 typedef struct vt_device_outputs {
     const uint32_t* id_a;

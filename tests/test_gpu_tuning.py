@@ -1,7 +1,7 @@
 """The autotuner's launch configurations change speed, never results.
 
-Warps per block of the FP32 contact kernel (2, 4, 8) and the grid cell scale (1, 1.25,
-1.5) are swept on one structure (single and periodic) and on a batch: every configuration
+Warps per block of the FP32 contact kernel (2, 4, 8), its persistent work-queue launch
+(chunks of 4 or 16 pairs) and the grid cell scale (1, 1.25, 1.5) are swept on one structure (single and periodic) and on a batch: every configuration
 gives bit-identical contacts and cells.  The autotuner then picks one of the candidates.
 """
 import numpy as np
@@ -33,16 +33,16 @@ def test_configurations_give_identical_results(periodic):
     d = torch.from_numpy(balls).cuda()
     torch.cuda.synchronize()
     ref = None
-    for w in (2, 4, 8):
-        for c in (1.0, 1.25, 1.5):
-            e.set_tuning(w, c)
-            assert e.tuning() == {"warps_per_block": w, "cell_scale": c}
-            e.compute_device(d.data_ptr(), len(balls), 1.4, box, precision="fp32")
-            r = e.download()
-            if ref is None:
-                ref = r
-            else:
-                _same(r, ref)
+    configs = [(w, c, 0) for w in (2, 4, 8) for c in (1.0, 1.25, 1.5)] + [(2, 1.0, 4), (8, 1.0, 16)]
+    for w, c, ch in configs:
+        e.set_tuning(w, c, ch)
+        assert e.tuning() == {"warps_per_block": w, "cell_scale": c, "chunk": ch}
+        e.compute_device(d.data_ptr(), len(balls), 1.4, box, precision="fp32")
+        r = e.download()
+        if ref is None:
+            ref = r
+        else:
+            _same(r, ref)
     with pytest.raises(V.VoronotaError):
         e.set_tuning(3, 1.0)
 
@@ -58,7 +58,7 @@ def test_autotune_on_a_batch():
     d = torch.from_numpy(balls).cuda()
     torch.cuda.synchronize()
     t = e.autotune_device(d.data_ptr(), len(balls), 1.4, precision="fp32", offsets=off)
-    assert t["warps_per_block"] in (2, 4, 8) and t["cell_scale"] in (1.0, 1.25, 1.5)
+    assert t["warps_per_block"] in (2, 4, 8) and t["cell_scale"] in (1.0, 1.25, 1.5) and t["chunk"] in (0, 4, 16)
     e.compute_batch_device(d.data_ptr(), off, 1.4, "fp32")
     got = e.download_batch()
     ref = V.compute_batch((balls, off), 1.4, "fp32")

@@ -26,51 +26,75 @@ constexpr int kWarps = VT_C32_WARPS;
 __device__ unsigned long long g_debug_sites[32];
 #endif
 
+// One pair: the FP32 contour and the descriptor, written to the pair's outputs.
+template <bool FULL, bool XM>
+__device__ __forceinline__ void contact_pair32(const DevBufs& b, uint32_t p, float band) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
+    const uint32_t off = b.nb_off[a], cnt = b.nb_cnt[a];
+    PairGeom<float> g;
+    const float Ra = (float)b.sph[a].w;
+    const float4 rb = b.nb_rel[eb];
+    g.A = {{0.f, 0.f, 0.f}, Ra};
+    g.B = {{rb.x, rb.y, rb.z}, rb.w};
+    g.a_id = a;
+    g.b_id = b.nb_id[eb];
+    g.S = Ra + rb.w;
+    g.e0 = band * g.S;
+    g.want_xm = b.p_arcm != nullptr;
+    const float4* rel = b.nb_rel + off;
+    const uint32_t* nid = b.nb_id + off;
+    auto nbf = [&](int e) {
+        Nb<float> r;
+        float4 v = rel[e];
+        r.s = {{v.x, v.y, v.z}, v.w};
+        r.id = nid[e];
+        return r;
+    };
+    WarpContact r = contact_warp<float, true, FULL, XM>(g, (int)cnt, (int)(eb - off), nbf);
+#ifdef VT_DEBUG_SITES
+    if (lane == 0 && r.unsure) atomicAdd(&g_debug_sites[r.site < 0 ? 31 : r.site], 1ull);
+#endif
+    if (lane == 0) {
+        uint8_t st = (r.valid ? kValid : 0) | (r.unsure ? kUnsure : 0) | (r.overflow ? kOverflow : 0);
+        b.p_status[p] = st;
+        b.p_area[p] = r.valid ? r.area : 0.0;
+        b.p_arc[p] = r.valid ? r.arc : 0.0;
+        b.p_central[p] = r.valid && r.central ? 1 : 0;
+        b.p_sa_a[p] = r.valid ? r.sa_a : 0.0;
+        b.p_sa_b[p] = r.valid ? r.sa_b : 0.0;
+        b.p_pv_a[p] = r.valid ? r.pv_a : 0.0;
+        b.p_pv_b[p] = r.valid ? r.pv_b : 0.0;
+        if (XM && b.p_arcm)
+            for (int k = 0; k < 3; ++k) b.p_arcm[3 * (size_t)p + k] = r.valid ? r.xm[k] : 0.0;
+    }
+}
+
 // W warps per block (chosen by the engine's autotuner); the minimum resident blocks keep
 // the register budget of a thread at 64 (80 with the arc moments) for every W.
+// queue == null: a grid-stride loop over the pairs.  Otherwise a persistent launch (one
+// wave of resident blocks) whose warps take chunks of `chunk` consecutive pairs from the
+// work counter *queue (zero at launch), so that costly pairs do not leave a tail of idle
+// SMs.
 template <bool FULL, bool XM, int W>
 __global__ void __launch_bounds__(W * 32, (XM ? 6 : VT_C32_MINB) * 4 / W)
-    k_contact32(DevBufs b, uint32_t P, float band) {
+    k_contact32(DevBufs b, uint32_t P, float band, uint32_t* queue, uint32_t chunk) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (uint32_t p = blockIdx.x * W + w; p < P; p += gridDim.x * W) {
-        const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
-        const uint32_t off = b.nb_off[a], cnt = b.nb_cnt[a];
-        PairGeom<float> g;
-        const float Ra = (float)b.sph[a].w;
-        const float4 rb = b.nb_rel[eb];
-        g.A = {{0.f, 0.f, 0.f}, Ra};
-        g.B = {{rb.x, rb.y, rb.z}, rb.w};
-        g.a_id = a;
-        g.b_id = b.nb_id[eb];
-        g.S = Ra + rb.w;
-        g.e0 = band * g.S;
-        g.want_xm = b.p_arcm != nullptr;
-        const float4* rel = b.nb_rel + off;
-        const uint32_t* nid = b.nb_id + off;
-        auto nbf = [&](int e) {
-            Nb<float> r;
-            float4 v = rel[e];
-            r.s = {{v.x, v.y, v.z}, v.w};
-            r.id = nid[e];
-            return r;
-        };
-        WarpContact r = contact_warp<float, true, FULL, XM>(g, (int)cnt, (int)(eb - off), nbf);
-#ifdef VT_DEBUG_SITES
-        if (lane == 0 && r.unsure) atomicAdd(&g_debug_sites[r.site < 0 ? 31 : r.site], 1ull);
-#endif
-        if (lane == 0) {
-            uint8_t st = (r.valid ? kValid : 0) | (r.unsure ? kUnsure : 0) | (r.overflow ? kOverflow : 0);
-            b.p_status[p] = st;
-            b.p_area[p] = r.valid ? r.area : 0.0;
-            b.p_arc[p] = r.valid ? r.arc : 0.0;
-            b.p_central[p] = r.valid && r.central ? 1 : 0;
-            b.p_sa_a[p] = r.valid ? r.sa_a : 0.0;
-            b.p_sa_b[p] = r.valid ? r.sa_b : 0.0;
-            b.p_pv_a[p] = r.valid ? r.pv_a : 0.0;
-            b.p_pv_b[p] = r.valid ? r.pv_b : 0.0;
-            if (XM && b.p_arcm)
-                for (int k = 0; k < 3; ++k) b.p_arcm[3 * (size_t)p + k] = r.valid ? r.xm[k] : 0.0;
+    // one loop (and one inlined copy of the contour code) for both launch forms
+    uint32_t p = queue ? 0u : blockIdx.x * W + w, end = queue ? 0u : P;
+    const uint32_t step = queue ? 1u : gridDim.x * W;
+    for (;;) {
+        if (p >= end) {
+            if (!queue) break;
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(queue, chunk);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base >= P) break;
+            p = base;
+            end = base + chunk < P ? base + chunk : P;
         }
+        contact_pair32<FULL, XM>(b, p, band);
+        p += step;
     }
 }
 
@@ -165,18 +189,36 @@ void launch_adjoint_f32(const DevBufs& b, uint32_t P, const double* u_contact, c
     count_launch();
 }
 
+template <bool FULL, bool XM, int W>
+void launch_c32_kernel(const DevBufs& b, uint32_t P, cudaStream_t s) {
+    uint32_t* queue = b.c32_chunk > 0 ? b.c32_queue : nullptr;
+    size_t g;
+    if (queue) {
+        static int blocks_per_sm = 0;  // resident blocks of this variant (per process)
+        if (blocks_per_sm == 0)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_contact32<FULL, XM, W>, W * 32, 0);
+        int sms = 148;
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        g = (size_t)sms * (size_t)(blocks_per_sm > 0 ? blocks_per_sm : 1);
+        cudaMemsetAsync(queue, 0, sizeof(uint32_t), s);
+    } else {
+        g = (P + W - 1) / W;
+        if (g > (size_t)148 * 16 * 32 / W) g = (size_t)148 * 16 * 32 / W;
+    }
+    if (g < 1) g = 1;
+    k_contact32<FULL, XM, W><<<(unsigned)g, W * 32, 0, s>>>(b, P, b.fp32_band, queue, (uint32_t)b.c32_chunk);
+    count_launch();
+}
+
 template <int W>
 void launch_c32(const DevBufs& b, uint32_t P, int full, cudaStream_t s) {
-    size_t g = (P + W - 1) / W;
-    if (g < 1) g = 1;
-    if (g > (size_t)148 * 16 * 32 / W) g = (size_t)148 * 16 * 32 / W;
     if (full && b.p_arcm)  // the updateable tessellation records arc moments
-        k_contact32<true, true, W><<<(unsigned)g, W * 32, 0, s>>>(b, P, b.fp32_band);
+        launch_c32_kernel<true, true, W>(b, P, s);
     else if (full)
-        k_contact32<true, false, W><<<(unsigned)g, W * 32, 0, s>>>(b, P, b.fp32_band);
+        launch_c32_kernel<true, false, W>(b, P, s);
     else
-        k_contact32<false, false, W><<<(unsigned)g, W * 32, 0, s>>>(b, P, b.fp32_band);
-    count_launch();
+        launch_c32_kernel<false, false, W>(b, P, s);
 }
 
 void launch_contact_f32(const DevBufs& b, uint32_t P, int full, cudaStream_t s) {

@@ -164,6 +164,7 @@ struct vt_engine {
     double fp32_band_ulps = 16.0;  // FP32 point error budget E, in float ulps of the pair scale
     // launch configuration, set by the autotuner or by hand
     int c32_warps = 4;        // warps per block of the FP32 contact kernel
+    int c32_chunk = 0;        // > 0: persistent FP32 contact launch, pairs taken in chunks
     double cell_scale = 1.0;  // grid cell edge / the minimum edge (2 max R + 0.25)
     // state of the last call
     vt_stats stats{};
@@ -271,6 +272,8 @@ struct vt_engine {
         b.n_groups = d_groups ? n_groups : 0;
         b.fp32_band = (float)(fp32_band_ulps * 1.1920928955078125e-07);
         b.c32_warps = c32_warps;
+        b.c32_chunk = c32_chunk;
+        b.c32_queue = words.p + 14;
 
         sph.ensure(max_slots);
         slot_id.ensure(max_slots);
@@ -615,7 +618,7 @@ struct vt_engine {
         timing = true;
         auto stage_sum = [&](std::initializer_list<int> ks, double* out) -> int {
             double best = 1e300;
-            for (int rep = 0; rep < 3; ++rep) {
+            for (int rep = 0; rep < 2; ++rep) {
                 int st = run(d_in, n, probe, pbox9, nullptr, 0, precision, 0, batch_off, S);
                 if (st != VT_OK) return st;
                 double t = 0.0;
@@ -627,10 +630,13 @@ struct vt_engine {
         };
         int st = VT_OK;
         if (precision == VT_FP32_FIXUP) {
-            int best_w = c32_warps;
+            // warps per block with the grid-stride launch, then the persistent launch's
+            // chunk size at the best width
+            int best_w = c32_warps, best_c = 0;
             double best_t = 1e300;
             for (int wv : {2, 4, 8}) {
                 c32_warps = wv;
+                c32_chunk = 0;
                 double t = 0.0;
                 st = stage_sum({5}, &t);
                 if (st != VT_OK) break;
@@ -640,6 +646,18 @@ struct vt_engine {
                 }
             }
             c32_warps = best_w;
+            for (int ch : {4, 16}) {
+                if (st != VT_OK) break;
+                c32_chunk = ch;
+                double t = 0.0;
+                st = stage_sum({5}, &t);
+                if (st != VT_OK) break;
+                if (t < best_t) {
+                    best_t = t;
+                    best_c = ch;
+                }
+            }
+            c32_chunk = best_c;
         }
         if (st == VT_OK) {
             double best_s = cell_scale, best_t = 1e300;
@@ -880,17 +898,20 @@ int vt_engine_autotune_device(vt_engine* e, const double* d_xyzr, uint64_t n, do
                            batch_offsets ? num_structures : 0);
     });
 }
-int vt_engine_get_tuning(const vt_engine* e, int* warps, double* cell_scale) {
+int vt_engine_get_tuning(const vt_engine* e, int* warps, double* cell_scale, int* chunk) {
     if (!e) return VT_ERR_INVALID;
     if (warps) *warps = e->c32_warps;
     if (cell_scale) *cell_scale = e->cell_scale;
+    if (chunk) *chunk = e->c32_chunk;
     return VT_OK;
 }
-int vt_engine_set_tuning(vt_engine* e, int warps, double cell_scale) {
-    if (!e || (warps != 2 && warps != 4 && warps != 8) || !(cell_scale >= 1.0) || !(cell_scale <= 4.0))
+int vt_engine_set_tuning(vt_engine* e, int warps, double cell_scale, int chunk) {
+    if (!e || (warps != 2 && warps != 4 && warps != 8) || !(cell_scale >= 1.0) || !(cell_scale <= 4.0) ||
+        chunk < 0 || chunk > 256)
         return VT_ERR_INVALID;
     e->c32_warps = warps;
     e->cell_scale = cell_scale;
+    e->c32_chunk = chunk;
     return VT_OK;
 }
 int vt_engine_grad_device(vt_engine* e, const double* d_w_sas, const double* d_u_contact, double* d_grad) {

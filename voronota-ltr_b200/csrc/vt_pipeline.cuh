@@ -132,6 +132,8 @@ struct DevBufs {
     const GridDev* grids;
     const uint32_t* cell_base;
     int c32_warps;  // warps per block of the FP32 contact kernel (2, 4 or 8; 0: 4)
+    int c32_chunk;  // > 0: persistent FP32 contact launch taking chunks of pairs from
+    uint32_t* c32_queue;  // this work counter
 };
 
 

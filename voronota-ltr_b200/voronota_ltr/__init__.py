@@ -146,8 +146,9 @@ def library():
     L.vt_engine_grad_device.argtypes = [_vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.vt_engine_autotune_device.argtypes = [_vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double, _f64p,
                                             ctypes.c_int, _u64p, ctypes.c_uint64]
-    L.vt_engine_get_tuning.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
-    L.vt_engine_set_tuning.argtypes = [_vp, ctypes.c_int, ctypes.c_double]
+    L.vt_engine_get_tuning.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                                       ctypes.POINTER(ctypes.c_int)]
+    L.vt_engine_set_tuning.argtypes = [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int]
     L.vt_grad.argtypes = [_f64p, ctypes.c_uint64, ctypes.c_double, _f64p, ctypes.c_int, _f64p, _f64p,
                           ctypes.c_uint64, _f64p]
     L.vt_status_string.argtypes = [ctypes.c_int]
@@ -518,12 +519,13 @@ class Engine:
         return self.tuning()
 
     def tuning(self) -> dict:
-        w, c = ctypes.c_int(), ctypes.c_double()
-        _check(self._L.vt_engine_get_tuning(self._h, ctypes.byref(w), ctypes.byref(c)))
-        return {"warps_per_block": w.value, "cell_scale": c.value}
+        w, c, ch = ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
+        _check(self._L.vt_engine_get_tuning(self._h, ctypes.byref(w), ctypes.byref(c), ctypes.byref(ch)))
+        return {"warps_per_block": w.value, "cell_scale": c.value, "chunk": ch.value}
 
-    def set_tuning(self, warps_per_block: int = 4, cell_scale: float = 1.0):
-        _check(self._L.vt_engine_set_tuning(self._h, int(warps_per_block), float(cell_scale)))
+    def set_tuning(self, warps_per_block: int = 4, cell_scale: float = 1.0, chunk: int = 0):
+        """chunk > 0: persistent contact launch taking `chunk` pairs per grab."""
+        _check(self._L.vt_engine_set_tuning(self._h, int(warps_per_block), float(cell_scale), int(chunk)))
 
     def grad_device(self, d_w_ptr, d_u_ptr, d_grad_ptr: int):
         """Adjoint of the last full tessellation: d_grad (N x 4 doubles on the device) =
