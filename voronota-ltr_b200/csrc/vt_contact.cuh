@@ -313,40 +313,35 @@ __device__ __forceinline__ double solid_angle(Dec<T, F>& d, const Sph<T>& a, con
         if (on) {
             const T pi = (T)kPi;
             // turn term at point p1: pi - dihedral (FP32: the supplement, in double)
-            auto turn_at = [&](V3<T> x1, V3<T> x2) -> double {
-                if constexpr (F)
-                    return dihedral_supplement(a.c, p1.p, x1, x2);
+            // the two directions of the turn at p1: along the arc's tangent where an arc
+            // ends or starts at p1, else towards the neighbouring points
+            V3<T> x1 = p0.p, x2 = p2.p;
+            const bool arc_in = p0.ang > (T)0, arc_out = !arc_in && p1.ang > (T)0;
+            if (arc_in || arc_out) {
+                const T ang = arc_in ? p0.ang : p1.ang;
+                V3<T> dd = cross(b.c - a.c, p1.p - ic.c);
+                V3<T> w = (arc_in ? p0.p : p2.p) - p1.p;
+                T dv = dot(dd, w);
+                if constexpr (F) {
+                    d.band(ang - pi, arc_in ? ea0 : ea1);
+                    d.band(dv, (T)2 * e0 * (norm(b.c - a.c) * norm(w) + (T)2 * norm(dd)));
+                }
+                bool flip = (ang < pi && dv < (T)0) || (ang > pi && dv > (T)0);
+                if (flip) dd = -dd;
+                if (arc_in)
+                    x1 = p1.p + dd;
                 else
-                    return pi - min_dihedral(a.c, p1.p, x1, x2);
-            };
-            if (p0.ang > (T)0) {
-                V3<T> dd = cross(b.c - a.c, p1.p - ic.c);
-                V3<T> w = p0.p - p1.p;
-                T dv = dot(dd, w);
-                if constexpr (F) {
-                    d.band(p0.ang - pi, ea0);
-                    d.band(dv, (T)2 * e0 * (norm(b.c - a.c) * norm(w) + (T)2 * norm(dd)));
-                }
-                bool flip = (p0.ang < pi && dv < (T)0) || (p0.ang > pi && dv > (T)0);
-                if (flip) dd = -dd;
-                t = turn_at(p1.p + dd, p2.p);
-            } else if (p1.ang > (T)0) {
-                V3<T> dd = cross(b.c - a.c, p1.p - ic.c);
-                V3<T> w = p2.p - p1.p;
-                T dv = dot(dd, w);
-                if constexpr (F) {
-                    d.band(p1.ang - pi, ea1);
-                    d.band(dv, (T)2 * e0 * (norm(b.c - a.c) * norm(w) + (T)2 * norm(dd)));
-                }
-                bool flip = (p1.ang < pi && dv < (T)0) || (p1.ang > pi && dv > (T)0);
-                if (flip) dd = -dd;
-                t = turn_at(p0.p, p1.p + dd);
+                    x2 = p1.p + dd;
+            }
+            if constexpr (F)
+                t = dihedral_supplement(a.c, p1.p, x1, x2);
+            else
+                t = pi - min_dihedral(a.c, p1.p, x1, x2);
+            if (arc_out) {
                 if constexpr (F)
                     t2 = (T)((double)p1.ang * ((double)norm_rn(ic.c - a.c) / (double)a.r));
                 else
                     t2 = p1.ang * (norm(ic.c - a.c) / a.r);
-            } else {
-                t = turn_at(p0.p, p2.p);
             }
         }
         if constexpr (F) {
@@ -806,9 +801,14 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
         Pt<T> p2 = shfl_pt(q, nxl);
         T ea0 = 0;
         if constexpr (F) ea0 = __shfl_sync(kFull, ang_err, pvl);
-        double sa = solid_angle(d, g.A, g.B, g.ic, p0, q, p2, on, len, e0, ea0, ang_err);
-        VT_SITE(12);
-        double sb = solid_angle(d, g.B, g.A, g.ic, p0, q, p2, on, len, e0, ea0, ang_err);
+        // one inlined copy of the solid angle for both sides (a, then b)
+        double sab[2];
+#pragma unroll 1
+        for (int side = 0; side < 2; ++side) {
+            const Sph<T> s0 = side ? g.B : g.A, s1 = side ? g.A : g.B;
+            sab[side] = solid_angle(d, s0, s1, g.ic, p0, q, p2, on, len, e0, ea0, ang_err);
+        }
+        const double sa = sab[0], sb = sab[1];
         VT_SITE(13);
         T sign_a = sa < 0.0 ? (T)-1 : (T)1;
         T sign_b = sb < 0.0 ? (T)-1 : (T)1;
