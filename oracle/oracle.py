@@ -53,6 +53,12 @@ def lib():
     L.vto_get_neighbors.argtypes = [vp, _u64p, _u64p, _f64p]
     L.vto_get_pairs.argtypes = [vp, _u64p, _u64p, _u8p, _f64p, _f64p, _u8p, _f64p, _f64p, _f64p, _f64p]
     L.vto_free.argtypes = [vp]
+    L.vto_set_network.argtypes = [ctypes.c_int]
+    for name in ("vto_num_vertices", "vto_num_edges"):
+        getattr(L, name).argtypes = [vp]
+        getattr(L, name).restype = ctypes.c_uint64
+    L.vto_get_vertices.argtypes = [vp, _u64p, _f64p]
+    L.vto_get_edges.argtypes = [vp, _u64p, _f64p]
     L.vto_upd_create.argtypes = [ctypes.c_int]
     L.vto_upd_create.restype = vp
     L.vto_upd_destroy.argtypes = [vp]
@@ -172,10 +178,17 @@ def set_faithful_grid_update(on: bool) -> None:
     lib().vto_set_faithful_grid_update(1 if on else 0)
 
 
+NET_NULL = np.uint64(0xFFFFFFFFFFFFFFFF)  # NULL_ID of a network element (types.rs:98)
+
+
 def compute(balls, probe: float, periodic_box=None, groups=None, contacts_only: bool = False,
-            internals: bool = False) -> OracleResult:
-    """compute_tessellation / compute_contacts_only on the CPU oracle."""
+            internals: bool = False, with_cell_vertices: bool = False) -> OracleResult:
+    """compute_tessellation / compute_contacts_only on the CPU oracle.  With
+    with_cell_vertices the result also holds the tessellation network: vertex_ids
+    (V, 4) and vertex_xyz (V, 3), edge_ids (E, 3) and edge_length (E,); NULL ids are
+    NET_NULL."""
     L = lib()
+    L.vto_set_network(1 if with_cell_vertices else 0)
     xyzr = np.ascontiguousarray(np.asarray(balls, dtype=np.float64).reshape(-1, 4))
     n = xyzr.shape[0]
     pb = pbox_vectors(periodic_box)
@@ -184,10 +197,20 @@ def compute(balls, probe: float, periodic_box=None, groups=None, contacts_only: 
     rc = L.vto_compute(_p(xyzr, _f64p), n, float(probe), None if pb is None else _p(pb, _f64p),
                        None if g is None else _p(g, _i32p), 0 if g is None else len(g),
                        1 if contacts_only else 0, ctypes.byref(h))
+    L.vto_set_network(0)
     if rc != 0:
         raise RuntimeError(f"oracle failed: {rc}")
     try:
-        return _read_result(L, h, internals)
+        res = _read_result(L, h, internals)
+        if with_cell_vertices:
+            nv, ne = L.vto_num_vertices(h), L.vto_num_edges(h)
+            res.vertex_ids = np.zeros((nv, 4), np.uint64)
+            res.vertex_xyz = np.zeros((nv, 3), np.float64)
+            res.edge_ids = np.zeros((ne, 3), np.uint64)
+            res.edge_length = np.zeros(ne, np.float64)
+            L.vto_get_vertices(h, _p(res.vertex_ids, _u64p), _p(res.vertex_xyz, _f64p))
+            L.vto_get_edges(h, _p(res.edge_ids, _u64p), _p(res.edge_length, _f64p))
+        return res
     finally:
         L.vto_free(h)
 

@@ -826,6 +826,92 @@ static bool contact_summary(const std::vector<Sphere>& sp, uint64_t a_id, uint64
     return true;
 }
 
+// Tessellation network elements (TessellationVertex / TessellationEdge, types.rs:456-570);
+// ids sorted, the NULL id (types.rs:98) is UINT64_MAX.
+struct NetVertex {
+    uint64_t ids[4];
+    double p[3];
+};
+struct NetEdge {
+    uint64_t ids[3];
+    double length;
+};
+
+constexpr uint64_t NET_NULL = UINT64_MAX;  // NULL_ID (types.rs:98)
+
+void sort_ids4(uint64_t* v) {  // TessellationVertex::sort_ids (types.rs:476-494), a sorting network
+    auto cs = [&](int i, int j) {
+        if (v[i] > v[j]) std::swap(v[i], v[j]);
+    };
+    cs(0, 1);
+    cs(2, 3);
+    cs(0, 2);
+    cs(1, 3);
+    cs(1, 2);
+}
+void sort_ids3(uint64_t* v) {  // TessellationEdge::sort_ids (types.rs:543-556)
+    auto cs = [&](int i, int j) {
+        if (v[i] > v[j]) std::swap(v[i], v[j]);
+    };
+    cs(0, 1);
+    cs(1, 2);
+    cs(0, 1);
+}
+
+// to_tessellation_elements (contact.rs:119-177) for a valid clipped contact of (a, b).
+void tessellation_elements(const Clipped& cl, uint64_t a_id, uint64_t b_id, std::vector<NetEdge>& E,
+                           std::vector<NetVertex>& Vs) {
+    if (cl.contour.empty()) {  // an uncut contact: one SAS edge, no vertices
+        NetEdge e{{a_id, b_id, NET_NULL}, cl.sum_arc * cl.ic.r};
+        sort_ids3(e.ids);
+        E.push_back(e);
+        return;
+    }
+    const size_t m = cl.contour.size();
+    for (size_t i = 0; i < m; ++i) {
+        const ContourPoint& cp = cl.contour[i];
+        const ContourPoint& nx = cl.contour[(i + 1) % m];
+        const bool arc = cp.right_id == a_id;
+        NetEdge e{{a_id, b_id, arc ? NET_NULL : cp.right_id}, arc ? cp.angle * cl.ic.r : norm(cp.p - nx.p)};
+        sort_ids3(e.ids);
+        E.push_back(e);
+        NetVertex v{{a_id, b_id, cp.left_id == a_id ? NET_NULL : cp.left_id, arc ? NET_NULL : cp.right_id},
+                    {cp.p.x, cp.p.y, cp.p.z}};
+        sort_ids4(v.ids);
+        Vs.push_back(v);
+    }
+}
+
+// assemble_tessellation_network (tessellation.rs:334-401): ids mod n for periodic images
+// (NULL kept), ids re-sorted, then elements sorted by ids and deduplicated.  The
+// reference sorts unstably, so which of several equal-id elements survives is
+// unspecified; here it is the first in pair and contour order (a stable sort).
+void assemble_network(std::vector<NetEdge>& E, std::vector<NetVertex>& Vs, bool periodic, uint64_t n) {
+    auto canon = [&](uint64_t id) { return (periodic && id != NET_NULL) ? id % n : id; };
+    for (auto& e : E) {
+        for (auto& id : e.ids) id = canon(id);
+        sort_ids3(e.ids);
+    }
+    for (auto& v : Vs) {
+        for (auto& id : v.ids) id = canon(id);
+        sort_ids4(v.ids);
+    }
+    std::stable_sort(E.begin(), E.end(), [](const NetEdge& x, const NetEdge& y) {
+        return std::lexicographical_compare(x.ids, x.ids + 3, y.ids, y.ids + 3);
+    });
+    std::stable_sort(Vs.begin(), Vs.end(), [](const NetVertex& x, const NetVertex& y) {
+        return std::lexicographical_compare(x.ids, x.ids + 4, y.ids, y.ids + 4);
+    });
+    E.erase(std::unique(E.begin(), E.end(),
+                        [](const NetEdge& x, const NetEdge& y) { return std::equal(x.ids, x.ids + 3, y.ids); }),
+            E.end());
+    Vs.erase(std::unique(Vs.begin(), Vs.end(),
+                         [](const NetVertex& x, const NetVertex& y) { return std::equal(x.ids, x.ids + 4, y.ids); }),
+             Vs.end());
+}
+
+bool g_network = false;  // vto_compute also builds the tessellation network
+
 inline bool same_group(const int32_t* g, uint64_t ng, uint64_t a, uint64_t b) {  // tessellation.rs:323-328
     return g && a < ng && b < ng && g[a] == g[b];
 }
@@ -835,6 +921,8 @@ inline bool same_group(const int32_t* g, uint64_t ng, uint64_t a, uint64_t b) { 
 // ---------------------------------------------------------------------------------------
 struct vto_result {
     uint64_t num_balls = 0;
+    std::vector<NetVertex> net_v;
+    std::vector<NetEdge> net_e;
     std::vector<uint64_t> c_a, c_b;
     std::vector<double> c_area, c_arc;
     std::vector<uint8_t> c_central;
@@ -1026,14 +1114,29 @@ int vto_compute(const double* xyzr, uint64_t n, double probe, const double* pbox
     size_t np = ctx.pairs.size();
     std::vector<ContactSummary> sums(np);
     std::vector<uint8_t> ok(np, 0);
+    const bool network = g_network && !contacts_only;
+    std::vector<std::vector<NetEdge>> pe(network ? np : 0);
+    std::vector<std::vector<NetVertex>> pv(network ? np : 0);
     parallel_for((int64_t)np, 256, [&](int64_t k) {
         uint64_t a = ctx.pairs[k].first, b = ctx.pairs[k].second;
         ContactSummary s;
         if (contact_summary(sp, a, b, ctx.all[a], contacts_only != 0, s)) {
             sums[k] = s;
             ok[k] = 1;
+            if (network) {
+                Clipped cl;
+                if (clip_contact(sp, a, b, ctx.all[a], cl)) tessellation_elements(cl, a, b, pe[k], pv[k]);
+            }
         }
     });
+    if (network) {
+        for (size_t k = 0; k < np; ++k)
+            if (ok[k] && sums[k].area > 0.0) {
+                r->net_e.insert(r->net_e.end(), pe[k].begin(), pe[k].end());
+                r->net_v.insert(r->net_v.end(), pv[k].begin(), pv[k].end());
+            }
+        assemble_network(r->net_e, r->net_v, ctx.periodic, n);
+    }
     r->p_a.resize(np);
     r->p_b.resize(np);
     r->p_valid = ok;
@@ -1097,6 +1200,21 @@ int vto_compute(const double* xyzr, uint64_t n, double probe, const double* pbox
     return 0;
 }
 
+void vto_set_network(int on) { g_network = on != 0; }
+uint64_t vto_num_vertices(const vto_result* r) { return r->net_v.size(); }
+uint64_t vto_num_edges(const vto_result* r) { return r->net_e.size(); }
+void vto_get_vertices(const vto_result* r, uint64_t* ids4, double* xyz3) {
+    for (size_t i = 0; i < r->net_v.size(); ++i) {
+        for (int k = 0; k < 4; ++k) ids4[4 * i + k] = r->net_v[i].ids[k];
+        for (int k = 0; k < 3; ++k) xyz3[3 * i + k] = r->net_v[i].p[k];
+    }
+}
+void vto_get_edges(const vto_result* r, uint64_t* ids3, double* length) {
+    for (size_t i = 0; i < r->net_e.size(); ++i) {
+        for (int k = 0; k < 3; ++k) ids3[3 * i + k] = r->net_e[i].ids[k];
+        length[i] = r->net_e[i].length;
+    }
+}
 uint64_t vto_num_balls(const vto_result* r) { return r->num_balls; }
 uint64_t vto_num_contacts(const vto_result* r) { return r->c_a.size(); }
 uint64_t vto_num_cells(const vto_result* r) { return r->cell_index.size(); }

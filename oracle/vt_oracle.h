@@ -57,6 +57,14 @@ void vto_get_pairs(const vto_result* r, uint64_t* a, uint64_t* b, uint8_t* valid
                    double* area, double* arc_length, uint8_t* central,
                    double* solid_a, double* solid_b, double* pyr_a, double* pyr_b);
 void vto_free(vto_result* r);
+/* Tessellation network (with_cell_vertices, contact.rs:119-177, tessellation.rs:334-401):
+ * when on, vto_compute (full tessellation) also builds the deduplicated vertices (4 sorted
+ * ball ids, NULL id = UINT64_MAX, and x, y, z) and edges (3 sorted ids and length). */
+void vto_set_network(int on);
+uint64_t vto_num_vertices(const vto_result* r);
+uint64_t vto_num_edges(const vto_result* r);
+void vto_get_vertices(const vto_result* r, uint64_t* ids4, double* xyz3);
+void vto_get_edges(const vto_result* r, uint64_t* ids3, double* length);
 
 /* UpdateableTessellation (updateable.rs:154-742). */
 vto_upd* vto_upd_create(int with_backup);

@@ -150,3 +150,26 @@ def test_thread_count_does_not_change_results():
     assert np.array_equal(r1.contacts_a, r4.contacts_a)
     assert np.array_equal(r1.contacts_area, r4.contacts_area)
     assert np.array_equal(r1.cells_sas, r4.cells_sas)
+
+
+def test_network_ring17():  # src/tessellation.rs:1347-1387 (C++ example output)
+    r = O.compute(RING_17, 1.0, with_cell_vertices=True)
+    on_sas = int((r.vertex_ids[:, 3] == O.NET_NULL).sum())
+    assert (len(r.vertex_ids), on_sas, len(r.vertex_ids) - on_sas) == (68, 32, 36)
+    assert len(r.edge_ids) > 0
+    # ids sorted within each element, elements sorted and unique
+    assert np.all(np.diff(r.vertex_ids.astype(np.float64), axis=1) >= 0)
+    keys = [tuple(v) for v in r.vertex_ids.tolist()]
+    assert keys == sorted(set(keys))
+
+
+def test_network_cs_1x1():  # src/tessellation.rs:1391-1510
+    r = O.compute(load_balls("cs_1x1"), 2.0, with_cell_vertices=True)
+    assert (len(r.vertex_ids), len(r.edge_ids)) == (65, 215)
+    assert int((r.vertex_ids[:, 3] == O.NET_NULL).sum()) > len(r.vertex_ids) // 2
+
+
+def test_network_full_circle_edge():  # src/tessellation.rs:1329-1344: an uncut contact
+    r = O.compute([(0.0, 0.0, 0.0, 1.5), (2.5, 0.0, 0.0, 1.5)], 0.5, with_cell_vertices=True)
+    assert len(r.vertex_ids) == 0 and len(r.edge_ids) == 1
+    assert r.edge_ids[0, 2] == O.NET_NULL
