@@ -19,7 +19,9 @@ geometry with FP64 recomputation of band pairs.  One step = one full tessellatio
 With torchrun (N > 1) each rank tessellates its own structure (seed = rank): independent
 replicas, no collective on the data path; value = all ranks' balls / max-over-ranks time
 (voronota_ltr.replicas).  The updateable, batched and differentiation legs run on every
-rank on its own inputs and report max-over-ranks times.
+rank on its own inputs and report max-over-ranks times; the network leg times
+compute_tessellation with with_cell_vertices on the main structure and checks its
+vertices and edges against the oracle.
 
 ``--impl reference`` times the reference's algorithm on the host cores instead (the CPU
 oracle port: the Rust reference cannot be built here) on the same workload.
@@ -58,6 +60,9 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--upd-n", type=int, default=200_000, help="balls of the periodic updateable trajectory")
     ap.add_argument("--no-upd", action="store_true", help="skip the updateable trajectory leg")
+    ap.add_argument("--no-network", action="store_true", help="skip the tessellation network leg")
+    ap.add_argument("--tuning", default=None,
+                    help="warps,cell_scale,chunk of the FP32 contact launch instead of autotuning (profiling)")
     ap.add_argument("--batch-count", type=int, default=4096, help="structures of the batched leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched leg")
     ap.add_argument("--grad-n", type=int, default=20_000, help="balls of the differentiation leg")
@@ -459,6 +464,59 @@ def grad_leg(args, rank, torch, V, R):
     return out
 
 
+def network_leg(args, rank, torch, V, R, balls):
+    """compute_tessellation with with_cell_vertices on the main structure: the device time
+    of the call with and without the network (CUDA events, inputs resident), and on rank 0
+    the network's ids checked bit for bit against the CPU oracle's, positions and lengths
+    within 1e-9 (1 + |x|)."""
+    n = balls.shape[0]
+    stream = torch.cuda.current_stream()
+    eng = V.Engine()
+    eng.set_stream(stream.cuda_stream)
+    d = torch.from_numpy(balls).cuda()
+
+    def timed(on, reps=5):
+        eng.set_network(on)
+        ts = []
+        for k in range(reps + 2):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            eng.compute_device(d.data_ptr(), n, PROBE, precision="fp32")
+            e1.record(stream)
+            e1.synchronize()
+            if k >= 2:
+                ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    base = R.max(timed(False))
+    with_net = R.max(timed(True))
+    r = eng.download()
+    eng.set_network(False)
+    eng.close()
+    out = {"ms_without_network": round(base, 3), "ms_with_network": round(with_net, 3),
+           "vertices": int(len(r.vertex_ids)), "edges": int(len(r.edge_ids))}
+    if rank == 0:
+        import oracle as O
+
+        o = O.compute(balls, PROBE, with_cell_vertices=True)
+        null32 = 0xFFFFFFFF
+
+        def oid(x):
+            y = x.astype(np.int64)
+            y[x == O.NET_NULL] = null32
+            return y
+
+        ok = (r.vertex_ids.shape == o.vertex_ids.shape and r.edge_ids.shape == o.edge_ids.shape
+              and np.array_equal(r.vertex_ids.astype(np.int64), oid(o.vertex_ids))
+              and np.array_equal(r.edge_ids.astype(np.int64), oid(o.edge_ids)))
+        out["ids_match_oracle"] = bool(ok)
+        if ok:
+            out["max_xyz_err"] = float(np.abs(r.vertex_xyz - o.vertex_xyz).max(initial=0.0))
+            out["max_len_rel_err"] = float((np.abs(r.edge_length - o.edge_length) / (1 + np.abs(o.edge_length)))
+                                           .max(initial=0.0))
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -512,7 +570,12 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
     eng = V.Engine(local)
     eng.set_stream(stream.cuda_stream)
-    tuning = eng.autotune_device(d_xyzr.data_ptr(), args.n, PROBE, precision="fp32")  # untimed set-up
+    if args.tuning:
+        w, c, ch = args.tuning.split(",")
+        eng.set_tuning(int(w), float(c), int(ch))
+        tuning = eng.tuning()
+    else:
+        tuning = eng.autotune_device(d_xyzr.data_ptr(), args.n, PROBE, precision="fp32")  # untimed set-up
     eng.set_timing(True)
 
     def device_leg(precision, steps, warmup, sample_clocks):
@@ -584,6 +647,7 @@ def run_ours(args):
     upd = None if args.no_upd else updateable_leg(args, rank, torch, V, R)
     bat = None if args.no_batch else batched_leg(args, rank, torch, V, R)
     grd = None if args.no_grad else grad_leg(args, rank, torch, V, R)
+    net = None if args.no_network else network_leg(args, rank, torch, V, R, balls)
 
     if rank == 0:
         line = {
@@ -614,6 +678,7 @@ def run_ours(args):
             "updateable": upd,
             "batched": bat,
             "differentiation": grd,
+            "network": net,
         }
         print(json.dumps(line), flush=True)
     eng.close()

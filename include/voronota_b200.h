@@ -54,6 +54,19 @@ int vt_compute_tessellation(const double* xyzr, uint64_t n, double probe, const 
 int vt_compute_contacts_only(const double* xyzr, uint64_t n, double probe, const double* periodic_box9,
                              const int32_t* groups, uint64_t n_groups, int precision, vt_result** out);
 
+/* compute_tessellation(..., with_cell_vertices = true) (src/tessellation.rs:37-48,
+ * 334-401): the result also holds the tessellation network -- cell vertices (4 ball ids
+ * in ascending order, 0xffffffff for NULL, i.e. a vertex on the SAS, and x, y, z) and
+ * cell edges (3 ids, NULL on the SAS, and the length), each sorted by ids and
+ * deduplicated (of several elements with equal ids the first in pair order is kept; the
+ * reference keeps an unspecified one).  Contours are recomputed in FP64 for the network. */
+int vt_compute_tessellation_network(const double* xyzr, uint64_t n, double probe, const double* periodic_box9,
+                                    const int32_t* groups, uint64_t n_groups, int precision, vt_result** out);
+uint64_t vt_result_num_vertices(const vt_result* r);
+uint64_t vt_result_num_edges(const vt_result* r);
+int vt_result_vertices(const vt_result* r, uint32_t* ids4, double* xyz3);
+int vt_result_edges(const vt_result* r, uint32_t* ids3, double* length);
+
 /* Result accessors: TessellationResult + the Results trait (src/types.rs:187-269). */
 uint64_t vt_result_num_balls(const vt_result* r);
 uint64_t vt_result_num_contacts(const vt_result* r);
@@ -99,6 +112,8 @@ int vt_engine_compute_host(vt_engine* e, const double* xyzr, uint64_t n, double 
                            const double* periodic_box9, const int32_t* groups, uint64_t n_groups,
                            int precision, int contacts_only);
 int vt_engine_download(vt_engine* e, vt_result** out);
+/* Engine calls also build the tessellation network (on) or not (off, the default). */
+int vt_engine_set_network(vt_engine* e, int on);
 
 typedef struct vt_stats {
     uint64_t num_balls, num_slots, num_entries, num_pairs, num_contacts, num_cells;

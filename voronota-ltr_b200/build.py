@@ -30,6 +30,7 @@ UNITS = {
     "vt_frontier.cu": ["--fmad=false"],
     "vt_batch.cu": ["--fmad=false"],
     "vt_adjoint.cu": ["--fmad=false"],
+    "vt_network.cu": ["--fmad=false"],
     "vt_updateable.cu": ["--fmad=false"],
 }
 

@@ -431,7 +431,8 @@ void set_hex_table() {
     cudaMemcpyToSymbol(c_hex_sin, hs, sizeof(hs));
     cudaMemcpyToSymbol(c_hex_cos, hc, sizeof(hc));
     cudaMemcpyToSymbol(c_hex_n, &n, sizeof(int));
-    set_hex_table_adjoint();  // the adjoint's translation unit holds its own copy
+    set_hex_table_adjoint();  // the adjoint's and the network's translation units hold
+    set_hex_table_network();  // their own copies
 }
 
 void launch_contact_f64(const DevBufs& b, uint32_t P, int full, int from_list, cudaStream_t s) {

@@ -152,6 +152,103 @@ struct vt_engine {
             }
         }
     }
+    // tessellation network (with_cell_vertices) of the last call
+    bool network = false;
+    uint64_t net_nv = 0, net_ne = 0;
+    DBuf<uint32_t> net_flags, net_voff, net_vcnt, net_ecnt, net_off_v, net_off_e, net_src, net_src2, net_uflags,
+        net_uoff;
+    DBuf<uint4> net_vids, net_eids;
+    DBuf<double> net_vxyz, net_elen;
+    DBuf<unsigned long long> net_hi, net_lo, net_ka, net_kb, net_hs, net_ls;
+    DBuf<uint32_t> net_ia, net_ib, net_order;
+    DBuf<uint8_t> net_temp;
+    DBuf<uint32_t> out_net_vid, out_net_eid;
+    DBuf<double> out_net_vxyz, out_net_elen;
+
+    // one element type: sort the dense keys, keep the first of equal ids, gather
+    uint64_t net_unique(uint32_t m, int vertices) {
+        if (m == 0) return 0;
+        net_ka.ensure(m);
+        net_kb.ensure(m);
+        net_hs.ensure(m);
+        net_ls.ensure(m);
+        net_ia.ensure(m);
+        net_ib.ensure(m);
+        net_order.ensure(m);
+        const size_t tb = net_sort_temp_bytes(m);
+        net_temp.ensure(tb);
+        NetSortBufs t{net_ka.p, net_kb.p, net_hs.p, net_ls.p, net_ia.p, net_ib.p, net_order.p, net_temp.p, tb};
+        net_sort(m, net_hi.p, net_lo.p, t, stream);
+        net_uflags.ensure(m + 1);
+        net_uoff.ensure(m + 2);
+        launch_net_unique(m, t, net_uflags.p, stream);
+        ensure_scan(m + 1);
+        scan_u32(net_uflags.p, net_uoff.p, m, scan_tmp.p, stream);
+        VT_CUDA(cudaMemcpyAsync(h_words + 15, net_uoff.p + m, 4, cudaMemcpyDeviceToHost, stream));
+        sync();
+        const uint32_t U = h_words[15];
+        net_src2.ensure(m);
+        if (vertices) {
+            out_net_vid.ensure(4 * (size_t)U + 4);
+            out_net_vxyz.ensure(3 * (size_t)U + 3);
+            launch_net_gather(m, net_uoff.p, net_order.p, net_src.p, net_src2.p, net_vids.p, net_vxyz.p, 1,
+                              out_net_vid.p, out_net_vxyz.p, stream);
+        } else {
+            out_net_eid.ensure(3 * (size_t)U + 3);
+            out_net_elen.ensure((size_t)U + 1);
+            launch_net_gather(m, net_uoff.p, net_order.p, net_src.p, net_src2.p, net_eids.p, net_elen.p, 0,
+                              out_net_eid.p, out_net_elen.p, stream);
+        }
+        return U;
+    }
+
+    // assemble_tessellation_network over the pairs of the last run (after compaction)
+    int build_network(uint32_t P) {
+        DevBufs& b = bufs;
+        net_nv = net_ne = 0;
+        if (P == 0) return VT_OK;
+        net_flags.ensure(P + 1);
+        net_voff.ensure(P + 2);
+        launch_valid_flags(b, P, net_flags.p, stream);
+        ensure_scan(P + 1);
+        scan_u32(net_flags.p, net_voff.p, P, scan_tmp.p, stream);
+        VT_CUDA(cudaMemcpyAsync(h_words + 15, net_voff.p + P, 4, cudaMemcpyDeviceToHost, stream));
+        sync();
+        const uint32_t V = h_words[15];
+        if (V == 0) return VT_OK;
+        const size_t cap = (size_t)V * net_slot_capacity();
+        net_vids.ensure(cap);
+        net_eids.ensure(cap);
+        net_vxyz.ensure(3 * cap);
+        net_elen.ensure(cap);
+        net_vcnt.ensure(V + 1);
+        net_ecnt.ensure(V + 1);
+        NetSlots sl{net_vids.p, net_vxyz.p, net_eids.p, net_elen.p, net_vcnt.p, net_ecnt.p};
+        launch_net_elements(b, P, net_voff.p, sl, stream);
+        net_off_v.ensure(V + 2);
+        net_off_e.ensure(V + 2);
+        ensure_scan(V + 1);
+        scan_u32(net_vcnt.p, net_off_v.p, V, scan_tmp.p, stream);
+        scan_u32(net_ecnt.p, net_off_e.p, V, scan_tmp.p, stream);
+        VT_CUDA(cudaMemcpyAsync(h_words + 13, net_off_v.p + V, 4, cudaMemcpyDeviceToHost, stream));
+        VT_CUDA(cudaMemcpyAsync(h_words + 14, net_off_e.p + V, 4, cudaMemcpyDeviceToHost, stream));
+        sync();
+        const uint32_t Mv = h_words[13], Me = h_words[14];
+        const uint32_t mmax = std::max(Mv, Me) + 1;
+        net_hi.ensure(mmax);
+        net_lo.ensure(mmax);
+        net_src.ensure(mmax);
+        if (Mv) {
+            launch_net_keys(V, net_vcnt.p, net_off_v.p, net_vids.p, 4, net_hi.p, net_lo.p, net_src.p, stream);
+            net_nv = net_unique(Mv, 1);
+        }
+        if (Me) {
+            launch_net_keys(V, net_ecnt.p, net_off_e.p, net_eids.p, 3, net_hi.p, net_lo.p, net_src.p, stream);
+            net_ne = net_unique(Me, 0);
+        }
+        return VT_OK;
+    }
+
     // batched call state
     bool batch = false;
     uint64_t batch_S = 0;
@@ -245,6 +342,7 @@ struct vt_engine {
         batch_S = batch ? S : 0;
         stats = vt_stats{};
         stats.num_balls = n64;
+        net_nv = net_ne = 0;
         const uint64_t launches0 = launch_count();
         for (int k = 0; k < VT_NUM_STAGES; ++k) {
             used[k] = false;
@@ -535,6 +633,11 @@ struct vt_engine {
         t_end(9);
         t_end(10);
 
+        net_nv = net_ne = 0;
+        if (network && !contacts_only && !batch) {
+            int nst = build_network(P);
+            if (nst != VT_OK) return nst;
+        }
         VT_CUDA(cudaMemcpyAsync(h_words + 5, keep_off.p + P, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         if (!contacts_only)
             VT_CUDA(cudaMemcpyAsync(h_words + 6, cell_off.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
@@ -560,7 +663,7 @@ struct vt_engine {
         stats.total_sas_area = contacts_only ? 0.0 : h_tot[0];
         stats.total_volume = contacts_only ? 0.0 : h_tot[1];
         stats.total_contact_area = h_tot[2];
-        if (h_words[7] & (kErrOverflow | kErrNeighborCap)) {
+        if (h_words[7] & (kErrOverflow | kErrNeighborCap | kErrNetwork)) {
             g_last_error = "contour or neighbour capacity exceeded";
             return VT_ERR_CAPACITY;
         }
@@ -600,6 +703,22 @@ struct vt_engine {
             VT_CUDA(cudaMemcpyAsync(r->cell_index.data(), out_cell_index.p, M * 4, cudaMemcpyDeviceToHost, stream));
             VT_CUDA(cudaMemcpyAsync(r->cell_sas.data(), out_cell_sas.p, M * 8, cudaMemcpyDeviceToHost, stream));
             VT_CUDA(cudaMemcpyAsync(r->cell_vol.data(), out_cell_vol.p, M * 8, cudaMemcpyDeviceToHost, stream));
+        }
+        if (network && !contacts_only && !batch) {
+            r->has_network = true;
+            const size_t V = net_nv, E = net_ne;
+            r->net_vid.resize(4 * V);
+            r->net_vxyz.resize(3 * V);
+            r->net_eid.resize(3 * E);
+            r->net_elen.resize(E);
+            if (V) {
+                VT_CUDA(cudaMemcpyAsync(r->net_vid.data(), out_net_vid.p, 16 * V, cudaMemcpyDeviceToHost, stream));
+                VT_CUDA(cudaMemcpyAsync(r->net_vxyz.data(), out_net_vxyz.p, 24 * V, cudaMemcpyDeviceToHost, stream));
+            }
+            if (E) {
+                VT_CUDA(cudaMemcpyAsync(r->net_eid.data(), out_net_eid.p, 12 * E, cudaMemcpyDeviceToHost, stream));
+                VT_CUDA(cudaMemcpyAsync(r->net_elen.data(), out_net_elen.p, 8 * E, cudaMemcpyDeviceToHost, stream));
+            }
         }
         sync();
         r->totals[0] = stats.total_sas_area;
@@ -985,6 +1104,43 @@ int vt_engine_download_batch(vt_engine* e, vt_batch_result** out) {
     if (!e || !out) return VT_ERR_INVALID;
     *out = nullptr;
     return guarded([&]() { return e->download_batch(out); });
+}
+
+int vt_compute_tessellation_network(const double* xyzr, uint64_t n, double probe, const double* periodic_box9,
+                                    const int32_t* groups, uint64_t n_groups, int precision, vt_result** out) {
+    if (!out) return VT_ERR_INVALID;
+    *out = nullptr;
+    return with_default_engine([&](vt_engine* e) -> int {
+        e->network = true;
+        int st = host_compute(e, xyzr, n, probe, periodic_box9, groups, n_groups, precision, 0);
+        e->network = false;
+        if (st != VT_OK) return st;
+        e->network = true;
+        st = e->download(out);
+        e->network = false;
+        return st;
+    });
+}
+int vt_engine_set_network(vt_engine* e, int on) {
+    if (!e) return VT_ERR_INVALID;
+    e->network = on != 0;
+    return VT_OK;
+}
+uint64_t vt_result_num_vertices(const vt_result* r) { return r ? r->net_vxyz.size() / 3 : 0; }
+uint64_t vt_result_num_edges(const vt_result* r) { return r ? r->net_elen.size() : 0; }
+int vt_result_vertices(const vt_result* r, uint32_t* ids4, double* xyz3) {
+    if (!r || !r->has_network) return VT_ERR_INVALID;
+    const size_t V = r->net_vxyz.size() / 3;
+    if (V && ids4) std::memcpy(ids4, r->net_vid.data(), 16 * V);
+    if (V && xyz3) std::memcpy(xyz3, r->net_vxyz.data(), 24 * V);
+    return VT_OK;
+}
+int vt_result_edges(const vt_result* r, uint32_t* ids3, double* length) {
+    if (!r || !r->has_network) return VT_ERR_INVALID;
+    const size_t E = r->net_elen.size();
+    if (E && ids3) std::memcpy(ids3, r->net_eid.data(), 12 * E);
+    if (E && length) std::memcpy(length, r->net_elen.data(), 8 * E);
+    return VT_OK;
 }
 
 uint64_t vt_result_num_balls(const vt_result* r) { return r ? r->num_balls : 0; }

@@ -127,4 +127,8 @@ struct vt_result {
     vt::HostArr<uint32_t> cell_index;
     vt::HostArr<double> cell_sas, cell_vol;
     double totals[3] = {0, 0, 0};
+    // tessellation network (with_cell_vertices): 4 / 3 ids per vertex / edge
+    bool has_network = false;
+    vt::HostArr<uint32_t> net_vid, net_eid;
+    vt::HostArr<double> net_vxyz, net_elen;
 };

@@ -24,6 +24,7 @@ enum DevErr : uint32_t {
     kErrOverflow = 2u,     // a contour exceeded the serial fallback's capacity
     kErrIdRange = 4u,      // ids do not fit 32 bits
     kErrInvalid = 8u,      // non-finite input value or negative radius
+    kErrNetwork = 64u,     // a network contour outgrew a warp (32 points): elements not emitted
 };
 
 // Per-pair status bits.
@@ -254,6 +255,39 @@ void launch_adjoint(const DevBufs& b, uint32_t P, const double* w_sas, const dou
 void launch_adjoint_f32(const DevBufs& b, uint32_t P, const double* u_contact, const double* w_eff, double* grad,
                         cudaStream_t s);
 
+// ---- tessellation network (vt_network.cu) ----
+// Per valid pair (slot = exclusive scan of the valid flags), up to net_slot_capacity()
+// vertices and edges: ids (NULL = 0xffffffff; edges use x, y, z of the uint4), positions,
+// lengths, and the counts.
+struct NetSlots {
+    uint4* v_ids;
+    double* v_xyz;
+    uint4* e_ids;
+    double* e_len;
+    uint32_t* v_cnt;
+    uint32_t* e_cnt;
+};
+struct NetSortBufs {
+    unsigned long long *key_a, *key_b, *hi_s, *lo_s;
+    uint32_t *idx_a, *idx_b, *order;
+    void* temp;
+    size_t temp_bytes;
+};
+void launch_valid_flags(const DevBufs& b, uint32_t P, uint32_t* flags, cudaStream_t s);
+void launch_net_elements(const DevBufs& b, uint32_t P, const uint32_t* voff, NetSlots slots, cudaStream_t s);
+size_t net_slot_capacity();
+// dense keys of V pairs' elements (off = exclusive scan of cnt) and their slot positions
+void launch_net_keys(uint32_t V, const uint32_t* cnt, const uint32_t* off, const uint4* ids, int nids,
+                     unsigned long long* key_hi, unsigned long long* key_lo, uint32_t* src, cudaStream_t s);
+size_t net_sort_temp_bytes(uint32_t m);
+void net_sort(uint32_t m, const unsigned long long* hi, const unsigned long long* lo, NetSortBufs t, cudaStream_t s);
+// flags[i] = 1 for the first of each run of equal keys
+void launch_net_unique(uint32_t m, const NetSortBufs& t, uint32_t* flags, cudaStream_t s);
+// unique sorted elements (uoff = exclusive scan of the flags) to the output arrays
+void launch_net_gather(uint32_t m, const uint32_t* uoff, const uint32_t* order, const uint32_t* src_dense,
+                       uint32_t* src_tmp, const uint4* ids, const double* vals, int vertices, uint32_t* out_ids,
+                       double* out_vals, cudaStream_t s);
+
 // ---- contact kernels (vt_contact64.cu / vt_contact32.cu) ----
 // mode: 0 = all pairs; 1 = pairs listed in redo_list (count on device)
 void launch_contact_f64(const DevBufs& b, uint32_t P, int full, int from_list, cudaStream_t s);
@@ -265,5 +299,6 @@ void set_hex_table();
 // The hexagon table's values (host C library) and the upload into the adjoint's unit.
 void hex_table_values(double* hs, double* hc, int* n);
 void set_hex_table_adjoint();
+void set_hex_table_network();
 
 }  // namespace vt

@@ -91,6 +91,13 @@ def library():
     L.vt_result_free.argtypes = [_vp]
     L.vt_result_free.restype = None
     L.vt_result_view_get.argtypes = [_vp, ctypes.POINTER(VtResultView)]
+    L.vt_compute_tessellation_network.argtypes = args7 + [ctypes.POINTER(_vp)]
+    for name in ("vt_result_num_vertices", "vt_result_num_edges"):
+        getattr(L, name).argtypes = [_vp]
+        getattr(L, name).restype = ctypes.c_uint64
+    L.vt_result_vertices.argtypes = [_vp, _u32p, _f64p]
+    L.vt_result_edges.argtypes = [_vp, _u32p, _f64p]
+    L.vt_engine_set_network.argtypes = [_vp, ctypes.c_int]
     L.vt_engine_create.argtypes = [ctypes.c_int, ctypes.POINTER(_vp)]
     L.vt_engine_destroy.argtypes = [_vp]
     L.vt_engine_destroy.restype = None
@@ -287,7 +294,19 @@ class Result:
         cv = _view(v.cell_volume, M, ctypes.c_double, np.float64, owner)
         t = (ctypes.c_double(), ctypes.c_double(), ctypes.c_double())
         L.vt_result_totals(h, ctypes.byref(t[0]), ctypes.byref(t[1]), ctypes.byref(t[2]))
-        return cls(L.vt_result_num_balls(h), a, b, ar, arc, ce, ci, cs, cv, (t[0].value, t[1].value, t[2].value))
+        r = cls(L.vt_result_num_balls(h), a, b, ar, arc, ce, ci, cs, cv, (t[0].value, t[1].value, t[2].value))
+        V, E = int(L.vt_result_num_vertices(h)), int(L.vt_result_num_edges(h))
+        vid, vxyz = np.empty((V, 4), np.uint32), np.empty((V, 3))
+        eid, elen = np.empty((E, 3), np.uint32), np.empty(E)
+        if L.vt_result_vertices(h, vid.ctypes.data_as(_u32p), vxyz.ctypes.data_as(_f64p)) == VT_OK:
+            _check(L.vt_result_edges(h, eid.ctypes.data_as(_u32p), elen.ctypes.data_as(_f64p)))
+            r.vertex_ids, r.vertex_xyz, r.edge_ids, r.edge_length = vid, vxyz, eid, elen
+        return r
+
+    # tessellation network (with_cell_vertices): ids (V, 4) / (E, 3) as uint32 with
+    # NULL_ID (on the SAS) = 0xffffffff, positions (V, 3), lengths (E,); None otherwise
+    vertex_ids = vertex_xyz = edge_ids = edge_length = None
+    NULL_ID = 0xFFFFFFFF
 
     def sas_areas(self):
         """Per-ball SAS area or None (Results::sas_areas, types.rs:207-213)."""
@@ -311,9 +330,18 @@ class Result:
         cells = [{"index": i, "sas_area": s, "volume": v}
                  for i, s, v in zip(self.cell_index.tolist(), self.cell_sas_area.tolist(),
                                     self.cell_volume.tolist())]
-        return {"num_balls": self.num_balls, "contacts": contacts, "cells": cells,
-                "total_sas_area": self.total_sas_area, "total_volume": self.total_volume,
-                "total_contact_area": self.total_contact_area}
+        d = {"num_balls": self.num_balls, "contacts": contacts, "cells": cells,
+             "total_sas_area": self.total_sas_area, "total_volume": self.total_volume,
+             "total_contact_area": self.total_contact_area}
+        if self.vertex_ids is not None:
+            # vertices_to_list / edges_to_list (python.rs:153-187)
+            def ids(row):
+                return [None if i == self.NULL_ID else i for i in row]
+            d["cell_vertices"] = [{"ball_indices": ids(v), "x": p[0], "y": p[1], "z": p[2], "is_on_sas": v[3] == self.NULL_ID}
+                                  for v, p in zip(self.vertex_ids.tolist(), self.vertex_xyz.tolist())]
+            d["cell_edges"] = [{"ball_indices": ids(e), "length": ln, "is_on_sas": e[2] == self.NULL_ID}
+                               for e, ln in zip(self.edge_ids.tolist(), self.edge_length.tolist())]
+        return d
 
 
 def _run(fn_name, balls, probe, periodic_box, groups, precision) -> Result:
@@ -330,17 +358,20 @@ def _run(fn_name, balls, probe, periodic_box, groups, precision) -> Result:
     return Result.from_handle(L, h)
 
 
-def compute_tessellation_result(balls, probe, periodic_box=None, groups=None, precision="fp32") -> Result:
-    """compute_tessellation returning a :class:`Result` of numpy arrays."""
-    return _run("vt_compute_tessellation", balls, probe, periodic_box, groups, precision)
+def compute_tessellation_result(balls, probe, periodic_box=None, groups=None, precision="fp32",
+                                with_cell_vertices=False) -> Result:
+    """compute_tessellation returning a :class:`Result` of numpy arrays; with
+    ``with_cell_vertices`` it also holds the tessellation network (vertex_ids, vertex_xyz,
+    edge_ids, edge_length)."""
+    fn = "vt_compute_tessellation_network" if with_cell_vertices else "vt_compute_tessellation"
+    return _run(fn, balls, probe, periodic_box, groups, precision)
 
 
 def compute_tessellation(balls, probe, periodic_box=None, groups=None, with_cell_vertices=False,
                          precision="fp32") -> dict[str, Any]:
-    """Radical tessellation of balls (python.rs:238-264); returns the reference's dict."""
-    if with_cell_vertices:
-        raise NotImplementedError("with_cell_vertices (tessellation network) is not part of the GPU path")
-    return compute_tessellation_result(balls, probe, periodic_box, groups, precision).to_dict()
+    """Radical tessellation of balls (python.rs:238-264); returns the reference's dict,
+    with "cell_vertices" and "cell_edges" when ``with_cell_vertices``."""
+    return compute_tessellation_result(balls, probe, periodic_box, groups, precision, with_cell_vertices).to_dict()
 
 
 def compute_contacts_only(balls, probe, periodic_box=None, groups=None, precision="fp32") -> list[dict]:
@@ -492,6 +523,10 @@ class Engine:
 
     def set_fp32_band(self, ulps: float):
         _check(self._L.vt_engine_set_fp32_band(self._h, float(ulps)))
+
+    def set_network(self, on: bool = True):
+        """Later compute calls also build the tessellation network (with_cell_vertices)."""
+        _check(self._L.vt_engine_set_network(self._h, 1 if on else 0))
 
     def set_timing(self, on: bool = True):
         _check(self._L.vt_engine_set_timing(self._h, 1 if on else 0))
