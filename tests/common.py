@@ -35,3 +35,14 @@ def central_golden():
 def contact_lookup(res_a, res_b, a, b):
     idx = np.where((np.asarray(res_a) == a) & (np.asarray(res_b) == b))[0]
     return int(idx[0]) if len(idx) else None
+
+
+def sunflower(k, R=4.0, d=5.0, rr=1.0, rho=3.6):
+    """Two large balls whose contact is cut by k small balls on a ring around it: the
+    contact's contour has k points (touching small balls) or 2k (arcs between them), more
+    than a warp holds for k > 32, which exercises the serial contour fallback."""
+    balls = [(0.0, 0.0, 0.0, R), (d, 0.0, 0.0, R)]
+    for i in range(k):
+        t = 2 * np.pi * i / k
+        balls.append((d / 2, rho * np.cos(t), rho * np.sin(t), rr))
+    return np.array(balls, float)

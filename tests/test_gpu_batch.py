@@ -5,6 +5,8 @@ it alone: the batched path runs the same kernels over a concatenated ball array 
 one grid per structure, so contacts (ids local to the structure, order, central bits,
 areas, arc lengths) and cells are compared bit for bit with single GPU calls, in both
 precisions; per-structure totals (a different summation tree) within 1e-12 relative.
+FP32 mode picks its contact kernel by the call's candidate-pair count (FP64 below 8192
+pairs), so the single calls force the FP32 kernel that the whole batch runs.
 Structures are also checked against the oracle, and uneven sizes, empty structures and
 malformed offsets are covered.
 """
@@ -13,7 +15,7 @@ import pytest
 
 import oracle as O
 import voronota_ltr as V
-from gpu_util import compare
+from gpu_util import compare, engine_run
 from voronota_ltr import workloads as W
 
 pytestmark = pytest.mark.gpu
@@ -43,7 +45,7 @@ def test_batch_equals_single_calls(precision):
     r = V.compute_batch(structs, 1.4, precision)
     assert len(r) == len(structs)
     for s, balls in enumerate(structs):
-        single = V.compute_tessellation_result(balls, 1.4, precision=precision)
+        single, _ = engine_run(balls, 1.4, precision, fp32_min_pairs=0)
         _same(r.structure(s), single)
 
 

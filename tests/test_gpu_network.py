@@ -11,7 +11,7 @@ import pytest
 
 import oracle as O
 import voronota_ltr as V
-from common import RING_17, THREE_LINE, goldens, load_balls
+from common import RING_17, THREE_LINE, goldens, load_balls, sunflower
 from gpu_util import compare
 from voronota_ltr import workloads as W
 
@@ -117,3 +117,15 @@ def test_network_does_not_change_the_rest():
     assert np.array_equal(a.id_a, b.id_a) and np.array_equal(a.id_b, b.id_b)
     assert np.array_equal(a.area, b.area) and np.array_equal(a.cell_sas_area, b.cell_sas_area)
     assert a.vertex_ids is None and b.vertex_ids is not None
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_contours_longer_than_a_warp(prec):
+    """Contours of 40, 80 and 120 points go through the serial contour kernel."""
+    for balls, probe in [(sunflower(40), 0.5), (sunflower(40, rr=0.1, rho=3.3), 0.1),
+                         (sunflower(120, rr=0.12, rho=3.3), 0.5)]:
+        r = check_network(balls, probe, prec)
+        on_pair = ((r.vertex_ids == 0).any(1) & (r.vertex_ids == 1).any(1)).sum()
+        assert on_pair == len(balls) - 2
+    box = {"corners": [(-10, -10, -10), (12, 10, 10)]}
+    check_network(sunflower(40, rr=0.1, rho=3.3), 0.1, prec, periodic_box=box)

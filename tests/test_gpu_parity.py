@@ -7,8 +7,9 @@ import pytest
 
 import oracle as O
 import voronota_ltr as V
-from common import CENTRAL_POINTS, RING_17, THREE_LINE, central_golden, contact_lookup, goldens, load_balls
-from gpu_util import compare, gpu
+from common import (CENTRAL_POINTS, RING_17, THREE_LINE, central_golden, contact_lookup, goldens, load_balls,
+                    sunflower)
+from gpu_util import compare, engine_run, gpu
 from voronota_ltr import workloads as W
 
 pytestmark = pytest.mark.gpu
@@ -136,6 +137,49 @@ def test_edge_cases(prec):
     ]:
         r = gpu(balls, probe, precision=prec)
         compare(r, O.compute(balls, probe), prec)
+
+
+SUNFLOWERS = [(sunflower(40), 0.5), (sunflower(40, rr=0.1, rho=3.3), 0.1), (sunflower(120, rr=0.12, rho=3.3), 0.5)]
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_serial_fallback_long_contours(prec):
+    """Contours of 40 to 120 points (more than a warp holds) through the serial kernel."""
+    for balls, probe in SUNFLOWERS:
+        r, st = engine_run(balls, probe, prec)
+        assert st.num_serial >= 1
+        compare(r, O.compute(balls, probe), prec)
+        r = gpu(balls, probe, precision=prec, contacts_only=True)
+        compare(r, O.compute(balls, probe, contacts_only=True), prec, contacts_only=True)
+
+
+def test_fp32_kernel_forced_on_small_inputs():
+    """The FP32 kernel (forced below its default minimum of 8192 candidate pairs) on the
+    small golden structures and edge cases: pair sets and central bits exact, values within
+    the FP32 tolerances."""
+    cases = [(RING_17, 1.0, None), (RING_17, G["ring17_periodic"]["probe"], {"corners": G["ring17_periodic"]["corners"]}),
+             (load_balls("cs_1x1"), 2.0, None), (THREE_LINE, 0.5, None),
+             ([(0, 0, 0, 1.0), (0, 0, 0, 0.5), (1, 0, 0, 1.0)], 0.5, None),
+             ([(0, 0, 0, 1), (0, 0, 1, 1), (0, 1, 0, 1), (0, 1, 1, 1), (1, 0, 0, 1), (1, 0, 1, 1), (1, 1, 0, 1),
+               (1, 1, 1, 1)], 2.0, None)]
+    for balls, probe, box in cases:
+        r, st = engine_run(balls, probe, "fp32", periodic_box=box, fp32_min_pairs=0)
+        assert st.fp32_kernel == 1
+        compare(r, O.compute(balls, probe, periodic_box=box), "fp32")
+        r, st = engine_run(balls, probe, "fp32", periodic_box=box)
+        assert st.fp32_kernel == 0  # below the default minimum: the FP64 kernel
+        compare(r, O.compute(balls, probe, periodic_box=box), "fp64")
+
+
+def test_fp32_kernel_coherent_rounding():
+    """Forced FP32 on the rotationally symmetric sunflowers: every small ball's contact has
+    the same geometry, so the FP32 rounding of the solid angles adds up coherently instead
+    of averaging out; the totals then stay within 1e-5 relative (not 1e-6), while pair
+    sets, central bits and per-contact values meet the FP32 tolerances."""
+    for balls, probe in SUNFLOWERS:
+        r, st = engine_run(balls, probe, "fp32", fp32_min_pairs=0)
+        assert st.fp32_kernel == 1
+        compare(r, O.compute(balls, probe), "fp32", total_rel=1e-5)
 
 
 def test_invalid_input_raises():

@@ -410,7 +410,64 @@ __global__ void k_contact_serial(DevBufs b, int full) {
     }
 }
 
+// Tessellation network of the pairs whose contour outgrew a warp: the serial contour, then
+// the elements k_net_elements writes for a warp contour (contact.rs:119-177), into the
+// overflow area of the element storage (kSerialCap elements per listed pair).
+__global__ void k_net_serial(DevBufs b, const uint32_t* __restrict__ voff, NetSlots sl) {
+    const uint32_t listed = *sl.ov_count;
+    const uint32_t count = listed < sl.ov_cap ? listed : sl.ov_cap;
+    const int periodic = b.periodic;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+        uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+        if (slot >= b.serial_slots) break;
+        const uint32_t p = sl.ov_list[t];
+        const uint32_t v = voff[p];
+        Contour c;
+        c.v = reinterpret_cast<SP*>(b.serial_scratch) + (size_t)slot * kSerialCap;
+        c.n = 0;
+        c.cap = kSerialCap;
+        c.overflow = false;
+        Sph<double> ic;
+        V3<double> axis, bary;
+        double sum_arc, area;
+        const bool ok = serial_clip(b, p, c, ic, axis, bary, sum_arc, area);
+        const uint32_t o = t * (uint32_t)kSerialCap;  // in the overflow area
+        sl.base[v] = sl.split + o;
+        if (!ok || c.overflow) {  // counts stay 0
+            atomicOr(b.err, (uint32_t)kErrNetwork);
+            continue;
+        }
+        const uint32_t a = b.pair_a[p], bid = b.nb_id[b.pair_e[p]];
+        if (c.n == 0) {  // an uncut contact: one SAS edge
+            sl.ov_e_ids[o] = net_edge_ids(a, bid, kNetNull, periodic, b.n);
+            sl.ov_e_len[o] = sum_arc * ic.r;
+            sl.e_cnt[v] = 1;
+            continue;
+        }
+        for (int k = 0; k < c.n; ++k) {
+            const SP& cp = c.v[k];
+            const SP& nx = c.v[k + 1 < c.n ? k + 1 : 0];
+            const bool arc = cp.rid == a;
+            sl.ov_e_ids[o + k] = net_edge_ids(a, bid, arc ? kNetNull : cp.rid, periodic, b.n);
+            sl.ov_e_len[o + k] = arc ? cp.ang * ic.r : norm(P3(cp) - P3(nx));
+            sl.ov_v_ids[o + k] =
+                net_vertex_ids(a, bid, cp.lid == a ? kNetNull : cp.lid, arc ? kNetNull : cp.rid, periodic, b.n);
+            sl.ov_v_xyz[3 * (size_t)(o + k)] = cp.x;
+            sl.ov_v_xyz[3 * (size_t)(o + k) + 1] = cp.y;
+            sl.ov_v_xyz[3 * (size_t)(o + k) + 2] = cp.z;
+        }
+        sl.v_cnt[v] = (uint32_t)c.n;
+        sl.e_cnt[v] = (uint32_t)c.n;
+    }
+}
+
 }  // namespace
+
+void launch_net_serial(const DevBufs& b, const uint32_t* voff, NetSlots sl, cudaStream_t s) {
+    unsigned threads = 128;
+    unsigned blocks = (b.serial_slots + threads - 1) / threads;
+    k_net_serial<<<blocks, threads, 0, s>>>(b, voff, sl); count_launch();
+}
 
 void hex_table_values(double* hs, double* hc, int* n) {
     // the reference's accumulation: rotation_angle = pi/3, += pi/3 while < 2 pi

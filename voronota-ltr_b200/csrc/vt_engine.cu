@@ -157,8 +157,10 @@ struct vt_engine {
     uint64_t net_nv = 0, net_ne = 0;
     DBuf<uint32_t> net_flags, net_voff, net_vcnt, net_ecnt, net_off_v, net_off_e, net_src, net_src2, net_uflags,
         net_uoff;
-    DBuf<uint4> net_vids, net_eids;
-    DBuf<double> net_vxyz, net_elen;
+    DBuf<uint4> net_vids, net_eids, net_ov_vids, net_ov_eids;
+    DBuf<double> net_vxyz, net_elen, net_ov_vxyz, net_ov_elen;
+    DBuf<uint32_t> net_base, net_ov_list;
+    NetSlots net_slots{};
     DBuf<unsigned long long> net_hi, net_lo, net_ka, net_kb, net_hs, net_ls;
     DBuf<uint32_t> net_ia, net_ib, net_order;
     DBuf<uint8_t> net_temp;
@@ -191,13 +193,13 @@ struct vt_engine {
         if (vertices) {
             out_net_vid.ensure(4 * (size_t)U + 4);
             out_net_vxyz.ensure(3 * (size_t)U + 3);
-            launch_net_gather(m, net_uoff.p, net_order.p, net_src.p, net_src2.p, net_vids.p, net_vxyz.p, 1,
-                              out_net_vid.p, out_net_vxyz.p, stream);
+            launch_net_gather(m, net_uoff.p, net_order.p, net_src.p, net_src2.p, net_slots, 1, out_net_vid.p,
+                              out_net_vxyz.p, stream);
         } else {
             out_net_eid.ensure(3 * (size_t)U + 3);
             out_net_elen.ensure((size_t)U + 1);
-            launch_net_gather(m, net_uoff.p, net_order.p, net_src.p, net_src2.p, net_eids.p, net_elen.p, 0,
-                              out_net_eid.p, out_net_elen.p, stream);
+            launch_net_gather(m, net_uoff.p, net_order.p, net_src.p, net_src2.p, net_slots, 0, out_net_eid.p,
+                              out_net_elen.p, stream);
         }
         return U;
     }
@@ -213,18 +215,37 @@ struct vt_engine {
         ensure_scan(P + 1);
         scan_u32(net_flags.p, net_voff.p, P, scan_tmp.p, stream);
         VT_CUDA(cudaMemcpyAsync(h_words + 15, net_voff.p + P, 4, cudaMemcpyDeviceToHost, stream));
+        VT_CUDA(cudaMemcpyAsync(h_words + 13, b.d_serial_count, 4, cudaMemcpyDeviceToHost, stream));
         sync();
         const uint32_t V = h_words[15];
         if (V == 0) return VT_OK;
-        const size_t cap = (size_t)V * net_slot_capacity();
+        // the pairs whose warp contour overflowed in the contact stage overflow here too
+        // (same FP64 contour arithmetic); a margin, and the kernel reports any excess
+        const uint32_t ov_cap = h_words[13] + 16;
+        const size_t cap = (size_t)V * net_slot_capacity(), ov = (size_t)ov_cap * kSerialCap;
+        if (cap + ov >= (size_t)UINT32_MAX) {
+            g_last_error = "tessellation network too large for 32-bit element indices";
+            return VT_ERR_CAPACITY;
+        }
         net_vids.ensure(cap);
         net_eids.ensure(cap);
         net_vxyz.ensure(3 * cap);
         net_elen.ensure(cap);
+        net_ov_vids.ensure(ov);
+        net_ov_eids.ensure(ov);
+        net_ov_vxyz.ensure(3 * ov);
+        net_ov_elen.ensure(ov);
         net_vcnt.ensure(V + 1);
         net_ecnt.ensure(V + 1);
-        NetSlots sl{net_vids.p, net_vxyz.p, net_eids.p, net_elen.p, net_vcnt.p, net_ecnt.p};
+        net_base.ensure(V + 1);
+        net_ov_list.ensure(ov_cap + 1);  // [ov_cap] is the counter
+        VT_CUDA(cudaMemsetAsync(net_ov_list.p + ov_cap, 0, 4, stream));
+        NetSlots& sl = net_slots;
+        sl = NetSlots{net_vids.p, net_vxyz.p, net_eids.p, net_elen.p, net_ov_vids.p, net_ov_vxyz.p, net_ov_eids.p,
+                      net_ov_elen.p, (uint32_t)cap, net_base.p, net_vcnt.p, net_ecnt.p, net_ov_list.p,
+                      net_ov_list.p + ov_cap, ov_cap};
         launch_net_elements(b, P, net_voff.p, sl, stream);
+        launch_net_serial(b, net_voff.p, sl, stream);
         net_off_v.ensure(V + 2);
         net_off_e.ensure(V + 2);
         ensure_scan(V + 1);
@@ -239,11 +260,11 @@ struct vt_engine {
         net_lo.ensure(mmax);
         net_src.ensure(mmax);
         if (Mv) {
-            launch_net_keys(V, net_vcnt.p, net_off_v.p, net_vids.p, 4, net_hi.p, net_lo.p, net_src.p, stream);
+            launch_net_keys(V, net_vcnt.p, net_off_v.p, sl, 1, net_hi.p, net_lo.p, net_src.p, stream);
             net_nv = net_unique(Mv, 1);
         }
         if (Me) {
-            launch_net_keys(V, net_ecnt.p, net_off_e.p, net_eids.p, 3, net_hi.p, net_lo.p, net_src.p, stream);
+            launch_net_keys(V, net_ecnt.p, net_off_e.p, sl, 0, net_hi.p, net_lo.p, net_src.p, stream);
             net_ne = net_unique(Me, 0);
         }
         return VT_OK;
@@ -259,6 +280,7 @@ struct vt_engine {
     std::vector<uint32_t> h_crange, h_mrange;
     std::vector<double> h_btot;
     double fp32_band_ulps = 16.0;  // FP32 point error budget E, in float ulps of the pair scale
+    uint64_t fp32_min_pairs = 8192;  // FP32 mode: fewer candidate pairs run the FP64 kernel
     // launch configuration, set by the autotuner or by hand
     int c32_warps = 4;        // warps per block of the FP32 contact kernel
     int c32_chunk = 0;        // > 0: persistent FP32 contact launch, pairs taken in chunks
@@ -492,7 +514,8 @@ struct vt_engine {
         }
 
         // 5. neighbour lists + pair list
-        const bool fp32 = precision == VT_FP32_FIXUP;
+        const bool fp32 = precision == VT_FP32_FIXUP && P >= fp32_min_pairs;
+        stats.fp32_kernel = fp32 ? 1 : 0;
         nb_id.ensure(E);
         nb_slot.ensure(E);
         nb_val.ensure(E);
@@ -1120,6 +1143,11 @@ int vt_compute_tessellation_network(const double* xyzr, uint64_t n, double probe
         e->network = false;
         return st;
     });
+}
+int vt_engine_set_fp32_min_pairs(vt_engine* e, uint64_t min_pairs) {
+    if (!e) return VT_ERR_INVALID;
+    e->fp32_min_pairs = min_pairs;
+    return VT_OK;
 }
 int vt_engine_set_network(vt_engine* e, int on) {
     if (!e) return VT_ERR_INVALID;

@@ -5,7 +5,8 @@
 //   1. every valid pair's contour is recomputed in FP64 (warp per pair) and emits one edge
 //      per contour segment -- ids (a, b, the cutting neighbour or NULL on an arc), length
 //      of the chord or arc -- and one vertex per contour point -- ids (a, b, left id,
-//      right id with a's id as NULL), position; an uncut contact emits one SAS edge;
+//      right id with a's id as NULL), position; an uncut contact emits one SAS edge; a
+//      contour that outgrows the warp is listed for the serial kernel (vt_contact64.cu);
 //   2. ids are taken mod n for periodic images and sorted within the element;
 //   3. elements are compacted, stably sorted by their ids (radix sort on two 64-bit key
 //      words, low word first) and deduplicated keeping the first of equal ids, i.e. the
@@ -21,18 +22,9 @@ namespace vt {
 namespace {
 
 constexpr int kWarps = 4;
-constexpr int kSlot = 32;                 // elements of one pair (a warp contour holds <= 32 points)
-constexpr uint32_t kNull = 0xffffffffu;   // NULL_ID of an element id
+constexpr int kSlot = 32;  // elements of one pair (a warp contour holds <= 32 points)
 
 __device__ __forceinline__ Sph<double> sph_of(double4 v) { return {{v.x, v.y, v.z}, v.w}; }
-
-__device__ __forceinline__ void cswap(uint32_t& x, uint32_t& y) {
-    if (x > y) {
-        uint32_t t = x;
-        x = y;
-        y = t;
-    }
-}
 
 __global__ void k_valid_flags(const uint8_t* __restrict__ status, uint32_t P, uint32_t* __restrict__ flags) {
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x)
@@ -40,12 +32,10 @@ __global__ void k_valid_flags(const uint8_t* __restrict__ status, uint32_t P, ui
 }
 
 __global__ void __launch_bounds__(kWarps * 32)
-    k_net_elements(DevBufs b, uint32_t P, const uint32_t* __restrict__ voff, uint4* __restrict__ v_ids,
-                   double* __restrict__ v_xyz, uint4* __restrict__ e_ids, double* __restrict__ e_len,
-                   uint32_t* __restrict__ v_cnt, uint32_t* __restrict__ e_cnt) {
+    k_net_elements(DevBufs b, uint32_t P, const uint32_t* __restrict__ voff, NetSlots sl) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t n = b.n;
-    auto canon = [&](uint32_t id) { return (b.periodic && id != kNull) ? id % n : id; };
+    const int periodic = b.periodic;
     for (uint32_t p = blockIdx.x * kWarps + w; p < P; p += gridDim.x * kWarps) {
         const uint32_t slot = voff[p];
         if (voff[p + 1] == slot) continue;  // no contact
@@ -69,25 +59,27 @@ __global__ void __launch_bounds__(kWarps * 32)
         };
         ContourOut<double> co;
         WarpContact r = contact_warp<double, false, false>(g, (int)cnt, (int)(eb - off), nbf, &co);
-        const size_t base = (size_t)slot * kSlot;
-        if (!r.valid) {
+        const uint32_t base = slot * (uint32_t)kSlot;
+        if (!r.valid) {  // the contour outgrew the warp: the serial kernel emits this pair
             if (lane == 0) {
-                atomicOr(b.err, kErrNetwork);
-                v_cnt[slot] = 0;
-                e_cnt[slot] = 0;
+                sl.v_cnt[slot] = 0;
+                sl.e_cnt[slot] = 0;
+                sl.base[slot] = base;
+                const uint32_t j = r.overflow ? atomicAdd(sl.ov_count, 1u) : sl.ov_cap;
+                if (j < sl.ov_cap)
+                    sl.ov_list[j] = p;
+                else
+                    atomicOr(b.err, kErrNetwork);
             }
             continue;
         }
         if (co.full) {  // an uncut contact: one SAS edge, no vertex
             if (lane == 0) {
-                uint32_t i0 = canon(a), i1 = canon(g.b_id), i2 = kNull;
-                cswap(i0, i1);
-                cswap(i1, i2);
-                cswap(i0, i1);
-                e_ids[base] = make_uint4(i0, i1, i2, 0u);
-                e_len[base] = kTau * co.ic.r;
-                v_cnt[slot] = 0;
-                e_cnt[slot] = 1;
+                sl.e_ids[base] = net_edge_ids(a, g.b_id, kNetNull, periodic, n);
+                sl.e_len[base] = kTau * co.ic.r;
+                sl.v_cnt[slot] = 0;
+                sl.e_cnt[slot] = 1;
+                sl.base[slot] = base;
             }
             continue;
         }
@@ -97,44 +89,34 @@ __global__ void __launch_bounds__(kWarps * 32)
         if (lane < len) {
             const Pt<double>& cp = co.q;
             const bool arc = cp.rid == a;
-            // edge (a, b, third)
-            uint32_t e0 = canon(a), e1 = canon(g.b_id), e2 = arc ? kNull : canon(cp.rid);
-            cswap(e0, e1);
-            cswap(e1, e2);
-            cswap(e0, e1);
-            e_ids[base + lane] = make_uint4(e0, e1, e2, 0u);
-            e_len[base + lane] = arc ? cp.ang * co.ic.r : norm(cp.p - nxt.p);
-            // vertex (a, b, left, right)
-            uint32_t v0 = canon(a), v1 = canon(g.b_id), v2 = cp.lid == a ? kNull : canon(cp.lid),
-                     v3 = arc ? kNull : canon(cp.rid);
-            cswap(v0, v1);
-            cswap(v2, v3);
-            cswap(v0, v2);
-            cswap(v1, v3);
-            cswap(v1, v2);
-            v_ids[base + lane] = make_uint4(v0, v1, v2, v3);
-            v_xyz[3 * (base + lane)] = cp.p.x;
-            v_xyz[3 * (base + lane) + 1] = cp.p.y;
-            v_xyz[3 * (base + lane) + 2] = cp.p.z;
+            sl.e_ids[base + lane] = net_edge_ids(a, g.b_id, arc ? kNetNull : cp.rid, periodic, n);
+            sl.e_len[base + lane] = arc ? cp.ang * co.ic.r : norm(cp.p - nxt.p);
+            sl.v_ids[base + lane] =
+                net_vertex_ids(a, g.b_id, cp.lid == a ? kNetNull : cp.lid, arc ? kNetNull : cp.rid, periodic, n);
+            sl.v_xyz[3 * (size_t)(base + lane)] = cp.p.x;
+            sl.v_xyz[3 * (size_t)(base + lane) + 1] = cp.p.y;
+            sl.v_xyz[3 * (size_t)(base + lane) + 2] = cp.p.z;
         }
         if (lane == 0) {
-            v_cnt[slot] = (uint32_t)len;
-            e_cnt[slot] = (uint32_t)len;
+            sl.v_cnt[slot] = (uint32_t)len;
+            sl.e_cnt[slot] = (uint32_t)len;
+            sl.base[slot] = base;
         }
     }
 }
 
-// dense arrays: key words (hi, lo) and the element's slot position
+// dense arrays: key words (hi, lo) and the element's index
 __global__ void k_net_compact(uint32_t V, const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ off,
-                              const uint4* __restrict__ ids, int nids, unsigned long long* __restrict__ key_hi,
+                              NetSlots sl, int vertices, unsigned long long* __restrict__ key_hi,
                               unsigned long long* __restrict__ key_lo, uint32_t* __restrict__ src) {
     for (uint32_t v = blockIdx.x; v < V; v += gridDim.x) {
-        const uint32_t c = cnt[v], o = off[v];
+        const uint32_t c = cnt[v], o = off[v], base = sl.base[v];
         for (uint32_t k = threadIdx.x; k < c; k += blockDim.x) {
-            const uint4 id = ids[(size_t)v * kSlot + k];
+            const uint32_t i = base + k;
+            const uint4 id = vertices ? net_vid(sl, i) : net_eid(sl, i);
             key_hi[o + k] = ((unsigned long long)id.x << 32) | id.y;
-            key_lo[o + k] = nids == 4 ? (((unsigned long long)id.z << 32) | id.w) : (unsigned long long)id.z;
-            src[o + k] = v * kSlot + k;
+            key_lo[o + k] = vertices ? (((unsigned long long)id.z << 32) | id.w) : (unsigned long long)id.z;
+            src[o + k] = i;
         }
     }
 }
@@ -144,30 +126,28 @@ __global__ void k_first_flags(const unsigned long long* __restrict__ hi, const u
         flags[i] = (i == 0 || hi[i] != hi[i - 1] || lo[i] != lo[i - 1]) ? 1u : 0u;
 }
 __global__ void k_net_gather_v(uint32_t m, const uint32_t* __restrict__ uoff, const uint32_t* __restrict__ src,
-                               const uint4* __restrict__ ids, const double* __restrict__ xyz,
-                               uint32_t* __restrict__ out_ids, double* __restrict__ out_xyz) {
+                               NetSlots sl, uint32_t* __restrict__ out_ids, double* __restrict__ out_xyz) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         if (uoff[i + 1] == uoff[i]) continue;
         const uint32_t o = uoff[i], s = src[i];
-        const uint4 id = ids[s];
+        const uint4 id = net_vid(sl, s);
         out_ids[4 * (size_t)o] = id.x;
         out_ids[4 * (size_t)o + 1] = id.y;
         out_ids[4 * (size_t)o + 2] = id.z;
         out_ids[4 * (size_t)o + 3] = id.w;
-        for (int k = 0; k < 3; ++k) out_xyz[3 * (size_t)o + k] = xyz[3 * (size_t)s + k];
+        for (int k = 0; k < 3; ++k) out_xyz[3 * (size_t)o + k] = net_vxyz(sl, s, k);
     }
 }
 __global__ void k_net_gather_e(uint32_t m, const uint32_t* __restrict__ uoff, const uint32_t* __restrict__ src,
-                               const uint4* __restrict__ ids, const double* __restrict__ len,
-                               uint32_t* __restrict__ out_ids, double* __restrict__ out_len) {
+                               NetSlots sl, uint32_t* __restrict__ out_ids, double* __restrict__ out_len) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         if (uoff[i + 1] == uoff[i]) continue;
         const uint32_t o = uoff[i], s = src[i];
-        const uint4 id = ids[s];
+        const uint4 id = net_eid(sl, s);
         out_ids[3 * (size_t)o] = id.x;
         out_ids[3 * (size_t)o + 1] = id.y;
         out_ids[3 * (size_t)o + 2] = id.z;
-        out_len[o] = len[s];
+        out_len[o] = net_elen(sl, s);
     }
 }
 
@@ -179,8 +159,7 @@ void launch_valid_flags(const DevBufs& b, uint32_t P, uint32_t* flags, cudaStrea
     k_valid_flags<<<gb(P), 256, 0, s>>>(b.p_status, P, flags); count_launch();
 }
 void launch_net_elements(const DevBufs& b, uint32_t P, const uint32_t* voff, NetSlots sl, cudaStream_t s) {
-    k_net_elements<<<grid_blocks(P, kWarps, 148 * 64), kWarps * 32, 0, s>>>(b, P, voff, sl.v_ids, sl.v_xyz, sl.e_ids,
-                                                                           sl.e_len, sl.v_cnt, sl.e_cnt);
+    k_net_elements<<<grid_blocks(P, kWarps, 148 * 64), kWarps * 32, 0, s>>>(b, P, voff, sl);
     count_launch();
 }
 size_t net_slot_capacity() { return kSlot; }
@@ -194,10 +173,10 @@ void set_hex_table_network() {
     cudaMemcpyToSymbol(c_hex_n, &n, sizeof(int));
 }
 
-void launch_net_keys(uint32_t V, const uint32_t* cnt, const uint32_t* off, const uint4* ids, int nids,
+void launch_net_keys(uint32_t V, const uint32_t* cnt, const uint32_t* off, const NetSlots& sl, int vertices,
                      unsigned long long* key_hi, unsigned long long* key_lo, uint32_t* src, cudaStream_t s) {
     int g = (int)(V < 148u * 16u ? (V > 0 ? V : 1) : 148u * 16u);
-    k_net_compact<<<g, 64, 0, s>>>(V, cnt, off, ids, nids, key_hi, key_lo, src); count_launch();
+    k_net_compact<<<g, 64, 0, s>>>(V, cnt, off, sl, vertices, key_hi, key_lo, src); count_launch();
 }
 
 size_t net_sort_temp_bytes(uint32_t m) {
@@ -253,13 +232,13 @@ void launch_net_unique(uint32_t m, const NetSortBufs& t, uint32_t* flags, cudaSt
     k_first_flags<<<gb(m), 256, 0, s>>>(t.hi_s, t.lo_s, m, flags); count_launch();
 }
 void launch_net_gather(uint32_t m, const uint32_t* uoff, const uint32_t* order, const uint32_t* src_dense,
-                       uint32_t* src_tmp, const uint4* ids, const double* vals, int vertices, uint32_t* out_ids,
-                       double* out_vals, cudaStream_t s) {
+                       uint32_t* src_tmp, const NetSlots& sl, int vertices, uint32_t* out_ids, double* out_vals,
+                       cudaStream_t s) {
     k_gather_u32<<<gb(m), 256, 0, s>>>(m, order, src_dense, src_tmp); count_launch();
     if (vertices)
-        k_net_gather_v<<<gb(m), 256, 0, s>>>(m, uoff, src_tmp, ids, vals, out_ids, out_vals);
+        k_net_gather_v<<<gb(m), 256, 0, s>>>(m, uoff, src_tmp, sl, out_ids, out_vals);
     else
-        k_net_gather_e<<<gb(m), 256, 0, s>>>(m, uoff, src_tmp, ids, vals, out_ids, out_vals);
+        k_net_gather_e<<<gb(m), 256, 0, s>>>(m, uoff, src_tmp, sl, out_ids, out_vals);
     count_launch();
 }
 

@@ -256,17 +256,79 @@ void launch_adjoint_f32(const DevBufs& b, uint32_t P, const double* u_contact, c
                         cudaStream_t s);
 
 // ---- tessellation network (vt_network.cu) ----
-// Per valid pair (slot = exclusive scan of the valid flags), up to net_slot_capacity()
-// vertices and edges: ids (NULL = 0xffffffff; edges use x, y, z of the uint4), positions,
-// lengths, and the counts.
+// Element storage.  Valid pair number v (slot = exclusive scan of the valid flags) owns
+// elements [base[v], base[v] + cnt[v]) of a two-part index space: [0, split) are the warp
+// slots (net_slot_capacity() = 32 elements per pair, split = 32 V); [split, ...) is the
+// overflow area, kSerialCap elements for each pair whose contour outgrew a warp, filled
+// by the serial kernel (launch_net_serial).  Ids: NULL = 0xffffffff; an edge uses the
+// x, y, z of its uint4.
+constexpr uint32_t kNetNull = 0xffffffffu;
 struct NetSlots {
-    uint4* v_ids;
+    uint4* v_ids;  // warp area
     double* v_xyz;
     uint4* e_ids;
     double* e_len;
+    uint4* ov_v_ids;  // overflow area
+    double* ov_v_xyz;
+    uint4* ov_e_ids;
+    double* ov_e_len;
+    uint32_t split;
+    uint32_t* base;
     uint32_t* v_cnt;
     uint32_t* e_cnt;
+    uint32_t* ov_list;   // pairs whose contour outgrew a warp, in no particular order
+    uint32_t* ov_count;  // device counter of ov_list
+    uint32_t ov_cap;
 };
+__device__ __forceinline__ uint4 net_vid(const NetSlots& s, uint32_t i) {
+    return i < s.split ? s.v_ids[i] : s.ov_v_ids[i - s.split];
+}
+__device__ __forceinline__ uint4 net_eid(const NetSlots& s, uint32_t i) {
+    return i < s.split ? s.e_ids[i] : s.ov_e_ids[i - s.split];
+}
+__device__ __forceinline__ double net_vxyz(const NetSlots& s, uint32_t i, int k) {
+    return i < s.split ? s.v_xyz[3 * (size_t)i + k] : s.ov_v_xyz[3 * (size_t)(i - s.split) + k];
+}
+__device__ __forceinline__ double net_elen(const NetSlots& s, uint32_t i) {
+    return i < s.split ? s.e_len[i] : s.ov_e_len[i - s.split];
+}
+__device__ __forceinline__ void net_cswap(uint32_t& x, uint32_t& y) {
+    if (x > y) {
+        const uint32_t t = x;
+        x = y;
+        y = t;
+    }
+}
+// ids of the edge (a, b, third) and of the vertex (a, b, left, right): periodic image ids
+// taken mod n (NULL kept), then sorted (contact.rs:119-177, tessellation.rs:334-360)
+__device__ __forceinline__ uint4 net_edge_ids(uint32_t a, uint32_t b, uint32_t third, int periodic, uint32_t n) {
+    uint32_t i0 = a, i1 = b, i2 = third;
+    if (periodic) {
+        i0 %= n;
+        i1 %= n;
+        if (i2 != kNetNull) i2 %= n;
+    }
+    net_cswap(i0, i1);
+    net_cswap(i1, i2);
+    net_cswap(i0, i1);
+    return make_uint4(i0, i1, i2, 0u);
+}
+__device__ __forceinline__ uint4 net_vertex_ids(uint32_t a, uint32_t b, uint32_t l, uint32_t r, int periodic,
+                                                uint32_t n) {
+    uint32_t v0 = a, v1 = b, v2 = l, v3 = r;
+    if (periodic) {
+        v0 %= n;
+        v1 %= n;
+        if (v2 != kNetNull) v2 %= n;
+        if (v3 != kNetNull) v3 %= n;
+    }
+    net_cswap(v0, v1);  // sorting network of 4
+    net_cswap(v2, v3);
+    net_cswap(v0, v2);
+    net_cswap(v1, v3);
+    net_cswap(v1, v2);
+    return make_uint4(v0, v1, v2, v3);
+}
 struct NetSortBufs {
     unsigned long long *key_a, *key_b, *hi_s, *lo_s;
     uint32_t *idx_a, *idx_b, *order;
@@ -275,9 +337,11 @@ struct NetSortBufs {
 };
 void launch_valid_flags(const DevBufs& b, uint32_t P, uint32_t* flags, cudaStream_t s);
 void launch_net_elements(const DevBufs& b, uint32_t P, const uint32_t* voff, NetSlots slots, cudaStream_t s);
+// the pairs of ov_list through the serial contour (vt_contact64.cu); at most ov_cap
+void launch_net_serial(const DevBufs& b, const uint32_t* voff, NetSlots slots, cudaStream_t s);
 size_t net_slot_capacity();
-// dense keys of V pairs' elements (off = exclusive scan of cnt) and their slot positions
-void launch_net_keys(uint32_t V, const uint32_t* cnt, const uint32_t* off, const uint4* ids, int nids,
+// dense keys of V pairs' elements (off = exclusive scan of cnt) and their element indices
+void launch_net_keys(uint32_t V, const uint32_t* cnt, const uint32_t* off, const NetSlots& slots, int vertices,
                      unsigned long long* key_hi, unsigned long long* key_lo, uint32_t* src, cudaStream_t s);
 size_t net_sort_temp_bytes(uint32_t m);
 void net_sort(uint32_t m, const unsigned long long* hi, const unsigned long long* lo, NetSortBufs t, cudaStream_t s);
@@ -285,8 +349,8 @@ void net_sort(uint32_t m, const unsigned long long* hi, const unsigned long long
 void launch_net_unique(uint32_t m, const NetSortBufs& t, uint32_t* flags, cudaStream_t s);
 // unique sorted elements (uoff = exclusive scan of the flags) to the output arrays
 void launch_net_gather(uint32_t m, const uint32_t* uoff, const uint32_t* order, const uint32_t* src_dense,
-                       uint32_t* src_tmp, const uint4* ids, const double* vals, int vertices, uint32_t* out_ids,
-                       double* out_vals, cudaStream_t s);
+                       uint32_t* src_tmp, const NetSlots& slots, int vertices, uint32_t* out_ids, double* out_vals,
+                       cudaStream_t s);
 
 // ---- contact kernels (vt_contact64.cu / vt_contact32.cu) ----
 // mode: 0 = all pairs; 1 = pairs listed in redo_list (count on device)

@@ -53,7 +53,8 @@ class VtStats(ctypes.Structure):
         "num_fp64_redo", "num_serial")] + [
         ("total_sas_area", ctypes.c_double), ("total_volume", ctypes.c_double),
         ("total_contact_area", ctypes.c_double), ("device_error_bits", ctypes.c_uint32),
-        ("num_kernel_launches", ctypes.c_uint64), ("num_cell_redo", ctypes.c_uint64)]
+        ("num_kernel_launches", ctypes.c_uint64), ("num_cell_redo", ctypes.c_uint64),
+        ("fp32_kernel", ctypes.c_uint64)]
 
 STAGES = ("prepare", "images", "grid", "neighbor_count", "neighbor_fill", "contact", "fp64_recompute",
           "serial_fallback", "cells", "output", "call")
@@ -98,6 +99,7 @@ def library():
     L.vt_result_vertices.argtypes = [_vp, _u32p, _f64p]
     L.vt_result_edges.argtypes = [_vp, _u32p, _f64p]
     L.vt_engine_set_network.argtypes = [_vp, ctypes.c_int]
+    L.vt_engine_set_fp32_min_pairs.argtypes = [_vp, ctypes.c_uint64]
     L.vt_engine_create.argtypes = [ctypes.c_int, ctypes.POINTER(_vp)]
     L.vt_engine_destroy.argtypes = [_vp]
     L.vt_engine_destroy.restype = None
@@ -523,6 +525,11 @@ class Engine:
 
     def set_fp32_band(self, ulps: float):
         _check(self._L.vt_engine_set_fp32_band(self._h, float(ulps)))
+
+    def set_fp32_min_pairs(self, min_pairs: int):
+        """FP32 mode runs the FP32 contact kernel only from this many candidate pairs
+        (default 8192; FP64 below); 0 forces the FP32 kernel."""
+        _check(self._L.vt_engine_set_fp32_min_pairs(self._h, int(min_pairs)))
 
     def set_network(self, on: bool = True):
         """Later compute calls also build the tessellation network (with_cell_vertices)."""
