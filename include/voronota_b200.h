@@ -67,6 +67,27 @@ uint64_t vt_result_num_edges(const vt_result* r);
 int vt_result_vertices(const vt_result* r, uint32_t* ids4, double* xyz3);
 int vt_result_edges(const vt_result* r, uint32_t* ids3, double* length);
 
+/* compute_solvent_spheres (src/solvent_spheres.rs:131-169): weighted pseudo-solvent
+ * spheres on the exposed surface.  Stage 1 tessellates the balls with `probe`; a sample
+ * point p = centre + v (r + probe) of an exposed ball (cell sas_area > 0), v one of the
+ * subdivided-icosahedron directions of `depth` (0..4: 12, 42, 162, 642, 2562; larger
+ * clamps to 4), is kept when it is strictly closer (distance minus radius) to its ball
+ * than to every contact partner; stage 2 tessellates the atoms (radius max(r - probe +
+ * volume_probe, 0.01)) and the spheres (radius probe + volume_probe) with probe 0, and a
+ * sphere's weight is its stage-2 cell volume (0 without a cell).  Spheres come in the
+ * reference's order: cells by ball index, then direction order.  VT_ERR_INVALID (with the
+ * reference's message in vt_last_error) for a negative or non-finite probe or volume
+ * probe, a negative depth, non-finite coordinates or a non-positive radius. */
+typedef struct vt_solvent_result vt_solvent_result;
+int vt_compute_solvent_spheres(const double* xyzr, uint64_t n, double probe, double volume_probe, int depth,
+                               const double* periodic_box9, int precision, vt_solvent_result** out);
+uint64_t vt_solvent_count(const vt_solvent_result* r);
+/* The unit sample directions of a depth (clamped to 0..4), x y z each; returns their count
+ * (12, 42, 162, 642, 2562).  Host code only: needs no GPU. */
+int vt_icosahedron(int depth, double* xyz3);
+int vt_solvent_get(const vt_solvent_result* r, double* xyz3, double* radius, double* weight, uint32_t* parent);
+void vt_solvent_free(vt_solvent_result* r);
+
 /* Result accessors: TessellationResult + the Results trait (src/types.rs:187-269). */
 uint64_t vt_result_num_balls(const vt_result* r);
 uint64_t vt_result_num_contacts(const vt_result* r);

@@ -75,6 +75,15 @@ def lib():
     L.vto_upd_get_affected.argtypes = [vp, _u64p]
     L.vto_upd_summary.argtypes = [vp]
     L.vto_upd_summary.restype = vp
+    L.vto_icosahedron.argtypes = [ctypes.c_int, _f64p]
+    L.vto_icosahedron.restype = ctypes.c_int
+    L.vto_solvent_spheres.argtypes = [_f64p, ctypes.c_uint64, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                      _f64p, ctypes.POINTER(vp)]
+    L.vto_solvent_spheres.restype = ctypes.c_int
+    L.vto_solvent_count.argtypes = [vp]
+    L.vto_solvent_count.restype = ctypes.c_uint64
+    L.vto_solvent_get.argtypes = [vp, _f64p, _u64p]
+    L.vto_solvent_free.argtypes = [vp]
     _lib = L
     return L
 
@@ -274,3 +283,42 @@ class OracleUpdateable:
             return _read_result(self._L, h, False)
         finally:
             self._L.vto_free(h)
+
+
+def icosahedron(depth: int) -> np.ndarray:
+    """Unit sample directions of SubdividedIcosahedron (subdivided_icosahedron.rs:53-125)."""
+    L = lib()
+    k = L.vto_icosahedron(int(depth), None)
+    out = np.zeros((k, 3))
+    L.vto_icosahedron(int(depth), _p(out, _f64p))
+    return out
+
+
+class SolventResult:
+    def __init__(self, xyz, radius, weight, parent):
+        self.xyz, self.radius, self.weight, self.parent = xyz, radius, weight, parent
+
+
+_SOLVENT_ERRORS = {1: "invalid probe radius", 2: "invalid volume probe", 3: "invalid ball"}
+
+
+def solvent_spheres(balls, probe: float, volume_probe: float = 0.0, subdivision_depth: int = 2,
+                    periodic_box=None) -> SolventResult:
+    """compute_solvent_spheres (solvent_spheres.rs:131-169) on the CPU."""
+    L = lib()
+    x = np.ascontiguousarray(np.asarray(balls, dtype=np.float64).reshape(-1, 4))
+    pb = pbox_vectors(periodic_box)
+    h = ctypes.c_void_p()
+    st = L.vto_solvent_spheres(_p(x, _f64p), x.shape[0], float(probe), float(volume_probe), int(subdivision_depth),
+                               None if pb is None else _p(pb, _f64p), ctypes.byref(h))
+    if st != 0:
+        raise ValueError(_SOLVENT_ERRORS.get(st, "invalid input"))
+    try:
+        k = L.vto_solvent_count(h)
+        v = np.zeros((k, 5))
+        par = np.zeros(k, np.uint64)
+        if k:
+            L.vto_solvent_get(h, _p(v, _f64p), _p(par, _u64p))
+    finally:
+        L.vto_solvent_free(h)
+    return SolventResult(v[:, :3].copy(), v[:, 3].copy(), v[:, 4].copy(), par)

@@ -24,6 +24,7 @@
 #include "vt_oracle.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -1763,5 +1764,165 @@ vto_result* vto_upd_summary(const vto_upd* h) {  // summary (:332-378)
     }
     return r;
 }
+
+}  // extern "C"
+
+// ---- compute_solvent_spheres (solvent_spheres.rs:131-330) ----------------------------
+// SubdividedIcosahedron::new (subdivided_icosahedron.rs:53-125): the 12 normalised
+// icosahedron vertices, then `depth` rounds that split every face in four; the midpoint
+// of an edge is appended (normalised) the first time the edge is met, visiting faces in
+// order and each face's edges as (v1,v2), (v0,v2), (v0,v1).
+static std::vector<V3> icosahedron_directions(int depth) {
+    const double t = (1.0 + std::sqrt(5.0)) / 2.0;
+    const double base[12][3] = {{t, 1.0, 0.0},  {-t, 1.0, 0.0},  {t, -1.0, 0.0}, {-t, -1.0, 0.0},
+                                {1.0, 0.0, t},  {1.0, 0.0, -t},  {-1.0, 0.0, t}, {-1.0, 0.0, -t},
+                                {0.0, t, 1.0},  {0.0, -t, 1.0},  {0.0, t, -1.0}, {0.0, -t, -1.0}};
+    std::vector<V3> v;
+    for (const auto& b : base) v.push_back(normalize(V3{b[0], b[1], b[2]}));
+    std::vector<std::array<size_t, 3>> faces = {
+        {0, 8, 4},  {1, 10, 7}, {2, 9, 11}, {7, 3, 1},  {0, 5, 10}, {3, 9, 6},  {3, 11, 9},
+        {8, 6, 4},  {2, 4, 9},  {3, 7, 11}, {4, 2, 0},  {9, 4, 6},  {2, 11, 5}, {0, 10, 8},
+        {5, 0, 2},  {10, 5, 7}, {1, 6, 8},  {1, 8, 10}, {6, 1, 3},  {11, 7, 5}};
+    for (int d = 0; d < depth; ++d) {
+        std::map<std::pair<size_t, size_t>, size_t> mids;
+        std::vector<std::array<size_t, 3>> next;
+        next.reserve(faces.size() * 4);
+        for (const auto& f : faces) {
+            const std::pair<size_t, size_t> edges[3] = {{f[1], f[2]}, {f[0], f[2]}, {f[0], f[1]}};
+            size_t m[3];
+            for (int k = 0; k < 3; ++k) {
+                auto key = edges[k].first < edges[k].second ? edges[k]
+                                                            : std::make_pair(edges[k].second, edges[k].first);
+                auto it = mids.find(key);
+                if (it == mids.end()) {
+                    v.push_back(normalize((v[edges[k].first] + v[edges[k].second]) * 0.5));
+                    it = mids.emplace(key, v.size() - 1).first;
+                }
+                m[k] = it->second;
+            }
+            next.push_back({f[0], m[1], m[2]});
+            next.push_back({f[1], m[0], m[2]});
+            next.push_back({f[2], m[0], m[1]});
+            next.push_back({m[0], m[1], m[2]});
+        }
+        faces.swap(next);
+    }
+    return v;
+}
+
+struct vto_solvent {
+    std::vector<double> x, y, z, radius, weight;
+    std::vector<uint64_t> parent;
+};
+
+extern "C" {
+
+int vto_icosahedron(int depth, double* xyz3) {
+    const auto v = icosahedron_directions(depth < 0 ? 0 : (depth > 4 ? 4 : depth));
+    if (xyz3)
+        for (size_t i = 0; i < v.size(); ++i) {
+            xyz3[3 * i] = v[i].x;
+            xyz3[3 * i + 1] = v[i].y;
+            xyz3[3 * i + 2] = v[i].z;
+        }
+    return (int)v.size();
+}
+
+int vto_solvent_spheres(const double* xyzr, uint64_t n, double probe, double volume_probe, int depth,
+                        const double* pbox9, vto_solvent** out) {
+    *out = nullptr;
+    // validate_params / validate_balls (:164-194)
+    if (!std::isfinite(probe) || probe < 0.0) return 1;
+    if (!std::isfinite(volume_probe) || volume_probe < 0.0) return 2;
+    for (uint64_t i = 0; i < n; ++i) {
+        const double* b = xyzr + 4 * i;
+        if (!std::isfinite(b[0]) || !std::isfinite(b[1]) || !std::isfinite(b[2])) return 3;
+        if (!std::isfinite(b[3]) || b[3] <= 0.0) return 3;
+    }
+    vto_solvent* res = new vto_solvent();
+    *out = res;
+    if (n == 0) return 0;
+    const bool net = g_network;
+    g_network = false;
+    // stage 1 (:149-150)
+    vto_result* r1 = nullptr;
+    vto_compute(xyzr, n, probe, pbox9, nullptr, 0, 0, &r1);
+    // build_neighbor_graph (:201-233): partners of each exposed ball (sas_area > 0); the
+    // reference sorts them by distance only to stop early, which does not change results
+    std::vector<char> exposed(n, 0);
+    for (size_t k = 0; k < r1->cell_index.size(); ++k)
+        if (r1->cell_sas[k] > 0.0) exposed[r1->cell_index[k]] = 1;
+    std::vector<std::vector<uint64_t>> nb(n);
+    for (size_t k = 0; k < r1->c_a.size(); ++k) {
+        const uint64_t a = r1->c_a[k], b = r1->c_b[k];
+        if (exposed[a]) nb[a].push_back(b);
+        if (exposed[b]) nb[b].push_back(a);
+    }
+    auto center = [&](uint64_t i) { return V3{xyzr[4 * i], xyzr[4 * i + 1], xyzr[4 * i + 2]}; };
+    // generate_solvent_spheres / is_valid_solvent_position (:236-289)
+    const auto dirs = icosahedron_directions(depth < 0 ? 0 : (depth > 4 ? 4 : depth));
+    for (size_t k = 0; k < r1->cell_index.size(); ++k) {
+        if (!(r1->cell_sas[k] > 0.0)) continue;
+        const uint64_t i = r1->cell_index[k];
+        const V3 c = center(i);
+        const double ri = xyzr[4 * i + 3], R = ri + probe;
+        for (const V3& v : dirs) {
+            const V3 p = c + v * R;
+            const double da = norm(p - c) - ri;
+            bool ok = true;
+            for (uint64_t j : nb[i])
+                if (norm(p - center(j)) - xyzr[4 * j + 3] <= da) {
+                    ok = false;
+                    break;
+                }
+            if (!ok) continue;
+            res->x.push_back(p.x);
+            res->y.push_back(p.y);
+            res->z.push_back(p.z);
+            res->radius.push_back(probe);
+            res->weight.push_back(0.0);
+            res->parent.push_back(i);
+        }
+    }
+    vto_free(r1);
+    const size_t S = res->x.size();
+    if (S > 0) {
+        // compute_solvent_weights (:292-345): adjusted atoms, then the solvent spheres,
+        // tessellated with probe 0; a solvent sphere's weight is its cell volume
+        std::vector<double> comb(4 * (n + S));
+        for (uint64_t i = 0; i < n; ++i) {
+            comb[4 * i] = xyzr[4 * i];
+            comb[4 * i + 1] = xyzr[4 * i + 1];
+            comb[4 * i + 2] = xyzr[4 * i + 2];
+            comb[4 * i + 3] = rmax(xyzr[4 * i + 3] - probe + volume_probe, 0.01);
+        }
+        for (size_t s = 0; s < S; ++s) {
+            double* c = comb.data() + 4 * (n + s);
+            c[0] = res->x[s];
+            c[1] = res->y[s];
+            c[2] = res->z[s];
+            c[3] = probe + volume_probe;
+        }
+        vto_result* r2 = nullptr;
+        vto_compute(comb.data(), n + S, 0.0, pbox9, nullptr, 0, 0, &r2);
+        for (size_t k = 0; k < r2->cell_index.size(); ++k)
+            if (r2->cell_index[k] >= n) res->weight[r2->cell_index[k] - n] = r2->cell_vol[k];
+        vto_free(r2);
+    }
+    g_network = net;
+    return 0;
+}
+uint64_t vto_solvent_count(const vto_solvent* s) { return s ? s->x.size() : 0; }
+void vto_solvent_get(const vto_solvent* s, double* xyzrw5, uint64_t* parent) {
+    for (size_t i = 0; i < s->x.size(); ++i) {
+        xyzrw5[5 * i] = s->x[i];
+        xyzrw5[5 * i + 1] = s->y[i];
+        xyzrw5[5 * i + 2] = s->z[i];
+        xyzrw5[5 * i + 3] = s->radius[i];
+        xyzrw5[5 * i + 4] = s->weight[i];
+        parent[i] = s->parent[i];
+    }
+}
+void vto_solvent_free(vto_solvent* s) { delete s; }
 
 }  // extern "C"

@@ -83,6 +83,17 @@ void vto_upd_get_affected(const vto_upd* h, uint64_t* ids);
 /* summary() (updateable.rs:332-378) as a result object; free with vto_free. */
 vto_result* vto_upd_summary(const vto_upd* h);
 
+/* compute_solvent_spheres (solvent_spheres.rs:131-169): 0 ok, 1 invalid probe,
+ * 2 invalid volume probe, 3 invalid ball.  Spheres in the reference's order (cells by
+ * index, then icosahedron vertex order); x, y, z, radius, weight per sphere. */
+typedef struct vto_solvent vto_solvent;
+int vto_icosahedron(int depth, double* xyz3);
+int vto_solvent_spheres(const double* xyzr, uint64_t n, double probe, double volume_probe, int depth,
+                        const double* pbox9, vto_solvent** out);
+uint64_t vto_solvent_count(const vto_solvent* s);
+void vto_solvent_get(const vto_solvent* s, double* xyzrw5, uint64_t* parent);
+void vto_solvent_free(vto_solvent* s);
+
 #ifdef __cplusplus
 }
 #endif

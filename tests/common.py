@@ -46,3 +46,14 @@ def sunflower(k, R=4.0, d=5.0, rr=1.0, rho=3.6):
         t = 2 * np.pi * i / k
         balls.append((d / 2, rho * np.cos(t), rho * np.sin(t), rr))
     return np.array(balls, float)
+
+
+def big_ball_in_lattice(big_r=10.0, spacing=2.5, half=14.0, small_r=1.6, seed=0):
+    """A ball of radius big_r at the origin inside a jittered lattice of small balls: the
+    big ball has several hundred neighbour candidates (more than a warp sorts at once)."""
+    rng = np.random.default_rng(seed)
+    g = np.arange(-half, half + 1e-9, spacing)
+    pts = np.array(np.meshgrid(g, g, g, indexing="ij")).reshape(3, -1).T
+    pts = pts + rng.uniform(-0.3, 0.3, pts.shape)
+    small = np.column_stack([pts, np.full(len(pts), small_r)])
+    return np.vstack([[0.0, 0.0, 0.0, big_r], small])

@@ -64,6 +64,9 @@ def compare(g, o, precision, contacts_only=False, ordered=True, total_rel=None):
     ds = np.abs(g.cell_sas_area - o.cells_sas)
     dv = np.abs(g.cell_volume - o.cells_vol)
     assert np.all(ds <= ts), f"max |d sas| {ds.max()}"
+    # exposure (sas_area > 0: what compute_solvent_spheres samples) decided as the oracle
+    expo = np.nonzero((g.cell_sas_area > 0) != (o.cells_sas > 0))[0]
+    assert len(expo) == 0, f"exposure differs at cells {g.cell_index[expo[:10]]}"
     assert np.all(dv <= tv), f"max |d vol| {dv.max()}"
     rs = abs(g.total_sas_area - o.total_sas_area) / max(abs(o.total_sas_area), 1e-300)
     rv = abs(g.total_volume - o.total_volume) / max(abs(o.total_volume), 1e-300)

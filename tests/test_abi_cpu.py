@@ -75,3 +75,24 @@ def test_no_device_fails_loudly():
     with pytest.raises(V.VoronotaError) as ei:
         V.compute_tessellation([(0, 0, 0, 1.5)], 1.4)
     assert ei.value.status == V.VT_ERR_NO_DEVICE
+
+
+def test_icosahedron_directions_match_oracle():
+    """The library's sample directions (host code) are the oracle's bit for bit."""
+    import oracle as O
+    for depth in range(6):
+        assert np.array_equal(V.icosahedron_directions(depth), O.icosahedron(depth))
+
+
+def test_solvent_input_validation_without_device():
+    """compute_solvent_spheres rejects bad parameters before any device work, with the
+    reference's ValueError (solvent_spheres.rs:164-194; tests/test_python.py:262-278)."""
+    for kw in [dict(balls=[(0.0, 0.0, 0.0, 1.5)], probe=-1.0), dict(balls=[(0.0, 0.0, 0.0, 1.5)], probe=float("nan")),
+               dict(balls=[(0.0, 0.0, 0.0, -1.0)], probe=1.4), dict(balls=[(0.0, 0.0, 0.0, 0.0)], probe=1.4),
+               dict(balls=[(float("inf"), 0.0, 0.0, 1.0)], probe=1.4),
+               dict(balls=[(0.0, 0.0, 0.0, 1.5)], probe=1.4, volume_probe=-0.5)]:
+        with pytest.raises(ValueError):
+            V.compute_solvent_spheres(**kw)
+    with pytest.raises(OverflowError):
+        V.compute_solvent_spheres([(0.0, 0.0, 0.0, 1.5)], 1.4, subdivision_depth=-1)
+    assert hasattr(V, "compute_solvent_spheres")

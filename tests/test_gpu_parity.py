@@ -182,6 +182,22 @@ def test_fp32_kernel_coherent_rounding():
         compare(r, O.compute(balls, probe), "fp32", total_rel=1e-5)
 
 
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_long_neighbour_lists(prec):
+    """A ball with 646 / 1190 neighbour candidates (beyond the 256 the warp sort holds):
+    its list is sorted by the block sort, pairs and contacts as the oracle's."""
+    from common import big_ball_in_lattice
+    for balls in (big_ball_in_lattice(), big_ball_in_lattice(big_r=14.0, half=20.0)):
+        compare(gpu(balls, 1.4, precision=prec), O.compute(balls, 1.4), prec)
+        r = gpu(balls, 1.4, precision=prec, contacts_only=True)
+        compare(r, O.compute(balls, 1.4, contacts_only=True), prec, contacts_only=True)
+    balls = big_ball_in_lattice()
+    box = {"corners": [(-16.0, -16.0, -16.0), (16.5, 16.5, 16.5)]}
+    compare(gpu(balls, 1.4, periodic_box=box, precision=prec), O.compute(balls, 1.4, periodic_box=box), prec)
+    groups = (balls[:, 0] > 0).astype(np.int32)
+    compare(gpu(balls, 1.4, groups=groups, precision=prec), O.compute(balls, 1.4, groups=groups), prec)
+
+
 def test_invalid_input_raises():
     for bad in ([(0, 0, float("nan"), 1.0)], [(0, 0, 0, -1.0)]):
         with pytest.raises(V.VoronotaError) as ei:

@@ -238,3 +238,20 @@ def test_device_api_matches_host_api():
         assert np.array_equal(a.area, b.area) and np.array_equal(a.cell_sas_area, b.cell_sas_area)
         assert h.affected_ids().tolist() == d.affected_ids().tolist()
         assert d.totals() == (b.total_sas_area, b.total_volume, b.total_contact_area)
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_long_neighbour_lists(precision):
+    """A big ball with 646 neighbours (beyond the warp sort buffer) moved and changed:
+    its frontier list goes through the block sort."""
+    from common import big_ball_in_lattice
+    balls = big_ball_in_lattice()
+    p = Pair(precision)
+    assert p.call("init", balls, 1.4, None)
+    p.check()
+    moved = balls.copy()
+    moved[0, :3] += (0.3, -0.2, 0.1)
+    moved[0, 3] += 0.4
+    moved[5, :3] += 0.2
+    assert p.call("update_with_changed", moved, [0, 5])
+    p.check()

@@ -173,3 +173,42 @@ def test_network_full_circle_edge():  # src/tessellation.rs:1329-1344: an uncut 
     r = O.compute([(0.0, 0.0, 0.0, 1.5), (2.5, 0.0, 0.0, 1.5)], 0.5, with_cell_vertices=True)
     assert len(r.vertex_ids) == 0 and len(r.edge_ids) == 1
     assert r.edge_ids[0, 2] == O.NET_NULL
+
+
+# ---- compute_solvent_spheres (solvent_spheres.rs:371-483, tests/test_python.py:199-293) ----
+def test_icosahedron_vertex_counts():  # subdivided_icosahedron.rs:143-152
+    for depth, k in enumerate((12, 42, 162, 642, 2562)):
+        v = O.icosahedron(depth)
+        assert v.shape == (k, 3)
+        assert np.abs(np.linalg.norm(v, axis=1) - 1.0).max() < 1e-10
+    assert len(O.icosahedron(7)) == 2562  # depth clamps to 4 (:29-38)
+
+
+def test_solvent_single_sphere():  # solvent_spheres.rs:371-386
+    r = O.solvent_spheres([(0.0, 0.0, 0.0, 1.5)], 1.4, subdivision_depth=0)
+    assert len(r.weight) == 12 and np.all(r.parent == 0)
+    assert np.all(np.abs(r.radius - 1.4) < 1e-10) and np.all(r.weight > 0)
+
+
+def test_solvent_two_separated_spheres_cpp_golden():  # solvent_spheres.rs:410-441 (C++ sihsolv)
+    r = O.solvent_spheres([(0.0, 0.0, 0.0, 1.5), (5.0, 0.0, 0.0, 1.5)], 1.4, 0.0, 0)
+    assert len(r.weight) == 24
+    assert (r.parent == 0).sum() == 12 and (r.parent == 1).sum() == 12
+    assert abs(r.weight.sum() - 249.1) < 5.0
+
+
+def test_solvent_touching_and_contained():  # solvent_spheres.rs:388-408, 443-461
+    r = O.solvent_spheres([(0.0, 0.0, 0.0, 1.5), (2.5, 0.0, 0.0, 1.5)], 1.4, subdivision_depth=0)
+    assert 0 < len(r.weight) < 24
+    r = O.solvent_spheres([(0.0, 0.0, 0.0, 3.0), (2.5, 0.0, 0.0, 1.0)], 1.4, subdivision_depth=0)
+    assert (r.parent == 0).sum() > (r.parent == 1).sum()
+
+
+def test_solvent_validation_and_empty():  # solvent_spheres.rs:463-483; tests/test_python.py:243-278
+    for balls, probe in [([(0.0, 0.0, 0.0, 1.5)], -1.0), ([(0.0, 0.0, 0.0, 1.5)], float("nan")),
+                         ([(0.0, 0.0, 0.0, -1.0)], 1.4), ([(float("nan"), 0.0, 0.0, 1.5)], 1.4)]:
+        with pytest.raises(ValueError):
+            O.solvent_spheres(balls, probe)
+    assert len(O.solvent_spheres(np.zeros((0, 4)), 1.4).weight) == 0
+    assert len(O.solvent_spheres([(0.0, 0.0, 0.0, 1.5), (5.0, 0.0, 0.0, 1.5)], 1.4, volume_probe=0.5,
+                                 subdivision_depth=0).weight) > 0

@@ -31,6 +31,7 @@ UNITS = {
     "vt_batch.cu": ["--fmad=false"],
     "vt_adjoint.cu": ["--fmad=false"],
     "vt_network.cu": ["--fmad=false"],
+    "vt_solvent.cu": ["--fmad=false"],
     "vt_updateable.cu": ["--fmad=false"],
 }
 

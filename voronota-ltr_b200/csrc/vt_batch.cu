@@ -150,6 +150,18 @@ __global__ void k_batch_localize_pair(uint32_t* __restrict__ a, uint32_t* __rest
     }
 }
 
+// pairs of structures with fewer than min_pairs candidate pairs: FP64 like a single call on
+// such a structure (marked unsure, so the FP64 recompute takes them)
+__global__ void k_batch_small_unsure(const uint32_t* __restrict__ pair_a, const uint32_t* __restrict__ bs,
+                                     const uint32_t* __restrict__ off, const uint32_t* __restrict__ pair_off,
+                                     uint32_t P, uint64_t min_pairs, uint8_t* __restrict__ status) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+        const uint32_t s = bs[pair_a[p]];
+        if ((uint64_t)(pair_off[off[s + 1]] - pair_off[off[s]]) < min_pairs && !(status[p] & kOverflow))
+            status[p] |= kUnsure;
+    }
+}
+
 __device__ __forceinline__ double block_sum(double v, double* sh) {
     const int t = threadIdx.x;
     sh[t] = v;
@@ -207,6 +219,12 @@ void launch_batch_grid(const DevBufs& b, uint32_t N, uint32_t total_cells, uint3
     cudaMemcpyAsync(b.cell_cursor, b.cell_start, sizeof(uint32_t) * total_cells, cudaMemcpyDeviceToDevice, s);
     k_batch_cell_scatter<<<gb(N), kBlock, 0, s>>>(b.sph, N, b.ball_struct, b.grids, b.cell_base, b.cell_cursor,
                                                   b.c_pos, b.c_id, b.c_slot);
+    count_launch();
+}
+void launch_batch_small_unsure(const DevBufs& b, const uint32_t* off, uint32_t P, uint64_t min_pairs,
+                               cudaStream_t s) {
+    if (P == 0 || min_pairs == 0) return;
+    k_batch_small_unsure<<<gb(P), kBlock, 0, s>>>(b.pair_a, b.ball_struct, off, b.pair_off, P, min_pairs, b.p_status);
     count_launch();
 }
 void launch_batch_outputs(const DevBufs& b, const uint32_t* off, uint32_t S, uint32_t P, int contacts_only,

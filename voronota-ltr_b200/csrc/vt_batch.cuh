@@ -20,6 +20,10 @@ void launch_batch_grid_setup(const uint32_t* off, uint32_t S, uint32_t N, const 
                              BBox* bboxes, GridDev* grids, uint32_t* ncell, double cell_scale, cudaStream_t s);
 // Counting sort of the balls into the concatenated grid (b.cell_base filled).
 void launch_batch_grid(const DevBufs& b, uint32_t N, uint32_t total_cells, uint32_t* scan_tmp, cudaStream_t s);
+// FP32 mode: the pairs of structures with fewer than min_pairs candidate pairs are marked
+// for the FP64 recompute (a single call on such a structure runs FP64).
+void launch_batch_small_unsure(const DevBufs& b, const uint32_t* off, uint32_t P, uint64_t min_pairs,
+                               cudaStream_t s);
 // Per-structure contact / cell ranges, local ids, per-structure totals (3 doubles per
 // structure: SAS area, volume, contact area).
 void launch_batch_outputs(const DevBufs& b, const uint32_t* off, uint32_t S, uint32_t P, int contacts_only,

@@ -23,6 +23,7 @@
 #include "vt_host.cuh"
 #include "vt_pipeline.cuh"
 #include "vt_batch.cuh"
+#include "vt_solvent.cuh"
 
 using namespace vt;
 
@@ -97,6 +98,12 @@ struct vt_batch_result {
     std::vector<double> totals;                   // 3 per structure
 };
 
+// Host copy of compute_solvent_spheres' output.
+struct vt_solvent_result {
+    std::vector<double> xyz, radius, weight;
+    std::vector<uint32_t> parent;
+};
+
 struct vt_engine {
     int device = 0;
     cudaStream_t own = nullptr;
@@ -114,7 +121,7 @@ struct vt_engine {
     DBuf<uint32_t> pair_a, pair_e;
     DBuf<uint8_t> p_status, p_central;
     DBuf<double> p_area, p_arc, p_sa_a, p_sa_b, p_pv_a, p_pv_b;
-    DBuf<uint32_t> redo_list, serial_list, keep, keep_off, cell_off, flags32;
+    DBuf<uint32_t> redo_list, serial_list, keep, keep_off, cell_off, flags32, big_list;
     DBuf<double> serial_scratch;
     DBuf<uint8_t> cell_flag, ball_dirty;
     DBuf<uint32_t> cell_redo;
@@ -267,6 +274,85 @@ struct vt_engine {
             launch_net_keys(V, net_ecnt.p, net_off_e.p, sl, 0, net_hi.p, net_lo.p, net_src.p, stream);
             net_ne = net_unique(Me, 0);
         }
+        return VT_OK;
+    }
+
+    // compute_solvent_spheres (solvent_spheres.rs:131-345): stage-1 tessellation, the kept
+    // sample points (vt_solvent.cu), stage-2 tessellation of atoms + spheres, weights
+    DBuf<uint8_t> sv_exposed;
+    DBuf<uint32_t> sv_deg, sv_poff, sv_cursor, sv_partners, sv_mask, sv_count, sv_soff, sv_parent;
+    DBuf<double> sv_dirs, sv_xyz, sv_weight, sv_combined;
+    int sv_depth = -1;
+    uint32_t sv_K = 0;
+    uint64_t sv_S = 0;
+
+    int solvent(const double* d_xyzr, uint64_t n, double probe, double volume_probe, int depth,
+                const double* pbox9, int precision) {
+        sv_S = 0;
+        int st = run(d_xyzr, n, probe, pbox9, nullptr, 0, precision, 0);
+        if (st != VT_OK || n == 0) return st;
+        if (depth != sv_depth) {
+            const std::vector<double> dirs = icosahedron_directions(depth);
+            sv_dirs.ensure(dirs.size());
+            VT_CUDA(cudaMemcpy(sv_dirs.p, dirs.data(), dirs.size() * sizeof(double), cudaMemcpyHostToDevice));
+            sv_K = (uint32_t)(dirs.size() / 3);
+            sv_depth = depth;
+        }
+        const uint32_t C = (uint32_t)stats.num_contacts, M = (uint32_t)stats.num_cells, nn = (uint32_t)n;
+        const uint32_t words = (sv_K + 31) / 32;
+        sv_exposed.ensure(n);
+        sv_deg.ensure(n + 1);
+        sv_poff.ensure(n + 2);
+        sv_cursor.ensure(n + 1);
+        sv_partners.ensure(2 * (size_t)C + 1);
+        sv_mask.ensure((size_t)M * words + 1);
+        sv_count.ensure(M + 1);
+        sv_soff.ensure(M + 2);
+        SolventBufs t{sv_exposed.p, sv_deg.p,  sv_poff.p,  sv_cursor.p, sv_partners.p, sv_dirs.p,
+                      sv_mask.p,    sv_count.p, sv_soff.p, nullptr,     nullptr};
+        ensure_scan(std::max<size_t>(n, M) + 1);
+        launch_solvent_partners(bufs.out_a, bufs.out_b, C, bufs.out_cell_index, bufs.out_cell_sas, M, nn, t,
+                                scan_tmp.p, stream);
+        launch_solvent_mask(d_xyzr, bufs.out_cell_index, bufs.out_cell_sas, M, t, sv_K, probe, stream);
+        scan_u32(sv_count.p, sv_soff.p, M, scan_tmp.p, stream);
+        VT_CUDA(cudaMemcpyAsync(h_words + 15, sv_soff.p + M, 4, cudaMemcpyDeviceToHost, stream));
+        sync();
+        const uint64_t S = M ? h_words[15] : 0;
+        if (S == 0) return VT_OK;
+        if (n + S >= (uint64_t)0xffffffffu / 27u) {
+            g_last_error = "too many solvent spheres for 32-bit ids";
+            return VT_ERR_CAPACITY;
+        }
+        sv_xyz.ensure(3 * S);
+        sv_parent.ensure(S);
+        sv_combined.ensure(4 * (n + S));
+        t.sol_xyz = sv_xyz.p;
+        t.sol_parent = sv_parent.p;
+        launch_solvent_write(d_xyzr, bufs.out_cell_index, M, t, sv_K, probe, volume_probe, nn, sv_combined.p, stream);
+        st = run(sv_combined.p, n + S, 0.0, pbox9, nullptr, 0, precision, 0);
+        if (st != VT_OK) return st;
+        sv_weight.ensure(S);
+        launch_solvent_weights(bufs.out_cell_index, bufs.out_cell_vol, (uint32_t)stats.num_cells, nn, (uint32_t)S,
+                               sv_weight.p, stream);
+        sv_S = S;
+        sync();
+        return VT_OK;
+    }
+
+    int download_solvent(double probe, vt_solvent_result** out) {
+        std::unique_ptr<vt_solvent_result> r(new vt_solvent_result());
+        const size_t S = sv_S;
+        r->xyz.resize(3 * S);
+        r->radius.assign(S, probe);
+        r->weight.resize(S);
+        r->parent.resize(S);
+        if (S) {
+            VT_CUDA(cudaMemcpyAsync(r->xyz.data(), sv_xyz.p, 24 * S, cudaMemcpyDeviceToHost, stream));
+            VT_CUDA(cudaMemcpyAsync(r->weight.data(), sv_weight.p, 8 * S, cudaMemcpyDeviceToHost, stream));
+            VT_CUDA(cudaMemcpyAsync(r->parent.data(), sv_parent.p, 4 * S, cudaMemcpyDeviceToHost, stream));
+            sync();
+        }
+        *out = r.release();
         return VT_OK;
     }
 
@@ -493,6 +579,9 @@ struct vt_engine {
         b.excluded = excluded.p;
         b.nb_off = nb_off.p;
         b.pair_off = pair_off.p;
+        big_list.ensure(n + 1);
+        b.big_list = big_list.p;
+        b.d_big_count = words.p + 6;
         t_begin(3);
         launch_search_count(b, stream);
         scan_u32(nb_cnt.p, nb_off.p, n, scan_tmp.p, stream);
@@ -502,8 +591,9 @@ struct vt_engine {
         VT_CUDA(cudaMemcpyAsync(h_words + 1, pair_off.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         VT_CUDA(cudaMemcpyAsync(h_words + 2, words.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         VT_CUDA(cudaMemcpyAsync(h_words + 3, b.d_nslots, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        VT_CUDA(cudaMemcpyAsync(h_words + 10, b.d_big_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         sync();
-        const uint32_t E = h_words[0], P = h_words[1];
+        const uint32_t E = h_words[0], P = h_words[1], n_big = h_words[10];
         stats.num_entries = E;
         stats.num_pairs = P;
         stats.num_slots = h_words[3];
@@ -531,7 +621,7 @@ struct vt_engine {
         b.pair_a = pair_a.p;
         b.pair_e = pair_e.p;
         t_begin(4);
-        launch_search_fill(b, fp32 ? 1 : 0, stream);
+        launch_search_fill(b, fp32 ? 1 : 0, n_big, stream);
         t_end(4);
 
         // 6. contacts
@@ -566,6 +656,7 @@ struct vt_engine {
                 launch_contact_f32(b, P, full, stream);
                 t_end(5);
                 t_begin(6);
+                if (batch) launch_batch_small_unsure(b, boff.p, P, fp32_min_pairs, stream);
                 launch_collect_redo(b, P, stream);
                 launch_contact_f64(b, P, full, 1, stream);
                 t_end(6);
@@ -1144,6 +1235,80 @@ int vt_compute_tessellation_network(const double* xyzr, uint64_t n, double probe
         return st;
     });
 }
+int vt_compute_solvent_spheres(const double* xyzr, uint64_t n, double probe, double volume_probe, int depth,
+                               const double* periodic_box9, int precision, vt_solvent_result** out) {
+    if (!out) return VT_ERR_INVALID;
+    *out = nullptr;
+    // validate_params / validate_balls (solvent_spheres.rs:164-194), same messages
+    char msg[160];
+    if (!std::isfinite(probe) || probe < 0.0) {
+        std::snprintf(msg, sizeof msg, "invalid probe radius: %g (must be non-negative and finite)", probe);
+        g_last_error = msg;
+        return VT_ERR_INVALID;
+    }
+    if (!std::isfinite(volume_probe) || volume_probe < 0.0) {
+        std::snprintf(msg, sizeof msg, "invalid volume probe: %g (must be non-negative and finite)", volume_probe);
+        g_last_error = msg;
+        return VT_ERR_INVALID;
+    }
+    if (depth < 0) {
+        g_last_error = "negative subdivision depth";
+        return VT_ERR_INVALID;
+    }
+    if (n > 0 && !xyzr) {
+        g_last_error = "null balls pointer";
+        return VT_ERR_INVALID;
+    }
+    for (uint64_t i = 0; i < n; ++i) {
+        const double* b = xyzr + 4 * i;
+        const char* why = nullptr;
+        if (!std::isfinite(b[0]) || !std::isfinite(b[1]) || !std::isfinite(b[2]))
+            why = "coordinates must be finite";
+        else if (!std::isfinite(b[3]) || b[3] <= 0.0)
+            why = "radius must be positive and finite";
+        if (why) {
+            std::snprintf(msg, sizeof msg, "invalid ball at index %llu: %s", (unsigned long long)i, why);
+            g_last_error = msg;
+            return VT_ERR_INVALID;
+        }
+    }
+    if (precision != VT_FP64 && precision != VT_FP32_FIXUP) {
+        g_last_error = "unknown precision";
+        return VT_ERR_INVALID;
+    }
+    return with_default_engine([&](vt_engine* e) -> int {
+        int st = validate_host(xyzr, n, probe, periodic_box9, nullptr, 0);
+        if (st != VT_OK) return st;
+        VT_CUDA(cudaSetDevice(e->device));
+        const double* d_in = nullptr;
+        if (n) {
+            e->xyzr.ensure(4 * n);
+            VT_CUDA(cudaMemcpyAsync(e->xyzr.p, xyzr, 4 * n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+            d_in = e->xyzr.p;
+        }
+        st = e->solvent(d_in, n, probe, volume_probe, depth > 4 ? 4 : depth, periodic_box9, precision);
+        if (st != VT_OK) return st;
+        return e->download_solvent(probe, out);
+    });
+}
+int vt_icosahedron(int depth, double* xyz3) {
+    const std::vector<double> d = icosahedron_directions(depth);
+    if (xyz3) std::memcpy(xyz3, d.data(), d.size() * sizeof(double));
+    return (int)(d.size() / 3);
+}
+uint64_t vt_solvent_count(const vt_solvent_result* r) { return r ? r->weight.size() : 0; }
+int vt_solvent_get(const vt_solvent_result* r, double* xyz3, double* radius, double* weight, uint32_t* parent) {
+    if (!r) return VT_ERR_INVALID;
+    const size_t S = r->weight.size();
+    if (!S) return VT_OK;
+    if (xyz3) std::memcpy(xyz3, r->xyz.data(), 24 * S);
+    if (radius) std::memcpy(radius, r->radius.data(), 8 * S);
+    if (weight) std::memcpy(weight, r->weight.data(), 8 * S);
+    if (parent) std::memcpy(parent, r->parent.data(), 4 * S);
+    return VT_OK;
+}
+void vt_solvent_free(vt_solvent_result* r) { delete r; }
+
 int vt_engine_set_fp32_min_pairs(vt_engine* e, uint64_t min_pairs) {
     if (!e) return VT_ERR_INVALID;
     e->fp32_min_pairs = min_pairs;

@@ -216,7 +216,12 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_search(DevBufs b, int wan
             r_incl[r] = __shfl_sync(0xffffffffu, incl, r);
             r_beg[r] = __shfl_sync(0xffffffffu, rbeg, r);
         }
-        uint32_t hits = 0;
+        // a row longer than the warp sort buffer is written unsorted to the CSR by the
+        // fill pass and sorted there by k_big_sort
+        const uint32_t row_cnt = FILL ? b.nb_cnt[row] : 0u;
+        const bool big = row_cnt > (uint32_t)kSortCap;
+        const uint32_t off = FILL ? b.nb_off[row] : 0u;
+        uint32_t hits = 0, np = 0;
         bool hidden = false;
         for (uint32_t t0 = 0; t0 < total && !hidden; t0 += 32) {
             uint32_t t = t0 + lane;
@@ -253,37 +258,40 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_search(DevBufs b, int wan
             }
             unsigned m = __ballot_sync(0xffffffffu, hit);
             uint32_t pos = hits + __popc(m & ((1u << lane) - 1u));
-            if (FILL && hit && pos < (uint32_t)kSortCap) {
-                s_val[w][pos] = val;
-                s_id[w][pos] = cid;
-                s_slot[w][pos] = cslot;
+            if (FILL && hit) {
+                if (big) {
+                    if (pos < row_cnt) {  // the count pass found exactly row_cnt
+                        b.nb_id[off + pos] = cid;
+                        b.nb_slot[off + pos] = cslot;
+                        b.nb_val[off + pos] = val;
+                    }
+                } else if (pos < (uint32_t)kSortCap) {
+                    s_val[w][pos] = val;
+                    s_id[w][pos] = cid;
+                    s_slot[w][pos] = cslot;
+                }
             }
-            if (!FILL && hit && pos < (uint32_t)kSortCap) s_id[w][pos] = cid;
+            if (!FILL) {  // pairs this ball generates (collect_collision_pairs, tessellation.rs:298-319)
+                const uint32_t bc = b.periodic ? cid % n : cid;
+                const bool gen = hit && !b.no_pairs && !same_group(b.groups, b.n_groups, i, bc) &&
+                                 ((b.periodic && cid >= n) || i < cid);
+                np += __popc(__ballot_sync(0xffffffffu, gen));
+            }
             hits += __popc(m);
         }
-        uint32_t cnt = hidden ? 0 : hits;
-        if (cnt > (uint32_t)kSortCap) {
-            if (lane == 0) atomicOr(b.err, (uint32_t)kErrNeighborCap);
-            cnt = 0;
-        }
+        const uint32_t cnt = hidden ? 0 : hits;
         __syncwarp();
         if (!FILL) {
-            uint32_t np = 0;
-            for (uint32_t e = lane; e < cnt && !b.no_pairs; e += 32) {
-                uint32_t bid = s_id[w][e];
-                uint32_t bc = b.periodic ? bid % n : bid;
-                bool gen = !same_group(b.groups, b.n_groups, i, bc) && ((b.periodic && bid >= n) || i < bid);
-                np += gen ? 1u : 0u;
-            }
-            for (int o = 16; o > 0; o >>= 1) np += __shfl_xor_sync(0xffffffffu, np, o);
             if (lane == 0) {
                 b.nb_cnt[row] = cnt;
-                if (!b.no_pairs) b.nb_npair[row] = np;
+                if (!b.no_pairs) b.nb_npair[row] = hidden ? 0u : np;
                 b.excluded[i] = hidden ? 1 : 0;
+                if (cnt > (uint32_t)kSortCap) b.big_list[atomicAdd(b.d_big_count, 1u)] = row;
             }
             __syncwarp();
             continue;
         }
+        if (big) continue;
         // bitonic sort of (value, id) (spheres_searcher.rs:324)
         uint32_t n2 = 2;
         while (n2 < cnt) n2 <<= 1;
@@ -318,7 +326,6 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_search(DevBufs b, int wan
                 }
             }
         }
-        const uint32_t off = b.nb_off[row];
         uint32_t prank = b.no_pairs ? 0u : b.pair_off[row];
         for (uint32_t e0 = 0; e0 < cnt; e0 += 32) {
             uint32_t e = e0 + lane;
@@ -351,6 +358,90 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_search(DevBufs b, int wan
             prank += __popc(m);
         }
         __syncwarp();
+    }
+}
+
+// ---- rows longer than the warp sort buffer: a block per row sorts the row in place in
+// global memory by (value, id) with an ascending bitonic network over the next power of
+// two (comparators reaching past the row's end are skipped: the missing elements act as
+// +infinity), then generates the row's pairs in sorted order (block scan of the flags).
+constexpr int kBigThreads = 1024;
+__device__ __forceinline__ void big_cmpswap(const DevBufs& b, uint32_t lo, uint32_t hi) {
+    const double vl = b.nb_val[lo], vh = b.nb_val[hi];
+    const uint32_t il = b.nb_id[lo], ih = b.nb_id[hi];
+    if (vless(vh, ih, vl, il)) {
+        const uint32_t sl = b.nb_slot[lo], sh = b.nb_slot[hi];
+        b.nb_val[lo] = vh;
+        b.nb_val[hi] = vl;
+        b.nb_id[lo] = ih;
+        b.nb_id[hi] = il;
+        b.nb_slot[lo] = sh;
+        b.nb_slot[hi] = sl;
+    }
+}
+__global__ void __launch_bounds__(kBigThreads) k_big_sort(DevBufs b, int want_rel) {
+    __shared__ uint32_t s_warp[kBigThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const uint32_t n = b.n, nbig = *b.d_big_count;
+    for (uint32_t k = blockIdx.x; k < nbig; k += gridDim.x) {
+        const uint32_t row = b.big_list[k];
+        const uint32_t i = b.frontier ? b.frontier[row] : row;
+        const uint32_t off = b.nb_off[row], cnt = b.nb_cnt[row];
+        uint32_t n2 = 1;
+        while (n2 < cnt) n2 <<= 1;
+        for (uint32_t size = 2; size <= n2; size <<= 1) {
+            const uint32_t half = size >> 1;
+            for (uint32_t t = tid; t < (n2 >> 1); t += kBigThreads) {  // flip step
+                const uint32_t g = t / half, p = t % half;
+                const uint32_t lo = g * size + p, hi = g * size + size - 1 - p;
+                if (hi < cnt) big_cmpswap(b, off + lo, off + hi);
+            }
+            __syncthreads();
+            for (uint32_t stride = half >> 1; stride > 0; stride >>= 1) {
+                for (uint32_t t = tid; t < (n2 >> 1); t += kBigThreads) {
+                    const uint32_t g = t / stride, p = t % stride;
+                    const uint32_t lo = g * 2 * stride + p, hi = lo + stride;
+                    if (hi < cnt) big_cmpswap(b, off + lo, off + hi);
+                }
+                __syncthreads();
+            }
+        }
+        const double4 A4 = b.sph[i];
+        uint32_t prank = b.no_pairs ? 0u : b.pair_off[row];
+        for (uint32_t base = 0; base < cnt; base += kBigThreads) {
+            const uint32_t e = base + tid;
+            bool gen = false;
+            uint32_t bid = 0;
+            if (e < cnt) {
+                bid = b.nb_id[off + e];
+                const uint32_t bc = b.periodic ? bid % n : bid;
+                gen = !b.no_pairs && !same_group(b.groups, b.n_groups, i, bc) && ((b.periodic && bid >= n) || i < bid);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, gen);
+            if (lane == 0) s_warp[w] = __popc(m);
+            __syncthreads();
+            uint32_t before = 0, total = 0;
+            for (int q = 0; q < kBigThreads / 32; ++q) {
+                before += q < w ? s_warp[q] : 0u;
+                total += s_warp[q];
+            }
+            if (e < cnt) {
+                int32_t pidx = -1;
+                if (gen) {
+                    pidx = (int32_t)(prank + before + __popc(m & ((1u << lane) - 1u)));
+                    b.pair_a[pidx] = i;
+                    b.pair_e[pidx] = off + e;
+                }
+                if (!b.no_pairs) b.nb_pair[off + e] = pidx;
+                if (want_rel) {
+                    const double4 C = b.sph[b.nb_slot[off + e]];
+                    b.nb_rel[off + e] = make_float4((float)(C.x - A4.x), (float)(C.y - A4.y), (float)(C.z - A4.z),
+                                                    (float)C.w);
+                }
+            }
+            prank += total;
+            __syncthreads();
+        }
     }
 }
 
@@ -719,12 +810,16 @@ void launch_grid(const DevBufs& b, uint32_t ncell, uint32_t max_slots, uint32_t*
                                          b.c_slot, b.slot_is_id); count_launch();
 }
 void launch_search_count(const DevBufs& b, cudaStream_t s) {
+    cudaMemsetAsync(b.d_big_count, 0, sizeof(uint32_t), s);
     int gb = grid_for(b.n, kSearchWarps, 148 * 64);
     k_search<false><<<gb, kSearchWarps * 32, 0, s>>>(b, 0); count_launch();
 }
-void launch_search_fill(const DevBufs& b, int want_rel, cudaStream_t s) {
+void launch_search_fill(const DevBufs& b, int want_rel, uint32_t n_big, cudaStream_t s) {
     int gb = grid_for(b.n, kSearchWarps, 148 * 64);
     k_search<true><<<gb, kSearchWarps * 32, 0, s>>>(b, want_rel); count_launch();
+    if (n_big) {
+        k_big_sort<<<n_big < 148u * 2u ? n_big : 148u * 2u, kBigThreads, 0, s>>>(b, want_rel); count_launch();
+    }
 }
 void launch_cells(const DevBufs& b, float cell_band, int only_dirty, cudaStream_t s) {
     int gb = grid_for(b.n, kCellWarps, 148 * 32);

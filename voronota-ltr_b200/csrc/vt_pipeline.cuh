@@ -34,7 +34,8 @@ enum PairStatus : uint8_t {
     kOverflow = 4,  // contour needed more than 32 points: recompute serially
 };
 
-constexpr int kSortCap = 256;       // neighbour list capacity of the warp sort buffer
+constexpr int kSortCap = 256;       // neighbour list capacity of the warp sort buffer (longer
+                                    // lists go through the block sort, without a limit)
 constexpr int kSerialCap = 256;     // contour capacity of the serial fallback
 
 // Host-visible bounding-box reduction result.
@@ -125,6 +126,10 @@ struct DevBufs {
     const uint32_t* frontier;  // search only these balls; per-ball CSR arrays are then
     uint32_t n_frontier;       // indexed by frontier position (excluded stays per ball)
     int no_pairs;              // fill pass writes the neighbour lists only
+    // rows with more neighbours than the warp sort holds (kSortCap): listed by the count
+    // pass, written unsorted by the fill pass, then sorted and paired by a block per row
+    uint32_t* big_list;
+    uint32_t* d_big_count;
     int slot_is_id;            // grid slots carry reference ids as their sph index
     int detached_excl;         // cells: an empty list is detached only when not excluded
     // batched structures (null for one structure): ball -> structure, the structure's
@@ -180,6 +185,9 @@ __device__ __forceinline__ void cell_from_sums(uint32_t count, double arc, doubl
     if (cell_band > 0.f && arc > 0.0) {
         double tol_sa = (double)cell_band * count;
         if (fabs(spos - sneg) <= tol_sa + 1e-10) *unsure = true;
+        // a nearly buried ball (positive dominance, 4 pi - (spos - sneg) about 0): the
+        // sign of its SAS area, i.e. whether it is exposed at all, is within the band
+        if (spos > sneg && fabs(fma(4.0, kPiD, -(spos - sneg))) <= tol_sa) *unsure = true;
         double sas_g = spos > sneg ? fma(4.0, kPiD, -(spos - sneg)) * r * r : (sneg - spos) * r * r;
         double vol_g = sas_g * r / 3.0 + ppos - pneg;
         double full_g = 4.0 / 3.0 * kPiD * r * r * r;
@@ -219,7 +227,8 @@ void launch_images(const DevBufs& b, double reach, const BBox* d_bbox, uint32_t*
 void launch_grid(const DevBufs& b, uint32_t ncell, uint32_t max_slots, uint32_t* scan_tmp, size_t scan_tmp_words,
                  cudaStream_t s);
 void launch_search_count(const DevBufs& b, cudaStream_t s);
-void launch_search_fill(const DevBufs& b, int want_rel, cudaStream_t s);
+// n_big: rows the count pass listed in big_list (read back by the caller)
+void launch_search_fill(const DevBufs& b, int want_rel, uint32_t n_big, cudaStream_t s);
 // cell_band > 0 (FP32 inputs): balls whose compute_sas branch decisions lie within
 // cell_band radians per contributing contact of their thresholds go to cell_redo_list.
 // only_dirty: recompute only balls flagged in ball_dirty.

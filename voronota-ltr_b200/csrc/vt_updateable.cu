@@ -43,6 +43,7 @@ enum Word : int {
     kWMore = 8,      // new neighbours of changed balls not yet affected
     kWOne = 9,       // constant 1 (a list length)
     kWId = 10,       // a one-element id list
+    kWBig = 11,      // rows of a search longer than the warp sort buffer
     kWords = 16,
 };
 
@@ -184,7 +185,7 @@ struct vt_updateable {
     DBuf<double4> sph, gsph, c_pos, changed_ball;
     DBuf<uint32_t> slot_id, gslot_id, cell_count, cell_start, cell_cursor, c_id, c_slot;
     DBuf<BBox> bbox_parts, bbox;
-    DBuf<uint32_t> img_cnt, img_off, scan_tmp, words;
+    DBuf<uint32_t> img_cnt, img_off, scan_tmp, words, big_rows;
     DBuf<uint64_t> ids_in;
     DBuf<double> src_in;
     DBuf<uint32_t> flags, flags_off, mark, row_of, list1, more_list, nflags, noff;
@@ -356,11 +357,15 @@ struct vt_updateable {
         b.no_pairs = 1;
         b.nb_cnt = L.cnt.p;
         b.nb_off = L.off.p;
+        big_rows.ensure(rows + 1);
+        b.big_list = big_rows.p;
+        b.d_big_count = w(kWBig);
         launch_search_count(b, stream);
         ensure_scan(rows + 1);
         scan_u32(L.cnt.p, L.off.p, rows, scan_tmp.p, stream);
         VT_CUDA(cudaMemcpyAsync(h_words, L.off.p + rows, 4, cudaMemcpyDeviceToHost, stream));
         VT_CUDA(cudaMemcpyAsync(h_words + 1, w(kWErr), 4, cudaMemcpyDeviceToHost, stream));
+        VT_CUDA(cudaMemcpyAsync(h_words + 3, w(kWBig), 4, cudaMemcpyDeviceToHost, stream));
         sync();
         if (h_words[1] & kErrNeighborCap) {
             set_last_error("a ball has more than 256 neighbour candidates");
@@ -374,7 +379,7 @@ struct vt_updateable {
         b.nb_slot = L.id.p;  // slots are ids: both writes store the same value
         b.nb_val = L.val.p;
         b.nb_rel = fp32 ? L.rel.p : nullptr;
-        launch_search_fill(b, fp32 ? 1 : 0, stream);
+        launch_search_fill(b, fp32 ? 1 : 0, h_words[3], stream);
         L.E = E;
         return VT_OK;
     }

@@ -47,6 +47,10 @@ class VoronotaError(RuntimeError):
         self.status = status
 
 
+class VoronotaInputError(VoronotaError, ValueError):
+    """Invalid input (VT_ERR_INVALID): a ValueError, as the reference's Python module raises."""
+
+
 class VtStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in (
         "num_balls", "num_slots", "num_entries", "num_pairs", "num_contacts", "num_cells",
@@ -100,6 +104,15 @@ def library():
     L.vt_result_edges.argtypes = [_vp, _u32p, _f64p]
     L.vt_engine_set_network.argtypes = [_vp, ctypes.c_int]
     L.vt_engine_set_fp32_min_pairs.argtypes = [_vp, ctypes.c_uint64]
+    L.vt_compute_solvent_spheres.argtypes = [_f64p, ctypes.c_uint64, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                             _f64p, ctypes.c_int, ctypes.POINTER(_vp)]
+    L.vt_icosahedron.argtypes = [ctypes.c_int, _f64p]
+    L.vt_icosahedron.restype = ctypes.c_int
+    L.vt_solvent_count.argtypes = [_vp]
+    L.vt_solvent_count.restype = ctypes.c_uint64
+    L.vt_solvent_get.argtypes = [_vp, _f64p, _f64p, _f64p, _u32p]
+    L.vt_solvent_free.argtypes = [_vp]
+    L.vt_solvent_free.restype = None
     L.vt_engine_create.argtypes = [ctypes.c_int, ctypes.POINTER(_vp)]
     L.vt_engine_destroy.argtypes = [_vp]
     L.vt_engine_destroy.restype = None
@@ -171,7 +184,7 @@ def _check(status: int) -> None:
     if status != VT_OK:
         L = library()
         msg = L.vt_last_error().decode(errors="replace") or L.vt_status_string(status).decode()
-        raise VoronotaError(status, msg)
+        raise (VoronotaInputError if status == VT_ERR_INVALID else VoronotaError)(status, msg)
 
 
 def _precision_code(precision) -> int:
@@ -404,6 +417,67 @@ def grad(balls, probe, w_sas=None, u_contact=None, periodic_box=None, precision=
                      None if w is None else w.ctypes.data_as(_f64p), None if u is None else u.ctypes.data_as(_f64p),
                      0 if u is None else len(u), out.ctypes.data_as(_f64p)))
     return out
+
+
+def icosahedron_directions(depth: int) -> np.ndarray:
+    """Sample directions of compute_solvent_spheres (SubdividedIcosahedron,
+    subdivided_icosahedron.rs:53-125) as computed by the library (host code)."""
+    L = library()
+    k = L.vt_icosahedron(int(depth), None)
+    out = np.empty((k, 3))
+    L.vt_icosahedron(int(depth), out.ctypes.data_as(_f64p))
+    return out
+
+
+class SolventSpheres:
+    """compute_solvent_spheres output as arrays: xyz (S, 3), radius, weight (S,), parent
+    (S,) ball index."""
+
+    def __init__(self, xyz, radius, weight, parent):
+        self.xyz, self.radius, self.weight, self.parent = xyz, radius, weight, parent
+
+    def __len__(self):
+        return len(self.weight)
+
+    def to_list(self) -> list[dict]:
+        """solvent_spheres_to_list (python.rs:326-342)."""
+        return [{"x": p[0], "y": p[1], "z": p[2], "radius": r, "weight": w, "parent_index": i}
+                for p, r, w, i in zip(self.xyz.tolist(), self.radius.tolist(), self.weight.tolist(),
+                                      self.parent.tolist())]
+
+
+def compute_solvent_spheres_result(balls, probe, volume_probe=None, subdivision_depth=None, periodic_box=None,
+                                   precision="fp32") -> SolventSpheres:
+    """compute_solvent_spheres returning arrays (see :func:`compute_solvent_spheres`)."""
+    L = library()
+    depth = 2 if subdivision_depth is None else int(subdivision_depth)
+    if depth < 0:  # the reference takes a u32
+        raise OverflowError("can't convert negative int to unsigned")
+    x = parse_balls(balls)
+    pb = None if periodic_box is None else parse_periodic_box(periodic_box)
+    h = _vp()
+    _check(L.vt_compute_solvent_spheres(x.ctypes.data_as(_f64p), x.shape[0], float(probe),
+                                        0.0 if volume_probe is None else float(volume_probe), depth,
+                                        None if pb is None else pb.ctypes.data_as(_f64p), _precision_code(precision),
+                                        ctypes.byref(h)))
+    try:
+        S = int(L.vt_solvent_count(h))
+        xyz, rad, w, par = np.empty((S, 3)), np.empty(S), np.empty(S), np.empty(S, np.uint32)
+        _check(L.vt_solvent_get(h, xyz.ctypes.data_as(_f64p), rad.ctypes.data_as(_f64p), w.ctypes.data_as(_f64p),
+                                par.ctypes.data_as(_u32p)))
+    finally:
+        L.vt_solvent_free(h)
+    return SolventSpheres(xyz, rad, w, par)
+
+
+def compute_solvent_spheres(balls, probe, volume_probe=None, subdivision_depth=None, periodic_box=None,
+                            precision="fp32") -> list[dict]:
+    """Weighted pseudo-solvent spheres on the exposed surface (python.rs:344-392): list of
+    dicts with x, y, z, radius, weight, parent_index.  Both tessellations run on the GPU
+    (``precision`` as for compute_tessellation); the sampling and the keep test between
+    them run in FP64 on the device with the reference's arithmetic."""
+    return compute_solvent_spheres_result(balls, probe, volume_probe, subdivision_depth, periodic_box,
+                                          precision).to_list()
 
 
 class BatchResult:
@@ -702,5 +776,6 @@ class UpdateableTessellation:
 
 
 __all__ = ["compute_tessellation", "compute_tessellation_result", "compute_contacts_only",
+           "compute_solvent_spheres", "compute_solvent_spheres_result", "SolventSpheres", "VoronotaInputError",
            "compute_contacts_only_result", "compute_batch", "BatchResult", "grad", "Engine", "Result", "UpdateableTessellation", "VoronotaError",
            "library", "parse_balls", "parse_periodic_box"]
