@@ -21,7 +21,8 @@ replicas, no collective on the data path; value = all ranks' balls / max-over-ra
 (voronota_ltr.replicas).  The updateable, batched and differentiation legs run on every
 rank on its own inputs and report max-over-ranks times; the network leg times
 compute_tessellation with with_cell_vertices on the main structure and checks its
-vertices and edges against the oracle.
+vertices and edges against the oracle; the solvent-sphere leg times compute_solvent_spheres
+through the C ABI against the CPU oracle.
 
 ``--impl reference`` times the reference's algorithm on the host cores instead (the CPU
 oracle port: the Rust reference cannot be built here) on the same workload.
@@ -61,6 +62,8 @@ def parse_args():
     ap.add_argument("--upd-n", type=int, default=200_000, help="balls of the periodic updateable trajectory")
     ap.add_argument("--no-upd", action="store_true", help="skip the updateable trajectory leg")
     ap.add_argument("--no-network", action="store_true", help="skip the tessellation network leg")
+    ap.add_argument("--no-solvent", action="store_true", help="skip the solvent-sphere leg")
+    ap.add_argument("--solvent-n", type=int, default=20_000, help="balls of the solvent-sphere leg")
     ap.add_argument("--tuning", default=None,
                     help="warps,cell_scale,chunk of the FP32 contact launch instead of autotuning (profiling)")
     ap.add_argument("--batch-count", type=int, default=4096, help="structures of the batched leg")
@@ -517,6 +520,44 @@ def network_leg(args, rank, torch, V, R, balls):
     return out
 
 
+def solvent_leg(args, rank, torch, V, R):
+    """compute_solvent_spheres on a lattice structure (depth 2, probe 1.4): the whole call
+    through the C ABI from host arrays (two tessellations and the sampling between them),
+    against the CPU oracle's time and output on rank 0."""
+    n = args.solvent_n
+    balls = workload(n, 11 + rank)
+    for _ in range(2):
+        V.compute_solvent_spheres_result(balls, PROBE, precision="fp32")
+    ts = {}
+    res = {}
+    for prec in ("fp32", "fp64"):
+        t = []
+        for _ in range(5):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res[prec] = V.compute_solvent_spheres_result(balls, PROBE, precision=prec)
+            t.append(time.perf_counter() - t0)
+        ts[prec] = R.max(1e3 * statistics.median(t))
+    out = {"workload": f"lattice {n} balls, probe 1.4, subdivision depth 2 (162 directions)",
+           "spheres": len(res["fp32"]), "ms_fp32": round(ts["fp32"], 3), "ms_fp64": round(ts["fp64"], 3)}
+    if rank == 0:
+        import oracle as O
+
+        t0 = time.perf_counter()
+        o = O.solvent_spheres(balls, PROBE)
+        out["cpu_oracle_ms"] = round(1e3 * (time.perf_counter() - t0), 1)
+        out["cpu_cores"] = O.get_threads()
+        g = res["fp64"]
+        out["fp64_positions_parents_match_oracle"] = bool(len(g) == len(o.weight) and np.array_equal(g.xyz, o.xyz)
+                                                          and np.array_equal(g.parent.astype(np.uint64), o.parent))
+        g32 = res["fp32"]
+        if len(g32) == len(o.weight) and len(g) == len(o.weight):
+            out["fp64_weight_max_rel_err"] = float((np.abs(g.weight - o.weight) / (1 + np.abs(o.weight))).max(initial=0))
+            out["fp32_total_weight_rel_err"] = float(abs(g32.weight.sum() - o.weight.sum()) / o.weight.sum())
+            out["fp32_positions_match_oracle"] = bool(np.array_equal(g32.xyz, o.xyz))
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -648,6 +689,7 @@ def run_ours(args):
     bat = None if args.no_batch else batched_leg(args, rank, torch, V, R)
     grd = None if args.no_grad else grad_leg(args, rank, torch, V, R)
     net = None if args.no_network else network_leg(args, rank, torch, V, R, balls)
+    sol = None if args.no_solvent else solvent_leg(args, rank, torch, V, R)
 
     if rank == 0:
         line = {
@@ -679,6 +721,7 @@ def run_ours(args):
             "batched": bat,
             "differentiation": grd,
             "network": net,
+            "solvent_spheres": sol,
         }
         print(json.dumps(line), flush=True)
     eng.close()

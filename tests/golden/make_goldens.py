@@ -8,6 +8,9 @@ src/input/mod.rs:117-143: the last four columns are x y z r) and the centrality 
 
 * ``balls_cs_1x1.npy``, ``balls_2zsk.npy``, ``balls_3dlb.npy`` -- (N, 4) float64 x y z r
 * ``central_golden.npy`` -- (20, 3) int64 rows (id_a, id_b, central)
+* ``assembly_1ctf.pdb1.gz``, ``assembly_1ctf.cif.gz``, ``1ctf_pdb_cells_reference.tsv.gz``,
+  ``custom_radii.txt.gz`` -- the reference's file-input test data (tests/data), gzipped,
+  for the file front end's end-to-end goldens
 
 The known answers the tests assert (counts and totals) are the numbers the reference's
 own tests assert; they are kept in ``goldens.json`` with the file:line they come from.
@@ -54,6 +57,18 @@ KNOWN_ANSWERS = {
     },
     "centrality": {"source": "tests/centrality_golden.rs:12-66; tests/data/central_golden.tsv",
                    "probe": 1.4, "radius": 1.5},
+    "file_1ctf_pdb": {"source": "tests/pdb_mmcif.rs:12-43,99-153; tests/test_python.py:303-315",
+                      "probe": 1.4, "balls": 492, "balls_without_hetero": 487, "contacts": 3078, "cells": 492,
+                      "total_sas_area": 4097.64, "total_contact_area": 10663.91, "tol": 0.01,
+                      "per_atom_tol": 0.01},
+    "file_1ctf_cif": {"source": "tests/pdb_mmcif.rs:45-97; tests/test_python.py:317-342",
+                      "probe": 1.4, "balls": 984, "contacts": 6354, "cells": 984},
+    "file_1ctf_custom_radii": {"source": "tests/pdb_mmcif.rs:216-246", "probe": 1.4, "balls": 984,
+                               "contacts": 6354, "total_sas_area": 7094.42, "total_contact_area": 21423.54,
+                               "tol": 0.01},
+    "radii_lookups": {"source": "tests/pdb_mmcif.rs:130-152",
+                      "cases": [["ALA", "CA", 1.90], ["ALA", "N", 1.70], ["ALA", "C", 1.75], ["ALA", "O", 1.49],
+                                ["ALA", "CB", 1.92], ["ARG", "NH1", 1.62], ["ZN", "ZN", 0.74]]},
 }
 
 
@@ -85,6 +100,13 @@ def main(ref_root):
             a, b, c = line.split()[:3]
             rows.append((int(a), int(b), int(c)))
     np.save(os.path.join(HERE, "central_golden.npy"), np.array(rows, dtype=np.int64))
+    import gzip
+    for name in ("assembly_1ctf.pdb1", "assembly_1ctf.cif", "1ctf_pdb_cells_reference.tsv", "custom_radii.txt"):
+        with open(os.path.join(ref_root, "tests", "data", name), "rb") as f:
+            data = f.read()
+        with gzip.GzipFile(os.path.join(HERE, name + ".gz"), "wb", mtime=0) as g:
+            g.write(data)
+        print(name, len(data))
     with open(os.path.join(HERE, "goldens.json"), "w") as f:
         json.dump(KNOWN_ANSWERS, f, indent=1, sort_keys=True)
     print("centrality rows", len(rows))

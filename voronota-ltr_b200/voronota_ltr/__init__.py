@@ -779,3 +779,8 @@ __all__ = ["compute_tessellation", "compute_tessellation_result", "compute_conta
            "compute_solvent_spheres", "compute_solvent_spheres_result", "SolventSpheres", "VoronotaInputError",
            "compute_contacts_only_result", "compute_batch", "BatchResult", "grad", "Engine", "Result", "UpdateableTessellation", "VoronotaError",
            "library", "parse_balls", "parse_periodic_box"]
+
+
+from .io import compute_tessellation_from_file  # noqa: E402  (file front end, voronota_ltr/io.py)
+
+__all__ += ["compute_tessellation_from_file"]
