@@ -160,11 +160,12 @@ int vt_engine_stats(const vt_engine* e, vt_stats* out);
  * more conservative (more pairs recomputed in FP64). */
 int vt_engine_set_fp32_band(vt_engine* e, double ulps);
 int vt_engine_set_timing(vt_engine* e, int on);
-/* FP32 mode runs the FP32 contact kernel only when a call has at least this many candidate
- * pairs (default 8192), and the FP64 kernel below it.  The FP32 kernel's absolute error
- * floor (about 5e-7 sr per solid angle, from float rounding of coordinates relative to the
- * ball centre) is above 1e-6 of the total SAS area of a small structure, and a small call
- * is latency bound, so FP64 costs it nothing measurable.  0 forces the FP32 kernel. */
+/* FP32 mode runs the FP32 contact kernel only when a call (or, in a batch, a structure)
+ * has at least this many candidate pairs (default 2048, about 130 balls), and the FP64
+ * kernel below it.  A tiny structure's total SAS area is the sum of few contacts, so the
+ * FP32 rounding of their solid angles is not averaged out (it adds up coherently on a
+ * symmetric input), and such a call is latency bound, so FP64 costs it nothing
+ * measurable.  0 forces the FP32 kernel. */
 int vt_engine_set_fp32_min_pairs(vt_engine* e, uint64_t min_pairs);
 int vt_engine_stage_times(const vt_engine* e, double* ms);
 

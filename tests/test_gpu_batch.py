@@ -5,7 +5,7 @@ it alone: the batched path runs the same kernels over a concatenated ball array 
 one grid per structure, so contacts (ids local to the structure, order, central bits,
 areas, arc lengths) and cells are compared bit for bit with single GPU calls, in both
 precisions; per-structure totals (a different summation tree) within 1e-12 relative.
-FP32 mode computes a structure with fewer than 8192 candidate pairs in FP64, alone or in
+FP32 mode computes a structure with fewer than 2048 candidate pairs in FP64, alone or in
 a batch (there its pairs go to the FP64 recompute), so the two agree bit for bit.
 Structures are also checked against the oracle, and uneven sizes, empty structures and
 malformed offsets are covered.

@@ -154,7 +154,7 @@ def test_serial_fallback_long_contours(prec):
 
 
 def test_fp32_kernel_forced_on_small_inputs():
-    """The FP32 kernel (forced below its default minimum of 8192 candidate pairs) on the
+    """The FP32 kernel (forced below its default minimum of 2048 candidate pairs) on the
     small golden structures and edge cases: pair sets and central bits exact, values within
     the FP32 tolerances."""
     cases = [(RING_17, 1.0, None), (RING_17, G["ring17_periodic"]["probe"], {"corners": G["ring17_periodic"]["corners"]}),

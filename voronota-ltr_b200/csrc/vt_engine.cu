@@ -366,7 +366,7 @@ struct vt_engine {
     std::vector<uint32_t> h_crange, h_mrange;
     std::vector<double> h_btot;
     double fp32_band_ulps = 16.0;  // FP32 point error budget E, in float ulps of the pair scale
-    uint64_t fp32_min_pairs = 8192;  // FP32 mode: fewer candidate pairs run the FP64 kernel
+    uint64_t fp32_min_pairs = 2048;  // FP32 mode: fewer candidate pairs run the FP64 kernel
     // launch configuration, set by the autotuner or by hand
     int c32_warps = 4;        // warps per block of the FP32 contact kernel
     int c32_chunk = 0;        // > 0: persistent FP32 contact launch, pairs taken in chunks

@@ -344,15 +344,17 @@ __device__ __forceinline__ T min_dihedral(V3<T> o, V3<T> a, V3<T> b1, V3<T> b2) 
     V3<T> d2 = b2 - (o + oa * dot(oa, b2 - o));
     return vec_angle(d1, d2);
 }
-// pi - min_dihedral_angle, computed directly (FP32 turn terms of the solid angle); the
-// unit vector uses correctly rounded square root and division.
+// pi - min_dihedral_angle for the FP32 turn terms of the solid angle, evaluated in double
+// from the widened float points: the dihedral at edge o-a between the half-planes
+// towards b1 and b2 is the angle between the normals (a-o) x (b1-o) and (a-o) x (b2-o).
+// Products of floats are exact in double, so a point b next to a (a vertex beside a short
+// contour edge) loses nothing to the cancellation of a float projection; the turn sum is
+// then the solid angle of the polygon with the float vertices.
 __device__ __forceinline__ double dihedral_supplement(V3<float> o, V3<float> a, V3<float> b1, V3<float> b2) {
-    V3<float> ao = a - o;
-    float l = __fsqrt_rn(norm2(ao));
-    V3<float> oa = {__fdiv_rn(ao.x, l), __fdiv_rn(ao.y, l), __fdiv_rn(ao.z, l)};
-    V3<float> d1 = b1 - (o + oa * dot(oa, b1 - o));
-    V3<float> d2 = b2 - (o + oa * dot(oa, b2 - o));
-    return vec_supplement(d1, d2);
+    const V3<double> O = widen(o);
+    const V3<double> ax = widen(a) - O, u1 = widen(b1) - O, u2 = widen(b2) - O;
+    const V3<double> n1 = cross(ax, u1), n2 = cross(ax, u2);
+    return atan2(norm(cross(n1, n2)), -dot(n1, n2));
 }
 
 }  // namespace vt

@@ -602,7 +602,7 @@ class Engine:
 
     def set_fp32_min_pairs(self, min_pairs: int):
         """FP32 mode runs the FP32 contact kernel only from this many candidate pairs
-        (default 8192; FP64 below); 0 forces the FP32 kernel."""
+        (default 2048; FP64 below); 0 forces the FP32 kernel."""
         _check(self._L.vt_engine_set_fp32_min_pairs(self._h, int(min_pairs)))
 
     def set_network(self, on: bool = True):
