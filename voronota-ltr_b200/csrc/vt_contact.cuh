@@ -46,8 +46,6 @@ namespace vt {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr float kF32Eps = 1.1920929e-7f;
-// FP32: contour edges shorter than kShortEdge * E send the pair to FP64
-constexpr float kShortEdge = 256.f;
 
 template <typename T>
 __device__ __forceinline__ T wsum(T v) {
@@ -537,6 +535,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
     }
 
     T sum_arc = 0, area = 0;
+    T area_tol = 0;  // FP32: band of the area <= 0 test (an uncut circle is far from it)
     V3<T> bary = mk<T>(0, 0, 0);
     bool on = false;
     T ang_err = 0;  // FP32: bound on this lane's arc-angle error
@@ -734,10 +733,15 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             if (q.ang > (T)0) t2 = g.ic.r * g.ic.r * (q.ang - sin(q.ang)) * (T)0.5;
         }
         area = lsum2(t, t2, len);
+        if constexpr (F) {
+            // moving each vertex by at most |d| changes the polygon area by at most |d| times
+            // the perimeter and an arc segment by at most 2 r |d|: the band of area <= 0
+            // is 4 E (perimeter + 2 r per arc), E the point error budget
+            T side = on ? norm(v.p - q.p) + (q.ang > (T)0 ? (T)2 * g.ic.r : (T)0) : (T)0;
+            area_tol = 4.f * e0 * wsum(side);
+        }
     }
     // area <= 0 -> None (contact.rs:329-331)
-    T area_tol = 0;
-    if constexpr (F) area_tol = 8.f * (float)kPi * g.ic.r * e0;
     bool area_none = d.less_eq(area, (T)0, area_tol);
     VT_SITE(9);
     if (area_none) {
@@ -763,8 +767,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                 T eerr = 0;
                 if constexpr (F) {
                     eerr = 4.f * e0;
-                    // a short edge's FP32 direction (and the turn terms at its ends) is unreliable
-                    if (el < kShortEdge * e0) d.unsure = true;
                 }
                 if (!d.less(el, fe, eerr)) {
                     V3<T> u = edge / el;
