@@ -10,7 +10,8 @@ geometry with FP64 recomputation of band pairs.  One step = one full tessellatio
          launching stream; a 256 MiB buffer is written between steps, outside the
          events, to flush the 126 MB L2)
   e2e    balls/s through the public C ABI (vt_compute_tessellation via the Python
-         front end) from pinned host memory, results copied back to host arrays
+         front end) from pinned host memory, results copied back to host arrays; wall
+         clock per call, median over the timed steps (mean and extremes reported beside)
   roofline  the contact kernel (the dominant kernel): algorithmic bytes per launch /
          its CUDA-event duration, against the measured HBM copy bandwidth
   cpu_baseline  the CPU oracle (a restatement of the reference's Rust code; Rust is not
@@ -669,7 +670,9 @@ def run_ours(args):
         res = V.compute_tessellation_result(host, PROBE, precision="fp32")
         e2e_t.append(time.perf_counter() - t0)
     barrier()
-    e2e_ms = max_over_ranks(1e3 * sum(e2e_t) / len(e2e_t))
+    # median over the steps: the host side of a shared machine shows rare stalls of a few
+    # hundred ms (a 197 ms step among 5.9 ms ones) that a mean would turn into the number
+    e2e_ms = max_over_ranks(1e3 * statistics.median(e2e_t))
     C, M = len(res.id_a), len(res.cell_index)
     d2h = C * (4 + 4 + 8 + 8 + 1) + M * (4 + 8 + 8) + 3 * 8
     h2d = balls.nbytes
@@ -700,7 +703,10 @@ def run_ours(args):
                        "balls_per_gpu": args.n, "probe": PROBE, "parallelism": f"replicas x{world}",
                        "l2": "256 MiB buffer written between timed steps (outside the per-step events)"},
             "e2e": {"value": world * args.n / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h, "ms_per_step_median": round(e2e_ms, 3),
+                    "ms_per_step_mean": round(1e3 * sum(e2e_t) / len(e2e_t), 3),
+                    "ms_per_step_min_median_max": [round(1e3 * x, 3) for x in
+                                                   (min(e2e_t), statistics.median(e2e_t), max(e2e_t))]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": "k_contact32",
                          "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": fp32["contact_ms"],

@@ -368,8 +368,10 @@ struct vt_engine {
     double fp32_band_ulps = 16.0;  // FP32 point error budget E, in float ulps of the pair scale
     uint64_t fp32_min_pairs = 2048;  // FP32 mode: fewer candidate pairs run the FP64 kernel
     // launch configuration, set by the autotuner or by hand
-    int c32_warps = 4;        // warps per block of the FP32 contact kernel
-    int c32_chunk = 0;        // > 0: persistent FP32 contact launch, pairs taken in chunks
+    // launch configuration of the FP32 contact kernel until the autotuner or the caller
+    // sets one: what the autotuner picks on protein-like inputs of 20k-200k balls
+    int c32_warps = 2;        // warps per block of the FP32 contact kernel
+    int c32_chunk = 4;        // > 0: persistent FP32 contact launch, pairs taken in chunks
     double cell_scale = 1.0;  // grid cell edge / the minimum edge (2 max R + 0.25)
     // state of the last call
     vt_stats stats{};
