@@ -292,13 +292,15 @@ struct WarpContact {
 
 // Solid angle (contact.rs:797-848) summed over the warp's contour.  ea0 / ea1 bound the
 // arc-angle errors of the previous and the own point (FP32).  FP64 follows the reference
-// term by term.  FP32 computes each turn term pi - dihedral as the supplement directly
+// term by term (half = 0: lanes hold the points).  FP32 with half != 0: each half-warp holds
+// the points of one side (contours of at most 16 points), summed within the half.  FP32
+// computes each turn term pi - dihedral as the supplement directly
 // (no float rounding of pi, which would bias every solid angle and so every SAS area)
 // and sums the terms in double.
 template <typename T, bool F>
 __device__ __forceinline__ double solid_angle(Dec<T, F>& d, const Sph<T>& a, const Sph<T>& b, const Sph<T>& ic,
                                               const Pt<T>& p0, const Pt<T>& p1, const Pt<T>& p2, bool on, int len,
-                                              T e0, T ea0, T ea1) {
+                                              T e0, T ea0, T ea1, int half = 0) {
     double sa;
     if (len == 0) {
         if constexpr (F)
@@ -343,7 +345,13 @@ __device__ __forceinline__ double solid_angle(Dec<T, F>& d, const Sph<T>& a, con
             }
         }
         if constexpr (F) {
-            sa = kTau - wsum(t + (double)t2);
+            // the sum over the lanes of this side: all 32, or 16 when each half-warp holds
+            // one side (half != 0)
+            double v = t + (double)t2;
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+            if (!half) v += __shfl_xor_sync(kFull, v, 16);
+            sa = kTau - v;
         } else {
             sa = kTau - lsum2(t, t2, len);
         }
@@ -803,12 +811,36 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
         Pt<T> p2 = shfl_pt(q, nxl);
         T ea0 = 0;
         if constexpr (F) ea0 = __shfl_sync(kFull, ang_err, pvl);
-        // one inlined copy of the solid angle for both sides (a, then b)
+        // one inlined copy of the solid angle for both sides.  FP64: side a, then side b.
+        // FP32: a contour of at most 16 points (almost all) computes both sides at once,
+        // lanes 0-15 side a and lanes 16-31 side b on the same points; longer ones take two
+        // passes with a lane per point.
         double sab[2];
+        if constexpr (F) {
+            const int split = len <= 16 ? 1 : 0;
 #pragma unroll 1
-        for (int side = 0; side < 2; ++side) {
-            const Sph<T> s0 = side ? g.B : g.A, s1 = side ? g.A : g.B;
-            sab[side] = solid_angle(d, s0, s1, g.ic, p0, q, p2, on, len, e0, ea0, ang_err);
+            for (int pass = 0; pass < 2 - split; ++pass) {
+                const int side = split ? (lane >> 4) : pass;
+                const int L = split ? (lane & 15) : lane;
+                const int pv = L > 0 ? L - 1 : (len > 0 ? len - 1 : 0);
+                const int nx = len > 0 ? (L + 1 < len ? L + 1 : 0) : 0;
+                const Pt<T> m1 = shfl_pt(q, L), m0 = shfl_pt(q, pv), m2 = shfl_pt(q, nx);
+                const T e1 = __shfl_sync(kFull, ang_err, L), em = __shfl_sync(kFull, ang_err, pv);
+                const Sph<T> s0 = side ? g.B : g.A, s1 = side ? g.A : g.B;
+                const double v = solid_angle(d, s0, s1, g.ic, m0, m1, m2, L < len, len, e0, em, e1, split);
+                if (split) {
+                    sab[0] = __shfl_sync(kFull, v, 0);
+                    sab[1] = __shfl_sync(kFull, v, 16);
+                } else {
+                    sab[pass] = v;
+                }
+            }
+        } else {
+#pragma unroll 1
+            for (int side = 0; side < 2; ++side) {
+                const Sph<T> s0 = side ? g.B : g.A, s1 = side ? g.A : g.B;
+                sab[side] = solid_angle(d, s0, s1, g.ic, p0, q, p2, on, len, e0, ea0, ang_err);
+            }
         }
         const double sa = sab[0], sb = sab[1];
         VT_SITE(13);
