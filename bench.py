@@ -206,9 +206,10 @@ def updateable_leg(args, rank, torch, V, R):
     balls, box, moves = trajectory(n, warm + steps, rank)
     stream = torch.cuda.current_stream()
 
-    def run(precision, nsteps):
+    def run(precision, nsteps, adjoint=True):
         u = V.UpdateableTessellation(False, precision)
         u.set_stream(stream.cuda_stream)
+        u.set_adjoint(adjoint)
         d = torch.from_numpy(balls).cuda()
         torch.cuda.synchronize()
         u.init_device(d.data_ptr(), n, PROBE, box)
@@ -223,7 +224,8 @@ def updateable_leg(args, rank, torch, V, R):
             u.update_with_changed_device(d.data_ptr(), n, ti.data_ptr(), len(ids))
             e1.record(stream)
             st = u.stats()
-            u.grad_sas_device(0, dg.data_ptr())  # adjoint of the total SAS
+            if adjoint:
+                u.grad_sas_device(0, dg.data_ptr())  # adjoint of the total SAS
             e2.record(stream)
             e2.synchronize()
             if t >= warm:
@@ -236,6 +238,7 @@ def updateable_leg(args, rank, torch, V, R):
 
     u32, d32, ms32, aff, pairs, redo, adj32 = run("fp32", steps)
     _, _, ms64, _, _, _, adj64 = run("fp64", max(3, steps // 2))
+    _, _, ms32na, _, _, _, _ = run("fp32", steps, adjoint=False)
     eng = V.Engine()
     eng.set_stream(stream.cuda_stream)
     full = []
@@ -249,6 +252,7 @@ def updateable_leg(args, rank, torch, V, R):
         full.append(e0.elapsed_time(e1))
     eng.close()
     t32 = R.max(statistics.median(ms32))
+    t32na = R.max(statistics.median(ms32na))
     t64 = R.max(statistics.median(ms64))
     a32 = R.max(statistics.median(adj32))
     a64 = R.max(statistics.median(adj64))
@@ -258,6 +262,7 @@ def updateable_leg(args, rank, torch, V, R):
                     "moved by N(0, 0.05 A) per axis, then update_with_changed on the device",
         "steps": steps, "warmup": warm,
         "ms_per_update_fp32": t32, "ms_per_update_fp64": t64,
+        "ms_per_update_fp32_adjoint_off": t32na,
         "ms_adjoint_total_sas_fp32": a32, "ms_adjoint_total_sas_fp64": a64,
         "ms_per_step_update_plus_adjoint_fp32": t32 + a32,
         "ms_full_recompute_fp32": tfull, "speedup_vs_full_recompute": tfull / t32,

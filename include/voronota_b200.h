@@ -295,8 +295,14 @@ int vt_upd_affected_ids(vt_updateable* h, uint64_t* out);
 /* Adjoint of sum_i w_sas[i] SAS_i over the current state (no counterpart in the
  * reference; the gradient of vt_engine_grad_device restricted to SAS terms): d_w_sas (n
  * doubles on the device, NULL: all 1, the total SAS) and d_grad (n x 4 doubles on the
- * device, overwritten with dL/d(x, y, z, r)). */
+ * device, overwritten with dL/d(x, y, z, r)).  VT_ERR_INVALID when an operation since
+ * the last full computation ran with the adjoint off (vt_upd_set_adjoint). */
 int vt_upd_grad_sas(vt_updateable* h, const double* d_w_sas, double* d_grad);
+/* Whether operations record the arc moments behind vt_upd_grad_sas (on by default; no
+ * counterpart in the reference).  Off saves about a tenth of an update's time; the
+ * adjoint is then refused until a full computation (init, or an update past the
+ * full-reinit threshold) has run with it on again. */
+int vt_upd_set_adjoint(vt_updateable* h, int on);
 /* counters of the last operation: list entries, pairs recomputed, FP64 redo, cells */
 int vt_upd_stats(const vt_updateable* h, vt_stats* out);
 

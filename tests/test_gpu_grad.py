@@ -188,3 +188,40 @@ def test_updateable_sas_adjoint_periodic_finite_differences():
 
     for i, c in _coords(len(balls), 10, 13):
         _check_fd(g[i, c], loss, balls, i, c)
+
+
+def test_updateable_adjoint_switch():
+    """With the adjoint off the updates give the same summary and grad_sas is refused until
+    an init with it on; back on, the adjoint equals a handle that always had it."""
+    import torch
+    balls, side = W.periodic_box_balls(1500, seed=13)
+    box = {"corners": [(0.0, 0.0, 0.0), (side, side, side)]}
+    d = torch.from_numpy(balls).cuda()
+    on = V.UpdateableTessellation(precision="fp32")
+    off = V.UpdateableTessellation(precision="fp32")
+    off.set_adjoint(False)
+    on.init_device(d.data_ptr(), len(balls), 1.4, box)
+    off.init_device(d.data_ptr(), len(balls), 1.4, box)
+    rng = np.random.default_rng(5)
+    ids = np.sort(rng.choice(len(balls), 15, replace=False)).astype(np.int64)
+    d[torch.from_numpy(ids).cuda(), :3] += 0.05
+    ti = torch.from_numpy(ids).cuda()
+    on.update_with_changed_device(d.data_ptr(), len(balls), ti.data_ptr(), len(ids))
+    off.update_with_changed_device(d.data_ptr(), len(balls), ti.data_ptr(), len(ids))
+    a, b = on.summary(), off.summary()
+    assert np.array_equal(a.id_a, b.id_a) and np.array_equal(a.area, b.area)
+    assert np.array_equal(a.cell_sas_area, b.cell_sas_area)
+    g = torch.empty((len(balls), 4), dtype=torch.float64, device="cuda")
+    with pytest.raises(V.VoronotaError):
+        off.grad_sas_device(0, g.data_ptr())
+    off.set_adjoint(True)
+    off.update_with_changed_device(d.data_ptr(), len(balls), ti.data_ptr(), len(ids))  # no change: still refused
+    with pytest.raises(V.VoronotaError):
+        off.grad_sas_device(0, g.data_ptr())
+    off.init_device(d.data_ptr(), len(balls), 1.4, box)
+    off.grad_sas_device(0, g.data_ptr())
+    g_on = torch.empty_like(g)
+    fresh = V.UpdateableTessellation(precision="fp32")
+    fresh.init_device(d.data_ptr(), len(balls), 1.4, box)
+    fresh.grad_sas_device(0, g_on.data_ptr())
+    assert torch.equal(g, g_on)

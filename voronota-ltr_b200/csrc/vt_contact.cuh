@@ -184,7 +184,9 @@ __device__ __forceinline__ V3<float> plane_segment_e(Dec<float, true>& d, V3<flo
     d.band(dd - (float)kEps, 2.f * E);
     if (dd < (float)kEps) return a;
     if (norm(b - a) > kCondMax * dd) d.unsure = true;  // cut grazing the edge
-    float t = da / (da - db);
+    // a cut point is an output vertex: a correctly rounded division (the kernel's
+    // approximate one is biased, moving every cut point the same way along its edge)
+    float t = __fdiv_rn(da, da - db);
     return a + (b - a) * t;
 }
 // intersect_segment_with_circle (geometry.rs:258-280)

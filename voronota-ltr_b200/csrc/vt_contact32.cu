@@ -71,13 +71,14 @@ __device__ __forceinline__ void contact_pair32(const DevBufs& b, uint32_t p, flo
 }
 
 // W warps per block (chosen by the engine's autotuner); the minimum resident blocks keep
-// the register budget of a thread at 64 (80 with the arc moments) for every W.
+// the register budget of a thread at 64 for every W (the arc-moment variant spills a few
+// bytes there, which costs less than the occupancy 80 registers would take).
 // queue == null: a grid-stride loop over the pairs.  Otherwise a persistent launch (one
 // wave of resident blocks) whose warps take chunks of `chunk` consecutive pairs from the
 // work counter *queue (zero at launch), so that costly pairs do not leave a tail of idle
 // SMs.
 template <bool FULL, bool XM, int W>
-__global__ void __launch_bounds__(W * 32, (XM ? 6 : VT_C32_MINB) * 4 / W)
+__global__ void __launch_bounds__(W * 32, VT_C32_MINB * 4 / W)
     k_contact32(DevBufs b, uint32_t P, float band, uint32_t* queue, uint32_t chunk) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     // one loop (and one inlined copy of the contour code) for both launch forms

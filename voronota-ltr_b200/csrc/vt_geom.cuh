@@ -291,7 +291,11 @@ __device__ __forceinline__ V3<float> ic_center(const Sph<float>& a, const Sph<fl
     V3<float> cv = b.c - a.c;
     float cm2 = norm2(cv);
     if (cm2 < (float)(kEps * kEps)) return a.c;
-    float h_over_cm = (a.r * a.r + cm2 - b.r * b.r) / (2.0f * cm2);
+    // a cutting plane's position fixes the cut points on it: a correctly rounded division
+    // (the kernel's approximate one, and a product with a rounded reciprocal, are biased:
+    // between two balls of one radius the plane sits at exactly 0.5 of the distance, and
+    // those land below it more often than above)
+    float h_over_cm = __fdiv_rn(a.r * a.r + cm2 - b.r * b.r, 2.0f * cm2);
     return a.c + cv * h_over_cm;
 }
 // distance_to_intersection_circle_center (:208-215)

@@ -114,6 +114,7 @@ struct UState {
     uint32_t n_changed = 0, n_affected = 0;
     bool affected_dups = false;  // affected keeps duplicated changed ids (no new neighbours)
     bool full = true;
+    bool adj_valid = false;  // the table's SAS adjoint coefficients describe this state
     // UpdateableResult::is_empty (updateable.rs:35-37)
     bool empty() const { return n == 0 || num_cells == 0; }
 };
@@ -153,6 +154,7 @@ void copy_state(UState& d, const UState& s, bool fp32, cudaStream_t st) {
     d.n_affected = s.n_affected;
     d.affected_dups = s.affected_dups;
     d.full = s.full;
+    d.adj_valid = s.adj_valid;
 }
 
 int check_host_balls(const double* xyzr, uint64_t n) {
@@ -173,6 +175,7 @@ struct vt_updateable {
     int device = 0;
     cudaStream_t own = nullptr, stream = nullptr;
     bool backup_enabled = false;
+    bool adjoint = true;  // record arc moments for the SAS adjoint (vt_upd_set_adjoint)
     bool fp32 = false;
     double fp32_band_ulps = 16.0;
     static constexpr float kCellBand = 4e-6f;  // per-contact band of the FP32 cell sums
@@ -437,7 +440,7 @@ struct vt_updateable {
         b.p_pv_a = p_pv_a.p;
         b.p_pv_b = p_pv_b.p;
         p_arcm.ensure(3 * (size_t)P + 3);
-        b.p_arcm = p_arcm.p;
+        b.p_arcm = adjoint ? p_arcm.p : nullptr;
         b.redo_list = redo_list.p;
         b.serial_list = serial_list.p;
         b.serial_scratch = serial_scratch.p;
@@ -600,6 +603,9 @@ struct vt_updateable {
     // table size, cell count and error bits after an operation
     int finish(UState& S) {
         const uint32_t n = S.n;
+        // coefficients are whole after a full computation with moments, and stay whole
+        // while every update records them
+        S.adj_valid = S.full ? adjoint : (S.adj_valid && adjoint);
         nflags.ensure(n + 1);
         noff.ensure(n + 2);
         launch_cell_flags_u32(S.cell_flag.p, n, nflags.p, stream);
@@ -887,6 +893,11 @@ struct vt_updateable {
         UState& S = *cur;
         const uint32_t n = S.n;
         if (n == 0) return VT_OK;
+        if (!S.adj_valid) {
+            set_last_error("SAS adjoint unavailable: an operation ran with the adjoint off "
+                           "(vt_upd_set_adjoint); enable it and init again");
+            return VT_ERR_INVALID;
+        }
         if (!sph_fresh) {
             int st = build_spheres(S);
             if (st != VT_OK) return st;
@@ -1158,6 +1169,11 @@ int vt_upd_grad_sas(vt_updateable* h, const double* d_w_sas, double* d_grad) {
         h->begin_op();
         return h->grad_sas(d_w_sas, d_grad);
     });
+}
+int vt_upd_set_adjoint(vt_updateable* h, int on) {
+    if (check_handle(h)) return VT_ERR_INVALID;
+    h->adjoint = on != 0;
+    return VT_OK;
 }
 int vt_upd_last_full_reinit(const vt_updateable* h) { return h && h->cur->full ? 1 : 0; }
 uint64_t vt_upd_num_changed(const vt_updateable* h) { return h ? h->cur->n_changed : 0; }

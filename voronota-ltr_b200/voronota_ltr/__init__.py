@@ -150,6 +150,7 @@ def library():
     L.vt_upd_num_affected.restype = ctypes.c_uint64
     L.vt_upd_affected_ids.argtypes = [_vp, _u64p]
     L.vt_upd_stats.argtypes = [_vp, ctypes.POINTER(VtStats)]
+    L.vt_upd_set_adjoint.argtypes = [_vp, ctypes.c_int]
     L.vt_upd_grad_sas.argtypes = [_vp, ctypes.c_void_p, ctypes.c_void_p]
     L.vt_compute_batch.argtypes = [_f64p, _u64p, ctypes.c_uint64, ctypes.c_double, ctypes.c_int,
                                    ctypes.POINTER(_vp)]
@@ -773,6 +774,12 @@ class UpdateableTessellation:
         """d_grad (N x 4 doubles on the device) = d(sum w SAS)/d(x, y, z, r) of the current
         state; d_w_ptr 0/None: the total SAS."""
         _check(self._L.vt_upd_grad_sas(self._h, d_w_ptr or None, d_grad_ptr))
+
+    def set_adjoint(self, on: bool = True):
+        """Record the arc moments behind grad_sas_device (default on).  Off makes updates
+        about a tenth faster; grad_sas_device then raises until a full computation ran
+        with it on again."""
+        _check(self._L.vt_upd_set_adjoint(self._h, 1 if on else 0))
 
 
 __all__ = ["compute_tessellation", "compute_tessellation_result", "compute_contacts_only",
