@@ -50,8 +50,9 @@ __global__ void k_sas_scale(uint32_t n, const double* __restrict__ w_eff, const 
         if (w_eff[i] != 0.0) grad[4 * (size_t)i + 3] += w_eff[i] * 2.0 * cell_sas[i] / sph[i].w;
 }
 
-// FP64 adjoint: all valid pairs, or (from_list) the pairs the FP32 adjoint listed.
-__global__ void __launch_bounds__(kWarps * 32)
+// FP64 adjoint: all valid pairs, or (from_list) the pairs the FP32 adjoint listed.  At
+// most 128 registers (4 resident blocks), like the FP64 contact kernel.
+__global__ void __launch_bounds__(kWarps * 32, 4)
     k_adjoint64(DevBufs b, uint32_t P, int from_list, const double* __restrict__ u_contact,
                 const double* __restrict__ w_eff, double* __restrict__ grad) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;

@@ -66,6 +66,7 @@ __device__ __forceinline__ float wmax(float v) {
 // uses a butterfly; its decisions near zero are inside the band and go to FP64.
 __device__ __forceinline__ double lsum(double v, int len) {
     double acc = 0.0;
+#pragma unroll 1  // code size: the FP64 kernel is bound by instruction fetch
     for (int k = 0; k < len; ++k) acc += __shfl_sync(kFull, v, k);
     return acc;
 }
@@ -73,6 +74,7 @@ __device__ __forceinline__ float lsum(float v, int) { return wsum(v); }
 // acc = (acc + u_k) + w_k for k in lane order (two additions per element)
 __device__ __forceinline__ double lsum2(double u, double w, int len) {
     double acc = 0.0;
+#pragma unroll 1
     for (int k = 0; k < len; ++k) {
         acc += __shfl_sync(kFull, u, k);
         acc += __shfl_sync(kFull, w, k);

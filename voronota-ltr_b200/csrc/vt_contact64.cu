@@ -29,8 +29,11 @@ __device__ __forceinline__ void write_pair(const DevBufs& b, uint32_t p, const W
         for (int k = 0; k < 3; ++k) b.p_arcm[3 * (size_t)p + k] = r.valid ? r.xm[k] : 0.0;
 }
 
-template <bool FULL>
-__global__ void __launch_bounds__(kWarps * 32) k_contact64(DevBufs b, uint32_t P, int from_list) {
+// 4 resident blocks per SM: at most 128 registers a thread (a few bytes of spill) for 16
+// warps per SM, against 12 at the 150 registers the kernel would take.  XM: compile in the
+// arc first moments (only when the caller records them).
+template <bool FULL, bool XM>
+__global__ void __launch_bounds__(kWarps * 32, 4) k_contact64(DevBufs b, uint32_t P, int from_list) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t count = from_list ? *b.d_redo_count : P;
     for (uint32_t it = blockIdx.x * kWarps + w; it < count; it += gridDim.x * kWarps) {
@@ -44,7 +47,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_contact64(DevBufs b, uint32_t P
         g.b_id = b.nb_id[eb];
         g.e0 = 0.0;
         g.S = g.A.r + g.B.r;
-        g.want_xm = b.p_arcm != nullptr;
+        g.want_xm = XM;
         const double4* sph = b.sph;
         const uint32_t* nslot = b.nb_slot + off;
         const uint32_t* nid = b.nb_id + off;
@@ -54,7 +57,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_contact64(DevBufs b, uint32_t P
             r.id = nid[e];
             return r;
         };
-        WarpContact r = contact_warp<double, false, FULL, true>(g, (int)cnt, (int)(eb - off), nbf);
+        WarpContact r = contact_warp<double, false, FULL, XM>(g, (int)cnt, (int)(eb - off), nbf);
         if (lane == 0) write_pair(b, p, r, r.overflow ? kOverflow : 0);
     }
 }
@@ -497,10 +500,12 @@ void launch_contact_f64(const DevBufs& b, uint32_t P, int full, int from_list, c
     size_t g = (work + kWarps - 1) / kWarps;
     if (g < 1) g = 1;
     if (g > 148 * 64) g = 148 * 64;
-    if (full)
-        k_contact64<true><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, from_list);
+    if (full && b.p_arcm)
+        k_contact64<true, true><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, from_list);
+    else if (full)
+        k_contact64<true, false><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, from_list);
     else
-        k_contact64<false><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, from_list);
+        k_contact64<false, false><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, from_list);
     count_launch();
 }
 
