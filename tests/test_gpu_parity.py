@@ -199,10 +199,21 @@ def test_long_neighbour_lists(prec):
 
 
 def test_invalid_input_raises():
-    for bad in ([(0, 0, float("nan"), 1.0)], [(0, 0, 0, -1.0)]):
+    """Bad balls are caught on the device before any other work; the host path's error
+    names the first bad ball; the engine stays usable afterwards."""
+    good = W.lattice_balls(500, 3)
+    for bad in ([(0, 0, float("nan"), 1.0)], [(0, 0, 0, -1.0)], np.vstack([good, [[1.0, float("inf"), 0.0, 1.5]]])):
         with pytest.raises(V.VoronotaError) as ei:
             V.compute_tessellation(bad, 1.4)
         assert ei.value.status == V.VT_ERR_INVALID
+        assert "ball %d" % (len(bad) - 1) in str(ei.value)
+    import torch
+    e = V.Engine()
+    d = torch.from_numpy(np.vstack([good, [[0.0, 0.0, float("nan"), 1.0]]])).cuda()
+    with pytest.raises(V.VoronotaError):
+        e.compute_device(d.data_ptr(), len(good) + 1, 1.4)
+    compare(V.compute_tessellation_result(good, 1.4, precision="fp64"), O.compute(good, 1.4), "fp64")
+    e.close()
 
 
 def test_fp32_large_lattice_pair_set_and_totals():

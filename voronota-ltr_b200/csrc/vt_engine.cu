@@ -501,7 +501,13 @@ struct vt_engine {
         launch_bbox_final(bbox_parts.p, nblk, bbox.p, stream);
         t_end(0);
         VT_CUDA(cudaMemcpyAsync(h_bbox, bbox.p, sizeof(BBox), cudaMemcpyDeviceToHost, stream));
+        VT_CUDA(cudaMemcpyAsync(h_words + 7, words.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         sync();
+        if (h_words[7] & kErrInvalid) {  // k_prepare's input check
+            stats.device_error_bits = h_words[7];
+            g_last_error = "non-finite input or negative radius";
+            return VT_ERR_INVALID;
+        }
         const BBox bb = *h_bbox;
         for (int k = 0; k < 3; ++k)
             if (!std::isfinite(bb.mn[k]) || !std::isfinite(bb.mx[k])) {
@@ -981,15 +987,21 @@ int validate_host(const double* xyzr, uint64_t n, double probe, const double* pb
                 g_last_error = "non-finite periodic box";
                 return VT_ERR_INVALID;
             }
+    return VT_OK;
+}
+
+// The balls themselves are checked on the device (k_prepare: a non-finite value or a
+// negative radius ends the call with VT_ERR_INVALID before any other work); a host
+// caller's error then names the first bad ball, found here.
+void name_invalid_ball(const double* xyzr, uint64_t n) {
     for (uint64_t i = 0; i < n; ++i) {
         const double* v = xyzr + 4 * i;
         if (!std::isfinite(v[0]) || !std::isfinite(v[1]) || !std::isfinite(v[2]) || !std::isfinite(v[3]) ||
             v[3] < 0.0) {
             g_last_error = "ball " + std::to_string(i) + ": non-finite value or negative radius";
-            return VT_ERR_INVALID;
+            return;
         }
     }
-    return VT_OK;
 }
 
 std::mutex g_engines_mu;
@@ -1036,7 +1048,9 @@ int host_compute(vt_engine* e, const double* xyzr, uint64_t n, double probe, con
                                 e->stream));
         d_g = e->groups.p;
     }
-    return e->run(d_in, n, probe, pbox9, d_g, n_groups, precision, contacts_only, batch_off, S);
+    st = e->run(d_in, n, probe, pbox9, d_g, n_groups, precision, contacts_only, batch_off, S);
+    if (st == VT_ERR_INVALID && (e->stats.device_error_bits & kErrInvalid)) name_invalid_ball(xyzr, n);
+    return st;
 }
 
 template <typename F>
