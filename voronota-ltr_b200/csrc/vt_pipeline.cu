@@ -292,16 +292,71 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_search(DevBufs b, int wan
             continue;
         }
         if (big) continue;
-        // bitonic sort of (value, id) (spheres_searcher.rs:324)
+        // bitonic sort of (value, id) (spheres_searcher.rs:324); keys are distinct within a
+        // row.  Up to 64 entries (nearly every ball): in registers, two per lane, partners
+        // exchanged by shuffles; longer rows: in shared memory.
         uint32_t n2 = 2;
         while (n2 < cnt) n2 <<= 1;
-        for (uint32_t e = cnt + lane; e < n2; e += 32) {
-            s_val[w][e] = INFINITY;
-            s_id[w][e] = 0xffffffffu;
-            s_slot[w][e] = 0;
-        }
-        __syncwarp();
-        if (cnt > 1) {
+        if (n2 <= 64) {
+            double v[2];
+            uint32_t id[2], sl[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint32_t t = lane + 32u * h;
+                v[h] = t < cnt ? s_val[w][t] : INFINITY;
+                id[h] = t < cnt ? s_id[w][t] : 0xffffffffu;
+                sl[h] = t < cnt ? s_slot[w][t] : 0u;
+            }
+            for (uint32_t k = 2; k <= n2; k <<= 1) {
+                for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
+                    if (jj == 32) {  // k = 64: element lane against lane + 32, ascending
+                        if (vless(v[1], id[1], v[0], id[0])) {
+                            const double tv = v[0];
+                            const uint32_t ti = id[0], ts = sl[0];
+                            v[0] = v[1];
+                            id[0] = id[1];
+                            sl[0] = sl[1];
+                            v[1] = tv;
+                            id[1] = ti;
+                            sl[1] = ts;
+                        }
+                        continue;
+                    }
+                    const bool lower = (lane & jj) == 0;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const uint32_t t = lane + 32u * h;
+                        const double pv = __shfl_xor_sync(0xffffffffu, v[h], jj);
+                        const uint32_t pi = __shfl_xor_sync(0xffffffffu, id[h], jj);
+                        const uint32_t ps = __shfl_xor_sync(0xffffffffu, sl[h], jj);
+                        const bool keep_min = lower == ((t & k) == 0);
+                        const bool take = keep_min ? vless(pv, pi, v[h], id[h]) : vless(v[h], id[h], pv, pi);
+                        if (take) {
+                            v[h] = pv;
+                            id[h] = pi;
+                            sl[h] = ps;
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint32_t t = lane + 32u * h;
+                if (t < cnt) {
+                    s_val[w][t] = v[h];
+                    s_id[w][t] = id[h];
+                    s_slot[w][t] = sl[h];
+                }
+            }
+            __syncwarp();
+        } else {
+            for (uint32_t e = cnt + lane; e < n2; e += 32) {
+                s_val[w][e] = INFINITY;
+                s_id[w][e] = 0xffffffffu;
+                s_slot[w][e] = 0;
+            }
+            __syncwarp();
             for (uint32_t k = 2; k <= n2; k <<= 1) {
                 for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
                     for (uint32_t t = lane; t < n2; t += 32) {
