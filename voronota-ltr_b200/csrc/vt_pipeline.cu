@@ -173,8 +173,10 @@ __device__ __forceinline__ bool vless(double va, uint32_t ia, double vb, uint32_
     return ia < ib;
 }
 
+// The count pass waits on candidate loads: 9 resident blocks (56 registers) hide a little
+// more of that latency than the 8 that 64 registers allow.
 template <bool FILL>
-__global__ void __launch_bounds__(kSearchWarps * 32) k_search(DevBufs b, int want_rel) {
+__global__ void __launch_bounds__(kSearchWarps * 32, FILL ? 1 : 9) k_search(DevBufs b, int want_rel) {
     __shared__ double s_val[kSearchWarps][kSortCap];
     __shared__ uint32_t s_id[kSearchWarps][kSortCap];
     __shared__ uint32_t s_slot[kSearchWarps][kSortCap];
