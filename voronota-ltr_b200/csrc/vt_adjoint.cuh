@@ -112,10 +112,11 @@ __device__ __forceinline__ void adjoint_pair(const AdjPair& G, bool full, int le
 // FP64 position of an FP32 contour vertex from the planes that define it: the radical
 // planes of (a, b), (a, lid), (a, rid), or the circle of (a, b) and one plane where lid
 // or rid is a.  y0 is the FP32 point relative to a; returns y0 when the construction is
-// ill-conditioned.  sphere_of(id) gives a neighbour's double sphere.
+// ill-conditioned (and then clears *ok when given).  sphere_of(id) gives a neighbour's
+// double sphere.
 template <typename SphereOf>
 __device__ __forceinline__ V3<double> snap_vertex(const AdjPair& G, V3<double> y0, uint32_t lid, uint32_t rid,
-                                                  SphereOf sphere_of) {
+                                                  SphereOf sphere_of, bool* ok = nullptr) {
     const V3<double> db = G.pb - G.pa;
     const double hb = 0.5 * (dot(db, db) + G.Ra * G.Ra - G.Rb * G.Rb);
     auto plane = [&](uint32_t c, V3<double>& d, double& h) {
@@ -128,29 +129,29 @@ __device__ __forceinline__ V3<double> snap_vertex(const AdjPair& G, V3<double> y
     if (lid != G.a && rid != G.a) {
         V3<double> d1, d2;
         double h1, h2;
-        if (!plane(lid, d1, h1) || !plane(rid, d2, h2)) return y0;
+        if (!plane(lid, d1, h1) || !plane(rid, d2, h2)) { if (ok) *ok = false; return y0; }
         // Cramer on rows db, d1, d2
         const V3<double> c12 = cross(d1, d2), c2b = cross(d2, db), cb1 = cross(db, d1);
         const double det = dot(db, c12);
         const double scale = norm(db) * norm(d1) * norm(d2);
-        if (!(fabs(det) > 1e-6 * scale)) return y0;
+        if (!(fabs(det) > 1e-6 * scale)) { if (ok) *ok = false; return y0; }
         return (c12 * hb + c2b * h1 + cb1 * h2) / det;
     }
     const uint32_t c = lid == G.a ? rid : lid;
-    if (c == G.a) return y0;
+    if (c == G.a) { if (ok) *ok = false; return y0; }
     V3<double> dc;
     double hc;
-    if (!plane(c, dc, hc)) return y0;
+    if (!plane(c, dc, hc)) { if (ok) *ok = false; return y0; }
     // the line of planes b and c: y = y_line + t * dir, then |y - q_rel| = rho
     const V3<double> dir = cross(db, dc);
     const double dd = dot(dir, dir);
-    if (!(dd > 1e-12 * dot(db, db) * dot(dc, dc))) return y0;
+    if (!(dd > 1e-12 * dot(db, db) * dot(dc, dc))) { if (ok) *ok = false; return y0; }
     const V3<double> y_line = (cross(dc, dir) * hb + cross(dir, db) * hc) / dd;
     const V3<double> qr = G.q - G.pa;
     const V3<double> w = y_line - qr;
     const double A = dd, B = 2.0 * dot(w, dir), Cq = dot(w, w) - G.rho * G.rho;
     const double disc = B * B - 4.0 * A * Cq;
-    if (!(disc >= 0.0)) return y0;
+    if (!(disc >= 0.0)) { if (ok) *ok = false; return y0; }
     const double sq = sqrt(disc);
     const double t1 = (-B - sq) / (2.0 * A), t2 = (-B + sq) / (2.0 * A);
     const V3<double> y1 = y_line + dir * t1, y2 = y_line + dir * t2;

@@ -291,6 +291,7 @@ struct WarpContact {
     double area, arc, sa_a, sa_b, pv_a, pv_b;
     double xm[3];  // first moment of the contact's arcs about a's centre (want_xm)
     bool central;
+    bool merged;  // two close points were merged (the kept point takes the other's id)
     int site;  // debug builds: first step with an unsure decision
 };
 
@@ -399,6 +400,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
     res.xm[0] = res.xm[1] = res.xm[2] = 0.0;
     res.central = false;
     res.site = -1;
+    res.merged = false;
 
     // contact.rs:206-218
     if (!sphere_intersects(d, g.A, g.B, (T)2 * g.S * e0) || sphere_contains(d, g.A, g.B, e0, (T)2 * g.S * e0) ||
@@ -531,6 +533,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             }
             VT_SITE(4);
             if (!(dse - (T)kEps > (T)0)) {
+                res.merged = true;
                 if (lane == ns) q.rid = erid;
                 int s2 = lane < ne ? lane : lane + 1;
                 s2 = s2 > 31 ? 31 : s2;

@@ -179,7 +179,143 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
     }
 }
 
+// Tessellation network elements from the FP32 contour (tessellation network of
+// vt_network.cu): the FP32 topology gives every vertex's defining planes, and the vertex
+// is placed in double from them (snap_vertex), so positions, chord lengths and arc
+// angles are FP64 values.  A pair whose FP32 contour is unsure, overflows, merged two
+// points (the kept point's ids no longer define it), or has a vertex the snap cannot
+// place is listed for the FP64 element kernel instead.
+__global__ void __launch_bounds__(kWarps * 32, 4)
+    k_net_elements32(DevBufs b, uint32_t P, float band, const uint32_t* __restrict__ voff, NetSlots sl,
+                     uint32_t* __restrict__ fp64_list, uint32_t* __restrict__ fp64_count) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t n = b.n;
+    const int periodic = b.periodic;
+    for (uint32_t p = blockIdx.x * kWarps + w; p < P; p += gridDim.x * kWarps) {
+        const uint32_t slot = voff[p];
+        if (voff[p + 1] == slot) continue;  // no contact
+        const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
+        const uint32_t bid = b.nb_id[eb];
+        const uint32_t off = b.nb_off[a], cnt = b.nb_cnt[a];
+        const double4 A4 = b.sph[a], B4 = b.sph[b.nb_slot[eb]];
+        PairGeom<float> g;
+        const float Ra = (float)A4.w;
+        const float4 rb = b.nb_rel[eb];
+        g.A = {{0.f, 0.f, 0.f}, Ra};
+        g.B = {{rb.x, rb.y, rb.z}, rb.w};
+        g.a_id = a;
+        g.b_id = bid;
+        g.S = Ra + rb.w;
+        g.e0 = band * g.S;
+        const float4* rel = b.nb_rel + off;
+        const uint32_t* nid = b.nb_id + off;
+        const uint32_t* nslot = b.nb_slot + off;
+        auto nbf = [&](int e) {
+            Nb<float> r;
+            float4 v = rel[e];
+            r.s = {{v.x, v.y, v.z}, v.w};
+            r.id = nid[e];
+            return r;
+        };
+        ContourOut<float> co;
+        WarpContact r = contact_warp<float, true, false>(g, (int)cnt, (int)(eb - off), nbf, &co);
+        bool fp64 = r.unsure || r.overflow || !r.valid || r.merged;
+        const Sph<double> A = {{A4.x, A4.y, A4.z}, A4.w}, B = {{B4.x, B4.y, B4.z}, B4.w};
+        const Sph<double> ic = intersection_circle(A, B);
+        const uint32_t base = slot * (uint32_t)kNetSlot;
+        if (!fp64 && co.full) {  // an uncut contact: one SAS edge, no vertex
+            if (lane == 0) {
+                sl.e_ids[base] = net_edge_ids(a, bid, kNetNull, periodic, n);
+                sl.e_len[base] = kTau * ic.r;
+                sl.v_cnt[slot] = 0;
+                sl.e_cnt[slot] = 1;
+                sl.base[slot] = base;
+            }
+            continue;
+        }
+        const int len = co.len;
+        V3<double> P0 = mk<double>(0, 0, 0), P1 = P0;
+        double ang = 0.0;
+        bool arc = false;
+        if (!fp64) {
+            AdjPair G;
+            G.pa = A.c;
+            G.pb = B.c;
+            G.Ra = A.r;
+            G.Rb = B.r;
+            G.q = ic.c;
+            G.rho = ic.r;
+            G.axis = normalize(B.c - A.c);
+            G.a = a;
+            G.bid = bid;
+            const double4* sph = b.sph;
+            auto sphere_of = [&](uint32_t c) {
+                for (uint32_t e = 0; e < cnt; ++e)
+                    if (nid[e] == c) return sph[nslot[e]];
+                return make_double4(0.0, 0.0, 0.0, 0.0);
+            };
+            bool ok = true;
+            V3<double> y = widen(co.q.p);
+            if (lane < len) y = snap_vertex(G, y, co.q.lid, co.q.rid, sphere_of, &ok);
+            P0 = A.c + y;
+            const int nx = len > 0 ? (lane + 1 < len ? lane + 1 : 0) : 0;
+            P1 = mk<double>(__shfl_sync(kFull, P0.x, nx), __shfl_sync(kFull, P0.y, nx), __shfl_sync(kFull, P0.z, nx));
+            const uint32_t nlid = __shfl_sync(kFull, co.q.lid, nx);
+            arc = lane < len && co.q.rid == a;
+            if (arc && nlid == a && co.q.ang > 0.f) {
+                const V3<double> v1 = P0 - G.q, v2 = P1 - G.q;
+                ang = atan2(dot(cross(v1, v2), G.axis), dot(v1, v2));
+                if (ang < 0.0) ang += kTau;
+                if (fabs((double)co.q.ang - ang) > 1e-3) ok = false;  // the 0 / 2 pi branch is unclear
+            }
+            // elements with equal ids inside one contour (arcs of one contact, both ends of
+            // an arc cut by the same ball): the network keeps the first in contour order,
+            // which the FP64 contour decides
+            const bool on = lane < len;
+            const uint32_t third = arc ? kNetNull : co.q.rid;
+            const uint32_t vl = co.q.lid == a ? kNetNull : co.q.lid;
+            const unsigned long long ek = on ? (unsigned long long)third : (1ull << 40) + lane;
+            const unsigned long long vk = on ? ((unsigned long long)vl << 32 | third) : (1ull << 63) + lane;
+            const bool dup = __popc(__match_any_sync(kFull, ek)) > 1 || __popc(__match_any_sync(kFull, vk)) > 1;
+            fp64 = __any_sync(kFull, !ok || dup);
+        }
+        if (fp64) {
+            if (lane == 0) {
+                sl.v_cnt[slot] = 0;
+                sl.e_cnt[slot] = 0;
+                sl.base[slot] = base;
+                fp64_list[atomicAdd(fp64_count, 1u)] = p;
+            }
+            continue;
+        }
+        if (lane < len) {
+            const Pt<float>& cp = co.q;
+            sl.e_ids[base + lane] = net_edge_ids(a, bid, arc ? kNetNull : cp.rid, periodic, n);
+            sl.e_len[base + lane] = arc ? ang * ic.r : norm(P1 - P0);
+            sl.v_ids[base + lane] =
+                net_vertex_ids(a, bid, cp.lid == a ? kNetNull : cp.lid, arc ? kNetNull : cp.rid, periodic, n);
+            sl.v_xyz[3 * (size_t)(base + lane)] = P0.x;
+            sl.v_xyz[3 * (size_t)(base + lane) + 1] = P0.y;
+            sl.v_xyz[3 * (size_t)(base + lane) + 2] = P0.z;
+        }
+        if (lane == 0) {
+            sl.v_cnt[slot] = (uint32_t)len;
+            sl.e_cnt[slot] = (uint32_t)len;
+            sl.base[slot] = base;
+        }
+    }
+}
+
 }  // namespace
+
+void launch_net_elements_f32(const DevBufs& b, uint32_t P, const uint32_t* voff, NetSlots sl, uint32_t* fp64_list,
+                             uint32_t* fp64_count, cudaStream_t s) {
+    size_t g = (P + kWarps - 1) / kWarps;
+    if (g < 1) g = 1;
+    if (g > 148 * 64) g = 148 * 64;
+    k_net_elements32<<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band, voff, sl, fp64_list, fp64_count);
+    count_launch();
+}
 
 void launch_adjoint_f32(const DevBufs& b, uint32_t P, const double* u_contact, const double* w_eff, double* grad,
                         cudaStream_t s) {

@@ -166,7 +166,7 @@ struct vt_engine {
         net_uoff;
     DBuf<uint4> net_vids, net_eids, net_ov_vids, net_ov_eids;
     DBuf<double> net_vxyz, net_elen, net_ov_vxyz, net_ov_elen;
-    DBuf<uint32_t> net_base, net_ov_list;
+    DBuf<uint32_t> net_base, net_ov_list, net_fp64_list;
     NetSlots net_slots{};
     DBuf<unsigned long long> net_hi, net_lo, net_ka, net_kb, net_hs, net_ls;
     DBuf<uint32_t> net_ia, net_ib, net_order;
@@ -251,7 +251,14 @@ struct vt_engine {
         sl = NetSlots{net_vids.p, net_vxyz.p, net_eids.p, net_elen.p, net_ov_vids.p, net_ov_vxyz.p, net_ov_eids.p,
                       net_ov_elen.p, (uint32_t)cap, net_base.p, net_vcnt.p, net_ecnt.p, net_ov_list.p,
                       net_ov_list.p + ov_cap, ov_cap};
-        launch_net_elements(b, P, net_voff.p, sl, stream);
+        if (b.nb_rel) {  // FP32 mode: FP32 contours with FP64-placed vertices, FP64 for the rest
+            net_fp64_list.ensure(V + 1);  // [V] is the counter
+            VT_CUDA(cudaMemsetAsync(net_fp64_list.p + V, 0, 4, stream));
+            launch_net_elements_f32(b, P, net_voff.p, sl, net_fp64_list.p, net_fp64_list.p + V, stream);
+            launch_net_elements(b, P, net_voff.p, sl, net_fp64_list.p, net_fp64_list.p + V, stream);
+        } else {
+            launch_net_elements(b, P, net_voff.p, sl, nullptr, nullptr, stream);
+        }
         launch_net_serial(b, net_voff.p, sl, stream);
         net_off_v.ensure(V + 2);
         net_off_e.ensure(V + 2);

@@ -22,7 +22,7 @@ namespace vt {
 namespace {
 
 constexpr int kWarps = 4;
-constexpr int kSlot = 32;  // elements of one pair (a warp contour holds <= 32 points)
+constexpr int kSlot = kNetSlot;  // elements of one pair (a warp contour holds <= 32 points)
 
 __device__ __forceinline__ Sph<double> sph_of(double4 v) { return {{v.x, v.y, v.z}, v.w}; }
 
@@ -32,11 +32,14 @@ __global__ void k_valid_flags(const uint8_t* __restrict__ status, uint32_t P, ui
 }
 
 __global__ void __launch_bounds__(kWarps * 32)
-    k_net_elements(DevBufs b, uint32_t P, const uint32_t* __restrict__ voff, NetSlots sl) {
+    k_net_elements(DevBufs b, uint32_t P, const uint32_t* __restrict__ voff, NetSlots sl,
+                   const uint32_t* __restrict__ list, const uint32_t* __restrict__ list_count) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t n = b.n;
     const int periodic = b.periodic;
-    for (uint32_t p = blockIdx.x * kWarps + w; p < P; p += gridDim.x * kWarps) {
+    const uint32_t count = list ? *list_count : P;
+    for (uint32_t it = blockIdx.x * kWarps + w; it < count; it += gridDim.x * kWarps) {
+        const uint32_t p = list ? list[it] : it;
         const uint32_t slot = voff[p];
         if (voff[p + 1] == slot) continue;  // no contact
         const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
@@ -158,8 +161,9 @@ int gb(size_t n) { return grid_blocks(n, 256, 148 * 16); }
 void launch_valid_flags(const DevBufs& b, uint32_t P, uint32_t* flags, cudaStream_t s) {
     k_valid_flags<<<gb(P), 256, 0, s>>>(b.p_status, P, flags); count_launch();
 }
-void launch_net_elements(const DevBufs& b, uint32_t P, const uint32_t* voff, NetSlots sl, cudaStream_t s) {
-    k_net_elements<<<grid_blocks(P, kWarps, 148 * 64), kWarps * 32, 0, s>>>(b, P, voff, sl);
+void launch_net_elements(const DevBufs& b, uint32_t P, const uint32_t* voff, NetSlots sl, const uint32_t* list,
+                         const uint32_t* count, cudaStream_t s) {
+    k_net_elements<<<grid_blocks(P, kWarps, 148 * 64), kWarps * 32, 0, s>>>(b, P, voff, sl, list, count);
     count_launch();
 }
 size_t net_slot_capacity() { return kSlot; }

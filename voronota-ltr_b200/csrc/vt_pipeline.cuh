@@ -272,6 +272,7 @@ void launch_adjoint_f32(const DevBufs& b, uint32_t P, const double* u_contact, c
 // by the serial kernel (launch_net_serial).  Ids: NULL = 0xffffffff; an edge uses the
 // x, y, z of its uint4.
 constexpr uint32_t kNetNull = 0xffffffffu;
+constexpr int kNetSlot = 32;  // elements of one pair in the warp area
 struct NetSlots {
     uint4* v_ids;  // warp area
     double* v_xyz;
@@ -345,7 +346,13 @@ struct NetSortBufs {
     size_t temp_bytes;
 };
 void launch_valid_flags(const DevBufs& b, uint32_t P, uint32_t* flags, cudaStream_t s);
-void launch_net_elements(const DevBufs& b, uint32_t P, const uint32_t* voff, NetSlots slots, cudaStream_t s);
+// FP64 elements of every valid pair, or (list != null) of the *count pairs listed
+void launch_net_elements(const DevBufs& b, uint32_t P, const uint32_t* voff, NetSlots slots, const uint32_t* list,
+                         const uint32_t* count, cudaStream_t s);
+// FP32 mode: elements from the FP32 contour with FP64-placed vertices (vt_contact32.cu);
+// pairs it cannot settle are listed for launch_net_elements
+void launch_net_elements_f32(const DevBufs& b, uint32_t P, const uint32_t* voff, NetSlots slots, uint32_t* fp64_list,
+                             uint32_t* fp64_count, cudaStream_t s);
 // the pairs of ov_list through the serial contour (vt_contact64.cu); at most ov_cap
 void launch_net_serial(const DevBufs& b, const uint32_t* voff, NetSlots slots, cudaStream_t s);
 size_t net_slot_capacity();
