@@ -129,3 +129,14 @@ def test_contours_longer_than_a_warp(prec):
         assert on_pair == len(balls) - 2
     box = {"corners": [(-10, -10, -10), (12, 10, 10)]}
     check_network(sunflower(40, rr=0.1, rho=3.3), 0.1, prec, periodic_box=box)
+
+
+def test_fp32_network_after_larger_calls():
+    """A warp of the FP32 element kernel handles several pairs in turn (more pairs than
+    resident warps); a slot it counts but leaves unwritten would show the elements of the
+    previous, larger calls that still sit in reused device memory."""
+    for seed in range(2):
+        V.compute_tessellation_result(W.lattice_balls(20000, seed), 1.4, precision="fp32", with_cell_vertices=True)
+    balls, side = W.periodic_box_balls(3000, 0.033, 1.52, seed=9)
+    for _ in range(2):
+        check_network(balls, 1.4, "fp32", periodic_box={"corners": [(0, 0, 0), (side, side, side)]})

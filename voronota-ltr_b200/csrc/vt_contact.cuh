@@ -108,6 +108,16 @@ template <typename T>
 __device__ __forceinline__ V3<T> shfl_v3(V3<T> v, int src) {
     return {__shfl_sync(kFull, v.x, src), __shfl_sync(kFull, v.y, src), __shfl_sync(kFull, v.z, src)};
 }
+// The same for the cut loop, where no point carries an arc angle yet (all 0).
+template <typename T>
+__device__ __forceinline__ Pt<T> shfl_pt_flat(const Pt<T>& q, int src) {
+    Pt<T> r;
+    r.p = shfl_v3(q.p, src);
+    r.lid = __shfl_sync(kFull, q.lid, src);
+    r.rid = __shfl_sync(kFull, q.rid, src);
+    r.ang = 0;
+    return r;
+}
 
 // sin and cos of the half rotation angles of init_contour (contact.rs:463-468): the
 // angles k pi/3 accumulate by repeated addition exactly as in the reference, and the
@@ -500,11 +510,11 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                 return res;
             }
             src = src < 0 ? 0 : (src > 31 ? 31 : src);
-            Pt<T> r = shfl_pt(q, src);
+            Pt<T> r = shfl_pt_flat(q, src);
             if (lane < n2) q = r;
             int il = ns > 0 ? ns - 1 : n2 - 1;
             int ir = ne + 1 < n2 ? ne + 1 : 0;
-            Pt<T> nbp = shfl_pt(q, lane == ns ? il : ir);
+            Pt<T> nbp = shfl_pt_flat(q, lane == ns ? il : ir);
             if (lane == ns || lane == ne) {
                 V3<T> ip;
                 if constexpr (F)
@@ -524,20 +534,25 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                 q.ang = 0;
             }
             VT_SITE(3);
-            // merge very close points (contact.rs:622-626)
-            V3<T> ps = shfl_v3(q.p, ns), pe = shfl_v3(q.p, ne);
-            uint32_t erid = __shfl_sync(kFull, q.rid, ne);
-            T dse = norm2(pe - ps);
-            if constexpr (F) {  // merge threshold: d^2 <= 1e-10, i.e. d <= 1e-5
-                if (fabsf(sqrtf(dse) - 1e-5f) <= 4.f * e0) d.unsure = true;
+            // merge very close points (contact.rs:622-626): lane ns holds the new point ps
+            // and takes pe from lane ne
+            const V3<T> pe = shfl_v3(q.p, ne);
+            bool close = false;
+            if (lane == ns) {
+                const T dse = norm2(pe - q.p);
+                if constexpr (F) {  // merge threshold: d^2 <= 1e-10, i.e. d <= 1e-5
+                    if (fabsf(sqrtf(dse) - 1e-5f) <= 4.f * e0) d.unsure = true;
+                }
+                close = !(dse - (T)kEps > (T)0);
             }
             VT_SITE(4);
-            if (!(dse - (T)kEps > (T)0)) {
+            if (__any_sync(kFull, close)) {
                 res.merged = true;
+                const uint32_t erid = __shfl_sync(kFull, q.rid, ne);
                 if (lane == ns) q.rid = erid;
                 int s2 = lane < ne ? lane : lane + 1;
                 s2 = s2 > 31 ? 31 : s2;
-                Pt<T> r2 = shfl_pt(q, s2);
+                Pt<T> r2 = shfl_pt_flat(q, s2);
                 if (lane < n2 - 1) q = r2;
                 n2 -= 1;
             }

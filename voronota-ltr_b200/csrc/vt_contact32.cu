@@ -276,7 +276,10 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
             const uint32_t vl = co.q.lid == a ? kNetNull : co.q.lid;
             const unsigned long long ek = on ? (unsigned long long)third : (1ull << 40) + lane;
             const unsigned long long vk = on ? ((unsigned long long)vl << 32 | third) : (1ull << 63) + lane;
-            const bool dup = __popc(__match_any_sync(kFull, ek)) > 1 || __popc(__match_any_sync(kFull, vk)) > 1;
+            // both matches on every lane: a collective that some lanes skip (a short-circuit
+            // ||) pairs the warp's later collectives wrongly
+            const unsigned me = __match_any_sync(kFull, ek), mv = __match_any_sync(kFull, vk);
+            const bool dup = __popc(me) > 1 || __popc(mv) > 1;
             fp64 = __any_sync(kFull, !ok || dup);
         }
         if (fp64) {
