@@ -19,7 +19,7 @@ def gpu(balls, probe, periodic_box=None, groups=None, precision="fp64", contacts
     return V.compute_tessellation_result(balls, probe, periodic_box, groups, precision)
 
 
-def compare(g, o, precision, contacts_only=False, ordered=True, total_rel=None):
+def compare(g, o, precision, contacts_only=False, ordered=True, total_rel=None, total_abs=None):
     """Pair sets and central bits bit-exact; values within the precision's tolerance.
 
     FP64: |d| <= 1e-9 (1 + |x|) everywhere (only the summation order of the warp
@@ -30,7 +30,8 @@ def compare(g, o, precision, contacts_only=False, ordered=True, total_rel=None):
     1e-4 (A^2, A^3) for tiny totals: a 17-ball periodic ring with 5 A^2 of SAS carries
     ~1e-5 A^2 of FP32 rounding in its nearly cancelling solid-angle sums (the FP32 kernel
     runs on such small inputs only when forced: fp32_engine below).  `total_rel`
-    overrides the relative bound on the totals.
+    overrides the relative bound on the totals; `total_abs` = (SAS, volume) absolute
+    allowances that replace the floor.
     """
     ga, gb = g.id_a.astype(np.int64), g.id_b.astype(np.int64)
     oa, ob = o.contacts_a.astype(np.int64), o.contacts_b.astype(np.int64)
@@ -74,8 +75,9 @@ def compare(g, o, precision, contacts_only=False, ordered=True, total_rel=None):
     rv = abs(g.total_volume - o.total_volume) / max(abs(o.total_volume), 1e-300)
     lim = total_rel if total_rel is not None else (1e-11 if precision == "fp64" else 1e-6)
     floor = 0.0 if precision == "fp64" else 1e-4
-    assert rs <= lim or abs(g.total_sas_area - o.total_sas_area) <= floor, f"total SAS rel err {rs}"
-    assert rv <= lim or abs(g.total_volume - o.total_volume) <= floor, f"total volume rel err {rv}"
+    fs, fv = total_abs if total_abs is not None else (floor, floor)
+    assert rs <= lim or abs(g.total_sas_area - o.total_sas_area) <= fs, f"total SAS rel err {rs}"
+    assert rv <= lim or abs(g.total_volume - o.total_volume) <= fv, f"total volume rel err {rv}"
     return {"max_dA": float(da.max(initial=0)), "rel_sas": rs, "rel_vol": rv}
 
 
