@@ -213,7 +213,7 @@ def updateable_leg(args, rank, torch, V, R):
         d = torch.from_numpy(balls).cuda()
         torch.cuda.synchronize()
         u.init_device(d.data_ptr(), n, PROBE, box)
-        ms, adj, pairs, redo = [], [], [], []
+        ms, adj, pairs, redo, cref = [], [], [], [], []
         dg = torch.empty((n, 4), dtype=torch.float64, device="cuda")
         for t, (ids, disp) in enumerate(moves[:warm + nsteps]):
             ti = torch.from_numpy(ids).cuda()
@@ -233,12 +233,13 @@ def updateable_leg(args, rank, torch, V, R):
                 adj.append(e1.elapsed_time(e2))
                 pairs.append(int(st.num_pairs))
                 redo.append(int(st.num_fp64_redo))
+                cref.append(int(st.num_cell_redo))
         aff = len(u.affected_ids())
-        return u, d, ms, aff, pairs, redo, adj
+        return u, d, ms, aff, pairs, redo, adj, cref
 
-    u32, d32, ms32, aff, pairs, redo, adj32 = run("fp32", steps)
-    _, _, ms64, _, _, _, adj64 = run("fp64", max(3, steps // 2))
-    _, _, ms32na, _, _, _, _ = run("fp32", steps, adjoint=False)
+    u32, d32, ms32, aff, pairs, redo, adj32, cref = run("fp32", steps)
+    _, _, ms64, _, _, _, adj64, _ = run("fp64", max(3, steps // 2))
+    _, _, ms32na, _, _, _, _, _ = run("fp32", steps, adjoint=False)
     eng = V.Engine()
     eng.set_stream(stream.cuda_stream)
     full = []
@@ -269,6 +270,7 @@ def updateable_leg(args, rank, torch, V, R):
         "balls_per_s_fp32": replica_throughput(n, R.world, t32), "max_over_ranks": R.world,
         "affected_per_update": aff, "pairs_per_update": int(statistics.median(pairs)),
         "fp64_redo_pairs_per_update": int(statistics.median(redo)),
+        "fp64_cell_refresh_per_update": int(statistics.median(cref)),
     }
     if rank == 0 and not args.no_cpu:
         out.update(updateable_cpu_check(balls, box, moves[:3], n, torch, V))

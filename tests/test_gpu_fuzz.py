@@ -74,3 +74,45 @@ def test_random_structure(k):
         np.testing.assert_allclose(r.vertex_xyz, o.vertex_xyz, rtol=0,
                                    atol=1e-9 * (1 + np.abs(o.vertex_xyz).max(initial=0)))
         assert np.all(np.abs(r.edge_length - o.edge_length) <= 1e-9 * (1 + np.abs(o.edge_length)))
+
+
+@pytest.fixture
+def fixed_grid():
+    O.set_faithful_grid_update(False)
+    yield
+    O.set_faithful_grid_update(True)
+
+
+def _allowance(balls, probe, s):
+    R = balls[s.cells_index.astype(np.int64), 3] + probe
+    exposed = s.cells_sas > 0
+    return 1e-7 * float((4 * np.pi * R[exposed] ** 2).sum()), 1e-7 * float((4 * np.pi * R[exposed] ** 3 / 3).sum())
+
+
+@pytest.mark.parametrize("k", [k for k in range(CASES) if k % 5 != 0][:16])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_random_trajectory(k, precision, fixed_grid):
+    """update_with_changed on a random trajectory: each step moves a random subset (1 ball
+    to 3% of them, or more than half, which reinitialises) by a random amount, some steps
+    also change radii; the GPU handle and the oracle's restatement of updateable.rs agree on
+    the return values, changed and affected ids, and the summary."""
+    balls, probe, box, _ = fuzz_case(k)
+    balls = balls.copy()
+    rng = np.random.default_rng(5000 + k)
+    g = V.UpdateableTessellation(with_backup=False, precision=precision)
+    o = O.OracleUpdateable(with_backup=False)
+    assert g.init(balls, probe, box) == o.init(balls, probe, box)
+    n = len(balls)
+    for step in range(5):
+        big = step == 3 and k % 3 == 0
+        m = int(rng.integers(n // 2 + 1, n)) if big else int(rng.integers(1, max(2, n // 30)))
+        ids = np.sort(rng.choice(n, size=m, replace=False))
+        balls[ids, :3] += rng.normal(0.0, float(rng.choice([0.01, 0.1, 0.5])), size=(m, 3))
+        if step == 2:
+            balls[ids[: max(1, m // 4)], 3] *= rng.uniform(0.9, 1.1, size=max(1, m // 4))
+        assert g.update_with_changed(balls, ids.tolist()) == o.update_with_changed(balls, ids.tolist())
+        assert g.last_update_was_full_reinit() == o.last_update_was_full_reinit()
+        assert g.changed_ids().tolist() == o.changed_ids().tolist()
+        assert g.affected_ids().tolist() == o.affected_ids().tolist()
+        so = o.summary()
+        compare(g.summary(), so, precision, total_abs=_allowance(balls, probe, so) if precision == "fp32" else None)

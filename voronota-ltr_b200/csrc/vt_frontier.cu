@@ -154,11 +154,12 @@ __global__ void __launch_bounds__(kWarps * 32)
 }
 
 // collect_collision_pairs (updateable.rs:516-561): a involved and not excluded; b's
-// canonical ball involved and not excluded; a < b, or b a periodic image.
+// canonical ball involved and not excluded; a < b, or b a periodic image.  need > 0: also
+// mark[a] >= need or mark[b's canonical ball] >= need.
 template <bool FILL>
 __global__ void __launch_bounds__(kWarps * 32)
     k_upd_pairs(const uint32_t* __restrict__ list, const uint32_t* __restrict__ count, uint32_t n, int periodic,
-                ListsRef L, const uint8_t* __restrict__ excl, const uint32_t* __restrict__ mark,
+                ListsRef L, const uint8_t* __restrict__ excl, const uint32_t* __restrict__ mark, uint32_t need,
                 uint32_t* __restrict__ npair, const uint32_t* __restrict__ pair_off, uint32_t* __restrict__ pair_a,
                 uint32_t* __restrict__ pair_e, int32_t* __restrict__ nb_pair) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -166,6 +167,7 @@ __global__ void __launch_bounds__(kWarps * 32)
     for (uint32_t t = blockIdx.x * kWarps + w; t < m; t += gridDim.x * kWarps) {
         const uint32_t a = list ? list[t] : t;
         const bool a_ok = !excl[a];
+        const bool a_need = need == 0 || mark[a] >= need;
         const uint32_t cnt = L.cnt[a], off = L.off[a];
         uint32_t rank = FILL ? pair_off[a] : 0u;
         for (uint32_t e0 = 0; e0 < cnt; e0 += 32) {
@@ -174,7 +176,8 @@ __global__ void __launch_bounds__(kWarps * 32)
             if (e < cnt && a_ok) {
                 const uint32_t bid = L.id[off + e];
                 const uint32_t bc = periodic ? bid % n : bid;
-                gen = (!mark || mark[bc]) && !excl[bc] && ((periodic && bid >= n) || a < bid);
+                gen = (!mark || mark[bc]) && !excl[bc] && ((periodic && bid >= n) || a < bid) &&
+                      (a_need || mark[bc] >= need);
             }
             const unsigned bal = __ballot_sync(0xffffffffu, gen);
             if (FILL && e < cnt) {
@@ -416,11 +419,41 @@ __global__ void __launch_bounds__(kWarps * 32)
         }
     }
 }
-__global__ void k_redo_unsure(NewContacts nc, const uint32_t* __restrict__ nc_count, const uint8_t* __restrict__ unsure,
-                              uint32_t* __restrict__ redo_list, uint32_t* __restrict__ d_redo_count) {
+__global__ void k_table_update(NewContacts nc, const uint32_t* __restrict__ nc_count, TableRef T,
+                               uint32_t* __restrict__ err) {
     const uint32_t m = *nc_count;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
-        if (unsure[nc.a[k]] || unsure[nc.b[k]]) redo_list[atomicAdd(d_redo_count, 1u)] = nc.pair[k];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        const uint32_t a = nc.a[k], b = nc.b[k];
+        for (int side = 0; side < (a == b ? 1 : 2); ++side) {
+            const uint32_t i = side ? b : a;
+            const bool own_a = i == a;
+            uint32_t d = T.off[i];
+            const uint32_t e = T.off[i + 1];
+            while (d < e && !(T.a[d] == a && T.b[d] == b)) ++d;
+            if (d == e) {
+                atomicOr(err, kErrRefresh);
+                continue;
+            }
+            T.area[d] = nc.area[k];
+            T.arc[d] = nc.arc[k];
+            T.sa[d] = own_a ? nc.sa_a[k] : nc.sa_b[k];
+            T.pv[d] = own_a ? nc.pv_a[k] : nc.pv_b[k];
+            T.flags[d] = (uint8_t)((T.flags[d] & ~1u) | (nc.central[k] ? 1u : 0u));
+            if (T.gA) {
+                T.gA[d] = own_a ? nc.gaa[k] : nc.gbb[k];
+                T.gB[d] = own_a ? nc.gba[k] : nc.gab[k];
+            }
+        }
+    }
+}
+__global__ void k_list_flagged(const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
+                               const uint8_t* __restrict__ flag, uint32_t* __restrict__ out,
+                               uint32_t* __restrict__ d_out) {
+    const uint32_t m = *count;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+        const uint32_t i = list[t];
+        if (flag[i]) out[atomicAdd(d_out, 1u)] = i;
+    }
 }
 __device__ __forceinline__ double sas_weight(const double* w, const uint8_t* cell_flag, const double* cell_sas,
                                              uint32_t i) {
@@ -547,15 +580,15 @@ void launch_splice_lists(uint32_t n, const uint32_t* mark, const uint32_t* row_o
     count_launch();
 }
 void launch_upd_pairs(int fill, const uint32_t* list, const uint32_t* count, uint32_t max_count, uint32_t n,
-                      int periodic, ListsRef lists, const uint8_t* excl, const uint32_t* mark, uint32_t* npair,
-                      const uint32_t* pair_off, uint32_t* pair_a, uint32_t* pair_e, int32_t* nb_pair,
-                      cudaStream_t s) {
+                      int periodic, ListsRef lists, const uint8_t* excl, const uint32_t* mark, uint32_t need,
+                      uint32_t* npair, const uint32_t* pair_off, uint32_t* pair_a, uint32_t* pair_e,
+                      int32_t* nb_pair, cudaStream_t s) {
     const uint32_t m = list ? max_count : n;
     if (fill)
-        k_upd_pairs<true><<<gw(m), kWarps * 32, 0, s>>>(list, count, n, periodic, lists, excl, mark, npair, pair_off,
-                                                        pair_a, pair_e, nb_pair);
+        k_upd_pairs<true><<<gw(m), kWarps * 32, 0, s>>>(list, count, n, periodic, lists, excl, mark, need, npair,
+                                                        pair_off, pair_a, pair_e, nb_pair);
     else
-        k_upd_pairs<false><<<gw(m), kWarps * 32, 0, s>>>(list, count, n, periodic, lists, excl, mark, npair,
+        k_upd_pairs<false><<<gw(m), kWarps * 32, 0, s>>>(list, count, n, periodic, lists, excl, mark, need, npair,
                                                          pair_off, pair_a, pair_e, nb_pair);
     count_launch();
 }
@@ -590,9 +623,13 @@ void launch_table_cells(const uint32_t* list, const uint32_t* count, uint32_t ma
                                                         cell_band, unsure);
     count_launch();
 }
-void launch_redo_unsure(const NewContacts& nc, const uint32_t* nc_count, uint32_t max_nc, const uint8_t* unsure,
-                        uint32_t* redo_list, uint32_t* d_redo_count, cudaStream_t s) {
-    k_redo_unsure<<<gb(max_nc), kBlock, 0, s>>>(nc, nc_count, unsure, redo_list, d_redo_count); count_launch();
+void launch_table_update(const NewContacts& nc, const uint32_t* nc_count, uint32_t max_nc, TableRef tab,
+                         uint32_t* err, cudaStream_t s) {
+    k_table_update<<<gb(max_nc), kBlock, 0, s>>>(nc, nc_count, tab, err); count_launch();
+}
+void launch_list_flagged(const uint32_t* list, const uint32_t* count, uint32_t max_count, const uint8_t* flag,
+                         uint32_t* out, uint32_t* d_out, cudaStream_t s) {
+    k_list_flagged<<<gb(max_count), kBlock, 0, s>>>(list, count, flag, out, d_out); count_launch();
 }
 void launch_table_grad(uint32_t n, TableRef tab, const double* w, const uint8_t* cell_flag, const double* cell_sas,
                        const double4* sph, double* grad, cudaStream_t s) {

@@ -108,10 +108,11 @@ void launch_splice_lists(uint32_t n, const uint32_t* mark, const uint32_t* row_o
 // collect_collision_pairs with involvement (updateable.rs:516-561) over the listed balls
 // (list == null: all n).  Count pass writes npair[a]; fill pass writes pair_a, pair_e
 // (list entry of b) and nb_pair (pair index or -1) for every entry of a listed ball.
+// need > 0 keeps only the pairs with an end whose mark is at least need.
 void launch_upd_pairs(int fill, const uint32_t* list, const uint32_t* count, uint32_t max_count, uint32_t n,
-                      int periodic, ListsRef lists, const uint8_t* excl, const uint32_t* mark, uint32_t* npair,
-                      const uint32_t* pair_off, uint32_t* pair_a, uint32_t* pair_e, int32_t* nb_pair,
-                      cudaStream_t s);
+                      int periodic, ListsRef lists, const uint8_t* excl, const uint32_t* mark, uint32_t need,
+                      uint32_t* npair, const uint32_t* pair_off, uint32_t* pair_a, uint32_t* pair_e,
+                      int32_t* nb_pair, cudaStream_t s);
 // Kept pairs (keep_off = exclusive scan of keep flags) as canonical contacts
 // (compute_contact_summaries_with_dedup + deduplicate_and_canonicalize_contacts,
 // updateable.rs:565-631).
@@ -136,9 +137,16 @@ void launch_table_write_new(uint32_t n, const NewContacts& nc, TableRef nw, cons
 void launch_table_cells(const uint32_t* list, const uint32_t* count, uint32_t max_count, TableRef tab,
                         const double4* sph, const uint8_t* excl, uint8_t* cell_flag, double* cell_sas,
                         double* cell_vol, float cell_band, uint8_t* unsure, cudaStream_t s);
-// Appends to redo_list the pair of every new contact with an unsure end.
-void launch_redo_unsure(const NewContacts& nc, const uint32_t* nc_count, uint32_t max_nc, const uint8_t* unsure,
-                        uint32_t* redo_list, uint32_t* d_redo_count, cudaStream_t s);
+// Contact-table bit: a recomputed contact found no entry to overwrite (launch_table_update).
+constexpr uint32_t kErrRefresh = 128u;
+// Overwrites the values of the existing entries (same canonical ids) of every contact in
+// nc; the entries keep their place in each ball's order.
+void launch_table_update(const NewContacts& nc, const uint32_t* nc_count, uint32_t max_nc, TableRef tab,
+                         uint32_t* err, cudaStream_t s);
+// Appends to out the listed balls whose flag is set (in no particular order; the count
+// goes to *d_out, zeroed by the caller).
+void launch_list_flagged(const uint32_t* list, const uint32_t* count, uint32_t max_count, const uint8_t* flag,
+                         uint32_t* out, uint32_t* d_out, cudaStream_t s);
 // grad (n x 4, overwritten) = d(sum_i w_i SAS_i)/d(x, y, z, r) from the table's adjoint
 // coefficients (w == null: all 1; balls without a cell or with zero SAS weigh 0).
 void launch_table_grad(uint32_t n, TableRef tab, const double* w, const uint8_t* cell_flag, const double* cell_sas,

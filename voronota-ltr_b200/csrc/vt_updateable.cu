@@ -44,6 +44,8 @@ enum Word : int {
     kWOne = 9,       // constant 1 (a list length)
     kWId = 10,       // a one-element id list
     kWBig = 11,      // rows of a search longer than the warp sort buffer
+    kWUnsure = 12,   // affected balls with an uncertain compute_sas branch (FP32)
+    kWMarked = 13,   // balls marked for their FP64 refresh
     kWords = 16,
 };
 
@@ -207,6 +209,7 @@ struct vt_updateable {
     DBuf<uint32_t> keep_cnt, new_cnt, tot_cnt, cursor, tmp_k;
     DBuf<uint32_t> cell_redo;
     DBuf<uint8_t> ball_dirty, unsure;
+    DBuf<uint32_t> ulist, mark2, nflags2, noff2, aff2;
     DBuf<uint32_t> sum_flags, sum_off, out_a, out_b, out_cell_index;
     DBuf<double> out_area, out_arc, out_cell_sas, out_cell_vol, totals, partials;
     DBuf<uint8_t> out_central;
@@ -388,13 +391,14 @@ struct vt_updateable {
     }
 
     // Pairs (a, b) of involved balls (mark == null: all), updateable.rs:516-561.
-    uint32_t gen_pairs(UState& S, const uint32_t* list, const uint32_t* d_count, uint32_t m, const uint32_t* mk) {
+    uint32_t gen_pairs(UState& S, const uint32_t* list, const uint32_t* d_count, uint32_t m, const uint32_t* mk,
+                       uint32_t need = 0) {
         const uint32_t n = S.n;
         npair.ensure(n + 1);
         pair_off.ensure(n + 1);
         zero(npair.p, (size_t)n * 4);
         const ListsRef L = S.lists.ref(false);
-        launch_upd_pairs(0, list, d_count, m, n, S.periodic ? 1 : 0, L, S.excl.p, mk, npair.p, nullptr, nullptr,
+        launch_upd_pairs(0, list, d_count, m, n, S.periodic ? 1 : 0, L, S.excl.p, mk, need, npair.p, nullptr, nullptr,
                          nullptr, nullptr, stream);
         ensure_scan(n + 1);
         scan_u32(npair.p, pair_off.p, n, scan_tmp.p, stream);
@@ -402,7 +406,7 @@ struct vt_updateable {
         pair_a.ensure(P + 1);
         pair_e.ensure(P + 1);
         nb_pair.ensure(S.lists.E + 1);
-        launch_upd_pairs(1, list, d_count, m, n, S.periodic ? 1 : 0, L, S.excl.p, mk, npair.p, pair_off.p, pair_a.p,
+        launch_upd_pairs(1, list, d_count, m, n, S.periodic ? 1 : 0, L, S.excl.p, mk, need, npair.p, pair_off.p, pair_a.p,
                          pair_e.p, nb_pair.p, stream);
         return P;
     }
@@ -575,6 +579,47 @@ struct vt_updateable {
         return VT_OK;
     }
 
+    // FP32 updates: an affected ball whose compute_sas branch is uncertain on its FP32 sums
+    // (cell_from_sums' bands) has every contact recomputed in FP64, the table entries kept
+    // from earlier operations included (their FP32 values take part in the same sums), and
+    // then the cells of the ball and its neighbours are recomputed.  The uncertain balls
+    // are marked 2 and their neighbours 1; the pairs with an end marked 2 are recomputed,
+    // and their FP64 values replace the entries' values in place, so the table keeps the
+    // reference's entry order.
+    void refresh_unsure_cells(UState& S, const uint32_t* d_count, uint32_t A) {
+        const uint32_t n = S.n;
+        ulist.ensure(A + 1);
+        zero(w(kWUnsure), 4);
+        launch_list_flagged(S.affected.p, d_count, A, unsure.p, ulist.p, w(kWUnsure), stream);
+        const uint32_t U = read_word(w(kWUnsure));
+        stats.num_cell_redo = U;
+        if (U == 0) return;
+        mark2.ensure(n + 1);
+        nflags2.ensure(n + 1);
+        noff2.ensure(n + 2);
+        aff2.ensure(n + 1);
+        zero(mark2.p, (size_t)n * 4);
+        launch_mark_list(ulist.p, w(kWUnsure), U, mark2.p, 2, w(kWMarked), stream);
+        launch_mark_neighbours(ulist.p, w(kWUnsure), U, nullptr, S.lists.ref(false), n, mark2.p, 1, w(kWMarked),
+                               nullptr, stream);
+        launch_nonzero(mark2.p, n, nflags2.p, stream);
+        ensure_scan(n + 1);
+        scan_u32(nflags2.p, noff2.p, n, scan_tmp.p, stream);
+        launch_compact_index(noff2.p, n, aff2.p, stream);
+        const uint32_t A2 = read_word(noff2.p + n);
+        const uint32_t P2 = gen_pairs(S, aff2.p, noff2.p + n, A2, mark2.p, 2);
+        DevBufs b = pair_bufs(S, P2);
+        if (P2) {
+            launch_contact_f64(b, P2, 1, 0, stream);
+            launch_collect_redo(b, P2, stream);
+            launch_contact_serial(b, P2, 1, stream);
+        }
+        extract_new(b, P2);
+        if (P2) launch_table_update(nc_ref(), keep_off.p + P2, P2, S.tab.ref(), w(kWErr), stream);
+        launch_table_cells(aff2.p, noff2.p + n, A2, S.tab.ref(), sph.p, S.excl.p, S.cell_flag.p, S.cell_sas.p,
+                           S.cell_vol.p, 0.f, nullptr, stream);
+    }
+
     // update_using_affected (updateable.rs:476-514) for the involved balls (mark != 0),
     // listed sorted in S.affected (count on the device at d_count)
     void update_using_affected(UState& S, const uint32_t* d_count, uint32_t A) {
@@ -587,17 +632,7 @@ struct vt_updateable {
         const float band = (fp32 && P > 0) ? kCellBand : 0.f;
         launch_table_cells(S.affected.p, d_count, A, S.tab.ref(), sph.p, S.excl.p, S.cell_flag.p, S.cell_sas.p,
                            S.cell_vol.p, band, band > 0.f ? unsure.p : nullptr, stream);
-        if (band > 0.f) {
-            // new contacts at a cell with an uncertain compute_sas branch: FP64 values, then
-            // the new table entries and the cells again (kept entries keep their values)
-            zero(w(kWRedo), 4);
-            launch_redo_unsure(nc_ref(), keep_off.p + P, P, unsure.p, redo_list.p, w(kWRedo), stream);
-            launch_contact_f64(b, P, 1, 1, stream);
-            launch_new_contacts(P, keep_off.p, b, nc_ref(), stream);
-            launch_table_write_new(S.n, nc_ref(), S.tab.ref(), keep_cnt.p, new_cnt.p, tmp_k.p, w(kWErr), stream);
-            launch_table_cells(S.affected.p, d_count, A, S.tab.ref(), sph.p, S.excl.p, S.cell_flag.p, S.cell_sas.p,
-                               S.cell_vol.p, 0.f, nullptr, stream);
-        }
+        if (band > 0.f) refresh_unsure_cells(S, d_count, A);
     }
 
     // table size, cell count and error bits after an operation
@@ -631,6 +666,10 @@ struct vt_updateable {
         if (h_words[2] & kErrInvalid) {
             set_last_error("non-finite input or negative radius");
             return VT_ERR_INVALID;
+        }
+        if (h_words[2] & kErrRefresh) {
+            set_last_error("internal: an FP64 cell refresh met a contact missing from the contact table");
+            return VT_ERR_CUDA;
         }
         return VT_OK;
     }
