@@ -116,3 +116,27 @@ def test_random_trajectory(k, precision, fixed_grid):
         assert g.affected_ids().tolist() == o.affected_ids().tolist()
         so = o.summary()
         compare(g.summary(), so, precision, total_abs=_allowance(balls, probe, so) if precision == "fp32" else None)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_random_batches(precision):
+    """Batched calls over random mixes of empty, tiny (1-6 balls), cloud and lattice
+    structures, one probe per batch; every structure's result equals the oracle's."""
+    rng = np.random.default_rng(77)
+    for batch, probe in enumerate((0.0, 0.5, 1.4, 2.0)):
+        structs = []
+        for _ in range(int(rng.integers(5, 40))):
+            kind = int(rng.integers(0, 4))
+            if kind == 0:
+                structs.append(np.zeros((0, 4)))
+            elif kind == 1 or kind == 2:
+                n = int(rng.integers(1, 7)) if kind == 1 else int(rng.integers(20, 600))
+                side = (max(n, 2) / rng.uniform(0.01, 0.05)) ** (1.0 / 3.0)
+                structs.append(np.column_stack([rng.uniform(0.0, side, (n, 3)), rng.uniform(0.8, 2.5, n)]))
+            else:
+                structs.append(W.lattice_balls(int(rng.integers(50, 1500)), 4000 + batch * 100 + len(structs)))
+        r = V.compute_batch(structs, probe, precision)
+        for s, balls in enumerate(structs):
+            o = O.compute(balls, probe)
+            allow = _allowance(balls, probe, o) if precision == "fp32" and len(balls) else None
+            compare(r.structure(s), o, precision, total_abs=allow)
