@@ -140,3 +140,24 @@ def test_random_batches(precision):
             o = O.compute(balls, probe)
             allow = _allowance(balls, probe, o) if precision == "fp32" and len(balls) else None
             compare(r.structure(s), o, precision, total_abs=allow)
+
+
+@pytest.mark.parametrize("k", range(12))
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_random_solvent_spheres(k, precision):
+    """compute_solvent_spheres on the random structures (depth 0-2, with and without a
+    volume probe): the kept spheres equal the oracle's bit for bit (they follow the
+    exposure decisions), weights within the cell tolerances."""
+    balls, probe, box, _ = fuzz_case(k)
+    probe = max(probe, 0.5)
+    depth, volume_probe = k % 3, (0.0, 0.5)[k % 2]
+    g = V.compute_solvent_spheres_result(balls, probe, volume_probe, depth, box, precision)
+    o = O.solvent_spheres(balls, probe, volume_probe, depth, box)
+    assert len(g) == len(o.weight)
+    assert np.array_equal(g.xyz, o.xyz) and np.array_equal(g.parent.astype(np.uint64), o.parent)
+    dw = np.abs(g.weight - o.weight)
+    if precision == "fp64":
+        assert np.all(dw <= 1e-9 * (1 + np.abs(o.weight)))
+    else:
+        assert np.all(dw <= 1e-2)
+        assert abs(g.weight.sum() - o.weight.sum()) <= max(1e-6 * abs(o.weight.sum()), 1e-4)
