@@ -186,20 +186,40 @@ struct PairGeom {
 // treated as ill-conditioned (the point could be off by more than E).
 constexpr float kCondMax = 64.f;
 
-// intersection_of_plane_and_segment (geometry.rs:134-148)
-__device__ __forceinline__ V3<float> plane_segment_e(Dec<float, true>& d, V3<float> pp, V3<float> n, V3<float> a,
+// FP32 forms with the plane given by its unit normal n and offset h = n . p: the side of
+// x (halfspace_of_point_unit, geometry.rs:118-131, with the same kEps margin and band)
+// and the cut point of segment a-b (intersection_of_plane_and_segment, geometry.rs:
+// 134-148).  The pre-tests' normal is already unit, so no re-normalisation.  Written with
+// explicit roundings, which the compiler neither contracts nor reorders, so that every
+// instantiation of the kernel (with or without the arc moments) gives the same values.
+__device__ __forceinline__ float plane_offset(V3<float> p, V3<float> n) {
+    return __fmaf_rn(p.z, n.z, __fmaf_rn(p.y, n.y, __fmul_rn(p.x, n.x)));
+}
+__device__ __forceinline__ float plane_side(V3<float> n, float h, V3<float> x) {  // n . x - h
+    return __fmaf_rn(n.z, x.z, __fmaf_rn(n.y, x.y, __fmaf_rn(n.x, x.x, -h)));
+}
+__device__ __forceinline__ int halfspace_h(Dec<float, true>& d, V3<float> n, float h, V3<float> x, float tol) {
+    const float sd = plane_side(n, h, x);
+    d.band(sd - (float)kEps, tol);
+    d.band(sd + (float)kEps, tol);
+    if (sd - (float)kEps > 0.f) return 1;
+    if (sd + (float)kEps < 0.f) return -1;
+    return 0;
+}
+__device__ __forceinline__ V3<float> plane_segment_h(Dec<float, true>& d, V3<float> n, float h, V3<float> a,
                                                      V3<float> b, float E) {
-    V3<float> nn = normalize(n);
-    float da = sd_plane_unit(pp, nn, a);
-    float db = sd_plane_unit(pp, nn, b);
-    float dd = fabsf(da - db);
+    const float da = plane_side(n, h, a);
+    const float db = plane_side(n, h, b);
+    const float den = __fsub_rn(da, db);
+    const float dd = fabsf(den);
     d.band(dd - (float)kEps, 2.f * E);
     if (dd < (float)kEps) return a;
-    if (norm(b - a) > kCondMax * dd) d.unsure = true;  // cut grazing the edge
+    const V3<float> ab = {__fsub_rn(b.x, a.x), __fsub_rn(b.y, a.y), __fsub_rn(b.z, a.z)};
+    if (norm(ab) > kCondMax * dd) d.unsure = true;  // cut grazing the edge
     // a cut point is an output vertex: a correctly rounded division (the kernel's
     // approximate one is biased, moving every cut point the same way along its edge)
-    float t = __fdiv_rn(da, da - db);
-    return a + (b - a) * t;
+    const float t = __fdiv_rn(da, den);
+    return {__fmaf_rn(ab.x, t, a.x), __fmaf_rn(ab.y, t, a.y), __fmaf_rn(ab.z, t, a.z)};
 }
 // intersect_segment_with_circle (geometry.rs:258-280)
 __device__ __forceinline__ bool segment_circle_e(Dec<float, true>& d, const Sph<float>& c, V3<float> p_in,
@@ -444,6 +464,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             cid = c.id;
             cls = pretest(d, g, c.s, pc, pn);
         }
+        if constexpr (F) pc.x = plane_offset(pc, pn);  // FP32: the cut loop takes the plane as (pn, pn . pc)
         VT_SITE(1);
         if (__any_sync(kFull, cls == kDiscard)) {
             discarded = true;
@@ -453,7 +474,11 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
         while (cutmask) {
             int j = __ffs(cutmask) - 1;
             cutmask &= cutmask - 1;
-            V3<T> PC = shfl_v3(pc, j), PN = shfl_v3(pn, j);
+            V3<T> PC, PN = shfl_v3(pn, j);
+            if constexpr (F)
+                PC.x = __shfl_sync(kFull, pc.x, j);  // the plane offset
+            else
+                PC = shfl_v3(pc, j);
             uint32_t CID = __shfl_sync(kFull, cid, j);
             if (!init) {
                 len = init_contour(q, lane, g.a_id, g.ic, g.axis, (float)e0);
@@ -466,7 +491,11 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                 if (!__any_sync(kFull, cut)) continue;
             }
             // mark_contour (contact.rs:506-521)
-            bool out = lane < len && halfspace(d, PC, PN, q.p, e0) >= 0;
+            bool out;
+            if constexpr (F)
+                out = lane < len && halfspace_h(d, PN, PC.x, q.p, e0) >= 0;
+            else
+                out = lane < len && halfspace(d, PC, PN, q.p, e0) >= 0;
             unsigned om = __ballot_sync(kFull, out);
             VT_SITE(2);
             if (om == 0) continue;
@@ -518,7 +547,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             if (lane == ns || lane == ne) {
                 V3<T> ip;
                 if constexpr (F)
-                    ip = plane_segment_e(d, PC, PN, q.p, nbp.p, e0);
+                    ip = plane_segment_h(d, PN, PC.x, q.p, nbp.p, e0);
                 else
                     ip = plane_segment(d, PC, PN, q.p, nbp.p, 0.0);
                 if (lane == ns) {

@@ -260,17 +260,19 @@ __global__ void __launch_bounds__(kSearchWarps * 32, FILL ? 1 : 9) k_search(DevB
             }
             unsigned m = __ballot_sync(0xffffffffu, hit);
             uint32_t pos = hits + __popc(m & ((1u << lane) - 1u));
-            if (FILL && hit) {
-                if (big) {
-                    if (pos < row_cnt) {  // the count pass found exactly row_cnt
-                        b.nb_id[off + pos] = cid;
-                        b.nb_slot[off + pos] = cslot;
-                        b.nb_val[off + pos] = val;
+            if constexpr (FILL) {
+                if (hit) {
+                    if (big) {
+                        if (pos < row_cnt) {  // the count pass found exactly row_cnt
+                            b.nb_id[off + pos] = cid;
+                            b.nb_slot[off + pos] = cslot;
+                            b.nb_val[off + pos] = val;
+                        }
+                    } else if (pos < (uint32_t)kSortCap) {
+                        s_val[w][pos] = val;
+                        s_id[w][pos] = cid;
+                        s_slot[w][pos] = cslot;
                     }
-                } else if (pos < (uint32_t)kSortCap) {
-                    s_val[w][pos] = val;
-                    s_id[w][pos] = cid;
-                    s_slot[w][pos] = cslot;
                 }
             }
             if (!FILL) {  // pairs this ball generates (collect_collision_pairs, tessellation.rs:298-319)
