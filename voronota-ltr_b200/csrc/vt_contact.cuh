@@ -479,7 +479,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                 PC.x = __shfl_sync(kFull, pc.x, j);  // the plane offset
             else
                 PC = shfl_v3(pc, j);
-            uint32_t CID = __shfl_sync(kFull, cid, j);
             if (!init) {
                 len = init_contour(q, lane, g.a_id, g.ic, g.axis, (float)e0);
                 init = true;
@@ -505,6 +504,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                 discarded = true;
                 break;
             }
+            const uint32_t CID = __shfl_sync(kFull, cid, j);  // needed only when the mark cuts
             if (out) q.lid = q.rid = CID;
             if (len < 3) continue;  // cut_contour returns early (contact.rs:530-532)
             // cut_contour (contact.rs:534-626)
