@@ -198,22 +198,25 @@ int vt_engine_device_outputs(const vt_engine* e, vt_device_outputs* out);
 
 /* ---- gradient ----
  * No counterpart in the reference: the adjoint of
- *     L = sum_i w_sas[i] SAS_i + sum_k u_contact[k] area_k
- * with respect to every ball's x, y, z and r (SAS_i of a ball without a cell counts as 0;
- * contact k is the k-th contact of the tessellation's output).  The backward pass
- * recomputes each contact's contour in FP64 and differentiates the final region
- * analytically (boundary velocities of its edges and arcs); it does not store contours.
- * Balls of periodic images accumulate into the ball they image; the box is fixed.
- * A contact whose contour needed more than 32 points is not differentiated
- * (VT_ERR_CAPACITY). */
+ *     L = sum_i w_sas[i] SAS_i + sum_i v_volume[i] V_i + sum_k u_contact[k] area_k
+ * with respect to every ball's x, y, z and r (SAS_i and V_i of a ball without a cell
+ * count as 0; contact k is the k-th contact of the tessellation's output; V_i is the
+ * cell volume of compute_sas, types.rs:623-663).  The backward pass recomputes each
+ * contact's contour and differentiates the final region analytically (boundary
+ * velocities of its edges and arcs; the pyramid volumes through the radical planes'
+ * distances); it does not store contours.  Balls of periodic images accumulate into the
+ * ball they image; the box is fixed.  A contact whose contour needed more than 32 points
+ * is not differentiated (VT_ERR_CAPACITY). */
 /* After vt_engine_compute_device/_host (full tessellation, one structure): device arrays
- * d_w_sas (n doubles) and d_u_contact (one per contact) may be NULL; d_grad: n x 4
- * doubles, overwritten. */
-int vt_engine_grad_device(vt_engine* e, const double* d_w_sas, const double* d_u_contact, double* d_grad);
+ * d_w_sas and d_v_volume (n doubles each) and d_u_contact (one per contact) may each be
+ * NULL (no such term); d_grad: n x 4 doubles, overwritten. */
+int vt_engine_grad_device(vt_engine* e, const double* d_w_sas, const double* d_v_volume, const double* d_u_contact,
+                          double* d_grad);
 /* Forward (as vt_compute_tessellation, no groups) + adjoint on host arrays; u_contact
  * must have num_contacts = the tessellation's contact count entries. */
 int vt_grad(const double* xyzr, uint64_t n, double probe, const double* periodic_box9, int precision,
-            const double* w_sas, const double* u_contact, uint64_t num_contacts, double* grad_out);
+            const double* w_sas, const double* v_volume, const double* u_contact, uint64_t num_contacts,
+            double* grad_out);
 
 /* ---- batched structures ----
  * No counterpart in the reference (which tessellates one structure per call): S
@@ -324,14 +327,18 @@ int vt_upd_stats(const vt_updateable* h, vt_stats* out);
  * four or none).  Results equal the regular FP64 path's for the same lists.
  *
  * Limit: every listed a must have at most VT_NOALLOC_MAX_NEIGHBORS neighbours (the
- * scratch holds 128 contour points per pair); otherwise the call returns
- * VT_ERR_CAPACITY before computing anything.  The first call on a device looks up the
+ * scratch holds 192 contour points per pair, the peak a 57-entry list can reach);
+ * otherwise the call returns VT_ERR_CAPACITY before computing anything.  Malformed input
+ * (a pair or neighbour index not below num_spheres, offsets not ascending within the
+ * index array of d_nb_offsets[num_spheres] entries, a non-finite coordinate or a
+ * negative radius among the spheres the pairs read) returns VT_ERR_INVALID, also before
+ * any contact is computed.  The first call on a device looks up the
  * scratch's device address and uploads a small table, so make it before any stream
  * capture.  Calls share the one scratch array: calls that overlap on the GPU race and
  * must be serialised (one stream, or host-side ordering).  The call returns after its
  * work on `stream` (a cudaStream_t, NULL for the default stream) has finished. */
 #define VT_NOALLOC_MAX_NEIGHBORS 57
-#define VT_NOALLOC_SCRATCH_BYTES 6291712
+#define VT_NOALLOC_SCRATCH_BYTES 9437440
 int vt_contact_descriptors_noalloc(const double* d_spheres, uint64_t num_spheres, const uint32_t* d_nb_offsets,
                                    const uint32_t* d_nb_index, const uint32_t* d_pair_a, const uint32_t* d_pair_b,
                                    uint64_t num_pairs, uint8_t* d_status, double* d_area, double* d_arc_length,

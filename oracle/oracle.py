@@ -322,3 +322,62 @@ def solvent_spheres(balls, probe: float, volume_probe: float = 0.0, subdivision_
     finally:
         L.vto_solvent_free(h)
     return SolventResult(v[:, :3].copy(), v[:, 3].copy(), v[:, 4].copy(), par)
+
+
+def loss_weights_by_pair(id_a, id_b, u, num_balls):
+    """(sorted pair keys, weights) of per-contact weights u attached to the contacts' ball
+    pairs, so that a loss can look a pair's weight up under any perturbation (a pair that
+    is not in the list weighs 0)."""
+    key = np.asarray(id_a, np.int64) * int(num_balls) + np.asarray(id_b, np.int64)
+    order = np.argsort(key)
+    return key[order], np.asarray(u, np.float64)[order]
+
+
+def finite_difference_local(balls, probe: float, i: int, c: int, h: float, w=None, v=None, upair=None) -> float:
+    """Central difference (L(x + h e) - L(x - h e)) / 2h of
+    L = sum_j w_j SAS_j + sum_j v_j V_j + sum_(a,b) u_ab area_ab at coordinate c (x, y, z,
+    r) of ball i, computed by the oracle on the sub-structure that determines the change.
+
+    Moving ball i changes only contacts whose ends both intersect ball i (a contact is cut
+    only by balls intersecting both of its balls) and the cells of the balls intersecting
+    i.  Those are computed exactly from the balls within three neighbour hops (each hop at
+    most 2 max R): a contact needs the complete neighbour list of its lower ball, and a
+    cell all of its contacts.  The terms of balls and contacts farther away are left out
+    (they do not change).  upair = loss_weights_by_pair(...) of the full structure; w, v
+    are per-ball weights of the full structure (None: no such term).  Non-periodic."""
+    balls = np.asarray(balls, np.float64)
+    R = balls[:, 3] + probe
+    reach = 2.0 * R.max()
+    d = np.linalg.norm(balls[:, :3] - balls[i, :3], axis=1)
+    sub = np.nonzero(d <= 3.0 * reach + 4.0 * abs(h) + 0.1)[0]
+    li = int(np.searchsorted(sub, i))
+    # balls whose cells and contacts may change: those intersecting ball i (with margin)
+    near = d[sub] <= R[sub] + R[i] + 4.0 * abs(h) + 0.01
+    n = len(balls)
+
+    def loss(x):
+        o = compute(x, probe)
+        total = 0.0
+        ci = o.cells_index.astype(np.int64)
+        keep = near[ci]
+        gi = sub[ci[keep]]
+        if w is not None:
+            total += float(np.dot(w[gi], o.cells_sas[keep]))
+        if v is not None:
+            total += float(np.dot(v[gi], o.cells_vol[keep]))
+        if upair is not None:
+            a = o.contacts_a.astype(np.int64)
+            b = o.contacts_b.astype(np.int64)
+            m = near[a] | near[b]
+            k = sub[a[m]] * n + sub[b[m]]
+            ks, us = upair
+            pos = np.clip(np.searchsorted(ks, k), 0, max(len(ks) - 1, 0))
+            uu = np.where(ks[pos] == k, us[pos], 0.0) if len(ks) else np.zeros(len(k))
+            total += float(np.dot(uu, o.contacts_area[m]))
+        return total
+
+    xp = balls[sub].copy()
+    xm = balls[sub].copy()
+    xp[li, c] += h
+    xm[li, c] -= h
+    return (loss(xp) - loss(xm)) / (2.0 * h)

@@ -1,6 +1,7 @@
 """The hand-written adjoint against central finite differences.
 
-L = sum_i w_i SAS_i + sum_(a,b) u_ab area_ab with seeded w ~ U(0, 1) and u ~ N(0, 1)
+L = sum_i w_i SAS_i + sum_(a,b) u_ab area_ab with seeded w ~ U(0, 1) and u ~ N(0, 1), and
+with a volume term sum_i v_i V_i (v ~ U(0, 1))
 (u attached to the contact's ball pair, so contacts that appear under a perturbation
 carry no weight).  The gradient with respect to x, y, z and r of randomly chosen balls is
 checked against central differences with h = 1e-4 A in f64 of the GPU FP64 forward and of
@@ -32,20 +33,23 @@ def _weights(balls, probe, seed, box=None):
     return w, u, upair
 
 
-def _loss(sas_idx, sas, ida, idb, area, w, upair):
+def _loss(sas_idx, sas, ida, idb, area, w, upair, vol=None, v=None):
     ls = float(np.dot(w[sas_idx], sas))
     la = sum(upair.get((int(a), int(b)), 0.0) * x for a, b, x in zip(ida, idb, area))
-    return ls + la
+    lv = float(np.dot(v[sas_idx], vol)) if v is not None else 0.0
+    return ls + la + lv
 
 
-def _loss_gpu(balls, probe, w, upair, box=None):
+def _loss_gpu(balls, probe, w, upair, box=None, v=None):
     r = V.compute_tessellation_result(balls, probe, box, precision="fp64")
-    return _loss(r.cell_index.astype(np.int64), r.cell_sas_area, r.id_a, r.id_b, r.area, w, upair)
+    return _loss(r.cell_index.astype(np.int64), r.cell_sas_area, r.id_a, r.id_b, r.area, w, upair,
+                 r.cell_volume, v)
 
 
-def _loss_oracle(balls, probe, w, upair, box=None):
+def _loss_oracle(balls, probe, w, upair, box=None, v=None):
     o = O.compute(balls, probe, periodic_box=box)
-    return _loss(o.cells_index.astype(np.int64), o.cells_sas, o.contacts_a, o.contacts_b, o.contacts_area, w, upair)
+    return _loss(o.cells_index.astype(np.int64), o.cells_sas, o.contacts_a, o.contacts_b, o.contacts_area, w, upair,
+                 o.cells_vol, v)
 
 
 def _coords(n, k, seed):
@@ -86,6 +90,53 @@ def test_adjoint_matches_oracle_finite_differences():
         _check_fd(g[i, c], lambda b: _loss_oracle(b, 1.4, w, upair), balls, i, c)
 
 
+def _check_fd_local(g, balls, i, c, w, v, upair):
+    fd = O.finite_difference_local(balls, 1.4, i, c, H, w, v, upair)
+    if abs(g - fd) <= TOL * (1 + abs(fd)):
+        return abs(g - fd) / (1 + abs(fd))
+    fd2 = O.finite_difference_local(balls, 1.4, i, c, H / 10, w, v, upair)
+    err = abs(g - fd2) / (1 + abs(fd2))
+    assert err <= TOL, f"ball {i} coord {c}: adjoint {g} vs oracle differences {fd} (h 1e-4), {fd2} (h 1e-5)"
+    return err
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_differentiation_config_256_coordinates_vs_oracle(precision):
+    """The differentiation workload: 20,000 lattice balls, L = sum w SAS + sum u area with
+    w ~ U(0, 1), u ~ N(0, 1); the adjoint after the FP32 and the FP64 forward against the
+    oracle's central differences (h = 1e-4 A, f64) at 256 random coordinates (x, y, z, r),
+    each difference taken on the sub-structure that determines it
+    (oracle.finite_difference_local)."""
+    balls = W.lattice_balls(20000, 7)
+    o = O.compute(balls, 1.4)
+    rng = np.random.default_rng(20)
+    w = rng.uniform(0.0, 1.0, len(balls))
+    u_o = rng.normal(0.0, 1.0, len(o.contacts_a))
+    upair = O.loss_weights_by_pair(o.contacts_a, o.contacts_b, u_o, len(balls))
+    r = V.compute_tessellation_result(balls, 1.4, precision=precision)
+    k = r.id_a.astype(np.int64) * len(balls) + r.id_b.astype(np.int64)
+    pos = np.clip(np.searchsorted(upair[0], k), 0, len(upair[0]) - 1)
+    u = np.where(upair[0][pos] == k, upair[1][pos], 0.0)
+    g = V.grad(balls, 1.4, w, u, precision=precision)
+    errs = [_check_fd_local(g[i, c], balls, i, c, w, None, upair) for i, c in _coords(len(balls), 256, 30)]
+    assert len(errs) == 256
+
+
+def test_volume_adjoint_256_coordinates_vs_oracle():
+    """The same 20,000-ball structure with the volume term: L = sum w SAS + sum v V +
+    sum u area, v ~ U(0, 1), 256 coordinates against the oracle's central differences."""
+    balls = W.lattice_balls(20000, 7)
+    o = O.compute(balls, 1.4)
+    rng = np.random.default_rng(21)
+    w = rng.uniform(0.0, 1.0, len(balls))
+    v = rng.uniform(0.0, 1.0, len(balls))
+    u = rng.normal(0.0, 1.0, len(o.contacts_a))
+    upair = O.loss_weights_by_pair(o.contacts_a, o.contacts_b, u, len(balls))
+    g = V.grad(balls, 1.4, w, u, precision="fp64", v_volume=v)
+    for i, c in _coords(len(balls), 256, 31):
+        _check_fd_local(g[i, c], balls, i, c, w, v, upair)
+
+
 def test_separate_terms_and_fp32_forward():
     balls = W.lattice_balls(1200, 23)
     w, u, upair = _weights(balls, 1.4, 5)
@@ -113,6 +164,57 @@ def test_periodic_adjoint():
         _check_fd(g[i, c], lambda b: _loss_gpu(b, 1.4, w, upair, box), balls, i, c)
 
 
+def _vweights(n, seed):
+    return np.random.default_rng(seed).uniform(0.0, 1.0, n)
+
+
+def test_volume_adjoint_matches_gpu_finite_differences():
+    balls = W.lattice_balls(1500, 31)
+    w, u, upair = _weights(balls, 1.4, 31)
+    v = _vweights(len(balls), 32)
+    g = V.grad(balls, 1.4, w, u, precision="fp64", v_volume=v)
+    for i, c in _coords(len(balls), 40, 33):
+        _check_fd(g[i, c], lambda b: _loss_gpu(b, 1.4, w, upair, v=v), balls, i, c)
+
+
+def test_volume_adjoint_alone_matches_oracle_finite_differences():
+    """Only the volume term (w = 0, u = 0), against the CPU oracle; includes exposed and
+    buried balls of a small structure and a radius coordinate of each kind."""
+    balls = W.lattice_balls(600, 34)
+    v = _vweights(len(balls), 35)
+    z = np.zeros(len(balls))
+    g = V.grad(balls, 1.4, None, None, precision="fp64", v_volume=v)
+    g_sum = V.grad(balls, 1.4, z, None, precision="fp64", v_volume=v)
+    assert np.allclose(g, g_sum, rtol=1e-12, atol=1e-12)
+    for i, c in _coords(len(balls), 16, 36):
+        _check_fd(g[i, c], lambda b: _loss_oracle(b, 1.4, z, {}, v=v), balls, i, c)
+
+
+def test_volume_terms_add_and_fp32_forward():
+    balls = W.lattice_balls(1200, 37)
+    w, u, upair = _weights(balls, 1.4, 37)
+    v = _vweights(len(balls), 38)
+    g_v = V.grad(balls, 1.4, None, None, precision="fp64", v_volume=v)
+    g_wu = V.grad(balls, 1.4, w, u, precision="fp64")
+    g = V.grad(balls, 1.4, w, u, precision="fp64", v_volume=v)
+    assert np.allclose(g, g_v + g_wu, rtol=1e-12, atol=1e-9)
+    g32 = V.grad(balls, 1.4, w, u, precision="fp32", v_volume=v)
+    # x, y, z: the FP32 adjoint snaps vertices to FP64; the volume terms use the forward's
+    # FP32 areas and SAS (relative error ~1e-6 per contact, ~1e-4 per cell SAS)
+    assert np.allclose(g32[:, :3], g[:, :3], rtol=1e-5, atol=1e-5)
+    assert np.allclose(g32[:, 3], g[:, 3], rtol=1e-4, atol=1e-4)
+
+
+def test_periodic_volume_adjoint():
+    balls, side = W.periodic_box_balls(1500, seed=39)
+    box = {"corners": [(0.0, 0.0, 0.0), (side, side, side)]}
+    w, u, upair = _weights(balls, 1.4, 39, box)
+    v = _vweights(len(balls), 40)
+    g = V.grad(balls, 1.4, w, u, box, precision="fp64", v_volume=v)
+    for i, c in _coords(len(balls), 16, 41):
+        _check_fd(g[i, c], lambda b: _loss_gpu(b, 1.4, w, upair, box, v=v), balls, i, c)
+
+
 def test_torch_autograd_matches_c_abi():
     import torch
 
@@ -120,13 +222,16 @@ def test_torch_autograd_matches_c_abi():
 
     balls = W.lattice_balls(1000, 24)
     w, u, _ = _weights(balls, 1.4, 10)
+    v = _vweights(len(balls), 11)
     x = torch.from_numpy(balls).cuda().requires_grad_(True)
-    sas, area, ida, idb = tessellate(x, 1.4, precision="fp64")
+    sas, vol, area, ida, idb = tessellate(x, 1.4, precision="fp64")
     r = V.compute_tessellation_result(balls, 1.4, precision="fp64")
     assert np.array_equal(ida.cpu().numpy(), r.id_a.astype(np.int64))
-    loss = (torch.from_numpy(w).cuda() * sas).sum() + (torch.from_numpy(u).cuda() * area).sum()
+    assert np.allclose(vol.detach().cpu().numpy()[r.cell_index.astype(np.int64)], r.cell_volume, rtol=1e-12)
+    loss = ((torch.from_numpy(w).cuda() * sas).sum() + (torch.from_numpy(u).cuda() * area).sum()
+            + (torch.from_numpy(v).cuda() * vol).sum())
     loss.backward()
-    g = V.grad(balls, 1.4, w, u, precision="fp64")
+    g = V.grad(balls, 1.4, w, u, precision="fp64", v_volume=v)
     assert np.allclose(x.grad.cpu().numpy(), g, rtol=1e-12, atol=1e-10)
 
 

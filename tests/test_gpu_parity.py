@@ -216,11 +216,50 @@ def test_invalid_input_raises():
     e.close()
 
 
+_ORACLE_100K = {}
+
+
+def _oracle_100k(kind):
+    """The oracle's results on the 100k-ball lattice (seed 0, probe 1.4), computed once:
+    'full' = compute_tessellation, 'groups' = compute_contacts_only with groups 0 for
+    x < 0 and 1 otherwise."""
+    if kind not in _ORACLE_100K:
+        balls = W.lattice_balls(100000, 0)
+        if kind == "full":
+            _ORACLE_100K[kind] = O.compute(balls, 1.4)
+        else:
+            _ORACLE_100K[kind] = O.compute(balls, 1.4, groups=W.x_sign_groups(balls), contacts_only=True)
+    return _ORACLE_100K[kind]
+
+
 def test_fp32_large_lattice_pair_set_and_totals():
     balls = W.lattice_balls(100000, 0)
-    o = O.compute(balls, 1.4)
+    o = _oracle_100k("full")
     stats = compare(gpu(balls, 1.4, precision="fp32"), o, "fp32")
     assert stats["rel_sas"] <= 1e-6
+
+
+def test_fp64_large_lattice():
+    """The 100k-ball drop-in configuration through the plain FP64 path."""
+    balls = W.lattice_balls(100000, 0)
+    compare(gpu(balls, 1.4, precision="fp64"), _oracle_100k("full"), "fp64")
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_large_lattice_contacts_only_with_groups(prec):
+    """compute_contacts_only on the 100k-ball lattice with groups 0 for x < 0 and 1
+    otherwise: the inter-group contact set bit-exact, areas within the precision's
+    tolerance, and each contact equal to the same pair's contact in the grouped full
+    tessellation (contacts-only == full, tests/contacts_only.rs)."""
+    balls = W.lattice_balls(100000, 0)
+    groups = W.x_sign_groups(balls)
+    r = gpu(balls, 1.4, groups=groups, precision=prec, contacts_only=True)
+    compare(r, _oracle_100k("groups"), prec, contacts_only=True)
+    g = balls[:, 0] < 0
+    assert len(r.id_a) > 1000 and np.all(g[r.id_a.astype(np.int64)] != g[r.id_b.astype(np.int64)])
+    full = gpu(balls, 1.4, groups=groups, precision=prec)
+    assert np.array_equal(full.id_a, r.id_a) and np.array_equal(full.id_b, r.id_b)
+    assert np.allclose(full.area, r.area, rtol=0, atol=1e-10 if prec == "fp64" else 1e-3)
 
 
 def test_engine_device_path_matches_host_path():

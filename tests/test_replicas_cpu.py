@@ -11,7 +11,10 @@ import socket
 import pytest
 import torch.multiprocessing as mp
 
-from voronota_ltr.replicas import Ranks, partition, replica_throughput
+import numpy as np
+
+from voronota_ltr import workloads as W
+from voronota_ltr.replicas import Ranks, partition, partition_weighted, replica_throughput
 
 
 def _free_port():
@@ -30,8 +33,12 @@ def _worker(rank, world, port, q):
     ms = 10.0 + 5.0 * rank  # rank 1 is the slowest
     m = R.max(ms)
     start, stop = partition(4096, world, rank)
+    sizes = W.batch_sizes(4096)
+    ws, we = partition_weighted(sizes, world, rank)
+    balls = float(sizes[ws:we].sum())
+    total = R.max(balls)
     R.close()
-    q.put((rank, m, start, stop))
+    q.put((rank, m, start, stop, ws, we, balls, total))
 
 
 def test_two_gloo_ranks():
@@ -46,8 +53,13 @@ def test_two_gloo_ranks():
         p.join(timeout=60)
         assert p.exitcode == 0
     assert [o[1] for o in out] == [15.0, 15.0]  # every rank sees the max
-    assert out[0][2:] == (0, 2048) and out[1][2:] == (2048, 4096)
+    assert out[0][2:4] == (0, 2048) and out[1][2:4] == (2048, 4096)
     assert replica_throughput(100_000, 2, out[0][1]) == pytest.approx(2 * 100_000 / 0.015)
+    # the batch split by balls: contiguous, complete, balanced
+    assert out[0][4] == 0 and out[0][5] == out[1][4] and out[1][5] == 4096
+    sizes = W.batch_sizes(4096)
+    assert out[0][6] + out[1][6] == float(sizes.sum())
+    assert abs(out[0][6] - out[1][6]) <= sizes.max()
 
 
 def test_partition_covers_everything_once():
@@ -60,6 +72,21 @@ def test_partition_covers_everything_once():
             assert max(sizes) - min(sizes) <= 1
     with pytest.raises(ValueError):
         partition(10, 2, 2)
+
+
+def test_partition_weighted_balances_and_covers():
+    sizes = W.batch_sizes(4096)
+    for world in (1, 2, 3, 4, 8):
+        blocks = [partition_weighted(sizes, world, r) for r in range(world)]
+        assert blocks[0][0] == 0 and blocks[-1][1] == len(sizes)
+        assert all(blocks[i][1] == blocks[i + 1][0] for i in range(world - 1))
+        loads = [sizes[a:b].sum() for a, b in blocks]
+        assert max(loads) - min(loads) <= 2 * sizes.max()
+    assert partition_weighted([], 4, 2) == (0, 0)
+    assert [partition_weighted([5], 3, r) for r in range(3)] in ([(0, 1), (1, 1), (1, 1)], [(0, 0), (0, 1), (1, 1)],
+                                                                  [(0, 0), (0, 0), (0, 1)])
+    with pytest.raises(ValueError):
+        partition_weighted([1, 2], 2, 2)
 
 
 def test_single_rank_needs_no_process_group():

@@ -1,5 +1,5 @@
 // vt_adjoint.cu -- hand-written adjoint of
-//     L = sum_i w_i SAS_i + sum_k u_k area_k
+//     L = sum_i w_i SAS_i + sum_i v_i V_i + sum_k u_k area_k
 // with respect to the centres and radii of the balls (no counterpart in the reference).
 //
 // The backward pass recomputes every contact's contour (FP64 warp kernel, the same
@@ -24,8 +24,21 @@
 //               / (D rho)          (per unit length on the unit sphere, times 1/R_a),
 //   giving d SAS_a = 2 R_a dR_a |E_a| + R_a^2 d|E_a|; the arcs bound E_b the same way.
 //
+// * The cell volume is V_a = SAS_a R_a / 3 + sum_b pyr_ab (types.rs:647-649) with the
+//   pyramid pyr_ab = |q_ab - p_a| area_ab / 3 signed by the solid angle (contact.rs:
+//   374-379).  That sign is negative exactly when the circle centre q_ab lies behind p_a
+//   as seen from p_b (contact.rs:839-845), so pyr_ab = t_ab area_ab / 3 with the signed
+//   distance t_ab = (D^2 + R_a^2 - R_b^2) / (2 D) from p_a to the radical plane.  Hence
+//   v_a V_a adds v_a R_a / 3 to the SAS weight of a, v_a SAS_a / 3 to dL/dR_a, and, per
+//   contact, (v_a t_ab + v_b t_ba) / 3 to its area weight plus area/3 times the
+//   derivatives of t_ab and t_ba (vt_adjoint.cuh).  Where compute_sas leaves SAS at 0
+//   (no arcs, or the full-sphere sanity reset of types.rs:651-657) V is the pyramid sum
+//   alone, which the zero SAS weight of such a cell gives; a detached ball (V = 4 pi R^3
+//   / 3, SAS = 4 pi R^2) gets dV/dR = SAS the same way.
+//
 // Periodic images contribute to the ball they image (id mod n); only balls with a cell
-// whose SAS is positive receive SAS terms.  Accumulation uses double atomics.
+// whose SAS is positive receive SAS terms, only balls with a cell volume terms.
+// Accumulation uses double atomics.
 #include <cmath>
 
 #include "vt_adjoint.cuh"
@@ -38,23 +51,36 @@ constexpr int kWarps = 4;
 
 __device__ __forceinline__ Sph<double> sph_of(double4 v) { return {{v.x, v.y, v.z}, v.w}; }
 
-__global__ void k_w_eff(uint32_t n, const double* __restrict__ w, const uint8_t* __restrict__ cell_flag,
-                        const double* __restrict__ cell_sas, double* __restrict__ w_eff) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        w_eff[i] = (w && cell_flag[i] && cell_sas[i] > 0.0) ? w[i] : 0.0;
+// w_eff: the SAS weight of each ball, w + v R / 3 (the SAS R / 3 part of its volume),
+// where the ball has a cell with a positive SAS; v_eff: the volume weight where it has a
+// cell (null without volume weights)
+__global__ void k_w_eff(uint32_t n, const double* __restrict__ w, const double* __restrict__ v,
+                        const uint8_t* __restrict__ cell_flag, const double* __restrict__ cell_sas,
+                        const double4* __restrict__ sph, double* __restrict__ w_eff, double* __restrict__ v_eff) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const bool cell = cell_flag[i] != 0;
+        const double vi = (v && cell) ? v[i] : 0.0;
+        w_eff[i] = (cell && cell_sas[i] > 0.0) ? (w ? w[i] : 0.0) + vi * sph[i].w / 3.0 : 0.0;
+        if (v_eff) v_eff[i] = vi;
+    }
 }
-// d SAS_i / d R_i at fixed exposed directions: 2 SAS_i / R_i
-__global__ void k_sas_scale(uint32_t n, const double* __restrict__ w_eff, const double* __restrict__ cell_sas,
-                            const double4* __restrict__ sph, double* __restrict__ grad) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        if (w_eff[i] != 0.0) grad[4 * (size_t)i + 3] += w_eff[i] * 2.0 * cell_sas[i] / sph[i].w;
+// d SAS_i / d R_i at fixed exposed directions: 2 SAS_i / R_i; and d(SAS_i R_i / 3) / dR_i
+// at fixed SAS: SAS_i / 3
+__global__ void k_sas_scale(uint32_t n, const double* __restrict__ w_eff, const double* __restrict__ v_eff,
+                            const double* __restrict__ cell_sas, const double4* __restrict__ sph,
+                            double* __restrict__ grad) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double vi = v_eff ? v_eff[i] : 0.0;
+        if (w_eff[i] != 0.0 || (vi != 0.0 && cell_sas[i] > 0.0))
+            grad[4 * (size_t)i + 3] += w_eff[i] * 2.0 * cell_sas[i] / sph[i].w + vi * cell_sas[i] / 3.0;
+    }
 }
 
 // FP64 adjoint: all valid pairs, or (from_list) the pairs the FP32 adjoint listed.  At
 // most 128 registers (4 resident blocks), like the FP64 contact kernel.
 __global__ void __launch_bounds__(kWarps * 32, 4)
     k_adjoint64(DevBufs b, uint32_t P, int from_list, const double* __restrict__ u_contact,
-                const double* __restrict__ w_eff, double* __restrict__ grad) {
+                const double* __restrict__ w_eff, const double* __restrict__ v_eff, double* __restrict__ grad) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t n = b.n;
     const uint32_t count = from_list ? *b.d_redo_count : P;
@@ -64,7 +90,7 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
         const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
         const uint32_t bid = b.nb_id[eb];
         AdjPair G;
-        if (!adjoint_weights(b, p, a, bid, u_contact, w_eff, G)) continue;
+        if (!adjoint_weights(b, p, a, bid, u_contact, w_eff, v_eff, G)) continue;
         const uint32_t off = b.nb_off[a], cnt = b.nb_cnt[a];
         PairGeom<double> g;
         g.A = sph_of(b.sph[a]);
@@ -122,23 +148,24 @@ void set_hex_table_adjoint() {
     cudaMemcpyToSymbol(c_hex_n, &n, sizeof(int));
 }
 
-void launch_adjoint(const DevBufs& b, uint32_t P, const double* w_sas, const double* u_contact, double* w_eff,
-                    double* grad, cudaStream_t s) {
+void launch_adjoint(const DevBufs& b, uint32_t P, const double* w_sas, const double* v_vol, const double* u_contact,
+                    double* w_eff, double* v_eff, double* grad, cudaStream_t s) {
     const uint32_t n = b.n;
+    double* ve = v_vol ? v_eff : nullptr;
     cudaMemsetAsync(grad, 0, 4 * sizeof(double) * n, s);
-    k_w_eff<<<gb(n), 256, 0, s>>>(n, w_sas, b.cell_flag, b.cell_sas, w_eff); count_launch();
+    k_w_eff<<<gb(n), 256, 0, s>>>(n, w_sas, v_vol, b.cell_flag, b.cell_sas, b.sph, w_eff, ve); count_launch();
     if (P) {
         if (b.nb_rel) {
             // FP32 contours; pairs with a decision in the band are redone in FP64
             cudaMemsetAsync(b.d_redo_count, 0, sizeof(uint32_t), s);
-            launch_adjoint_f32(b, P, u_contact, w_eff, grad, s);
-            k_adjoint64<<<grid_blocks(P, kWarps, 148 * 64), kWarps * 32, 0, s>>>(b, P, 1, u_contact, w_eff, grad);
+            launch_adjoint_f32(b, P, u_contact, w_eff, ve, grad, s);
+            k_adjoint64<<<grid_blocks(P, kWarps, 148 * 64), kWarps * 32, 0, s>>>(b, P, 1, u_contact, w_eff, ve, grad);
         } else {
-            k_adjoint64<<<grid_blocks(P, kWarps, 148 * 64), kWarps * 32, 0, s>>>(b, P, 0, u_contact, w_eff, grad);
+            k_adjoint64<<<grid_blocks(P, kWarps, 148 * 64), kWarps * 32, 0, s>>>(b, P, 0, u_contact, w_eff, ve, grad);
         }
         count_launch();
     }
-    k_sas_scale<<<gb(n), 256, 0, s>>>(n, w_eff, b.cell_sas, b.sph, grad); count_launch();
+    k_sas_scale<<<gb(n), 256, 0, s>>>(n, w_eff, ve, b.cell_sas, b.sph, grad); count_launch();
 }
 
 }  // namespace vt

@@ -1,7 +1,8 @@
 // vt_adjoint.cuh -- the adjoint epilogue shared by the FP64 and FP32 adjoint kernels
 // (vt_adjoint.cu, vt_contact32.cu): from a contact's final contour, the gradient of
-// u * area + w_a * SAS_a + w_b * SAS_b with respect to the balls' centres and radii.
-// The formulas are derived in vt_adjoint.cu.
+// u * area + w_a * SAS_a + w_b * SAS_b + v_a * pyr_a + v_b * pyr_b with respect to the
+// balls' centres and radii (pyr_a = t_ab area / 3, the contact's pyramid volume seen from
+// a).  The formulas are derived in vt_adjoint.cu.
 #pragma once
 #include "vt_contact.cuh"
 #include "vt_pipeline.cuh"
@@ -30,7 +31,9 @@ struct AdjPair {
     V3<double> pa, pb, q, axis;  // centres, circle centre, unit axis a -> b
     double Ra, Rb, rho;
     uint32_t a, bid;
-    double u, wa, wb;
+    double u, wa, wb;  // area weight (output contact), SAS weights of a and b
+    double va, vb;     // volume weights of a and b (0 without a cell, or b an image)
+    double area;       // the forward's area of the contact
 };
 
 // Warp-collective: every lane calls it.  Lane k < len holds contour point P (absolute),
@@ -43,9 +46,14 @@ __device__ __forceinline__ void adjoint_pair(const AdjPair& G, bool full, int le
                                              double* grad, uint32_t n) {
     const int lane = threadIdx.x & 31;
     const V3<double> pa = G.pa, pb = G.pb, q = G.q;
-    const double Ra = G.Ra, Rb = G.Rb, rho = G.rho, u = G.u, wa = G.wa, wb = G.wb;
+    const double Ra = G.Ra, Rb = G.Rb, rho = G.rho, wa = G.wa, wb = G.wb;
     const V3<double> dab = pb - pa;
     const double D2 = dot(dab, dab), D = sqrt(D2);
+    // the pyramid volumes t_ab A / 3 and t_ba A / 3 weigh the area like u does
+    // (t_ab = (D^2 + Ra^2 - Rb^2) / (2 D): signed distance from p_a to the radical plane)
+    const double dRR = Ra * Ra - Rb * Rb;
+    const double t_ab = 0.5 * D + dRR / (2.0 * D), t_ba = D - t_ab;
+    const double u = G.u + (G.va * t_ab + G.vb * t_ba) / 3.0;
     V3<double> ga = mk<double>(0, 0, 0), gb = mk<double>(0, 0, 0);
     double gra = 0.0, grb = 0.0, Lk = 0.0;
     V3<double> Xk = mk<double>(0, 0, 0);
@@ -104,6 +112,18 @@ __device__ __forceinline__ void adjoint_pair(const AdjPair& G, bool full, int le
             gra += wa * L * cmix * s - wb * Rb * Ra * L * s;
             grb += wb * L * cmix * s - wa * Ra * Rb * L * s;
         }
+        if (G.va != 0.0 || G.vb != 0.0) {
+            // pyramid volumes through t_ab and t_ba at fixed area:
+            // dt_ab/dD = 1/2 - dRR/(2 D^2), dt_ab/dRa = Ra/D, dt_ab/dRb = -Rb/D, t_ba = D - t_ab
+            const double c = G.area / 3.0;
+            const double k = dRR / (2.0 * D2);
+            const double gD = c * (G.va * (0.5 - k) + G.vb * (0.5 + k));
+            const V3<double> nh = dab / D;
+            ga = ga - nh * gD;
+            gb = gb + nh * gD;
+            gra += c * (G.va - G.vb) * Ra / D;
+            grb += c * (G.vb - G.va) * Rb / D;
+        }
         adj_add_grad(grad, G.a, n, ga, gra);
         adj_add_grad(grad, G.bid, n, gb, grb);
     }
@@ -158,14 +178,19 @@ __device__ __forceinline__ V3<double> snap_vertex(const AdjPair& G, V3<double> y
     return norm2(y1 - y0) <= norm2(y2 - y0) ? y1 : y2;
 }
 
-// Weight of pair p's contact: u of its output contact (kept pairs), w of both ends.
+// Weights of pair p's contact: u of its output contact (kept pairs), w and v of both
+// ends (a periodic image's cell is its own ball's, reached through that ball's pairs).
 __device__ __forceinline__ bool adjoint_weights(const DevBufs& b, uint32_t p, uint32_t a, uint32_t bid,
-                                                const double* u_contact, const double* w_eff, AdjPair& G) {
+                                                const double* u_contact, const double* w_eff,
+                                                const double* v_eff, AdjPair& G) {
     const bool kept = b.keep_off[p + 1] != b.keep_off[p];
     G.u = (u_contact && kept) ? u_contact[b.keep_off[p]] : 0.0;
     G.wa = w_eff[a];
     G.wb = bid < b.n ? w_eff[bid] : 0.0;
-    return G.u != 0.0 || G.wa != 0.0 || G.wb != 0.0;
+    G.va = v_eff ? v_eff[a] : 0.0;
+    G.vb = (v_eff && bid < b.n) ? v_eff[bid] : 0.0;
+    G.area = b.p_area[p];
+    return G.u != 0.0 || G.wa != 0.0 || G.wb != 0.0 || G.va != 0.0 || G.vb != 0.0;
 }
 
 }  // namespace vt

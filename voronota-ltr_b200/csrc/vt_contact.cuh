@@ -29,21 +29,6 @@
 
 namespace vt {
 
-// Debug builds (-DVT_DEBUG_SITES) record the first pipeline step at which an FP32
-// decision became unsure; product builds compile the markers away.
-#ifdef VT_DEBUG_SITES
-#define VT_SITE(k)                                             \
-    do {                                                       \
-        if constexpr (F) {                                     \
-            if (res.site < 0 && __any_sync(kFull, d.unsure)) res.site = (k); \
-        }                                                      \
-    } while (0)
-#else
-#define VT_SITE(k) \
-    do {           \
-    } while (0)
-#endif
-
 constexpr unsigned kFull = 0xffffffffu;
 constexpr float kF32Eps = 1.1920929e-7f;
 
@@ -322,7 +307,6 @@ struct WarpContact {
     double xm[3];  // first moment of the contact's arcs about a's centre (want_xm)
     bool central;
     bool merged;  // two close points were merged (the kept point takes the other's id)
-    int site;  // debug builds: first step with an unsure decision
 };
 
 // Solid angle (contact.rs:797-848) summed over the warp's contour.  ea0 / ea1 bound the
@@ -429,7 +413,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
     res.area = res.arc = res.sa_a = res.sa_b = res.pv_a = res.pv_b = 0.0;
     res.xm[0] = res.xm[1] = res.xm[2] = 0.0;
     res.central = false;
-    res.site = -1;
     res.merged = false;
 
     // contact.rs:206-218
@@ -441,7 +424,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
     g.ic = intersection_circle(g.A, g.B);
     g.axis = normalize(g.B.c - g.A.c);
     if (d.less_eq(g.ic.r, (T)0, e0)) {
-        VT_SITE(0);
         res.unsure = __any_sync(kFull, d.unsure);
         return res;
     }
@@ -465,7 +447,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             cls = pretest(d, g, c.s, pc, pn);
         }
         if constexpr (F) pc.x = plane_offset(pc, pn);  // FP32: the cut loop takes the plane as (pn, pn . pc)
-        VT_SITE(1);
         if (__any_sync(kFull, cls == kDiscard)) {
             discarded = true;
             break;
@@ -496,7 +477,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             else
                 out = lane < len && halfspace(d, PC, PN, q.p, e0) >= 0;
             unsigned om = __ballot_sync(kFull, out);
-            VT_SITE(2);
             if (om == 0) continue;
             int nout = __popc(om);
             if (nout >= len) {  // mark_and_cut_contour clears (contact.rs:496-499)
@@ -562,7 +542,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                 q.p = ip;
                 q.ang = 0;
             }
-            VT_SITE(3);
             // merge very close points (contact.rs:622-626): lane ns holds the new point ps
             // and takes pe from lane ne
             const V3<T> pe = shfl_v3(q.p, ne);
@@ -574,7 +553,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                 }
                 close = !(dse - (T)kEps > (T)0);
             }
-            VT_SITE(4);
             if (__any_sync(kFull, close)) {
                 res.merged = true;
                 const uint32_t erid = __shfl_sync(kFull, q.rid, ne);
@@ -614,7 +592,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             in = d.less_eq(dc2, r2, tol);
         }
         unsigned outm = __ballot_sync(kFull, lane < len && !in);
-        VT_SITE(5);
         if (outm != 0) {
             int nx = lane + 1 < len ? lane + 1 : 0;
             Pt<T> v = shfl_pt(q, nx);
@@ -691,7 +668,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                     }
                 }
             }
-            VT_SITE(6);
             int insertions = __reduce_add_sync(kFull, (unsigned)k);
             if (insertions == 0) {
                 res.unsure = __any_sync(kFull, d.unsure);
@@ -768,7 +744,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                 }
                 a = directed_angle(d, g.ic.c, q.p, v2.p, g.ic.c + g.axis, tol_dir);
             }
-            VT_SITE(7);
             q.ang = a;
             sum_arc = lsum(a, len);
             // full circle after all (contact.rs:765-768): contour cleared, area stays 0
@@ -779,7 +754,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                 return res;
             }
         }
-        VT_SITE(8);
         int nx = lane + 1 < len ? lane + 1 : 0;
         Pt<T> v = shfl_pt(q, nx);
         // calculate_contour_area (contact.rs:773-793)
@@ -802,7 +776,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
     }
     // area <= 0 -> None (contact.rs:329-331)
     bool area_none = d.less_eq(area, (T)0, area_tol);
-    VT_SITE(9);
     if (area_none) {
         res.unsure = __any_sync(kFull, d.unsure);
         return res;
@@ -813,7 +786,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
     {
         const T fe = (T)1e-10;
         bool reflex = on && d.greater(q.ang - fe, (T)kPi, ang_err);
-        VT_SITE(10);
         if (__any_sync(kFull, reflex)) {
             central = true;
         } else {
@@ -839,7 +811,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                 }
             }
             central = !__any_sync(kFull, bad);
-            VT_SITE(11);
         }
     }
 
@@ -894,7 +865,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             }
         }
         const double sa = sab[0], sb = sab[1];
-        VT_SITE(13);
         T sign_a = sa < 0.0 ? (T)-1 : (T)1;
         T sign_b = sb < 0.0 ? (T)-1 : (T)1;
         res.sa_a = sa;

@@ -22,10 +22,6 @@ namespace {
 #endif
 constexpr int kWarps = VT_C32_WARPS;
 
-#ifdef VT_DEBUG_SITES
-__device__ unsigned long long g_debug_sites[32];
-#endif
-
 // One pair: the FP32 contour and the descriptor, written to the pair's outputs.
 template <bool FULL, bool XM>
 __device__ __forceinline__ void contact_pair32(const DevBufs& b, uint32_t p, float band) {
@@ -52,9 +48,6 @@ __device__ __forceinline__ void contact_pair32(const DevBufs& b, uint32_t p, flo
         return r;
     };
     WarpContact r = contact_warp<float, true, FULL, XM>(g, (int)cnt, (int)(eb - off), nbf);
-#ifdef VT_DEBUG_SITES
-    if (lane == 0 && r.unsure) atomicAdd(&g_debug_sites[r.site < 0 ? 31 : r.site], 1ull);
-#endif
     if (lane == 0) {
         uint8_t st = (r.valid ? kValid : 0) | (r.unsure ? kUnsure : 0) | (r.overflow ? kOverflow : 0);
         b.p_status[p] = st;
@@ -104,7 +97,7 @@ __global__ void __launch_bounds__(W * 32, VT_C32_MINB * 4 / W)
 // the FP64 adjoint.
 __global__ void __launch_bounds__(kWarps * 32, 4)
     k_adjoint32(DevBufs b, uint32_t P, float band, const double* __restrict__ u_contact,
-                const double* __restrict__ w_eff, double* __restrict__ grad) {
+                const double* __restrict__ w_eff, const double* __restrict__ v_eff, double* __restrict__ grad) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t n = b.n;
     for (uint32_t p = blockIdx.x * kWarps + w; p < P; p += gridDim.x * kWarps) {
@@ -112,7 +105,7 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
         const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
         const uint32_t bid = b.nb_id[eb];
         AdjPair G;
-        if (!adjoint_weights(b, p, a, bid, u_contact, w_eff, G)) continue;
+        if (!adjoint_weights(b, p, a, bid, u_contact, w_eff, v_eff, G)) continue;
         const uint32_t off = b.nb_off[a], cnt = b.nb_cnt[a];
         const double4 A4 = b.sph[a], B4 = b.sph[b.nb_slot[eb]];
         PairGeom<float> g;
@@ -320,12 +313,12 @@ void launch_net_elements_f32(const DevBufs& b, uint32_t P, const uint32_t* voff,
     count_launch();
 }
 
-void launch_adjoint_f32(const DevBufs& b, uint32_t P, const double* u_contact, const double* w_eff, double* grad,
-                        cudaStream_t s) {
+void launch_adjoint_f32(const DevBufs& b, uint32_t P, const double* u_contact, const double* w_eff,
+                        const double* v_eff, double* grad, cudaStream_t s) {
     size_t g = (P + kWarps - 1) / kWarps;
     if (g < 1) g = 1;
     if (g > 148 * 64) g = 148 * 64;
-    k_adjoint32<<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band, u_contact, w_eff, grad);
+    k_adjoint32<<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band, u_contact, w_eff, v_eff, grad);
     count_launch();
 }
 
@@ -372,12 +365,3 @@ void launch_contact_f32(const DevBufs& b, uint32_t P, int full, cudaStream_t s) 
 
 }  // namespace vt
 
-#ifdef VT_DEBUG_SITES
-// Debug builds only: histogram of the first unsure step per flagged pair (read and clear).
-extern "C" int vt_debug_flag_sites(unsigned long long* out32) {
-    cudaMemcpyFromSymbol(out32, vt::g_debug_sites, 32 * sizeof(unsigned long long));
-    unsigned long long z[32] = {0};
-    cudaMemcpyToSymbol(vt::g_debug_sites, z, sizeof(z));
-    return 0;
-}
-#endif

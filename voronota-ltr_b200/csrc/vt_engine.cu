@@ -926,8 +926,8 @@ struct vt_engine {
     }
 
     // adjoint of the last full tessellation (device arrays)
-    DBuf<double> w_eff, grad_w, grad_u, grad_out;
-    int grad_device(const double* d_w, const double* d_u, double* d_grad) {
+    DBuf<double> w_eff, v_eff, grad_w, grad_v, grad_u, grad_out;
+    int grad_device(const double* d_w, const double* d_v, const double* d_u, double* d_grad) {
         if (!have_result || contacts_only || batch) {
             g_last_error = "the gradient needs the result of a full single-structure tessellation";
             return VT_ERR_INVALID;
@@ -936,8 +936,9 @@ struct vt_engine {
         const uint32_t n = (uint32_t)stats.num_balls;
         if (n == 0) return VT_OK;
         w_eff.ensure(n);
+        v_eff.ensure(n);
         VT_CUDA(cudaMemsetAsync(words.p, 0, sizeof(uint32_t), stream));
-        launch_adjoint(bufs, (uint32_t)stats.num_pairs, d_w, d_u, w_eff.p, d_grad, stream);
+        launch_adjoint(bufs, (uint32_t)stats.num_pairs, d_w, d_v, d_u, w_eff.p, v_eff.p, d_grad, stream);
         VT_CUDA(cudaMemcpyAsync(h_words + 13, words.p, 4, cudaMemcpyDeviceToHost, stream));
         sync();
         VT_CUDA(cudaGetLastError());
@@ -1170,12 +1171,14 @@ int vt_engine_set_tuning(vt_engine* e, int warps, double cell_scale, int chunk) 
     e->c32_chunk = chunk;
     return VT_OK;
 }
-int vt_engine_grad_device(vt_engine* e, const double* d_w_sas, const double* d_u_contact, double* d_grad) {
+int vt_engine_grad_device(vt_engine* e, const double* d_w_sas, const double* d_v_volume, const double* d_u_contact,
+                          double* d_grad) {
     if (!e || !d_grad) return VT_ERR_INVALID;
-    return guarded([&]() { return e->grad_device(d_w_sas, d_u_contact, d_grad); });
+    return guarded([&]() { return e->grad_device(d_w_sas, d_v_volume, d_u_contact, d_grad); });
 }
 int vt_grad(const double* xyzr, uint64_t n, double probe, const double* periodic_box9, int precision,
-            const double* w_sas, const double* u_contact, uint64_t num_contacts, double* grad_out) {
+            const double* w_sas, const double* v_volume, const double* u_contact, uint64_t num_contacts,
+            double* grad_out) {
     if (n && !grad_out) return VT_ERR_INVALID;
     return with_default_engine([&](vt_engine* e) -> int {
         int st = host_compute(e, xyzr, n, probe, periodic_box9, nullptr, 0, precision, 0);
@@ -1187,13 +1190,17 @@ int vt_grad(const double* xyzr, uint64_t n, double probe, const double* periodic
             return VT_ERR_INVALID;
         }
         e->grad_w.ensure(n);
+        e->grad_v.ensure(n);
         e->grad_u.ensure(num_contacts + 1);
         e->grad_out.ensure(4 * n);
         if (w_sas)
             VT_CUDA(cudaMemcpyAsync(e->grad_w.p, w_sas, 8 * n, cudaMemcpyHostToDevice, e->stream));
+        if (v_volume)
+            VT_CUDA(cudaMemcpyAsync(e->grad_v.p, v_volume, 8 * n, cudaMemcpyHostToDevice, e->stream));
         if (u_contact && num_contacts)
             VT_CUDA(cudaMemcpyAsync(e->grad_u.p, u_contact, 8 * num_contacts, cudaMemcpyHostToDevice, e->stream));
-        st = e->grad_device(w_sas ? e->grad_w.p : nullptr, u_contact ? e->grad_u.p : nullptr, e->grad_out.p);
+        st = e->grad_device(w_sas ? e->grad_w.p : nullptr, v_volume ? e->grad_v.p : nullptr,
+                            u_contact ? e->grad_u.p : nullptr, e->grad_out.p);
         if (st != VT_OK) return st;
         VT_CUDA(cudaMemcpyAsync(grad_out, e->grad_out.p, 32 * n, cudaMemcpyDeviceToHost, e->stream));
         e->sync();

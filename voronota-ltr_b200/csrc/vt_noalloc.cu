@@ -10,10 +10,18 @@
 // file-scope __device__ array that exists for the life of the process on every GPU that
 // loads the library.
 //
-// Limits: 1024 resident threads, each with room for 128 contour points.  A contour
-// started from the 7-point hexagon grows by at most one point per cut and at most doubles
-// in the restriction to the circle, so every pair whose `a` has at most 57 neighbours fits;
-// longer neighbour lists are rejected before any work with VT_ERR_CAPACITY.
+// Limits: 1024 resident threads, each with room for 192 contour points.  The contour
+// starts as the 7-point hexagon at the first cutting neighbour and each cut adds at most
+// one point (a single outside point becomes two; a run of outside points collapses to
+// two), so after the cuts a pair whose `a` lists at most 57 neighbours holds at most
+// 7 + 56 = 63 points.  The restriction to the circle keeps the outside points while it
+// inserts up to two points per edge, so its peak is 3 x 63 = 189 <= 192 points.  Longer
+// neighbour lists are rejected before any work with VT_ERR_CAPACITY; a contour that still
+// outgrew its slot would make the call return VT_ERR_CAPACITY as well (error bit 4).
+// Malformed input (a pair or neighbour index not below num_spheres, offsets that are not
+// ascending, a non-finite coordinate or a negative radius among the spheres a pair
+// reads) is rejected with VT_ERR_INVALID before the contact kernel runs, as the regular
+// path rejects it.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -34,9 +42,16 @@ namespace {
 using namespace vt;
 
 constexpr int kSlots = 1024;  // threads launched, one contour slot each
-constexpr int kCap = 128;     // contour points per slot
-constexpr int kMaxNeighbors = (kCap - 14) / 2;
+constexpr int kCap = 192;     // contour points per slot
+constexpr int kMaxNeighbors = 57;
+static_assert(3 * (7 + kMaxNeighbors - 1) <= kCap, "the peak contour of a 57-neighbour list must fit a slot");
 static_assert(kMaxNeighbors == VT_NOALLOC_MAX_NEIGHBORS, "header and kernel disagree");
+
+// bits of the error word (scratch word 0)
+constexpr uint32_t kNaCapacity = 1u;  // a listed a has more than kMaxNeighbors neighbours
+constexpr uint32_t kNaIndex = 2u;     // a pair / neighbour index or the offsets are malformed
+constexpr uint32_t kNaOverflow = 4u;  // a contour outgrew its slot (not expected within the limit)
+constexpr uint32_t kNaValue = 8u;     // a non-finite coordinate or a negative radius
 
 struct NP {  // one contour point (contact.rs:36-47)
     double x, y, z, ang;
@@ -50,7 +65,7 @@ constexpr size_t kCtrlBytes = 256;  // word 0: error flag
 constexpr size_t kScratchBytes = kCtrlBytes + (size_t)kSlots * kCap * sizeof(NP);
 static_assert(kScratchBytes == VT_NOALLOC_SCRATCH_BYTES, "header and kernel disagree");
 
-// The scratch itself (6,291,712 bytes per device).  Host code must not use this name as
+// The scratch itself (9,437,440 bytes per device).  Host code must not use this name as
 // an address: it is a host-side shadow; the device address comes from
 // cudaGetSymbolAddress at set-up.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
@@ -339,15 +354,43 @@ __device__ bool central(V3<double> center, const Contour& c, V3<double> bary) {
     return true;
 }
 
+__device__ __forceinline__ bool sphere_ok(const In& in, uint32_t i) {
+    const double* s = in.sph + 4 * (size_t)i;
+    return isfinite(s[0]) && isfinite(s[1]) && isfinite(s[2]) && isfinite(s[3]) && s[3] >= 0.0;
+}
+
+// Every read the contact kernel will make, checked first: the pair's ids, a's offsets
+// (ascending and within the index array, whose length is off[num_spheres]), a's
+// neighbour ids, and the spheres of a, b and the neighbours.
 __global__ void k_check_lists(In in, unsigned char* scratch) {
     uint32_t* err = reinterpret_cast<uint32_t*>(scratch);
+    const uint32_t total = in.off[in.ns];
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < in.np; p += gridDim.x * blockDim.x) {
-        uint32_t a = in.pa[p], b = in.pb[p];
+        const uint32_t a = in.pa[p], b = in.pb[p];
         if (a >= in.ns || b >= in.ns) {
-            atomicOr(err, 2u);
+            atomicOr(err, kNaIndex);
             continue;
         }
-        if (in.off[a + 1] - in.off[a] > (uint32_t)kMaxNeighbors) atomicOr(err, 1u);
+        const uint32_t lo = in.off[a], hi = in.off[a + 1];
+        if (lo > hi || hi > total) {
+            atomicOr(err, kNaIndex);
+            continue;
+        }
+        if (hi - lo > (uint32_t)kMaxNeighbors) {
+            atomicOr(err, kNaCapacity);
+            continue;
+        }
+        uint32_t bits = 0;
+        if (!sphere_ok(in, a) || !sphere_ok(in, b)) bits |= kNaValue;
+        for (uint32_t e = lo; e < hi; ++e) {
+            const uint32_t c = in.nbi[e];
+            if (c >= in.ns) {
+                bits |= kNaIndex;
+                break;
+            }
+            if (!sphere_ok(in, c)) bits |= kNaValue;
+        }
+        if (bits) atomicOr(err, bits);
     }
 }
 
@@ -367,7 +410,8 @@ __global__ void __launch_bounds__(128) k_contact_noalloc(In in, unsigned char* s
         V3<double> bary;
         double sum_arc = 0.0, ar = 0.0;
         bool ok = clip(in, a, b, c, ic, bary, sum_arc, ar) && !c.overflow;
-        st[p] = ok ? 1 : (c.overflow ? 4 : 0);
+        if (c.overflow) atomicOr(reinterpret_cast<uint32_t*>(scratch), kNaOverflow);
+        st[p] = ok ? 1 : 0;
         area[p] = ok ? ar : 0.0;
         arc[p] = ok ? sum_arc * ic.r : 0.0;
         cen[p] = ok && central(ic.c, c, bary) ? 1 : 0;
@@ -469,22 +513,32 @@ extern "C" int vt_contact_descriptors_noalloc(const double* d_spheres, uint64_t 
         vt::set_last_error(std::string("CUDA: ") + cudaGetErrorString(e));
         return VT_ERR_CUDA;
     }
-    if (h_err & 2u) {
-        vt::set_last_error("a pair index is not below num_spheres");
+    if (h_err & kNaIndex) {
+        vt::set_last_error("a pair or neighbour index is not below num_spheres, or the neighbour offsets are not "
+                           "ascending within the index array");
         return VT_ERR_INVALID;
     }
-    if (h_err & 1u) {
-        vt::set_last_error("a neighbour list has more than 57 entries; the no-allocation scratch holds 128 contour "
+    if (h_err & kNaValue) {
+        vt::set_last_error("a sphere read by a pair has a non-finite coordinate or a negative radius");
+        return VT_ERR_INVALID;
+    }
+    if (h_err & kNaCapacity) {
+        vt::set_last_error("a neighbour list has more than 57 entries; the no-allocation scratch holds 192 contour "
                 "points per pair (use vt_compute_tessellation for such inputs)");
         return VT_ERR_CAPACITY;
     }
     k_contact_noalloc<<<kSlots / 128, 128, 0, s>>>(in, scratch, d_status, d_area, d_arc_length, d_central,
                                                    d_solid_a, d_solid_b, d_pyramid_a, d_pyramid_b);
     e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, scratch, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         vt::set_last_error(std::string("CUDA: ") + cudaGetErrorString(e));
         return VT_ERR_CUDA;
+    }
+    if (h_err & kNaOverflow) {
+        vt::set_last_error("a contour outgrew the 192 points of its scratch slot; its contact is not computed");
+        return VT_ERR_CAPACITY;
     }
     return VT_OK;
 }

@@ -255,14 +255,15 @@ size_t scan_tmp_words_needed(size_t n);
 void scan_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* tmp, cudaStream_t s);
 
 // ---- adjoint (vt_adjoint.cu): grad (n x 4, overwritten) = dL/d(x, y, z, r) for
-// L = sum_i w_sas[i] SAS_i + sum_k u_contact[k] area_k over the last full tessellation in
-// b (w_sas, u_contact: device arrays or null; w_eff: n doubles of scratch).
-void launch_adjoint(const DevBufs& b, uint32_t P, const double* w_sas, const double* u_contact, double* w_eff,
-                    double* grad, cudaStream_t s);
+// L = sum_i w_sas[i] SAS_i + sum_i v_vol[i] V_i + sum_k u_contact[k] area_k over the last
+// full tessellation in b (w_sas, v_vol, u_contact: device arrays or null; w_eff, v_eff:
+// n doubles of scratch each).
+void launch_adjoint(const DevBufs& b, uint32_t P, const double* w_sas, const double* v_vol, const double* u_contact,
+                    double* w_eff, double* v_eff, double* grad, cudaStream_t s);
 // FP32 adjoint over all valid pairs (vt_contact32.cu); lists the pairs it cannot decide
-// in redo_list for the FP64 adjoint.
-void launch_adjoint_f32(const DevBufs& b, uint32_t P, const double* u_contact, const double* w_eff, double* grad,
-                        cudaStream_t s);
+// in redo_list for the FP64 adjoint.  v_eff may be null (no volume term).
+void launch_adjoint_f32(const DevBufs& b, uint32_t P, const double* u_contact, const double* w_eff,
+                        const double* v_eff, double* grad, cudaStream_t s);
 
 // ---- tessellation network (vt_network.cu) ----
 // Element storage.  Valid pair number v (slot = exclusive scan of the valid flags) owns

@@ -166,13 +166,13 @@ def library():
     L.vt_batch_totals.argtypes = [_vp, _f64p]
     L.vt_batch_free.argtypes = [_vp]
     L.vt_batch_free.restype = None
-    L.vt_engine_grad_device.argtypes = [_vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.vt_engine_grad_device.argtypes = [_vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.vt_engine_autotune_device.argtypes = [_vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double, _f64p,
                                             ctypes.c_int, _u64p, ctypes.c_uint64]
     L.vt_engine_get_tuning.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
                                        ctypes.POINTER(ctypes.c_int)]
     L.vt_engine_set_tuning.argtypes = [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int]
-    L.vt_grad.argtypes = [_f64p, ctypes.c_uint64, ctypes.c_double, _f64p, ctypes.c_int, _f64p, _f64p,
+    L.vt_grad.argtypes = [_f64p, ctypes.c_uint64, ctypes.c_double, _f64p, ctypes.c_int, _f64p, _f64p, _f64p,
                           ctypes.c_uint64, _f64p]
     L.vt_status_string.argtypes = [ctypes.c_int]
     L.vt_status_string.restype = ctypes.c_char_p
@@ -400,23 +400,33 @@ def compute_contacts_only_result(balls, probe, periodic_box=None, groups=None, p
     return _run("vt_compute_contacts_only", balls, probe, periodic_box, groups, precision)
 
 
-def grad(balls, probe, w_sas=None, u_contact=None, periodic_box=None, precision="fp64") -> np.ndarray:
-    """dL/d(x, y, z, r) (an (N, 4) array) of L = sum_i w_sas[i] SAS_i + sum_k u_contact[k]
-    area_k, contact k being the k-th contact of compute_tessellation on the same input
-    (no counterpart in the reference).  The forward runs in ``precision``; the adjoint
-    recomputes the contours in FP64."""
+def grad(balls, probe, w_sas=None, u_contact=None, periodic_box=None, precision="fp64",
+         v_volume=None) -> np.ndarray:
+    """dL/d(x, y, z, r) (an (N, 4) array) of L = sum_i w_sas[i] SAS_i + sum_i v_volume[i]
+    V_i + sum_k u_contact[k] area_k, contact k being the k-th contact of
+    compute_tessellation on the same input and V_i the cell volume (no counterpart in the
+    reference).  The forward runs in ``precision``; the adjoint recomputes the contours."""
     L = library()
     x = parse_balls(balls)
     pb = None if periodic_box is None else parse_periodic_box(periodic_box)
-    w = None if w_sas is None else np.ascontiguousarray(np.asarray(w_sas, dtype=np.float64).reshape(-1))
+
+    def per_ball(a, name):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1))
+        if len(a) != x.shape[0]:
+            raise ValueError(f"{name} needs one weight per ball")
+        return a
+
+    w = per_ball(w_sas, "w_sas")
+    v = per_ball(v_volume, "v_volume")
     u = None if u_contact is None else np.ascontiguousarray(np.asarray(u_contact, dtype=np.float64).reshape(-1))
-    if w is not None and len(w) != x.shape[0]:
-        raise ValueError("w_sas needs one weight per ball")
     out = np.zeros((x.shape[0], 4), np.float64)
     _check(L.vt_grad(x.ctypes.data_as(_f64p), x.shape[0], float(probe),
                      None if pb is None else pb.ctypes.data_as(_f64p), _precision_code(precision),
-                     None if w is None else w.ctypes.data_as(_f64p), None if u is None else u.ctypes.data_as(_f64p),
-                     0 if u is None else len(u), out.ctypes.data_as(_f64p)))
+                     None if w is None else w.ctypes.data_as(_f64p), None if v is None else v.ctypes.data_as(_f64p),
+                     None if u is None else u.ctypes.data_as(_f64p), 0 if u is None else len(u),
+                     out.ctypes.data_as(_f64p)))
     return out
 
 
@@ -644,10 +654,12 @@ class Engine:
         """chunk > 0: persistent contact launch taking `chunk` pairs per grab."""
         _check(self._L.vt_engine_set_tuning(self._h, int(warps_per_block), float(cell_scale), int(chunk)))
 
-    def grad_device(self, d_w_ptr, d_u_ptr, d_grad_ptr: int):
+    def grad_device(self, d_w_ptr, d_u_ptr, d_grad_ptr: int, d_v_ptr=None):
         """Adjoint of the last full tessellation: d_grad (N x 4 doubles on the device) =
-        dL/d(x, y, z, r), L = sum w SAS + sum u area (device pointers; 0/None = no term)."""
-        _check(self._L.vt_engine_grad_device(self._h, d_w_ptr or None, d_u_ptr or None, d_grad_ptr))
+        dL/d(x, y, z, r), L = sum w SAS + sum v volume + sum u area (device pointers;
+        0/None = no term)."""
+        _check(self._L.vt_engine_grad_device(self._h, d_w_ptr or None, d_v_ptr or None, d_u_ptr or None,
+                                             d_grad_ptr))
 
     def compute_batch_device(self, d_xyzr_ptr: int, offsets, probe: float, precision="fp32",
                              contacts_only: bool = False):

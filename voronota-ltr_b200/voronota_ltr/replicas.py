@@ -3,8 +3,9 @@
 A tessellation does not shard usefully below one structure (the work per structure is
 local and small next to a halo exchange), so several GPUs run independent structures:
 each rank tessellates its own inputs, and the only collectives are the barriers around
-the timed region and the max-over-ranks of the measured times.  Structures of a batch are
-split into contiguous blocks, one per rank.
+the timed region and the max-over-ranks of the measured times.  The structures of one
+batch are split into contiguous blocks, one per rank, of about equal ball counts
+(``partition_weighted``): each rank runs its block as one batched call.
 
 ``Ranks`` reads RANK / WORLD_SIZE / LOCAL_RANK from the environment (torchrun) and joins a
 process group when WORLD_SIZE > 1 (``nccl`` on GPUs; ``gloo`` for the CPU tests).
@@ -23,6 +24,32 @@ def partition(count: int, world: int, rank: int) -> tuple[int, int]:
     base, extra = divmod(count, world)
     start = rank * base + min(rank, extra)
     return start, start + base + (1 if rank < extra else 0)
+
+
+def partition_weighted(weights, world: int, rank: int) -> tuple[int, int]:
+    """Contiguous block [start, stop) of the items for `rank` of `world` ranks, cut where
+    the running sum of `weights` (e.g. balls per structure) crosses k / world of the
+    total, so every rank gets about the same weight; the blocks cover every item exactly
+    once, in order."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("bad world / rank")
+    import numpy as np
+
+    w = np.asarray(weights, dtype=np.float64)
+    if len(w) == 0:
+        return 0, 0
+    c = np.cumsum(w)
+    total = c[-1]
+
+    def cut(k):
+        if k <= 0:
+            return 0
+        if k >= world:
+            return len(w)
+        return int(np.searchsorted(c, total * k / world, side="left")) + 1
+
+    start, stop = cut(rank), cut(rank + 1)
+    return min(start, len(w)), min(max(stop, start), len(w))
 
 
 def replica_throughput(units_per_rank: float, world: int, max_ms: float) -> float:
