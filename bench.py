@@ -268,10 +268,11 @@ def updateable_leg(args, rank, torch, V, R):
         u = V.UpdateableTessellation(False, precision)
         u.set_stream(stream.cuda_stream)
         u.set_adjoint(adjoint)
+        u.set_timing(checks)
         d = torch.from_numpy(balls).cuda()
         torch.cuda.synchronize()
         u.init_device(d.data_ptr(), n, PROBE, box)
-        ms, adj, pairs, redo, cref, drift = [], [], [], [], [], []
+        ms, adj, pairs, redo, cref, drift, stages, syncs = [], [], [], [], [], [], [], []
         dg = torch.empty((n, 4), dtype=torch.float64, device="cuda")
         for t, (ids, disp) in enumerate(moves[:warm + nsteps]):
             ti = torch.from_numpy(ids).cuda()
@@ -282,6 +283,8 @@ def updateable_leg(args, rank, torch, V, R):
             u.update_with_changed_device(d.data_ptr(), n, ti.data_ptr(), len(ids))
             e1.record(stream)
             st = u.stats()
+            if checks:
+                stages.append(u.stage_times())
             if adjoint:
                 u.grad_sas_device(0, dg.data_ptr())  # adjoint of the total SAS
             e2.record(stream)
@@ -292,6 +295,7 @@ def updateable_leg(args, rank, torch, V, R):
                 pairs.append(int(st.num_pairs))
                 redo.append(int(st.num_fp64_redo))
                 cref.append(int(st.num_cell_redo))
+                syncs.append(int(st.num_host_syncs))
                 k = t - warm + 1
                 if checks and (k % check == 0 or k == nsteps):
                     mid = k == (nsteps // (2 * check)) * check or k == nsteps
@@ -300,12 +304,13 @@ def updateable_leg(args, rank, torch, V, R):
                     dd["step"] = k
                     drift.append(dd)
         aff = len(u.affected_ids())
-        return u, d, ms, aff, pairs, redo, adj, cref, drift
+        stage_med = {k: statistics.median(x[k] for x in stages[warm:]) for k in stages[0]} if stages else None
+        return u, d, ms, aff, pairs, redo, adj, cref, drift, stage_med, syncs
 
-    u32, d32, ms32, aff, pairs, redo, adj32, cref, drift = run("fp32", steps, checks=True)
+    u32, d32, ms32, aff, pairs, redo, adj32, cref, drift, ustages, usyncs = run("fp32", steps, checks=True)
     short = min(steps, 100)
-    _, _, ms64, _, _, _, adj64, _, _ = run("fp64", short)
-    _, _, ms32na, _, _, _, _, _, _ = run("fp32", short, adjoint=False)
+    ms64, adj64 = run("fp64", short)[2:7:4]
+    ms32na = run("fp32", short, adjoint=False)[2]
     eng = V.Engine()
     eng.set_stream(stream.cuda_stream)
     full = []
@@ -342,6 +347,8 @@ def updateable_leg(args, rank, torch, V, R):
         "affected_per_update": aff, "pairs_per_update": int(statistics.median(pairs)),
         "fp64_redo_pairs_per_update": int(statistics.median(redo)),
         "fp64_cell_refresh_per_update": int(statistics.median(cref)),
+        "stages_ms_fp32_median": {k: round(v, 4) for k, v in ustages.items()} if ustages else None,
+        "host_gaps_fp32": host_gaps(ustages, ustages["call"], int(statistics.median(usyncs))) if ustages else None,
         "drift_checks": drift,
         "drift_summary": {"checkpoints": len(drift), "contacts_identical_to_full_fp64_at_every_checkpoint": gpu_ok,
                           "max_rel_err_total_sas_vs_full_fp64": worst,

@@ -145,6 +145,7 @@ typedef struct vt_stats {
     uint64_t num_kernel_launches; /* kernels this library launched during the call */
     uint64_t num_cell_redo;       /* FP32 path: cells whose SAS branch needed FP64 inputs */
     uint64_t fp32_kernel;         /* 1 when the FP32 contact kernel ran */
+    uint64_t num_host_syncs;      /* waits of the host for the stream (each reads device counts) */
 } vt_stats;
 int vt_engine_stats(const vt_engine* e, vt_stats* out);
 
@@ -301,13 +302,33 @@ int vt_upd_affected_ids(vt_updateable* h, uint64_t* out);
  * device, overwritten with dL/d(x, y, z, r)).  VT_ERR_INVALID when an operation since
  * the last full computation ran with the adjoint off (vt_upd_set_adjoint). */
 int vt_upd_grad_sas(vt_updateable* h, const double* d_w_sas, double* d_grad);
-/* Whether operations record the arc moments behind vt_upd_grad_sas (on by default; no
- * counterpart in the reference).  Off saves about a tenth of an update's time; the
- * adjoint is then refused until a full computation (init, or an update past the
- * full-reinit threshold) has run with it on again. */
+/* Adjoint of sum_i w_sas[i] SAS_i + sum_i v_volume[i] V_i over the current state (no
+ * counterpart in the reference): d_w_sas and d_v_volume (n doubles each on the device)
+ * may each be NULL (no such term); d_grad (n x 4 doubles on the device) is overwritten
+ * with dL/d(x, y, z, r).  V_i is the cell volume of the handle's summary; its adjoint
+ * integrates the normal velocity of the cell's boundary (each contact face moves with
+ * its radical plane, the exposed sphere with the ball), from per-entry coefficients that
+ * the operations record with the SAS ones (vt_upd_set_adjoint).  Same refusal as
+ * vt_upd_grad_sas. */
+int vt_upd_grad(vt_updateable* h, const double* d_w_sas, const double* d_v_volume, double* d_grad);
+/* Whether operations record the arc and face moments behind vt_upd_grad_sas and
+ * vt_upd_grad (on by default; no counterpart in the reference).  Off saves about a tenth
+ * of an update's time; the adjoint is then refused until a full computation (init, or an
+ * update past the full-reinit threshold) has run with it on again. */
 int vt_upd_set_adjoint(vt_updateable* h, int on);
 /* counters of the last operation: list entries, pairs recomputed, FP64 redo, cells */
 int vt_upd_stats(const vt_updateable* h, vt_stats* out);
+/* Per-stage device times (CUDA events on the handle's stream) of the last
+ * update_with_changed / update that did not fall back to a full reinit, when timing is
+ * on (no counterpart in the reference):  [0] changed filter and marks  [1] apply, spheres,
+ * images, grid  [2] frontier neighbour searches  [3] list splice and affected set
+ * [4] pair generation  [5] contacts (FP32 or FP64, band recompute, serial)  [6] dedup,
+ * contact-table splice, cells  [7] FP64 refresh of uncertain cells  [8] cell count,
+ * error word  [9] the whole update (first to last event, including the host's reads of
+ * device counts between stages).  Unused stages are 0. */
+#define VT_UPD_NUM_STAGES 10
+int vt_upd_set_timing(vt_updateable* h, int on);
+int vt_upd_stage_times(const vt_updateable* h, double* ms);
 
 /* ---- contact descriptors without device allocation ----
  * No counterpart in the reference: an entry point for callers that cannot call

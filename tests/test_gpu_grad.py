@@ -268,6 +268,68 @@ def test_updateable_sas_adjoint_matches_stateless(precision):
     assert np.allclose(dg.cpu().numpy()[:, :3], g1[:, :3], rtol=tol_xyz, atol=tol_xyz)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_updateable_volume_adjoint_matches_stateless(precision):
+    """The handle's adjoint of sum w SAS + sum v V (per-entry face coefficients gathered,
+    Reynolds' transport form) against the stateless adjoint (pyramid-volume form) on the
+    same positions after a few updates: two derivations of one gradient."""
+    import torch
+
+    balls = W.lattice_balls(2000, 26)
+    t = V.UpdateableTessellation(precision=precision)
+    assert t.init(balls, 1.4)
+    rng = np.random.default_rng(6)
+    for _ in range(3):
+        ids = np.sort(rng.choice(len(balls), 20, replace=False))
+        balls[ids, :3] += rng.normal(0.0, 0.05, (20, 3))
+        assert t.update_with_changed(balls, ids)
+    w = rng.uniform(0.0, 1.0, len(balls))
+    v = rng.uniform(0.0, 1.0, len(balls))
+    dw, dv = torch.from_numpy(w).cuda(), torch.from_numpy(v).cuda()
+    dg = torch.empty((len(balls), 4), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    t.grad_device(0, dv.data_ptr(), dg.data_ptr())
+    g_v = V.grad(balls, 1.4, None, None, precision=precision, v_volume=v)
+    tol = 1e-8 if precision == "fp64" else 1e-4
+    assert np.allclose(dg.cpu().numpy(), g_v, rtol=tol, atol=tol)
+    t.grad_device(dw.data_ptr(), dv.data_ptr(), dg.data_ptr())
+    g = V.grad(balls, 1.4, w, None, precision=precision, v_volume=v)
+    assert np.allclose(dg.cpu().numpy(), g, rtol=tol, atol=tol)
+    # the SAS-only entry point is the w-only case
+    t.grad_sas_device(dw.data_ptr(), dg.data_ptr())
+    t2 = torch.empty_like(dg)
+    t.grad_device(dw.data_ptr(), 0, t2.data_ptr())
+    assert torch.equal(dg, t2)
+
+
+def test_updateable_volume_adjoint_periodic_finite_differences():
+    import torch
+
+    balls, side = W.periodic_box_balls(1500, seed=14)
+    box = {"corners": [(0.0, 0.0, 0.0), (side, side, side)]}
+    t = V.UpdateableTessellation(precision="fp64")
+    assert t.init(balls, 1.4, box)
+    rng = np.random.default_rng(7)
+    for _ in range(2):
+        ids = np.sort(rng.choice(len(balls), 15, replace=False))
+        balls[ids, :3] += rng.normal(0.0, 0.05, (15, 3))
+        assert t.update_with_changed(balls, ids)
+    v = rng.uniform(0.0, 1.0, len(balls))
+    dv = torch.from_numpy(v).cuda()
+    dg = torch.empty((len(balls), 4), dtype=torch.float64, device="cuda")
+    t.grad_device(0, dv.data_ptr(), dg.data_ptr())
+    g = dg.cpu().numpy()
+
+    def loss(b):
+        u = V.UpdateableTessellation(precision="fp64")
+        u.init(b, 1.4, box)
+        s = u.summary()
+        return float(np.dot(v[s.cell_index.astype(np.int64)], s.cell_volume))
+
+    for i, c in _coords(len(balls), 12, 15):
+        _check_fd(g[i, c], loss, balls, i, c)
+
+
 def test_updateable_sas_adjoint_periodic_finite_differences():
     import torch
 

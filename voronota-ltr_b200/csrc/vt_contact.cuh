@@ -163,7 +163,9 @@ struct PairGeom {
     uint32_t a_id, b_id;
     T e0;  // FP32: error budget E of a contour point coordinate (A); 0 in FP64
     T S;   // length scale of the pair (R_a + R_b)
-    bool want_xm = false;  // FULL: also the first moment of the arcs (the SAS adjoint)
+    // FULL and XM: lane 0 writes the contact's first moments here (6 doubles: the arcs'
+    // and the area's about a's centre, for the SAS and volume adjoints); null: not wanted
+    double* xm_out = nullptr;
 };
 
 // ---- FP32 constructions: decisions banded by the point error budget E ----
@@ -304,7 +306,10 @@ struct WarpContact {
     bool unsure;
     bool overflow;
     double area, arc, sa_a, sa_b, pv_a, pv_b;
-    double xm[3];  // first moment of the contact's arcs about a's centre (want_xm)
+    // serial kernel: xm[0..2] first moment of the contact's arcs about a's centre (the SAS
+    // adjoint), xm[3..5] first moment of the contact's area about a's centre (the volume
+    // adjoint); the warp kernel writes them to PairGeom::xm_out instead
+    double xm[6];
     bool central;
     bool merged;  // two close points were merged (the kept point takes the other's id)
 };
@@ -399,7 +404,7 @@ struct ContourOut {
     V3<T> axis;
 };
 
-// XM: compile in the arc first moment (computed when g.want_xm).
+// XM: compile in the first moments (computed and written when g.xm_out is set).
 template <typename T, bool F, bool FULL, bool XM = false, typename NbFn>
 __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn nb, ContourOut<T>* co = nullptr) {
     const int lane = threadIdx.x & 31;
@@ -411,7 +416,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
     res.unsure = false;
     res.overflow = false;
     res.area = res.arc = res.sa_a = res.sa_b = res.pv_a = res.pv_b = 0.0;
-    res.xm[0] = res.xm[1] = res.xm[2] = 0.0;
+    for (int k = 0; k < 6; ++k) res.xm[k] = 0.0;
     res.central = false;
     res.merged = false;
 
@@ -876,24 +881,67 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             res.pv_a = (double)(norm(g.ic.c - g.A.c) * area / (T)3 * sign_a);
             res.pv_b = (double)(norm(g.ic.c - g.B.c) * area / (T)3 * sign_b);
         }
-        if (XM && g.want_xm) {
+        if (XM && g.xm_out) {
             // integral of (x - a) over the arcs: an arc of angle t from e1 (unit, from the
             // circle centre) around the axis contributes (q - a) rho t + rho^2 (sin t e1 +
-            // (1 - cos t) axis x e1), with cos t = e1.e2, sin t = e2.(axis x e1)
+            // (1 - cos t) axis x e1), with cos t = e1.e2, sin t = e2.(axis x e1).
+            // integral of (x - a) over the area: the triangles (bary, p_k, p_k+1) of the
+            // area sum contribute their area times their centroid; the circular segment of
+            // an arc its area rho^2 (t - sin t) / 2 at q plus rho^3 (1 - cos t) / 6 (sin t e1
+            // + (1 - cos t) axis x e1) (the segment's centroid lies 4 rho sin^3(t/2) /
+            // (3 (t - sin t)) from q along the arc's bisector); sin t and cos t come from the
+            // arc's end points, as for the arcs' moment
             const double rho = (double)g.ic.r;
-            const V3<double> qa = wide3(g.ic.c - g.A.c);
-            V3<double> xk = mk<double>(0, 0, 0);
-            if (!init) {
-                if (lane == 0) xk = qa * (kTau * rho);
-            } else if (on && q.ang > (T)0 && rho > 0.0) {
+            const V3<double> aw = wide3(g.A.c);
+            const V3<double> qa = wide3(g.ic.c) - aw;
+            const bool arc = init && on && q.ang > (T)0 && rho > 0.0;
+            // the arc's sin t e1 + (1 - cos t) axis x e1 and cos t (one lane per arc)
+            auto arc_terms = [&](V3<double>& m, double& ct) {
                 const V3<double> qc = wide3(g.ic.c);
                 const V3<double> e1 = (wide3(q.p) - qc) / rho, e2 = (wide3(p2.p) - qc) / rho;
                 const V3<double> f = cross(wide3(g.axis), e1);
-                xk = qa * (rho * (double)q.ang) + (e1 * dot(e2, f) + f * (1.0 - dot(e2, e1))) * (rho * rho);
+                ct = dot(e2, e1);
+                m = e1 * dot(e2, f) + f * (1.0 - ct);
+                return dot(e2, f);
+            };
+            {  // the arcs (two passes keep fewer doubles live at once)
+                V3<double> xk = mk<double>(0, 0, 0);
+                if (!init) {
+                    if (lane == 0) xk = qa * (kTau * rho);
+                } else if (arc) {
+                    V3<double> m;
+                    double ct;
+                    arc_terms(m, ct);
+                    xk = qa * (rho * (double)q.ang) + m * (rho * rho);
+                }
+                const double xx = wsum(xk.x);
+                if (lane == 0) g.xm_out[0] = xx;
+                const double xy = wsum(xk.y);
+                if (lane == 0) g.xm_out[1] = xy;
+                const double xz = wsum(xk.z);
+                if (lane == 0) g.xm_out[2] = xz;
             }
-            res.xm[0] = wsum(xk.x);
-            res.xm[1] = wsum(xk.y);
-            res.xm[2] = wsum(xk.z);
+            {  // the area
+                V3<double> ak = mk<double>(0, 0, 0);
+                if (!init) {
+                    if (lane == 0) ak = qa * (double)area;
+                } else if (on) {
+                    const V3<double> bw = wide3(bary) - aw, pk = wide3(q.p) - aw, pn = wide3(p2.p) - aw;
+                    ak = (bw + pk + pn) * (0.5 * norm(cross(pk - bw, pn - bw)) / 3.0);
+                    if (arc) {
+                        V3<double> m;
+                        double ct;
+                        const double st = arc_terms(m, ct), th = (double)q.ang;
+                        ak = ak + qa * (0.5 * rho * rho * (th - st)) + m * (rho * rho * rho * (1.0 - ct) / 6.0);
+                    }
+                }
+                const double ax = wsum(ak.x);
+                if (lane == 0) g.xm_out[3] = ax;
+                const double ay = wsum(ak.y);
+                if (lane == 0) g.xm_out[4] = ay;
+                const double az = wsum(ak.z);
+                if (lane == 0) g.xm_out[5] = az;
+            }
         }
     }
     res.unsure = __any_sync(kFull, d.unsure);

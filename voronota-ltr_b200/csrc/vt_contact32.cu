@@ -37,7 +37,7 @@ __device__ __forceinline__ void contact_pair32(const DevBufs& b, uint32_t p, flo
     g.b_id = b.nb_id[eb];
     g.S = Ra + rb.w;
     g.e0 = band * g.S;
-    g.want_xm = b.p_arcm != nullptr;
+    if (XM && b.p_arcm) g.xm_out = b.p_arcm + 6 * (size_t)p;
     const float4* rel = b.nb_rel + off;
     const uint32_t* nid = b.nb_id + off;
     auto nbf = [&](int e) {
@@ -58,8 +58,6 @@ __device__ __forceinline__ void contact_pair32(const DevBufs& b, uint32_t p, flo
         b.p_sa_b[p] = r.valid ? r.sa_b : 0.0;
         b.p_pv_a[p] = r.valid ? r.pv_a : 0.0;
         b.p_pv_b[p] = r.valid ? r.pv_b : 0.0;
-        if (XM && b.p_arcm)
-            for (int k = 0; k < 3; ++k) b.p_arcm[3 * (size_t)p + k] = r.valid ? r.xm[k] : 0.0;
     }
 }
 

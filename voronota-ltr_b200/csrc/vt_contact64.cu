@@ -25,8 +25,6 @@ __device__ __forceinline__ void write_pair(const DevBufs& b, uint32_t p, const W
     b.p_sa_b[p] = r.valid ? r.sa_b : 0.0;
     b.p_pv_a[p] = r.valid ? r.pv_a : 0.0;
     b.p_pv_b[p] = r.valid ? r.pv_b : 0.0;
-    if (b.p_arcm)
-        for (int k = 0; k < 3; ++k) b.p_arcm[3 * (size_t)p + k] = r.valid ? r.xm[k] : 0.0;
 }
 
 // 4 resident blocks per SM: at most 128 registers a thread (a few bytes of spill) for 16
@@ -47,7 +45,7 @@ __global__ void __launch_bounds__(kWarps * 32, 4) k_contact64(DevBufs b, uint32_
         g.b_id = b.nb_id[eb];
         g.e0 = 0.0;
         g.S = g.A.r + g.B.r;
-        g.want_xm = XM;
+        if (XM && b.p_arcm) g.xm_out = b.p_arcm + 6 * (size_t)p;
         const double4* sph = b.sph;
         const uint32_t* nslot = b.nb_slot + off;
         const uint32_t* nid = b.nb_id + off;
@@ -380,23 +378,34 @@ __global__ void k_contact_serial(DevBufs b, int full) {
         r.arc = sum_arc * ic.r;
         r.central = r.valid ? serial_central(ic.c, c, bary) : false;
         r.sa_a = r.sa_b = r.pv_a = r.pv_b = 0.0;
-        r.xm[0] = r.xm[1] = r.xm[2] = 0.0;
-        if (r.valid && full && b.p_arcm) {  // first moment of the arcs about a
+        for (int k = 0; k < 6; ++k) r.xm[k] = 0.0;
+        if (r.valid && full && b.p_arcm) {  // first moments of the arcs and of the area about a
             const V3<double> pa = sph_of(b.sph[b.pair_a[p]]).c;
-            V3<double> X = mk<double>(0, 0, 0);
+            const V3<double> qa = ic.c - pa;
+            V3<double> X = mk<double>(0, 0, 0), M = mk<double>(0, 0, 0);
             if (c.n == 0) {
-                X = (ic.c - pa) * (kTau * ic.r);
+                X = qa * (kTau * ic.r);
+                M = qa * area;
             } else {
+                const double rho = ic.r;
                 for (int k = 0; k < c.n; ++k) {
+                    const V3<double> pk = P3(c.v[k]) - pa, pn = P3(c.v[(k + 1) % c.n]) - pa, bw = bary - pa;
+                    M = M + (bw + pk + pn) * (0.5 * norm(cross(pk - bw, pn - bw)) / 3.0);
                     if (!(c.v[k].ang > 0.0)) continue;
-                    const V3<double> e1 = (P3(c.v[k]) - ic.c) / ic.r, e2 = (P3(c.v[(k + 1) % c.n]) - ic.c) / ic.r;
+                    const V3<double> e1 = (P3(c.v[k]) - ic.c) / rho, e2 = (P3(c.v[(k + 1) % c.n]) - ic.c) / rho;
                     const V3<double> f = cross(axis, e1);
-                    X = X + (ic.c - pa) * (ic.r * c.v[k].ang) + (e1 * dot(e2, f) + f * (1.0 - dot(e2, e1))) * (ic.r * ic.r);
+                    const double ct = dot(e2, e1), st = dot(e2, f), th = c.v[k].ang;
+                    const V3<double> m = e1 * st + f * (1.0 - ct);
+                    X = X + qa * (rho * th) + m * (rho * rho);
+                    M = M + qa * (0.5 * rho * rho * (th - st)) + m * (rho * rho * rho * (1.0 - ct) / 6.0);
                 }
             }
             r.xm[0] = X.x;
             r.xm[1] = X.y;
             r.xm[2] = X.z;
+            r.xm[3] = M.x;
+            r.xm[4] = M.y;
+            r.xm[5] = M.z;
         }
         if (r.valid && full) {
             const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
@@ -410,6 +419,8 @@ __global__ void k_contact_serial(DevBufs b, int full) {
         }
         if (c.overflow) atomicOr(b.err, (uint32_t)kErrOverflow);
         write_pair(b, p, r, 0);
+        if (full && b.p_arcm)
+            for (int k = 0; k < 6; ++k) b.p_arcm[6 * (size_t)p + k] = r.xm[k];
     }
 }
 

@@ -443,7 +443,10 @@ struct vt_engine {
         if (own) cudaStreamDestroy(own);
     }
 
-    void sync() { VT_CUDA(cudaStreamSynchronize(stream)); }
+    void sync() {
+        ++stats.num_host_syncs;
+        VT_CUDA(cudaStreamSynchronize(stream));
+    }
 
     void ensure_scan(size_t n) { scan_tmp.ensure(scan_tmp_words_needed(n) + 8); }
 

@@ -235,8 +235,8 @@ __global__ void k_new_contacts(uint32_t P, const uint32_t* __restrict__ keep_off
             const V3<double> dab = mk<double>(B4.x - A4.x, B4.y - A4.y, B4.z - A4.z);
             const double Ra = A4.w, Rb = B4.w, D2 = dot(dab, dab), D = sqrt(D2);
             const double L = b.p_arc[p];
-            const V3<double> Xa = mk<double>(b.p_arcm[3 * (size_t)p], b.p_arcm[3 * (size_t)p + 1],
-                                             b.p_arcm[3 * (size_t)p + 2]);
+            const double* xm = b.p_arcm + 6 * (size_t)p;
+            const V3<double> Xa = mk<double>(xm[0], xm[1], xm[2]);
             double4 aa = make_double4(0, 0, 0, 0), ab = aa, ba = aa, bb = aa;
             const double da = D > 0.0 ? (D2 + Ra * Ra - Rb * Rb) / (2.0 * D) : 0.0;
             const double rho = sqrt(fmax(Ra * Ra - da * da, 0.0));
@@ -253,6 +253,33 @@ __global__ void k_new_contacts(uint32_t P, const uint32_t* __restrict__ keep_off
             nc.gab[k] = swap ? ba : ab;
             nc.gba[k] = swap ? ab : ba;
             nc.gbb[k] = swap ? aa : bb;
+            // the volume adjoint through the contact's face (Reynolds' transport theorem:
+            // a cell's volume changes by the normal velocity of its boundary).  The face lies
+            // on the radical plane, whose point x moves towards b by ((x - a).dp_a -
+            // (x - b).dp_b + Ra dRa - Rb dRb) / D; over the face that integrates to the
+            // face's area A and first moment M_a = integral of (x - a) (M_b = M_a - A (b - a)):
+            //   dV_a/dp_a = M_a / D - A n,  dV_a/dR_a = A Ra / D,   n = (b - a) / D,
+            //   dV_b/dp_a = -M_a / D,       dV_b/dR_a = -A Ra / D,
+            // and a <-> b with n -> -n.  The -A n term is the exposed sphere's share: the
+            // cell's boundary is closed, so the integral of the outward normal over the
+            // exposed part of sphere a is minus the sum of A n over a's faces; its radius
+            // term (the exposed area) is added per ball by the gather.
+            double4 vaa = make_double4(0, 0, 0, 0), vab = vaa, vba = vaa, vbb = vaa;
+            const double A = b.p_area[p];
+            if (A > 0.0 && D > 0.0) {
+                const V3<double> Ma = mk<double>(xm[3], xm[4], xm[5]);
+                const V3<double> Mb = Ma - dab * A;
+                const V3<double> nh = dab / D;
+                const V3<double> ca = Ma / D - nh * A, cb = Mb / D + nh * A;
+                vaa = make_double4(ca.x, ca.y, ca.z, A * Ra / D);  // dV_a / d(a)
+                vba = make_double4(-Ma.x / D, -Ma.y / D, -Ma.z / D, -A * Ra / D);  // dV_b / d(a)
+                vbb = make_double4(cb.x, cb.y, cb.z, A * Rb / D);  // dV_b / d(b)
+                vab = make_double4(-Mb.x / D, -Mb.y / D, -Mb.z / D, -A * Rb / D);  // dV_a / d(b)
+            }
+            nc.vaa[k] = swap ? vbb : vaa;
+            nc.vab[k] = swap ? vba : vab;
+            nc.vba[k] = swap ? vab : vba;
+            nc.vbb[k] = swap ? vaa : vbb;
         }
     }
 }
@@ -299,6 +326,8 @@ __device__ __forceinline__ void copy_entry(const TableRef& o, uint32_t q, const 
     if (w.gA) {
         w.gA[d] = o.gA[q];
         w.gB[d] = o.gB[q];
+        w.vA[d] = o.vA[q];
+        w.vB[d] = o.vB[q];
     }
 }
 __global__ void __launch_bounds__(kWarps * 32)
@@ -369,6 +398,8 @@ __global__ void __launch_bounds__(kWarps * 32)
             if (w.gA) {
                 w.gA[d] = own_a ? nc.gaa[k] : nc.gbb[k];
                 w.gB[d] = own_a ? nc.gba[k] : nc.gab[k];
+                w.vA[d] = own_a ? nc.vaa[k] : nc.vbb[k];
+                w.vB[d] = own_a ? nc.vba[k] : nc.vab[k];
             }
         }
         __syncwarp();
@@ -442,6 +473,8 @@ __global__ void k_table_update(NewContacts nc, const uint32_t* __restrict__ nc_c
             if (T.gA) {
                 T.gA[d] = own_a ? nc.gaa[k] : nc.gbb[k];
                 T.gB[d] = own_a ? nc.gba[k] : nc.gab[k];
+                T.vA[d] = own_a ? nc.vaa[k] : nc.vbb[k];
+                T.vB[d] = own_a ? nc.vba[k] : nc.vab[k];
             }
         }
     }
@@ -455,33 +488,49 @@ __global__ void k_list_flagged(const uint32_t* __restrict__ list, const uint32_t
         if (flag[i]) out[atomicAdd(d_out, 1u)] = i;
     }
 }
-__device__ __forceinline__ double sas_weight(const double* w, const uint8_t* cell_flag, const double* cell_sas,
-                                             uint32_t i) {
-    return (cell_flag[i] && cell_sas[i] > 0.0) ? (w ? w[i] : 1.0) : 0.0;
+// w == null: every SAS weight is `w_default` (1 for the total SAS, 0 for no SAS term)
+__device__ __forceinline__ double sas_weight(const double* w, double w_default, const uint8_t* cell_flag,
+                                             const double* cell_sas, uint32_t i) {
+    return (cell_flag[i] && cell_sas[i] > 0.0) ? (w ? w[i] : w_default) : 0.0;
+}
+__device__ __forceinline__ double vol_weight(const double* v, const uint8_t* cell_flag, uint32_t i) {
+    return (v && cell_flag[i]) ? v[i] : 0.0;
 }
 __global__ void __launch_bounds__(kWarps * 32)
-    k_table_grad(uint32_t n, TableRef T, const double* __restrict__ w, const uint8_t* __restrict__ cell_flag,
-                 const double* __restrict__ cell_sas, const double4* __restrict__ sph, double* __restrict__ grad) {
+    k_table_grad(uint32_t n, TableRef T, const double* __restrict__ w, double w_default, const double* __restrict__ v,
+                 const uint8_t* __restrict__ cell_flag, const double* __restrict__ cell_sas,
+                 const double4* __restrict__ sph, double* __restrict__ grad) {
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     for (uint32_t i = blockIdx.x * kWarps + wp; i < n; i += gridDim.x * kWarps) {
-        const double wi = sas_weight(w, cell_flag, cell_sas, i);
+        const double wi = sas_weight(w, w_default, cell_flag, cell_sas, i);
+        const double vi = vol_weight(v, cell_flag, i);
         double gx = 0, gy = 0, gz = 0, gr = 0;
         for (uint32_t q = T.off[i] + lane; q < T.off[i + 1]; q += 32) {
             const uint32_t other = T.a[q] == i ? T.b[q] : T.a[q];
-            const double wo = sas_weight(w, cell_flag, cell_sas, other);
+            const double wo = sas_weight(w, w_default, cell_flag, cell_sas, other);
             const double4 A = T.gA[q], B = T.gB[q];
             gx += wi * A.x + wo * B.x;
             gy += wi * A.y + wo * B.y;
             gz += wi * A.z + wo * B.z;
             gr += wi * A.w + wo * B.w;
+            if (v) {
+                const double vo = vol_weight(v, cell_flag, other);
+                const double4 VA = T.vA[q], VB = T.vB[q];
+                gx += vi * VA.x + vo * VB.x;
+                gy += vi * VA.y + vo * VB.y;
+                gz += vi * VA.z + vo * VB.z;
+                gr += vi * VA.w + vo * VB.w;
+            }
         }
         gx = wsum(gx);
         gy = wsum(gy);
         gz = wsum(gz);
         gr = wsum(gr);
         if (lane == 0) {
-            // radius scaling of the exposed area: dSAS/dR = 2 SAS / R at fixed directions
+            // radius scaling of the exposed area: dSAS/dR = 2 SAS / R at fixed directions;
+            // the exposed sphere's share of dV/dR is the exposed area itself
             if (wi != 0.0) gr += wi * 2.0 * cell_sas[i] / sph[i].w;
+            if (vi != 0.0) gr += vi * cell_sas[i];
             grad[4 * (size_t)i] = gx;
             grad[4 * (size_t)i + 1] = gy;
             grad[4 * (size_t)i + 2] = gz;
@@ -631,9 +680,11 @@ void launch_list_flagged(const uint32_t* list, const uint32_t* count, uint32_t m
                          uint32_t* out, uint32_t* d_out, cudaStream_t s) {
     k_list_flagged<<<gb(max_count), kBlock, 0, s>>>(list, count, flag, out, d_out); count_launch();
 }
-void launch_table_grad(uint32_t n, TableRef tab, const double* w, const uint8_t* cell_flag, const double* cell_sas,
+void launch_table_grad(uint32_t n, TableRef tab, const double* w, double w_default, const double* v,
+                       const uint8_t* cell_flag, const double* cell_sas,
                        const double4* sph, double* grad, cudaStream_t s) {
-    k_table_grad<<<gw(n), kWarps * 32, 0, s>>>(n, tab, w, cell_flag, cell_sas, sph, grad); count_launch();
+    k_table_grad<<<gw(n), kWarps * 32, 0, s>>>(n, tab, w, w_default, v, cell_flag, cell_sas, sph, grad);
+    count_launch();
 }
 void launch_owner_flags(const uint8_t* flags, uint32_t M, uint32_t* out, cudaStream_t s) {
     k_owner_flags<<<gb(M), kBlock, 0, s>>>(flags, M, out); count_launch();

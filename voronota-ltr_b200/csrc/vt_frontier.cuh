@@ -39,9 +39,12 @@ struct TableRef {
     double* pv;
     uint8_t* flags;
     // optional: SAS adjoint coefficients of the entry (x, y, z, r): gA = dSAS_owner /
-    // d(owner), gB = dSAS_other / d(owner)
+    // d(owner), gB = dSAS_other / d(owner); volume adjoint coefficients through the
+    // entry's contact face: vA = dV_owner / d(owner), vB = dV_other / d(owner)
     double4* gA;
     double4* gB;
+    double4* vA;
+    double4* vB;
 };
 
 // Contacts computed by one pass, deduplicated and canonicalised, in the reference's
@@ -57,11 +60,16 @@ struct NewContacts {
     double* pv_b;
     uint8_t* central;
     uint32_t* pair;
-    // optional: SAS adjoint coefficients, dSAS_x / d(y) for x, y in {a, b}
+    // optional: SAS adjoint coefficients, dSAS_x / d(y) for x, y in {a, b}, and volume
+    // adjoint coefficients dV_x / d(y) through the contact's face
     double4* gaa;
     double4* gab;
     double4* gba;
     double4* gbb;
+    double4* vaa;
+    double4* vab;
+    double4* vba;
+    double4* vbb;
 };
 
 // Every periodic image at id (g+1) n + j (populate_periodic_spheres, types.rs:351-375).
@@ -147,10 +155,12 @@ void launch_table_update(const NewContacts& nc, const uint32_t* nc_count, uint32
 // goes to *d_out, zeroed by the caller).
 void launch_list_flagged(const uint32_t* list, const uint32_t* count, uint32_t max_count, const uint8_t* flag,
                          uint32_t* out, uint32_t* d_out, cudaStream_t s);
-// grad (n x 4, overwritten) = d(sum_i w_i SAS_i)/d(x, y, z, r) from the table's adjoint
-// coefficients (w == null: all 1; balls without a cell or with zero SAS weigh 0).
-void launch_table_grad(uint32_t n, TableRef tab, const double* w, const uint8_t* cell_flag, const double* cell_sas,
-                       const double4* sph, double* grad, cudaStream_t s);
+// grad (n x 4, overwritten) = d(sum_i w_i SAS_i + sum_i v_i V_i)/d(x, y, z, r) from the
+// table's adjoint coefficients (w == null: every w_i = w_default; v == null: no volume
+// term; balls without a cell, or with zero SAS for the SAS term, weigh 0).
+void launch_table_grad(uint32_t n, TableRef tab, const double* w, double w_default, const double* v,
+                       const uint8_t* cell_flag, const double* cell_sas, const double4* sph, double* grad,
+                       cudaStream_t s);
 // Summary (updateable.rs:332-378): entries owned by their id a, in table order.
 void launch_owner_flags(const uint8_t* flags, uint32_t M, uint32_t* out, cudaStream_t s);
 void launch_summary_contacts(TableRef tab, uint32_t M, const uint32_t* off, uint32_t* a, uint32_t* b, double* area,

@@ -88,7 +88,7 @@ struct DevBufs {
     double* p_sa_b;
     double* p_pv_a;
     double* p_pv_b;
-    double* p_arcm;  // optional: first moment of each contact's arcs about a (3 per pair)
+    double* p_arcm;  // optional: first moments of each contact's arcs and area about a (6 per pair)
     // recompute lists
     uint32_t* redo_list;
     uint32_t* d_redo_count;

@@ -70,11 +70,14 @@ struct Table {
     DBuf<double> area, arc, sa, pv;
     DBuf<uint8_t> flags;
     DBuf<double4> gA, gB;  // SAS adjoint coefficients per entry
+    DBuf<double4> vA, vB;  // volume adjoint coefficients per entry
     uint64_t M = 0;
-    TableRef ref() const { return {off.p, a.p, b.p, area.p, arc.p, sa.p, pv.p, flags.p, gA.p, gB.p}; }
+    TableRef ref() const { return {off.p, a.p, b.p, area.p, arc.p, sa.p, pv.p, flags.p, gA.p, gB.p, vA.p, vB.p}; }
     void ensure(size_t n, size_t m) {
         gA.ensure(m);
         gB.ensure(m);
+        vA.ensure(m);
+        vB.ensure(m);
         off.ensure(n + 1);
         a.ensure(m);
         b.ensure(m);
@@ -95,6 +98,8 @@ struct Table {
         flags.swap(o.flags);
         gA.swap(o.gA);
         gB.swap(o.gB);
+        vA.swap(o.vA);
+        vB.swap(o.vB);
         std::swap(M, o.M);
     }
 };
@@ -145,6 +150,8 @@ void copy_state(UState& d, const UState& s, bool fp32, cudaStream_t st) {
     d.tab.flags.copy_from(s.tab.flags, s.tab.M, st);
     d.tab.gA.copy_from(s.tab.gA, s.tab.M, st);
     d.tab.gB.copy_from(s.tab.gB, s.tab.M, st);
+    d.tab.vA.copy_from(s.tab.vA, s.tab.M, st);
+    d.tab.vB.copy_from(s.tab.vB, s.tab.M, st);
     d.tab.M = s.tab.M;
     d.cell_flag.copy_from(s.cell_flag, n, st);
     d.cell_sas.copy_from(s.cell_sas, n, st);
@@ -203,7 +210,7 @@ struct vt_updateable {
     DBuf<uint32_t> nc_a, nc_b, nc_pair;
     DBuf<double> nc_area, nc_arc, nc_sa_a, nc_sa_b, nc_pv_a, nc_pv_b;
     DBuf<uint8_t> nc_central;
-    DBuf<double4> nc_gaa, nc_gab, nc_gba, nc_gbb;
+    DBuf<double4> nc_gaa, nc_gab, nc_gba, nc_gbb, nc_vaa, nc_vab, nc_vba, nc_vbb;
     DBuf<double> p_arcm;
     Table next_tab;
     DBuf<uint32_t> keep_cnt, new_cnt, tot_cnt, cursor, tmp_k;
@@ -242,10 +249,49 @@ struct vt_updateable {
         if (h_bbox) cudaFreeHost(h_bbox);
         cur.reset();
         bak.reset();
+        for (int k = 0; k < VT_UPD_NUM_STAGES; ++k) {
+            if (ev0[k]) cudaEventDestroy(ev0[k]);
+            if (ev1[k]) cudaEventDestroy(ev1[k]);
+        }
         if (own) cudaStreamDestroy(own);
     }
 
-    void sync() { VT_CUDA(cudaStreamSynchronize(stream)); }
+    void sync() {
+        ++stats.num_host_syncs;
+        VT_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    // stage timing of updates (vt_upd_set_timing)
+    bool timing = false;
+    cudaEvent_t ev0[VT_UPD_NUM_STAGES] = {}, ev1[VT_UPD_NUM_STAGES] = {};
+    bool used[VT_UPD_NUM_STAGES] = {};
+    double stage_ms[VT_UPD_NUM_STAGES] = {};
+    void t_reset() {
+        for (int k = 0; k < VT_UPD_NUM_STAGES; ++k) used[k] = false;
+    }
+    void t_begin(int k) {
+        if (!timing) return;
+        if (!ev0[k]) {
+            VT_CUDA(cudaEventCreate(&ev0[k]));
+            VT_CUDA(cudaEventCreate(&ev1[k]));
+        }
+        VT_CUDA(cudaEventRecord(ev0[k], stream));
+        used[k] = true;
+    }
+    void t_end(int k) {
+        if (timing && used[k]) VT_CUDA(cudaEventRecord(ev1[k], stream));
+    }
+    // after the operation's final sync
+    void t_collect() {
+        for (int k = 0; k < VT_UPD_NUM_STAGES; ++k) {
+            stage_ms[k] = 0.0;
+            if (timing && used[k]) {
+                float ms = 0.f;
+                VT_CUDA(cudaEventElapsedTime(&ms, ev0[k], ev1[k]));
+                stage_ms[k] = ms;
+            }
+        }
+    }
     uint32_t* w(int k) { return words.p + k; }
     void ensure_scan(size_t n) { scan_tmp.ensure(scan_tmp_words_needed(n) + 8); }
     void zero(void* p, size_t bytes) {
@@ -443,7 +489,7 @@ struct vt_updateable {
         b.p_sa_b = p_sa_b.p;
         b.p_pv_a = p_pv_a.p;
         b.p_pv_b = p_pv_b.p;
-        p_arcm.ensure(3 * (size_t)P + 3);
+        p_arcm.ensure(6 * (size_t)P + 6);
         b.p_arcm = adjoint ? p_arcm.p : nullptr;
         b.redo_list = redo_list.p;
         b.serial_list = serial_list.p;
@@ -475,7 +521,8 @@ struct vt_updateable {
 
     NewContacts nc_ref() {
         return {nc_a.p,    nc_b.p,      nc_area.p,  nc_arc.p,   nc_sa_a.p,  nc_sa_b.p, nc_pv_a.p,
-                nc_pv_b.p, nc_central.p, nc_pair.p, nc_gaa.p, nc_gab.p, nc_gba.p, nc_gbb.p};
+                nc_pv_b.p, nc_central.p, nc_pair.p, nc_gaa.p, nc_gab.p, nc_gba.p, nc_gbb.p,
+                nc_vaa.p,  nc_vab.p,    nc_vba.p,   nc_vbb.p};
     }
 
     // kept contacts of this pass (periodic dedup) as canonical new contacts; the count is
@@ -497,6 +544,10 @@ struct vt_updateable {
         nc_gab.ensure(P + 1);
         nc_gba.ensure(P + 1);
         nc_gbb.ensure(P + 1);
+        nc_vaa.ensure(P + 1);
+        nc_vab.ensure(P + 1);
+        nc_vba.ensure(P + 1);
+        nc_vbb.ensure(P + 1);
         if (P == 0) {
             zero(keep_off.p, 4);
             return;
@@ -623,16 +674,26 @@ struct vt_updateable {
     // update_using_affected (updateable.rs:476-514) for the involved balls (mark != 0),
     // listed sorted in S.affected (count on the device at d_count)
     void update_using_affected(UState& S, const uint32_t* d_count, uint32_t A) {
+        t_begin(4);
         const uint32_t P = gen_pairs(S, S.affected.p, d_count, A, mark.p);
         stats.num_pairs = P;
         DevBufs b = pair_bufs(S, P);
+        t_end(4);
+        t_begin(5);
         contacts(b, P);
+        t_end(5);
+        t_begin(6);
         extract_new(b, P);
         splice_table(S, mark.p, false, P);
         const float band = (fp32 && P > 0) ? kCellBand : 0.f;
         launch_table_cells(S.affected.p, d_count, A, S.tab.ref(), sph.p, S.excl.p, S.cell_flag.p, S.cell_sas.p,
                            S.cell_vol.p, band, band > 0.f ? unsure.p : nullptr, stream);
-        if (band > 0.f) refresh_unsure_cells(S, d_count, A);
+        t_end(6);
+        if (band > 0.f) {
+            t_begin(7);
+            refresh_unsure_cells(S, d_count, A);
+            t_end(7);
+        }
     }
 
     // table size, cell count and error bits after an operation
@@ -641,6 +702,7 @@ struct vt_updateable {
         // coefficients are whole after a full computation with moments, and stay whole
         // while every update records them
         S.adj_valid = S.full ? adjoint : (S.adj_valid && adjoint);
+        t_begin(8);
         nflags.ensure(n + 1);
         noff.ensure(n + 2);
         launch_cell_flags_u32(S.cell_flag.p, n, nflags.p, stream);
@@ -649,8 +711,11 @@ struct vt_updateable {
         VT_CUDA(cudaMemcpyAsync(h_words + 0, S.tab.off.p + n, 4, cudaMemcpyDeviceToHost, stream));
         VT_CUDA(cudaMemcpyAsync(h_words + 1, noff.p + n, 4, cudaMemcpyDeviceToHost, stream));
         VT_CUDA(cudaMemcpyAsync(h_words + 2, w(kWErr), 4, cudaMemcpyDeviceToHost, stream));
+        t_end(8);
+        t_end(9);
         sync();
         VT_CUDA(cudaGetLastError());
+        t_collect();
         S.tab.M = h_words[0];
         S.num_cells = h_words[1];
         stats.device_error_bits = h_words[2];
@@ -676,6 +741,7 @@ struct vt_updateable {
 
     void begin_op() {
         VT_CUDA(cudaSetDevice(device));
+        t_reset();
         zero(words.p, kWords * 4);
         const uint32_t one = 1;
         VT_CUDA(cudaMemcpyAsync(w(kWOne), &one, 4, cudaMemcpyHostToDevice, stream));
@@ -740,6 +806,8 @@ struct vt_updateable {
         const uint32_t n = S.n;
         const uint32_t thr = std::max<uint32_t>(n / 2, 10);  // size_threshold_for_full_reinit
         if (k == 0 || n == 0) return VT_OK;
+        t_begin(9);
+        t_begin(0);
         flags.ensure(k + 1);
         flags_off.ensure(k + 2);
         S.changed.ensure(k + 1);
@@ -758,17 +826,22 @@ struct vt_updateable {
         VT_CUDA(cudaMemcpyAsync(h_words + 0, d_kc, 4, cudaMemcpyDeviceToHost, stream));
         VT_CUDA(cudaMemcpyAsync(h_words + 1, w(kWDistinct), 4, cudaMemcpyDeviceToHost, stream));
         VT_CUDA(cudaMemcpyAsync(h_words + 2, w(kWNbrNew), 4, cudaMemcpyDeviceToHost, stream));
+        t_end(0);
         sync();
         const uint32_t kc = h_words[0], distinct = h_words[1], nbr_new = h_words[2];
         if (kc == 0) return VT_OK;  // no change: update returns false
         if (kc > thr || (uint64_t)kc + nbr_new > thr) {
+            t_reset();  // a full reinit follows: no update stages to report
             *need_full = true;
             return VT_OK;
         }
         // apply, rebuild spheres and grid, search the frontier (changed + old neighbours)
+        t_begin(1);
         launch_apply_changed(S.changed.p, changed_ball.p, d_kc, k, S.balls.p, stream);
         int st = build_spheres(S);
+        t_end(1);
         if (st != VT_OK) return st;
+        t_begin(2);
         const uint32_t A1 = distinct + nbr_new;
         nflags.ensure(n + 1);
         noff.ensure(n + 2);
@@ -791,7 +864,9 @@ struct vt_updateable {
             st = search(S, more_list.p, more, t2);
             if (st != VT_OK) return st;
         }
+        t_end(2);
         // splice the neighbour lists
+        t_begin(3);
         next_lists.cnt.ensure(n + 1);
         next_lists.off.ensure(n + 1);
         launch_splice_counts(n, mark.p, row_of.p, S.lists.cnt.p, t1.cnt.p, more ? t2.cnt.p : nullptr,
@@ -817,6 +892,7 @@ struct vt_updateable {
         S.n_affected = A;
         S.affected_dups = more == 0 && kc > distinct;
         S.full = false;
+        t_end(3);
         update_using_affected(S, noff.p + n, A);
         st = finish(S);
         if (st != VT_OK) return st;
@@ -926,14 +1002,15 @@ struct vt_updateable {
         return VT_OK;
     }
 
-    // adjoint of sum_i w_i SAS_i over the current state (w == null: every w_i = 1), a
-    // gather over the table's per-entry coefficients (no contour is recomputed)
-    int grad_sas(const double* d_w, double* d_grad) {
+    // adjoint of sum_i w_i SAS_i + sum_i v_i V_i over the current state (w == null: every
+    // w_i = w_default; v == null: no volume term), a gather over the table's per-entry
+    // coefficients (no contour is recomputed)
+    int grad(const double* d_w, double w_default, const double* d_v, double* d_grad) {
         UState& S = *cur;
         const uint32_t n = S.n;
         if (n == 0) return VT_OK;
         if (!S.adj_valid) {
-            set_last_error("SAS adjoint unavailable: an operation ran with the adjoint off "
+            set_last_error("adjoint unavailable: an operation ran with the adjoint off "
                            "(vt_upd_set_adjoint); enable it and init again");
             return VT_ERR_INVALID;
         }
@@ -941,7 +1018,7 @@ struct vt_updateable {
             int st = build_spheres(S);
             if (st != VT_OK) return st;
         }
-        launch_table_grad(n, S.tab.ref(), d_w, S.cell_flag.p, S.cell_sas.p, sph.p, d_grad, stream);
+        launch_table_grad(n, S.tab.ref(), d_w, w_default, d_v, S.cell_flag.p, S.cell_sas.p, sph.p, d_grad, stream);
         sync();
         VT_CUDA(cudaGetLastError());
         return VT_OK;
@@ -1206,7 +1283,14 @@ int vt_upd_grad_sas(vt_updateable* h, const double* d_w_sas, double* d_grad) {
     if (check_handle(h) || !d_grad) return VT_ERR_INVALID;
     return guarded([&]() -> int {
         h->begin_op();
-        return h->grad_sas(d_w_sas, d_grad);
+        return h->grad(d_w_sas, 1.0, nullptr, d_grad);
+    });
+}
+int vt_upd_grad(vt_updateable* h, const double* d_w_sas, const double* d_v_volume, double* d_grad) {
+    if (check_handle(h) || !d_grad) return VT_ERR_INVALID;
+    return guarded([&]() -> int {
+        h->begin_op();
+        return h->grad(d_w_sas, 0.0, d_v_volume, d_grad);
     });
 }
 int vt_upd_set_adjoint(vt_updateable* h, int on) {
@@ -1247,6 +1331,16 @@ int vt_upd_affected_ids(vt_updateable* h, uint64_t* out) {
 int vt_upd_stats(const vt_updateable* h, vt_stats* out) {
     if (check_handle(h) || !out) return VT_ERR_INVALID;
     *out = h->stats;
+    return VT_OK;
+}
+int vt_upd_set_timing(vt_updateable* h, int on) {
+    if (check_handle(h)) return VT_ERR_INVALID;
+    h->timing = on != 0;
+    return VT_OK;
+}
+int vt_upd_stage_times(const vt_updateable* h, double* ms) {
+    if (check_handle(h) || !ms) return VT_ERR_INVALID;
+    for (int k = 0; k < VT_UPD_NUM_STAGES; ++k) ms[k] = h->stage_ms[k];
     return VT_OK;
 }
 

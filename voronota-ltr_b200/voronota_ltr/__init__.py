@@ -58,10 +58,12 @@ class VtStats(ctypes.Structure):
         ("total_sas_area", ctypes.c_double), ("total_volume", ctypes.c_double),
         ("total_contact_area", ctypes.c_double), ("device_error_bits", ctypes.c_uint32),
         ("num_kernel_launches", ctypes.c_uint64), ("num_cell_redo", ctypes.c_uint64),
-        ("fp32_kernel", ctypes.c_uint64)]
+        ("fp32_kernel", ctypes.c_uint64), ("num_host_syncs", ctypes.c_uint64)]
 
 STAGES = ("prepare", "images", "grid", "neighbor_count", "neighbor_fill", "contact", "fp64_recompute",
           "serial_fallback", "cells", "output", "call")
+UPD_STAGES = ("changed", "grid", "search", "lists", "pairs", "contacts", "table_cells", "cell_refresh", "finish",
+              "call")
 
 
 class VtDeviceOutputs(ctypes.Structure):
@@ -150,8 +152,11 @@ def library():
     L.vt_upd_num_affected.restype = ctypes.c_uint64
     L.vt_upd_affected_ids.argtypes = [_vp, _u64p]
     L.vt_upd_stats.argtypes = [_vp, ctypes.POINTER(VtStats)]
+    L.vt_upd_set_timing.argtypes = [_vp, ctypes.c_int]
+    L.vt_upd_stage_times.argtypes = [_vp, _f64p]
     L.vt_upd_set_adjoint.argtypes = [_vp, ctypes.c_int]
     L.vt_upd_grad_sas.argtypes = [_vp, ctypes.c_void_p, ctypes.c_void_p]
+    L.vt_upd_grad.argtypes = [_vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.vt_compute_batch.argtypes = [_f64p, _u64p, ctypes.c_uint64, ctypes.c_double, ctypes.c_int,
                                    ctypes.POINTER(_vp)]
     L.vt_engine_compute_batch_device.argtypes = [_vp, ctypes.c_void_p, _u64p, ctypes.c_uint64, ctypes.c_double,
@@ -787,10 +792,25 @@ class UpdateableTessellation:
         state; d_w_ptr 0/None: the total SAS."""
         _check(self._L.vt_upd_grad_sas(self._h, d_w_ptr or None, d_grad_ptr))
 
+    def set_timing(self, on: bool = True):
+        """Record per-stage CUDA events in later updates (stage_times)."""
+        _check(self._L.vt_upd_set_timing(self._h, 1 if on else 0))
+
+    def stage_times(self) -> dict:
+        """Device milliseconds per stage of the last update (UPD_STAGES), with timing on."""
+        buf = (ctypes.c_double * len(UPD_STAGES))()
+        _check(self._L.vt_upd_stage_times(self._h, buf))
+        return dict(zip(UPD_STAGES, list(buf)))
+
+    def grad_device(self, d_w_ptr, d_v_ptr, d_grad_ptr: int):
+        """d_grad (N x 4 doubles on the device) = d(sum w SAS + sum v volume)/d(x, y, z, r)
+        of the current state; a 0/None weight pointer leaves its term out."""
+        _check(self._L.vt_upd_grad(self._h, d_w_ptr or None, d_v_ptr or None, d_grad_ptr))
+
     def set_adjoint(self, on: bool = True):
-        """Record the arc moments behind grad_sas_device (default on).  Off makes updates
-        about a tenth faster; grad_sas_device then raises until a full computation ran
-        with it on again."""
+        """Record the arc and face moments behind grad_sas_device / grad_device (default
+        on).  Off makes updates about a tenth faster; the adjoints then raise until a full
+        computation ran with it on again."""
         _check(self._L.vt_upd_set_adjoint(self._h, 1 if on else 0))
 
 
