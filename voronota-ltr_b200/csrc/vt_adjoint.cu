@@ -78,6 +78,7 @@ __global__ void k_sas_scale(uint32_t n, const double* __restrict__ w_eff, const 
 
 // FP64 adjoint: all valid pairs, or (from_list) the pairs the FP32 adjoint listed.  At
 // most 128 registers (4 resident blocks), like the FP64 contact kernel.
+template <bool VOL>
 __global__ void __launch_bounds__(kWarps * 32, 4)
     k_adjoint64(DevBufs b, uint32_t P, int from_list, const double* __restrict__ u_contact,
                 const double* __restrict__ w_eff, const double* __restrict__ v_eff, double* __restrict__ grad) {
@@ -131,11 +132,20 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
                 if (nid[e] == c) return sph[nslot[e]];
             return make_double4(0.0, 0.0, 0.0, 0.0);
         };
-        adjoint_pair(G, co.full, len, co.q.p, nxt.p, co.q.ang, co.q.rid, nxt.lid, sphere_of, grad, n);
+        adjoint_pair<VOL>(G, co.full, len, co.q.p, nxt.p, co.q.ang, co.q.rid, nxt.lid, sphere_of, grad, n);
     }
 }
 
 int gb(size_t n) { return grid_blocks(n, 256, 148 * 16); }
+
+void launch_adjoint64(const DevBufs& b, uint32_t P, int from_list, const double* u_contact, const double* w_eff,
+                      const double* v_eff, double* grad, cudaStream_t s) {
+    const int g = grid_blocks(P, kWarps, 148 * 64);
+    if (v_eff)
+        k_adjoint64<true><<<g, kWarps * 32, 0, s>>>(b, P, from_list, u_contact, w_eff, v_eff, grad);
+    else
+        k_adjoint64<false><<<g, kWarps * 32, 0, s>>>(b, P, from_list, u_contact, w_eff, v_eff, grad);
+}
 
 }  // namespace
 
@@ -159,9 +169,9 @@ void launch_adjoint(const DevBufs& b, uint32_t P, const double* w_sas, const dou
             // FP32 contours; pairs with a decision in the band are redone in FP64
             cudaMemsetAsync(b.d_redo_count, 0, sizeof(uint32_t), s);
             launch_adjoint_f32(b, P, u_contact, w_eff, ve, grad, s);
-            k_adjoint64<<<grid_blocks(P, kWarps, 148 * 64), kWarps * 32, 0, s>>>(b, P, 1, u_contact, w_eff, ve, grad);
+            launch_adjoint64(b, P, 1, u_contact, w_eff, ve, grad, s);
         } else {
-            k_adjoint64<<<grid_blocks(P, kWarps, 148 * 64), kWarps * 32, 0, s>>>(b, P, 0, u_contact, w_eff, ve, grad);
+            launch_adjoint64(b, P, 0, u_contact, w_eff, ve, grad, s);
         }
         count_launch();
     }

@@ -36,11 +36,12 @@ struct AdjPair {
     double area;       // the forward's area of the contact
 };
 
-// Warp-collective: every lane calls it.  Lane k < len holds contour point P (absolute),
+// Warp-collective: every lane calls it.  VOL: the pair carries volume weights (va, vb,
+// area); without them the pyramid terms are compiled out.  Lane k < len holds contour point P (absolute),
 // the next point Pn, the arc angle of its segment, its rid and the next point's lid;
 // full: no cut (the whole circle).  sphere_of(id) returns the double sphere of a's
 // neighbour with that reference id (w = 0 if not found).
-template <typename SphereOf>
+template <bool VOL, typename SphereOf>
 __device__ __forceinline__ void adjoint_pair(const AdjPair& G, bool full, int len, V3<double> P, V3<double> Pn,
                                              double ang, uint32_t rid, uint32_t nlid, SphereOf sphere_of,
                                              double* grad, uint32_t n) {
@@ -52,8 +53,11 @@ __device__ __forceinline__ void adjoint_pair(const AdjPair& G, bool full, int le
     // the pyramid volumes t_ab A / 3 and t_ba A / 3 weigh the area like u does
     // (t_ab = (D^2 + Ra^2 - Rb^2) / (2 D): signed distance from p_a to the radical plane)
     const double dRR = Ra * Ra - Rb * Rb;
-    const double t_ab = 0.5 * D + dRR / (2.0 * D), t_ba = D - t_ab;
-    const double u = G.u + (G.va * t_ab + G.vb * t_ba) / 3.0;
+    double u = G.u;
+    if constexpr (VOL) {
+        const double t_ab = 0.5 * D + dRR / (2.0 * D), t_ba = D - t_ab;
+        u += (G.va * t_ab + G.vb * t_ba) / 3.0;
+    }
     V3<double> ga = mk<double>(0, 0, 0), gb = mk<double>(0, 0, 0);
     double gra = 0.0, grb = 0.0, Lk = 0.0;
     V3<double> Xk = mk<double>(0, 0, 0);
@@ -112,7 +116,7 @@ __device__ __forceinline__ void adjoint_pair(const AdjPair& G, bool full, int le
             gra += wa * L * cmix * s - wb * Rb * Ra * L * s;
             grb += wb * L * cmix * s - wa * Ra * Rb * L * s;
         }
-        if (G.va != 0.0 || G.vb != 0.0) {
+        if (VOL && (G.va != 0.0 || G.vb != 0.0)) {
             // pyramid volumes through t_ab and t_ba at fixed area:
             // dt_ab/dD = 1/2 - dRR/(2 D^2), dt_ab/dRa = Ra/D, dt_ab/dRb = -Rb/D, t_ba = D - t_ab
             const double c = G.area / 3.0;
@@ -179,7 +183,8 @@ __device__ __forceinline__ V3<double> snap_vertex(const AdjPair& G, V3<double> y
 }
 
 // Weights of pair p's contact: u of its output contact (kept pairs), w and v of both
-// ends (a periodic image's cell is its own ball's, reached through that ball's pairs).
+// ends (a periodic image's cell is its own ball's, reached through that ball's pairs);
+// v_eff null: no volume term.
 __device__ __forceinline__ bool adjoint_weights(const DevBufs& b, uint32_t p, uint32_t a, uint32_t bid,
                                                 const double* u_contact, const double* w_eff,
                                                 const double* v_eff, AdjPair& G) {
@@ -189,7 +194,7 @@ __device__ __forceinline__ bool adjoint_weights(const DevBufs& b, uint32_t p, ui
     G.wb = bid < b.n ? w_eff[bid] : 0.0;
     G.va = v_eff ? v_eff[a] : 0.0;
     G.vb = (v_eff && bid < b.n) ? v_eff[bid] : 0.0;
-    G.area = b.p_area[p];
+    G.area = v_eff ? b.p_area[p] : 0.0;
     return G.u != 0.0 || G.wa != 0.0 || G.wb != 0.0 || G.va != 0.0 || G.vb != 0.0;
 }
 

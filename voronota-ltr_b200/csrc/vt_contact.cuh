@@ -891,56 +891,38 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             // + (1 - cos t) axis x e1) (the segment's centroid lies 4 rho sin^3(t/2) /
             // (3 (t - sin t)) from q along the arc's bisector); sin t and cos t come from the
             // arc's end points, as for the arcs' moment
-            const double rho = (double)g.ic.r;
-            const V3<double> aw = wide3(g.A.c);
-            const V3<double> qa = wide3(g.ic.c) - aw;
-            const bool arc = init && on && q.ang > (T)0 && rho > 0.0;
-            // the arc's sin t e1 + (1 - cos t) axis x e1 and cos t (one lane per arc)
-            auto arc_terms = [&](V3<double>& m, double& ct) {
-                const V3<double> qc = wide3(g.ic.c);
-                const V3<double> e1 = (wide3(q.p) - qc) / rho, e2 = (wide3(p2.p) - qc) / rho;
-                const V3<double> f = cross(wide3(g.axis), e1);
-                ct = dot(e2, e1);
-                m = e1 * dot(e2, f) + f * (1.0 - ct);
-                return dot(e2, f);
-            };
-            {  // the arcs (two passes keep fewer doubles live at once)
-                V3<double> xk = mk<double>(0, 0, 0);
-                if (!init) {
-                    if (lane == 0) xk = qa * (kTau * rho);
-                } else if (arc) {
-                    V3<double> m;
-                    double ct;
-                    arc_terms(m, ct);
-                    xk = qa * (rho * (double)q.ang) + m * (rho * rho);
+            // Formed in the contour's own precision (the FP32 kernel's coordinates are
+            // relative to a, so the moments carry no large offsets), one lane per contour
+            // point, then summed over the warp and widened.
+            const T rho = g.ic.r;
+            const V3<T> qa = g.ic.c - g.A.c;
+            V3<T> xk = mk<T>(0, 0, 0), ak = mk<T>(0, 0, 0);
+            if (!init) {
+                if (lane == 0) {
+                    xk = qa * ((T)kTau * rho);
+                    ak = qa * area;
                 }
-                const double xx = wsum(xk.x);
-                if (lane == 0) g.xm_out[0] = xx;
-                const double xy = wsum(xk.y);
-                if (lane == 0) g.xm_out[1] = xy;
-                const double xz = wsum(xk.z);
-                if (lane == 0) g.xm_out[2] = xz;
+            } else if (on) {
+                const V3<T> bw = bary - g.A.c, pk = q.p - g.A.c, pn = p2.p - g.A.c;
+                ak = (bw + pk + pn) * ((T)0.5 * norm(cross(pk - bw, pn - bw)) / (T)3);
+                if (q.ang > (T)0 && rho > (T)0) {
+                    const V3<T> e1 = (q.p - g.ic.c) / rho, e2 = (p2.p - g.ic.c) / rho;
+                    const V3<T> f = cross(g.axis, e1);
+                    const T ct = dot(e2, e1), st = dot(e2, f);
+                    const V3<T> m = e1 * st + f * ((T)1 - ct);
+                    xk = qa * (rho * q.ang) + m * (rho * rho);
+                    ak = ak + qa * ((T)0.5 * rho * rho * (q.ang - st)) + m * (rho * rho * rho * ((T)1 - ct) / (T)6);
+                }
             }
-            {  // the area
-                V3<double> ak = mk<double>(0, 0, 0);
-                if (!init) {
-                    if (lane == 0) ak = qa * (double)area;
-                } else if (on) {
-                    const V3<double> bw = wide3(bary) - aw, pk = wide3(q.p) - aw, pn = wide3(p2.p) - aw;
-                    ak = (bw + pk + pn) * (0.5 * norm(cross(pk - bw, pn - bw)) / 3.0);
-                    if (arc) {
-                        V3<double> m;
-                        double ct;
-                        const double st = arc_terms(m, ct), th = (double)q.ang;
-                        ak = ak + qa * (0.5 * rho * rho * (th - st)) + m * (rho * rho * rho * (1.0 - ct) / 6.0);
-                    }
-                }
-                const double ax = wsum(ak.x);
-                if (lane == 0) g.xm_out[3] = ax;
-                const double ay = wsum(ak.y);
-                if (lane == 0) g.xm_out[4] = ay;
-                const double az = wsum(ak.z);
-                if (lane == 0) g.xm_out[5] = az;
+            const T s0 = wsum(xk.x), s1 = wsum(xk.y), s2 = wsum(xk.z);
+            const T s3 = wsum(ak.x), s4 = wsum(ak.y), s5 = wsum(ak.z);
+            if (lane == 0) {
+                g.xm_out[0] = (double)s0;
+                g.xm_out[1] = (double)s1;
+                g.xm_out[2] = (double)s2;
+                g.xm_out[3] = (double)s3;
+                g.xm_out[4] = (double)s4;
+                g.xm_out[5] = (double)s5;
             }
         }
     }

@@ -93,6 +93,7 @@ __global__ void __launch_bounds__(W * 32, VT_C32_MINB * 4 / W)
 // FP32 adjoint: the contour recomputed in FP32 (relative to a), the gradient formed in
 // double from its points; pairs whose recomputation is unsure or overflows are listed for
 // the FP64 adjoint.
+template <bool VOL>
 __global__ void __launch_bounds__(kWarps * 32, 4)
     k_adjoint32(DevBufs b, uint32_t P, float band, const double* __restrict__ u_contact,
                 const double* __restrict__ w_eff, const double* __restrict__ v_eff, double* __restrict__ grad) {
@@ -166,7 +167,7 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
             // a nearly full or nearly empty arc keeps the FP32 branch of the angle
             if (fabs((double)co.q.ang - ang) > 1.0) ang = (double)co.q.ang;
         }
-        adjoint_pair(G, co.full, len, P0, P1, ang, co.q.rid, nlid, sphere_of, grad, n);
+        adjoint_pair<VOL>(G, co.full, len, P0, P1, ang, co.q.rid, nlid, sphere_of, grad, n);
     }
 }
 
@@ -316,7 +317,10 @@ void launch_adjoint_f32(const DevBufs& b, uint32_t P, const double* u_contact, c
     size_t g = (P + kWarps - 1) / kWarps;
     if (g < 1) g = 1;
     if (g > 148 * 64) g = 148 * 64;
-    k_adjoint32<<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band, u_contact, w_eff, v_eff, grad);
+    if (v_eff)
+        k_adjoint32<true><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band, u_contact, w_eff, v_eff, grad);
+    else
+        k_adjoint32<false><<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band, u_contact, w_eff, v_eff, grad);
     count_launch();
 }
 

@@ -46,6 +46,7 @@ enum Word : int {
     kWBig = 11,      // rows of a search longer than the warp sort buffer
     kWUnsure = 12,   // affected balls with an uncertain compute_sas branch (FP32)
     kWMarked = 13,   // balls marked for their FP64 refresh
+    kWQueue = 14,    // work counter of the persistent FP32 contact launch
     kWords = 16,
 };
 
@@ -389,6 +390,11 @@ struct vt_updateable {
         b.d_cell_redo_count = w(kWCellRedo);
         b.fp32_band = (float)(fp32_band_ulps * 1.1920928955078125e-07);
         b.slot_is_id = 1;
+        // FP32 contact launch: 2 warps per block, persistent, pairs taken 4 at a time (the
+        // form the engine's autotuner picks on the benchmark structures)
+        b.c32_warps = 2;
+        b.c32_chunk = 4;
+        b.c32_queue = w(kWQueue);
         return b;
     }
 
