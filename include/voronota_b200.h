@@ -174,9 +174,11 @@ int vt_engine_stage_times(const vt_engine* e, double* ms);
  * this input and keeps the fastest for later calls of the engine -- warps per block of the
  * FP32 contact kernel (2, 4 or 8; one warp per pair), its launch form (grid-stride, or
  * persistent with warps taking chunks of 4 or 16 pairs from a work counter; chunk 0 is
- * grid-stride) and the grid cell edge as a multiple of the minimum edge 2 max R + 0.25
- * (1, 1.25 or 1.5).  Results do not depend on any of them.  A new engine (and the one
- * behind the stateless calls) starts with 2 warps, chunks of 4 pairs and scale 1.
+ * grid-stride) and the grid cell edge as a multiple of the reach 2 max R + 0.25 (0.5,
+ * 0.75, 1 or 1.25; below 1 the neighbour search scans a 5 x 5 x 5 cell stencil culled to
+ * the rows and x-ranges within reach).  Results do not depend on any of them.  A new
+ * engine (and the one behind the stateless calls) starts with 2 warps, chunks of 4 pairs
+ * and scale 0.5.  vt_engine_set_tuning accepts scales in [0.5, 4].
  * batch_offsets: NULL for one structure, else as vt_engine_compute_batch_device. */
 int vt_engine_autotune_device(vt_engine* e, const double* d_xyzr, uint64_t n, double probe,
                               const double* periodic_box9, int precision, const uint64_t* batch_offsets,

@@ -33,7 +33,7 @@ def test_configurations_give_identical_results(periodic):
     d = torch.from_numpy(balls).cuda()
     torch.cuda.synchronize()
     ref = None
-    configs = [(w, c, 0) for w in (2, 4, 8) for c in (1.0, 1.25, 1.5)] + [(2, 1.0, 4), (8, 1.0, 16)]
+    configs = [(w, c, 0) for w in (2, 4, 8) for c in (0.5, 1.0, 1.5)] + [(2, 0.75, 4), (8, 1.0, 16), (2, 0.5, 4)]
     for w, c, ch in configs:
         e.set_tuning(w, c, ch)
         assert e.tuning() == {"warps_per_block": w, "cell_scale": c, "chunk": ch}
@@ -45,6 +45,8 @@ def test_configurations_give_identical_results(periodic):
             _same(r, ref)
     with pytest.raises(V.VoronotaError):
         e.set_tuning(3, 1.0)
+    with pytest.raises(V.VoronotaError):
+        e.set_tuning(2, 0.4)  # finer than half the reach: the stencil would exceed 5^3
 
 
 def test_autotune_on_a_batch():
@@ -58,7 +60,7 @@ def test_autotune_on_a_batch():
     d = torch.from_numpy(balls).cuda()
     torch.cuda.synchronize()
     t = e.autotune_device(d.data_ptr(), len(balls), 1.4, precision="fp32", offsets=off)
-    assert t["warps_per_block"] in (2, 4, 8) and t["cell_scale"] in (1.0, 1.25, 1.5) and t["chunk"] in (0, 4, 16)
+    assert t["warps_per_block"] in (2, 4, 8) and t["cell_scale"] in (0.5, 0.75, 1.0, 1.25) and t["chunk"] in (0, 4, 16)
     e.compute_batch_device(d.data_ptr(), off, 1.4, "fp32")
     got = e.download_batch()
     ref = V.compute_batch((balls, off), 1.4, "fp32")

@@ -60,8 +60,8 @@ __global__ void k_struct_bbox(const double4* __restrict__ sph, const uint32_t* _
     }
 }
 
-// plan_grid per structure: cell edge = max(2 max R + 0.25, 1), coarsened so that the
-// structure's grid has at most 8 n_s + 4096 cells
+// plan_grid per structure: cell edge = cell_scale x max(2 max R + 0.25, 1) (cell_scale >=
+// 0.5), coarsened so that the structure's grid has at most 8 n_s + 4096 cells
 __global__ void k_struct_grid(const BBox* __restrict__ bb, const uint32_t* __restrict__ off, uint32_t S,
                               double cell_scale, GridDev* __restrict__ grids, uint32_t* __restrict__ ncell) {
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
@@ -69,6 +69,8 @@ __global__ void k_struct_grid(const BBox* __restrict__ bb, const uint32_t* __res
         GridDev g{};
         if (ns == 0) {
             g.cell = 1.0;
+            g.reach = 1.0;
+            g.half = 1;
             g.dx = g.dy = g.dz = 1;
             grids[s] = g;
             ncell[s] = 0;
@@ -78,7 +80,7 @@ __global__ void k_struct_grid(const BBox* __restrict__ bb, const uint32_t* __res
         const double reach = fmax(2.0 * b.max_r + 0.25, 1.0);
         double ext[3];
         for (int k = 0; k < 3; ++k) ext[k] = (b.mx[k] - b.mn[k]) + 2.0 * reach;
-        double cell = reach * cell_scale;
+        double cell = reach * (cell_scale > 0.5 ? cell_scale : 0.5);
         int d[3];
         for (int k = 0; k < 3; ++k) d[k] = (int)floor(ext[k] / cell) + 1;
         double vol = (double)d[0] * d[1] * d[2];
@@ -89,6 +91,8 @@ __global__ void k_struct_grid(const BBox* __restrict__ bb, const uint32_t* __res
             vol = (double)d[0] * d[1] * d[2];
         }
         g.cell = cell;
+        g.reach = reach;
+        g.half = cell >= reach ? 1 : 2;
         g.ox = b.mn[0] - reach;
         g.oy = b.mn[1] - reach;
         g.oz = b.mn[2] - reach;

@@ -379,7 +379,7 @@ struct vt_engine {
     // sets one: what the autotuner picks on protein-like inputs of 20k-200k balls
     int c32_warps = 2;        // warps per block of the FP32 contact kernel
     int c32_chunk = 4;        // > 0: persistent FP32 contact launch, pairs taken in chunks
-    double cell_scale = 1.0;  // grid cell edge / the minimum edge (2 max R + 0.25)
+    double cell_scale = 0.5;  // grid cell edge / the reach 2 max R + 0.25 (0.5 .. 4; below 1: a 5^3 stencil)
     // state of the last call
     vt_stats stats{};
     bool contacts_only = false;
@@ -912,7 +912,7 @@ struct vt_engine {
         }
         if (st == VT_OK) {
             double best_s = cell_scale, best_t = 1e300;
-            for (double sc : {1.0, 1.25, 1.5}) {
+            for (double sc : {0.5, 0.75, 1.0, 1.25}) {
                 cell_scale = sc;
                 double t = 0.0;
                 st = stage_sum({2, 3, 4}, &t);
@@ -1166,7 +1166,7 @@ int vt_engine_get_tuning(const vt_engine* e, int* warps, double* cell_scale, int
     return VT_OK;
 }
 int vt_engine_set_tuning(vt_engine* e, int warps, double cell_scale, int chunk) {
-    if (!e || (warps != 2 && warps != 4 && warps != 8) || !(cell_scale >= 1.0) || !(cell_scale <= 4.0) ||
+    if (!e || (warps != 2 && warps != 4 && warps != 8) || !(cell_scale >= 0.5) || !(cell_scale <= 4.0) ||
         chunk < 0 || chunk > 256)
         return VT_ERR_INVALID;
     e->c32_warps = warps;

@@ -200,27 +200,37 @@ __global__ void __launch_bounds__(kSearchWarps * 32, FILL ? 7 : 9) k_search(DevB
         const Sph<double> A = sph_of(A4);
         int cx = cell_coord(A4.x, g.ox, g.cell, g.dx), cy = cell_coord(A4.y, g.oy, g.cell, g.dy),
             cz = cell_coord(A4.z, g.oz, g.cell, g.dz);
+        // stencil rows (y, z) of up to 2 half + 1 cells in x, one per lane; a row whose y and
+        // z slabs lie beyond the reach from the centre is empty, and a row's x-range is cut
+        // to the cells within reach (every intersecting ball is closer than the reach, and
+        // floor is monotone, so the cut loses none)
+        const int side = 2 * g.half + 1;
         uint32_t rbeg = 0, rcnt = 0;
-        if (lane < 9) {
-            int y = cy + lane / 3 - 1, z = cz + lane % 3 - 1;
+        if (lane < side * side) {
+            const int y = cy + lane / side - g.half, z = cz + lane % side - g.half;
             if (y >= 0 && y < g.dy && z >= 0 && z < g.dz) {
-                int x0 = cx > 0 ? cx - 1 : 0, x1 = cx + 1 < g.dx ? cx + 1 : g.dx - 1;
-                rbeg = b.cell_start[cbase + cell_key(g, x0, y, z)];
-                rcnt = b.cell_start[cbase + cell_key(g, x1, y, z) + 1] - rbeg;
+                const double ylo = g.oy + y * g.cell, zlo = g.oz + z * g.cell;
+                const double ey = fmax(fmax(ylo - A4.y, A4.y - (ylo + g.cell)), 0.0);
+                const double ez = fmax(fmax(zlo - A4.z, A4.z - (zlo + g.cell)), 0.0);
+                const double rem = g.reach * g.reach - ey * ey - ez * ez;
+                if (rem >= 0.0) {
+                    const double ext = sqrt(rem);
+                    int x0 = cell_coord(A4.x - ext, g.ox, g.cell, g.dx), x1 = cell_coord(A4.x + ext, g.ox, g.cell, g.dx);
+                    x0 = x0 > cx - g.half ? x0 : cx - g.half;
+                    x1 = x1 < cx + g.half ? x1 : cx + g.half;
+                    if (x0 <= x1) {
+                        rbeg = b.cell_start[cbase + cell_key(g, x0, y, z)];
+                        rcnt = b.cell_start[cbase + cell_key(g, x1, y, z) + 1] - rbeg;
+                    }
+                }
             }
         }
         uint32_t incl = rcnt;
-        for (int o = 1; o < 16; o <<= 1) {
+        for (int o = 1; o < 32; o <<= 1) {
             uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += t;
         }
-        uint32_t total = __shfl_sync(0xffffffffu, incl, 8);
-        uint32_t r_incl[9], r_beg[9];
-#pragma unroll
-        for (int r = 0; r < 9; ++r) {
-            r_incl[r] = __shfl_sync(0xffffffffu, incl, r);
-            r_beg[r] = __shfl_sync(0xffffffffu, rbeg, r);
-        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
         // a row longer than the warp sort buffer is written unsorted to the CSR by the
         // fill pass and sorted there by k_big_sort
         const uint32_t row_cnt = FILL ? b.nb_cnt[row] : 0u;
@@ -233,13 +243,19 @@ __global__ void __launch_bounds__(kSearchWarps * 32, FILL ? 7 : 9) k_search(DevB
             bool hit = false, hid = false;
             double val = 0.0;
             uint32_t cid = 0, cslot = 0;
-            if (t < total) {
-                int r = 0;
+            // candidate t lies in the first row whose inclusive count exceeds it
+            int r = 0;
 #pragma unroll
-                for (int k = 0; k < 8; ++k)
-                    if (r_incl[k] <= t) r = k + 1;
-                uint32_t prev = r == 0 ? 0 : r_incl[r - 1];
-                uint32_t idx = r_beg[r] + (t - prev);
+            for (int step = 16; step > 0; step >>= 1) {
+                const uint32_t v = __shfl_sync(0xffffffffu, incl, r + step - 1);
+                if (v <= t) r += step;
+            }
+            r = r > 31 ? 31 : r;
+            const uint32_t r_end = __shfl_sync(0xffffffffu, incl, r);
+            const uint32_t r_cnt = __shfl_sync(0xffffffffu, rcnt, r);
+            const uint32_t r_beg = __shfl_sync(0xffffffffu, rbeg, r);
+            if (t < total) {
+                uint32_t idx = r_beg + (t - (r_end - r_cnt));
                 cid = b.c_id[idx];
                 if (cid != i) {
                     const Sph<double> C = sph_of(b.c_pos[idx]);
@@ -537,7 +553,9 @@ __device__ __forceinline__ int32_t incident_pair(const DevBufs& b, uint32_t i, d
     return -1;
 }
 
-__global__ void __launch_bounds__(kCellWarps * 32) k_cells(DevBufs b, float cell_band, int only_dirty) {
+// 5 resident blocks per SM (48 registers, no spill): the kernel waits on dependent loads
+// (the binary searches), so warps in flight matter more than registers
+__global__ void __launch_bounds__(kCellWarps * 32, 5) k_cells(DevBufs b, float cell_band, int only_dirty) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t n = b.n;
     for (uint32_t i = blockIdx.x * kCellWarps + w; i < n; i += gridDim.x * kCellWarps) {
@@ -929,7 +947,7 @@ void launch_sums3(const double* x0, const uint32_t* cnt0, const double* x1, cons
 int grid_blocks(size_t n, int block, int cap) { return grid_for(n, block, cap); }
 
 GridDev plan_grid(const BBox& bb, double reach, size_t max_slots, uint32_t* ncell, double cell_scale) {
-    double ext[3], cell = reach * (cell_scale > 1.0 ? cell_scale : 1.0);
+    double ext[3], cell = reach * (cell_scale > 0.5 ? cell_scale : 0.5);
     for (int k = 0; k < 3; ++k) ext[k] = (bb.mx[k] - bb.mn[k]) + 2.0 * reach;
     auto dims_for = [&](double c, int* d) {
         for (int k = 0; k < 3; ++k) d[k] = (int)std::floor(ext[k] / c) + 1;
@@ -945,6 +963,8 @@ GridDev plan_grid(const BBox& bb, double reach, size_t max_slots, uint32_t* ncel
     }
     GridDev g;
     g.cell = cell;
+    g.reach = reach;
+    g.half = cell >= reach ? 1 : 2;  // cell >= reach / 2 always
     g.ox = bb.mn[0] - reach;
     g.oy = bb.mn[1] - reach;
     g.oz = bb.mn[2] - reach;

@@ -43,9 +43,13 @@ struct BBox {
     double mn[3], mx[3], max_r;
 };
 
+// Uniform grid: cells of edge `cell` from (ox, oy, oz), dx x dy x dz of them.  reach is an
+// upper bound of R_a + R_c over intersecting balls (2 max R + 0.25), and half = the stencil
+// half-width in cells (cell * half >= reach): 1 for cells of at least the reach, 2 for
+// cells of half of it (a 5 x 5 x 5 stencil, culled to the rows and x-ranges within reach).
 struct GridDev {
-    double ox, oy, oz, cell;
-    int dx, dy, dz;
+    double ox, oy, oz, cell, reach;
+    int dx, dy, dz, half;
 };
 
 struct DevBufs {

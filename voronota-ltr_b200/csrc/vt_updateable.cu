@@ -347,7 +347,7 @@ struct vt_updateable {
         } else {
             VT_CUDA(cudaMemcpyAsync(w(kWSlots), &S.n, 4, cudaMemcpyHostToDevice, stream));
         }
-        grid = plan_grid(bb, reach, nslots_max, &ncell);
+        grid = plan_grid(bb, reach, nslots_max, &ncell, 0.5);  // cells of half the reach, 5^3 stencil
         g.grid = grid;
         cell_count.ensure(ncell);
         cell_start.ensure(ncell + 1);

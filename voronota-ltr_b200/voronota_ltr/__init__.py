@@ -655,7 +655,7 @@ class Engine:
         _check(self._L.vt_engine_get_tuning(self._h, ctypes.byref(w), ctypes.byref(c), ctypes.byref(ch)))
         return {"warps_per_block": w.value, "cell_scale": c.value, "chunk": ch.value}
 
-    def set_tuning(self, warps_per_block: int = 2, cell_scale: float = 1.0, chunk: int = 4):
+    def set_tuning(self, warps_per_block: int = 2, cell_scale: float = 0.5, chunk: int = 4):
         """chunk > 0: persistent contact launch taking `chunk` pairs per grab."""
         _check(self._L.vt_engine_set_tuning(self._h, int(warps_per_block), float(cell_scale), int(chunk)))
 
