@@ -51,6 +51,16 @@ def _stale(target: str, deps: list[str]) -> bool:
 def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
+    # one build at a time: two concurrent builds could link objects compiled against
+    # different versions of the shared headers (struct layouts passed to kernels by value)
+    import fcntl
+
+    with open(os.path.join(BUILD, ".lock"), "w") as lock:
+        fcntl.flock(lock, fcntl.LOCK_EX)
+        return _build_locked(verbose, ptxas_info)
+
+
+def _build_locked(verbose: bool, ptxas_info: bool) -> str:
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
     headers.append(os.path.join(os.path.dirname(HERE), "include", "voronota_b200.h"))
     objs = []

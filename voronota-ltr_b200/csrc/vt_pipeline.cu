@@ -174,13 +174,11 @@ __device__ __forceinline__ bool vless(double va, uint32_t ia, double vb, uint32_
     return ia < ib;
 }
 
-// The count pass waits on candidate loads: 9 resident blocks (56 registers) hide a little
-// more of that latency than the 8 that 64 registers allow.
-// Resident blocks per SM: the count pass at 9 (56 registers); the fill pass at 7, as many as
+// Resident blocks per SM: the count pass at 8 (64 registers, no spill); the fill pass at 7, as many as
 // its 16 KB of sort buffers allow under the default carveout (71 registers, no spill; 95
 // registers and 5 blocks left it latency bound: 0.57 -> 0.47 ms at 100k balls).
 template <bool FILL>
-__global__ void __launch_bounds__(kSearchWarps * 32, FILL ? 7 : 9) k_search(DevBufs b, int want_rel) {
+__global__ void __launch_bounds__(kSearchWarps * 32, FILL ? 7 : 8) k_search(DevBufs b, int want_rel) {
     __shared__ double s_val[kSearchWarps][kSortCap];
     __shared__ uint32_t s_id[kSearchWarps][kSortCap];
     __shared__ uint32_t s_slot[kSearchWarps][kSortCap];
