@@ -82,9 +82,7 @@ template <bool VOL>
 __global__ void __launch_bounds__(kWarps * 32, 4)
     k_adjoint64(DevBufs b, uint32_t P, int from_list, const double* __restrict__ u_contact,
                 const double* __restrict__ w_eff, const double* __restrict__ v_eff, double* __restrict__ grad) {
-    __shared__ uint32_t s_hkey[kWarps][kAdjHash], s_hpos[kWarps][kAdjHash];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    uint32_t hash_of = 0xffffffffu;  // the ball whose list the warp's table holds
     const uint32_t n = b.n;
     const uint32_t count = from_list ? *b.d_redo_count : P;
     for (uint32_t it = blockIdx.x * kWarps + w; it < count; it += gridDim.x * kWarps) {
@@ -129,12 +127,11 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
         const int len = co.len;
         const int nx = len > 0 ? (lane + 1 < len ? lane + 1 : 0) : 0;
         const Pt<double> nxt = shfl_pt(co.q, nx);
-        NbHash nh{s_hkey[w], s_hpos[w], nid, nslot, sph, cnt};
-        if (hash_of != a) {  // consecutive pairs mostly share a
-            nh.build(lane);
-            hash_of = a;
-        }
-        auto sphere_of = [&](uint32_t c) { return nh.find(c); };
+        auto sphere_of = [&](uint32_t c) {
+            for (uint32_t e = 0; e < cnt; ++e)
+                if (nid[e] == c) return sph[nslot[e]];
+            return make_double4(0.0, 0.0, 0.0, 0.0);
+        };
         adjoint_pair<VOL>(G, co.full, len, co.q.p, nxt.p, co.q.ang, co.q.rid, nxt.lid, sphere_of, grad, n);
     }
 }

@@ -182,56 +182,6 @@ __device__ __forceinline__ V3<double> snap_vertex(const AdjPair& G, V3<double> y
     return norm2(y1 - y0) <= norm2(y2 - y0) ? y1 : y2;
 }
 
-// Sphere of a neighbour of `a` by its reference id: a per-warp open-addressing table in
-// shared memory (id -> list position), built by the warp for each pair, replaces a linear
-// scan of the list per lookup (three lookups per contour point: the edge's plane and the
-// two planes that place the vertex).  Lists longer than kAdjHashMax entries (rare: the
-// table must keep empty slots for its probes to end) fall back to the scan.
-constexpr int kAdjHash = 128;  // slots per warp
-constexpr uint32_t kAdjHashMax = 96;
-struct NbHash {
-    uint32_t* key;  // kAdjHash ids (0xffffffff: empty)
-    uint32_t* pos;  // list position of each key
-    const uint32_t* nid;
-    const uint32_t* nslot;
-    const double4* sph;
-    uint32_t cnt;
-    __device__ static uint32_t slot_of(uint32_t id) { return (id * 2654435761u) >> 25; }  // 7 bits
-    // warp-collective: every lane calls it
-    __device__ void build(int lane) {
-        for (int k = lane; k < kAdjHash; k += 32) key[k] = 0xffffffffu;
-        __syncwarp();
-        if (cnt <= kAdjHashMax)
-            for (uint32_t e = lane; e < cnt; e += 32) {
-                const uint32_t id = nid[e];
-                uint32_t h = slot_of(id);
-                for (int probe = 0; probe < kAdjHash; ++probe) {  // ends: the table has empty slots
-                    if (atomicCAS(&key[h], 0xffffffffu, id) == 0xffffffffu) {
-                        pos[h] = e;
-                        break;
-                    }
-                    h = (h + 1) & (kAdjHash - 1);
-                }
-            }
-        __syncwarp();
-    }
-    __device__ double4 find(uint32_t c) const {
-        if (cnt <= kAdjHashMax) {
-            uint32_t h = slot_of(c);
-            for (int probe = 0; probe < kAdjHash; ++probe) {
-                const uint32_t k = key[h];
-                if (k == c) return sph[nslot[pos[h]]];
-                if (k == 0xffffffffu) break;
-                h = (h + 1) & (kAdjHash - 1);
-            }
-            return make_double4(0.0, 0.0, 0.0, 0.0);
-        }
-        for (uint32_t e = 0; e < cnt; ++e)
-            if (nid[e] == c) return sph[nslot[e]];
-        return make_double4(0.0, 0.0, 0.0, 0.0);
-    }
-};
-
 // Weights of pair p's contact: u of its output contact (kept pairs), w and v of both
 // ends (a periodic image's cell is its own ball's, reached through that ball's pairs);
 // v_eff null: no volume term.

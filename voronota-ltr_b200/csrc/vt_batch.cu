@@ -115,14 +115,12 @@ __global__ void k_batch_cell_hist(const double4* __restrict__ sph, uint32_t N, c
 __global__ void k_batch_cell_scatter(const double4* __restrict__ sph, uint32_t N, const uint32_t* __restrict__ bs,
                                      const GridDev* __restrict__ grids, const uint32_t* __restrict__ base,
                                      uint32_t* __restrict__ cursor, double4* __restrict__ c_pos,
-                                     uint32_t* __restrict__ c_id, uint32_t* __restrict__ c_slot,
-                                     float4* __restrict__ c_pos32) {
+                                     uint32_t* __restrict__ c_id, uint32_t* __restrict__ c_slot) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         const uint32_t s = bs[i];
         const double4 p = sph[i];
         const uint32_t at = atomicAdd(&cursor[base[s] + slot_cell(grids[s], p)], 1u);
         c_pos[at] = p;
-        if (c_pos32) c_pos32[at] = make_float4((float)p.x, (float)p.y, (float)p.z, (float)p.w);
         c_id[at] = i;
         c_slot[at] = i;
     }
@@ -224,7 +222,7 @@ void launch_batch_grid(const DevBufs& b, uint32_t N, uint32_t total_cells, uint3
     scan_u32(b.cell_count, b.cell_start, total_cells, scan_tmp, s);
     cudaMemcpyAsync(b.cell_cursor, b.cell_start, sizeof(uint32_t) * total_cells, cudaMemcpyDeviceToDevice, s);
     k_batch_cell_scatter<<<gb(N), kBlock, 0, s>>>(b.sph, N, b.ball_struct, b.grids, b.cell_base, b.cell_cursor,
-                                                  b.c_pos, b.c_id, b.c_slot, b.c_pos32);
+                                                  b.c_pos, b.c_id, b.c_slot);
     count_launch();
 }
 void launch_batch_small_unsure(const DevBufs& b, const uint32_t* off, uint32_t P, uint64_t min_pairs,

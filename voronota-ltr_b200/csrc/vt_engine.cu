@@ -112,7 +112,6 @@ struct vt_engine {
     DBuf<double> xyzr;
     DBuf<int32_t> groups;
     DBuf<double4> sph, c_pos;
-    DBuf<float4> c_pos32;
     DBuf<uint32_t> slot_id, c_id, c_slot, cell_count, cell_start, cell_cursor;
     DBuf<uint32_t> nb_cnt, nb_npair, nb_off, pair_off, nb_id, nb_slot;
     DBuf<uint8_t> excluded;
@@ -424,7 +423,6 @@ struct vt_engine {
         groups.release();
         sph.release();
         c_pos.release();
-        c_pos32.release();
         excluded.release();
         nb_pair.release();
         nb_rel.release();
@@ -574,12 +572,10 @@ struct vt_engine {
         c_pos.ensure(max_slots);
         c_id.ensure(max_slots);
         c_slot.ensure(max_slots);
-        if (precision == VT_FP32_FIXUP) c_pos32.ensure(max_slots);
         b.cell_count = cell_count.p;
         b.cell_start = cell_start.p;
         b.cell_cursor = cell_cursor.p;
         b.c_pos = c_pos.p;
-        b.c_pos32 = precision == VT_FP32_FIXUP ? c_pos32.p : nullptr;
         b.c_id = c_id.p;
         b.c_slot = c_slot.p;
         ensure_scan(std::max<size_t>(ncell, n) + 1);

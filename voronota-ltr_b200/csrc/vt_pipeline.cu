@@ -150,13 +150,12 @@ __global__ void k_cell_hist(const double4* __restrict__ sph, const uint32_t* __r
 __global__ void k_cell_scatter(const double4* __restrict__ sph, const uint32_t* __restrict__ slot_id,
                                const uint32_t* __restrict__ d_nslots, GridDev g, uint32_t* __restrict__ cursor,
                                double4* __restrict__ c_pos, uint32_t* __restrict__ c_id, uint32_t* __restrict__ c_slot,
-                               int slot_is_id, float4* __restrict__ c_pos32) {
+                               int slot_is_id) {
     uint32_t ns = *d_nslots;
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < ns; s += gridDim.x * blockDim.x) {
         double4 p = sph[s];
         uint32_t at = atomicAdd(&cursor[slot_cell(g, p)], 1u);
         c_pos[at] = p;
-        if (c_pos32) c_pos32[at] = make_float4((float)p.x, (float)p.y, (float)p.z, (float)p.w);
         c_id[at] = slot_id[s];
         c_slot[at] = slot_is_id ? slot_id[s] : s;
     }
@@ -174,11 +173,13 @@ __device__ __forceinline__ bool vless(double va, uint32_t ia, double vb, uint32_
     return ia < ib;
 }
 
-// Resident blocks per SM: the count pass at 8 (64 registers, no spill); the fill pass at 7, as many as
+// The count pass waits on candidate loads: 9 resident blocks (56 registers) hide a little
+// more of that latency than the 8 that 64 registers allow.
+// Resident blocks per SM: the count pass at 9 (56 registers); the fill pass at 7, as many as
 // its 16 KB of sort buffers allow under the default carveout (71 registers, no spill; 95
 // registers and 5 blocks left it latency bound: 0.57 -> 0.47 ms at 100k balls).
 template <bool FILL>
-__global__ void __launch_bounds__(kSearchWarps * 32, FILL ? 7 : 8) k_search(DevBufs b, int want_rel) {
+__global__ void __launch_bounds__(kSearchWarps * 32, FILL ? 7 : 9) k_search(DevBufs b, int want_rel) {
     __shared__ double s_val[kSearchWarps][kSortCap];
     __shared__ uint32_t s_id[kSearchWarps][kSortCap];
     __shared__ uint32_t s_slot[kSearchWarps][kSortCap];
@@ -197,12 +198,6 @@ __global__ void __launch_bounds__(kSearchWarps * 32, FILL ? 7 : 8) k_search(DevB
         }
         const double4 A4 = b.sph[i];
         const Sph<double> A = sph_of(A4);
-        // float prefilter (c_pos32): a candidate whose float distance exceeds the float
-        // R_a + R_c by the margin m is out of reach in double as well (coordinates rounded
-        // to float move by at most 6e-8 of their magnitude, |c| <= |a| + 2 reach inside the
-        // stencil, and m allows 30 times that); every other candidate takes the FP64 tests
-        const float4 A32 = make_float4((float)A4.x, (float)A4.y, (float)A4.z, (float)A4.w);
-        const float m32 = 4e-6f * (fmaxf(fmaxf(fabsf(A32.x), fabsf(A32.y)), fabsf(A32.z)) + 2.f * (float)g.reach) + 1e-6f;
         int cx = cell_coord(A4.x, g.ox, g.cell, g.dx), cy = cell_coord(A4.y, g.oy, g.cell, g.dy),
             cz = cell_coord(A4.z, g.oz, g.cell, g.dz);
         // stencil rows (y, z) of up to 2 half + 1 cells in x, one per lane; a row whose y and
@@ -262,14 +257,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32, FILL ? 7 : 8) k_search(DevB
             if (t < total) {
                 uint32_t idx = r_beg + (t - (r_end - r_cnt));
                 cid = b.c_id[idx];
-                bool near = cid != i;
-                if (near && b.c_pos32) {
-                    const float4 c = b.c_pos32[idx];
-                    const float dx = c.x - A32.x, dy = c.y - A32.y, dz = c.z - A32.z;
-                    const float S = A32.w + c.w + m32;
-                    near = dx * dx + dy * dy + dz * dz <= S * S;
-                }
-                if (near) {
+                if (cid != i) {
                     const Sph<double> C = sph_of(b.c_pos[idx]);
                     if (sphere_intersects(d, A, C, 0.0)) {
                         // hidden central ball (spheres_searcher.rs:295-303)
@@ -899,7 +887,7 @@ void launch_grid(const DevBufs& b, uint32_t ncell, uint32_t max_slots, uint32_t*
     scan_u32(b.cell_count, b.cell_start, ncell, scan_tmp, s);
     cudaMemcpyAsync(b.cell_cursor, b.cell_start, sizeof(uint32_t) * ncell, cudaMemcpyDeviceToDevice, s);
     k_cell_scatter<<<gb, kBlock, 0, s>>>(b.sph, b.slot_id, b.d_nslots, b.grid, b.cell_cursor, b.c_pos, b.c_id,
-                                         b.c_slot, b.slot_is_id, b.c_pos32); count_launch();
+                                         b.c_slot, b.slot_is_id); count_launch();
 }
 void launch_search_count(const DevBufs& b, cudaStream_t s) {
     cudaMemsetAsync(b.d_big_count, 0, sizeof(uint32_t), s);

@@ -68,9 +68,6 @@ struct DevBufs {
     uint32_t* cell_start;
     uint32_t* cell_cursor;
     double4* c_pos;
-    // optional (FP32+fixup calls): float copy of c_pos; the search then rejects the
-    // candidates that are clearly out of reach in float and loads c_pos only for the rest
-    float4* c_pos32;
     uint32_t* c_id;
     uint32_t* c_slot;
     // CSR

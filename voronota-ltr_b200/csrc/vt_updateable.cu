@@ -196,7 +196,6 @@ struct vt_updateable {
 
     // workspace
     DBuf<double4> sph, gsph, c_pos, changed_ball;
-    DBuf<float4> c_pos32;  // FP32 handles: the search's float prefilter
     DBuf<uint32_t> slot_id, gslot_id, cell_count, cell_start, cell_cursor, c_id, c_slot;
     DBuf<BBox> bbox_parts, bbox;
     DBuf<uint32_t> img_cnt, img_off, scan_tmp, words, big_rows;
@@ -354,14 +353,12 @@ struct vt_updateable {
         cell_start.ensure(ncell + 1);
         cell_cursor.ensure(ncell);
         c_pos.ensure(nslots_max);
-        if (fp32) c_pos32.ensure(nslots_max);
         c_id.ensure(nslots_max);
         c_slot.ensure(nslots_max);
         g.cell_count = cell_count.p;
         g.cell_start = cell_start.p;
         g.cell_cursor = cell_cursor.p;
         g.c_pos = c_pos.p;
-        g.c_pos32 = fp32 ? c_pos32.p : nullptr;
         g.c_id = c_id.p;
         g.c_slot = c_slot.p;
         ensure_scan(std::max<size_t>(ncell, n) + 1);
@@ -383,7 +380,6 @@ struct vt_updateable {
         b.cell_start = cell_start.p;
         b.cell_cursor = cell_cursor.p;
         b.c_pos = c_pos.p;
-        b.c_pos32 = fp32 ? c_pos32.p : nullptr;
         b.c_id = c_id.p;
         b.c_slot = c_slot.p;
         b.excluded = S.excl.p;
