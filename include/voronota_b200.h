@@ -208,8 +208,9 @@ int vt_engine_device_outputs(const vt_engine* e, vt_device_outputs* out);
  * contact's contour and differentiates the final region analytically (boundary
  * velocities of its edges and arcs; the pyramid volumes through the radical planes'
  * distances); it does not store contours.  Balls of periodic images accumulate into the
- * ball they image; the box is fixed.  A contact whose contour needed more than 32 points
- * is not differentiated (VT_ERR_CAPACITY). */
+ * ball they image; the box is fixed.  Contours of more than 32 points (beyond a warp) are
+ * differentiated by a serial kernel; a contour beyond its 256 points is not
+ * (VT_ERR_CAPACITY). */
 /* After vt_engine_compute_device/_host (full tessellation, one structure): device arrays
  * d_w_sas and d_v_volume (n doubles each) and d_u_contact (one per contact) may each be
  * NULL (no such term); d_grad: n x 4 doubles, overwritten. */

@@ -137,6 +137,27 @@ def test_volume_adjoint_256_coordinates_vs_oracle():
         _check_fd_local(g[i, c], balls, i, c, w, v, upair)
 
 
+@pytest.mark.parametrize("k, rr, rho, probe", [(40, 0.1, 3.3, 0.1), (48, 1.0, 3.6, 0.5)])
+def test_adjoint_of_contours_beyond_a_warp(k, rr, rho, probe):
+    """A contact cut by k small balls on a ring (contours of 40 to 96 points, more than a
+    warp holds): the serial adjoint against central differences of the GPU forward and of
+    the oracle, for the SAS, area and volume terms (the ring jittered so that no step of
+    the differences meets a symmetric degeneracy)."""
+    from common import sunflower
+
+    balls = sunflower(k, rr=rr, rho=rho)
+    rng = np.random.default_rng(k)
+    balls[2:, :3] += rng.uniform(-0.03, 0.03, (k, 3))
+    w, u, upair = _weights(balls, probe, 50 + k)
+    v = _vweights(len(balls), 60 + k)
+    g = V.grad(balls, probe, w, u, precision="fp64", v_volume=v)
+    coords = [(0, 0), (0, 1), (0, 3), (1, 0), (1, 2), (1, 3)] + _coords(len(balls), 6, 70 + k)
+    for i, c in coords:
+        _check_fd(g[i, c], lambda b: _loss_gpu(b, probe, w, upair, v=v), balls, i, c)
+    for i, c in coords[:6]:
+        _check_fd(g[i, c], lambda b: _loss_oracle(b, probe, w, upair, v=v), balls, i, c)
+
+
 def test_separate_terms_and_fp32_forward():
     balls = W.lattice_balls(1200, 23)
     w, u, upair = _weights(balls, 1.4, 5)

@@ -111,8 +111,8 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
         };
         ContourOut<double> co;
         WarpContact r = contact_warp<double, false, false>(g, (int)cnt, (int)(eb - off), nbf, &co);
-        if (!r.valid) {
-            if (lane == 0 && r.overflow) atomicOr(b.err, kErrAdjoint);
+        if (!r.valid) {  // a contour beyond the warp's 32 points goes to the serial adjoint
+            if (lane == 0 && r.overflow) b.serial_list[atomicAdd(b.d_serial_count, 1u)] = p;
             continue;
         }
         G.pa = g.A.c;
@@ -163,6 +163,7 @@ void launch_adjoint(const DevBufs& b, uint32_t P, const double* w_sas, const dou
     const uint32_t n = b.n;
     double* ve = v_vol ? v_eff : nullptr;
     cudaMemsetAsync(grad, 0, 4 * sizeof(double) * n, s);
+    cudaMemsetAsync(b.d_serial_count, 0, sizeof(uint32_t), s);
     k_w_eff<<<gb(n), 256, 0, s>>>(n, w_sas, v_vol, b.cell_flag, b.cell_sas, b.sph, w_eff, ve); count_launch();
     if (P) {
         if (b.nb_rel) {
@@ -174,6 +175,7 @@ void launch_adjoint(const DevBufs& b, uint32_t P, const double* w_sas, const dou
             launch_adjoint64(b, P, 0, u_contact, w_eff, ve, grad, s);
         }
         count_launch();
+        launch_adjoint_serial(b, u_contact, w_eff, ve, grad, s);
     }
     k_sas_scale<<<gb(n), 256, 0, s>>>(n, w_eff, ve, b.cell_sas, b.sph, grad); count_launch();
 }

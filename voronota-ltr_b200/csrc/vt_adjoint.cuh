@@ -36,59 +36,116 @@ struct AdjPair {
     double area;       // the forward's area of the contact
 };
 
+// The pair's area weight with the pyramid volumes t_ab A / 3 and t_ba A / 3 folded in
+// (t_ab = (D^2 + Ra^2 - Rb^2) / (2 D): signed distance from p_a to the radical plane).
+template <bool VOL>
+__device__ __forceinline__ double adj_area_weight(const AdjPair& G) {
+    double u = G.u;
+    if constexpr (VOL) {
+        const V3<double> dab = G.pb - G.pa;
+        const double D = sqrt(dot(dab, dab));
+        const double t_ab = 0.5 * D + (G.Ra * G.Ra - G.Rb * G.Rb) / (2.0 * D), t_ba = D - t_ab;
+        u += (G.va * t_ab + G.vb * t_ba) / 3.0;
+    }
+    return u;
+}
+
+// One contour point's share: point P, the next point Pn, the arc angle of its segment,
+// its rid and the next point's lid.  An arc adds its length and first moment to (Lk, Xk);
+// a straight edge (on the radical plane of a and c = rid) adds the area weight u times its
+// boundary velocity to the gradients of a and b (ga, gra, gb, grb) and of c (directly).
+template <typename SphereOf>
+__device__ __forceinline__ void adj_point(const AdjPair& G, double u, V3<double> P, V3<double> Pn, double ang,
+                                          uint32_t rid, uint32_t nlid, SphereOf sphere_of, double* grad, uint32_t n,
+                                          V3<double>& ga, double& gra, V3<double>& gb, double& grb, double& Lk,
+                                          V3<double>& Xk) {
+    const V3<double> pa = G.pa, pb = G.pb, q = G.q;
+    if (rid == G.a && nlid == G.a) {
+        if (ang > 0.0) {
+            const V3<double> e1 = normalize(P - q);
+            const double h = 0.5 * ang;
+            const V3<double> mm = e1 * cos(h) + cross(G.axis, e1) * sin(h);
+            const double l = G.rho * ang;
+            Lk += l;
+            Xk = Xk + q * l + mm * (2.0 * G.rho * G.rho * sin(h));
+        }
+    } else if (u != 0.0) {
+        const double4 C = sphere_of(rid);
+        if (C.w > 0.0) {
+            const V3<double> dab = pb - pa;
+            const double D2 = dot(dab, dab);
+            const V3<double> pc = mk<double>(C.x, C.y, C.z);
+            const V3<double> dac = pc - pa;
+            const double kap = dot(dac, dab) / D2;
+            const V3<double> perp = (dac - dab * kap) * 2.0;
+            const double lam = 1.0 / norm(perp);
+            const V3<double> xm = (P + Pn) * 0.5;
+            const double coef = u * norm(Pn - P) * lam;
+            adj_add_grad(grad, rid, n, (xm - pc) * (-2.0 * coef), -2.0 * C.w * coef);
+            ga = ga + (xm - pa) * (2.0 * coef * (1.0 - kap));
+            gra += 2.0 * G.Ra * coef * (1.0 - kap);
+            gb = gb + (xm - pb) * (2.0 * coef * kap);
+            grb += 2.0 * G.Rb * coef * kap;
+        }
+    }
+}
+
+// The pair's terms through its arcs (total length L, first moment X) and pyramids, added
+// to the edge terms (ga, gra, gb, grb) and accumulated into a's and b's gradients.
+template <bool VOL>
+__device__ __forceinline__ void adj_finish(const AdjPair& G, double u, double L, V3<double> X, V3<double> ga,
+                                           double gra, V3<double> gb, double grb, double* grad, uint32_t n) {
+    const V3<double> pa = G.pa, pb = G.pb, q = G.q;
+    const double Ra = G.Ra, Rb = G.Rb, rho = G.rho, wa = G.wa, wb = G.wb;
+    const V3<double> dab = pb - pa;
+    const double D2 = dot(dab, dab), D = sqrt(D2);
+    if (L > 0.0 && rho > 0.0) {
+        const double kG = dot(q - pa, dab) / D2;
+        const V3<double> Xa = X - pa * L, Xb = X - pb * L;
+        // area through the arcs
+        ga = ga + Xa * (u * (1.0 - kG) / rho);
+        gra += u * (1.0 - kG) * Ra * L / rho;
+        gb = gb + Xb * (u * kG / rho);
+        grb += u * kG * Rb * L / rho;
+        // SAS of a and of b through the same arcs
+        const double s = 1.0 / (D * rho);
+        const double cmix = (Ra * Ra + Rb * Rb - D2) * 0.5;
+        ga = ga + Xb * (wa * Ra * s) - Xa * (wb * Rb * s);
+        gb = gb - Xb * (wa * Ra * s) + Xa * (wb * Rb * s);
+        gra += wa * L * cmix * s - wb * Rb * Ra * L * s;
+        grb += wb * L * cmix * s - wa * Ra * Rb * L * s;
+    }
+    if (VOL && (G.va != 0.0 || G.vb != 0.0)) {
+        // pyramid volumes through t_ab and t_ba at fixed area:
+        // dt_ab/dD = 1/2 - dRR/(2 D^2), dt_ab/dRa = Ra/D, dt_ab/dRb = -Rb/D, t_ba = D - t_ab
+        const double c = G.area / 3.0;
+        const double k = (Ra * Ra - Rb * Rb) / (2.0 * D2);
+        const double gD = c * (G.va * (0.5 - k) + G.vb * (0.5 + k));
+        const V3<double> nh = dab / D;
+        ga = ga - nh * gD;
+        gb = gb + nh * gD;
+        gra += c * (G.va - G.vb) * Ra / D;
+        grb += c * (G.vb - G.va) * Rb / D;
+    }
+    adj_add_grad(grad, G.a, n, ga, gra);
+    adj_add_grad(grad, G.bid, n, gb, grb);
+}
+
 // Warp-collective: every lane calls it.  VOL: the pair carries volume weights (va, vb,
-// area); without them the pyramid terms are compiled out.  Lane k < len holds contour point P (absolute),
-// the next point Pn, the arc angle of its segment, its rid and the next point's lid;
-// full: no cut (the whole circle).  sphere_of(id) returns the double sphere of a's
-// neighbour with that reference id (w = 0 if not found).
+// area); without them the pyramid terms are compiled out.  Lane k < len holds contour
+// point P (absolute), the next point Pn, the arc angle of its segment, its rid and the
+// next point's lid; full: no cut (the whole circle).  sphere_of(id) returns the double
+// sphere of a's neighbour with that reference id (w = 0 if not found).
 template <bool VOL, typename SphereOf>
 __device__ __forceinline__ void adjoint_pair(const AdjPair& G, bool full, int len, V3<double> P, V3<double> Pn,
                                              double ang, uint32_t rid, uint32_t nlid, SphereOf sphere_of,
                                              double* grad, uint32_t n) {
     const int lane = threadIdx.x & 31;
-    const V3<double> pa = G.pa, pb = G.pb, q = G.q;
-    const double Ra = G.Ra, Rb = G.Rb, rho = G.rho, wa = G.wa, wb = G.wb;
-    const V3<double> dab = pb - pa;
-    const double D2 = dot(dab, dab), D = sqrt(D2);
-    // the pyramid volumes t_ab A / 3 and t_ba A / 3 weigh the area like u does
-    // (t_ab = (D^2 + Ra^2 - Rb^2) / (2 D): signed distance from p_a to the radical plane)
-    const double dRR = Ra * Ra - Rb * Rb;
-    double u = G.u;
-    if constexpr (VOL) {
-        const double t_ab = 0.5 * D + dRR / (2.0 * D), t_ba = D - t_ab;
-        u += (G.va * t_ab + G.vb * t_ba) / 3.0;
-    }
+    const double u = adj_area_weight<VOL>(G);
     V3<double> ga = mk<double>(0, 0, 0), gb = mk<double>(0, 0, 0);
     double gra = 0.0, grb = 0.0, Lk = 0.0;
     V3<double> Xk = mk<double>(0, 0, 0);
-    if (!full && lane < len) {
-        if (rid == G.a && nlid == G.a) {
-            if (ang > 0.0) {
-                const V3<double> e1 = normalize(P - q);
-                const double h = 0.5 * ang;
-                const V3<double> mm = e1 * cos(h) + cross(G.axis, e1) * sin(h);
-                Lk = rho * ang;
-                Xk = q * Lk + mm * (2.0 * rho * rho * sin(h));
-            }
-        } else if (u != 0.0) {
-            // straight edge on the radical plane of a and c = rid
-            const double4 C = sphere_of(rid);
-            if (C.w > 0.0) {
-                const V3<double> pc = mk<double>(C.x, C.y, C.z);
-                const V3<double> dac = pc - pa;
-                const double kap = dot(dac, dab) / D2;
-                const V3<double> perp = (dac - dab * kap) * 2.0;
-                const double lam = 1.0 / norm(perp);
-                const V3<double> xm = (P + Pn) * 0.5;
-                const double coef = u * norm(Pn - P) * lam;
-                adj_add_grad(grad, rid, n, (xm - pc) * (-2.0 * coef), -2.0 * C.w * coef);
-                ga = (xm - pa) * (2.0 * coef * (1.0 - kap));
-                gra = 2.0 * Ra * coef * (1.0 - kap);
-                gb = (xm - pb) * (2.0 * coef * kap);
-                grb = 2.0 * Rb * coef * kap;
-            }
-        }
-    }
+    if (!full && lane < len) adj_point(G, u, P, Pn, ang, rid, nlid, sphere_of, grad, n, ga, gra, gb, grb, Lk, Xk);
     double L = adj_wsum(Lk);
     V3<double> X = adj_wsum3(Xk);
     ga = adj_wsum3(ga);
@@ -96,41 +153,10 @@ __device__ __forceinline__ void adjoint_pair(const AdjPair& G, bool full, int le
     gra = adj_wsum(gra);
     grb = adj_wsum(grb);
     if (full) {
-        L = 2.0 * kPi * rho;
-        X = q * L;
+        L = 2.0 * kPi * G.rho;
+        X = G.q * L;
     }
-    if (lane == 0) {
-        if (L > 0.0 && rho > 0.0) {
-            const double kG = dot(q - pa, dab) / D2;
-            const V3<double> Xa = X - pa * L, Xb = X - pb * L;
-            // area through the arcs
-            ga = ga + Xa * (u * (1.0 - kG) / rho);
-            gra += u * (1.0 - kG) * Ra * L / rho;
-            gb = gb + Xb * (u * kG / rho);
-            grb += u * kG * Rb * L / rho;
-            // SAS of a and of b through the same arcs
-            const double s = 1.0 / (D * rho);
-            const double cmix = (Ra * Ra + Rb * Rb - D2) * 0.5;
-            ga = ga + Xb * (wa * Ra * s) - Xa * (wb * Rb * s);
-            gb = gb - Xb * (wa * Ra * s) + Xa * (wb * Rb * s);
-            gra += wa * L * cmix * s - wb * Rb * Ra * L * s;
-            grb += wb * L * cmix * s - wa * Ra * Rb * L * s;
-        }
-        if (VOL && (G.va != 0.0 || G.vb != 0.0)) {
-            // pyramid volumes through t_ab and t_ba at fixed area:
-            // dt_ab/dD = 1/2 - dRR/(2 D^2), dt_ab/dRa = Ra/D, dt_ab/dRb = -Rb/D, t_ba = D - t_ab
-            const double c = G.area / 3.0;
-            const double k = dRR / (2.0 * D2);
-            const double gD = c * (G.va * (0.5 - k) + G.vb * (0.5 + k));
-            const V3<double> nh = dab / D;
-            ga = ga - nh * gD;
-            gb = gb + nh * gD;
-            gra += c * (G.va - G.vb) * Ra / D;
-            grb += c * (G.vb - G.va) * Rb / D;
-        }
-        adj_add_grad(grad, G.a, n, ga, gra);
-        adj_add_grad(grad, G.bid, n, gb, grb);
-    }
+    if (lane == 0) adj_finish<VOL>(G, u, L, X, ga, gra, gb, grb, grad, n);
 }
 
 // FP64 position of an FP32 contour vertex from the planes that define it: the radical

@@ -5,6 +5,7 @@
 //                    contour lives in a per-thread slice of a global scratch buffer.
 #include <cmath>
 
+#include "vt_adjoint.cuh"
 #include "vt_contact.cuh"
 #include "vt_pipeline.cuh"
 
@@ -475,7 +476,83 @@ __global__ void k_net_serial(DevBufs b, const uint32_t* __restrict__ voff, NetSl
     }
 }
 
+// Adjoint of the pairs whose contour outgrew a warp (listed by the FP64 adjoint in
+// serial_list): the serial contour, then the same per-point and per-pair terms as the warp
+// adjoint (vt_adjoint.cuh), summed in contour order by one thread.
+template <bool VOL>
+__global__ void k_adjoint_serial(DevBufs b, const double* __restrict__ u_contact, const double* __restrict__ w_eff,
+                                 const double* __restrict__ v_eff, double* __restrict__ grad) {
+    const uint32_t count = *b.d_serial_count;
+    const uint32_t n = b.n;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+        const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+        if (slot >= b.serial_slots) break;
+        const uint32_t p = b.serial_list[t];
+        const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
+        const uint32_t bid = b.nb_id[eb];
+        AdjPair G;
+        if (!adjoint_weights(b, p, a, bid, u_contact, w_eff, v_eff, G)) continue;
+        Contour c;
+        c.v = reinterpret_cast<SP*>(b.serial_scratch) + (size_t)slot * kSerialCap;
+        c.n = 0;
+        c.cap = kSerialCap;
+        c.overflow = false;
+        Sph<double> ic;
+        V3<double> axis, bary;
+        double sum_arc, area;
+        const bool ok = serial_clip(b, p, c, ic, axis, bary, sum_arc, area);
+        if (!ok || c.overflow) {
+            if (c.overflow) atomicOr(b.err, kErrAdjoint);
+            continue;
+        }
+        const Sph<double> A = sph_of(b.sph[a]), B = sph_of(b.sph[b.nb_slot[eb]]);
+        G.pa = A.c;
+        G.pb = B.c;
+        G.Ra = A.r;
+        G.Rb = B.r;
+        G.q = ic.c;
+        G.rho = ic.r;
+        G.axis = axis;
+        G.a = a;
+        G.bid = bid;
+        const uint32_t off = b.nb_off[a], cnt = b.nb_cnt[a];
+        const uint32_t* nid = b.nb_id + off;
+        const uint32_t* nslot = b.nb_slot + off;
+        const double4* sph = b.sph;
+        auto sphere_of = [&](uint32_t cid) {
+            for (uint32_t e = 0; e < cnt; ++e)
+                if (nid[e] == cid) return sph[nslot[e]];
+            return make_double4(0.0, 0.0, 0.0, 0.0);
+        };
+        const double u = adj_area_weight<VOL>(G);
+        V3<double> ga = mk<double>(0, 0, 0), gb = mk<double>(0, 0, 0), X = mk<double>(0, 0, 0);
+        double gra = 0.0, grb = 0.0, L = 0.0;
+        if (c.n == 0) {
+            L = 2.0 * kPi * G.rho;
+            X = G.q * L;
+        } else {
+            for (int k = 0; k < c.n; ++k) {
+                const SP& cp = c.v[k];
+                const SP& nx = c.v[k + 1 < c.n ? k + 1 : 0];
+                adj_point(G, u, P3(cp), P3(nx), cp.ang, cp.rid, nx.lid, sphere_of, grad, n, ga, gra, gb, grb, L, X);
+            }
+        }
+        adj_finish<VOL>(G, u, L, X, ga, gra, gb, grb, grad, n);
+    }
+}
+
 }  // namespace
+
+void launch_adjoint_serial(const DevBufs& b, const double* u_contact, const double* w_eff, const double* v_eff,
+                           double* grad, cudaStream_t s) {
+    const unsigned threads = 128;
+    const unsigned blocks = (b.serial_slots + threads - 1) / threads;
+    if (v_eff)
+        k_adjoint_serial<true><<<blocks, threads, 0, s>>>(b, u_contact, w_eff, v_eff, grad);
+    else
+        k_adjoint_serial<false><<<blocks, threads, 0, s>>>(b, u_contact, w_eff, v_eff, grad);
+    count_launch();
+}
 
 void launch_net_serial(const DevBufs& b, const uint32_t* voff, NetSlots sl, cudaStream_t s) {
     unsigned threads = 128;

@@ -946,7 +946,7 @@ struct vt_engine {
         sync();
         VT_CUDA(cudaGetLastError());
         if (h_words[13] & 32u) {
-            g_last_error = "a contact whose contour has more than 32 points is not differentiated";
+            g_last_error = "a contact whose contour has more than 256 points is not differentiated";
             return VT_ERR_CAPACITY;
         }
         return VT_OK;

@@ -266,6 +266,10 @@ void launch_adjoint(const DevBufs& b, uint32_t P, const double* w_sas, const dou
                     double* w_eff, double* v_eff, double* grad, cudaStream_t s);
 // FP32 adjoint over all valid pairs (vt_contact32.cu); lists the pairs it cannot decide
 // in redo_list for the FP64 adjoint.  v_eff may be null (no volume term).
+// Adjoint of the pairs the FP64 adjoint listed in serial_list (contours beyond a warp),
+// with the serial contour (vt_contact64.cu).
+void launch_adjoint_serial(const DevBufs& b, const double* u_contact, const double* w_eff, const double* v_eff,
+                           double* grad, cudaStream_t s);
 void launch_adjoint_f32(const DevBufs& b, uint32_t P, const double* u_contact, const double* w_eff,
                         const double* v_eff, double* grad, cudaStream_t s);
 
