@@ -177,7 +177,10 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
 // angles are FP64 values.  A pair whose FP32 contour is unsure, overflows, merged two
 // points (the kept point's ids no longer define it), or has a vertex the snap cannot
 // place is listed for the FP64 element kernel instead.
-__global__ void __launch_bounds__(kWarps * 32, 4)
+#ifndef VT_NET32_MINB
+#define VT_NET32_MINB 4
+#endif
+__global__ void __launch_bounds__(kWarps * 32, VT_NET32_MINB)
     k_net_elements32(DevBufs b, uint32_t P, float band, const uint32_t* __restrict__ voff, NetSlots sl,
                      uint32_t* __restrict__ fp64_list, uint32_t* __restrict__ fp64_count) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;

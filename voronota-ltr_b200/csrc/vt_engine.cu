@@ -187,7 +187,8 @@ struct vt_engine {
         const size_t tb = net_sort_temp_bytes(m);
         net_temp.ensure(tb);
         NetSortBufs t{net_ka.p, net_kb.p, net_hs.p, net_ls.p, net_ia.p, net_ib.p, net_order.p, net_temp.p, tb};
-        net_sort(m, net_hi.p, net_lo.p, t, stream);
+        const int B = net_key_bits(bufs.n);
+        net_sort(m, net_hi.p, net_lo.p, 2 * B, vertices ? 2 * B : B, t, stream);
         net_uflags.ensure(m + 1);
         net_uoff.ensure(m + 2);
         launch_net_unique(m, t, net_uflags.p, stream);
@@ -274,11 +275,11 @@ struct vt_engine {
         net_lo.ensure(mmax);
         net_src.ensure(mmax);
         if (Mv) {
-            launch_net_keys(V, net_vcnt.p, net_off_v.p, sl, 1, net_hi.p, net_lo.p, net_src.p, stream);
+            launch_net_keys(V, net_vcnt.p, net_off_v.p, sl, 1, b.n, net_hi.p, net_lo.p, net_src.p, stream);
             net_nv = net_unique(Mv, 1);
         }
         if (Me) {
-            launch_net_keys(V, net_ecnt.p, net_off_e.p, sl, 0, net_hi.p, net_lo.p, net_src.p, stream);
+            launch_net_keys(V, net_ecnt.p, net_off_e.p, sl, 0, b.n, net_hi.p, net_lo.p, net_src.p, stream);
             net_ne = net_unique(Me, 0);
         }
         return VT_OK;

@@ -8,10 +8,11 @@
 //      right id with a's id as NULL), position; an uncut contact emits one SAS edge; a
 //      contour that outgrows the warp is listed for the serial kernel (vt_contact64.cu);
 //   2. ids are taken mod n for periodic images and sorted within the element;
-//   3. elements are compacted, stably sorted by their ids (radix sort on two 64-bit key
-//      words, low word first) and deduplicated keeping the first of equal ids, i.e. the
-//      first in pair and contour order (the reference sorts unstably and keeps an
-//      unspecified one).
+//   3. elements are compacted, stably sorted by their ids (radix sort on two key words,
+//      low word first; an id takes B = bits(n) bits with NULL mapped to n, so it still
+//      sorts after every ball id, and a word holds two ids: 2B bits instead of 64) and
+//      deduplicated keeping the first of equal ids, i.e. the first in pair and contour
+//      order (the reference sorts unstably and keeps an unspecified one).
 #include <cub/cub.cuh>
 
 #include "vt_contact.cuh"
@@ -108,17 +109,21 @@ __global__ void __launch_bounds__(kWarps * 32)
     }
 }
 
-// dense arrays: key words (hi, lo) and the element's index
+// dense arrays: key words (hi, lo) and the element's index; thread per pair.  An id
+// takes B bits, NULL (0xffffffff) becoming n, above every ball id.
+__device__ __forceinline__ unsigned long long net_key_id(uint32_t id, uint32_t n) {
+    return id == kNetNull ? (unsigned long long)n : (unsigned long long)id;
+}
 __global__ void k_net_compact(uint32_t V, const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ off,
-                              NetSlots sl, int vertices, unsigned long long* __restrict__ key_hi,
+                              NetSlots sl, int vertices, uint32_t n, int B, unsigned long long* __restrict__ key_hi,
                               unsigned long long* __restrict__ key_lo, uint32_t* __restrict__ src) {
-    for (uint32_t v = blockIdx.x; v < V; v += gridDim.x) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
         const uint32_t c = cnt[v], o = off[v], base = sl.base[v];
-        for (uint32_t k = threadIdx.x; k < c; k += blockDim.x) {
+        for (uint32_t k = 0; k < c; ++k) {
             const uint32_t i = base + k;
             const uint4 id = vertices ? net_vid(sl, i) : net_eid(sl, i);
-            key_hi[o + k] = ((unsigned long long)id.x << 32) | id.y;
-            key_lo[o + k] = vertices ? (((unsigned long long)id.z << 32) | id.w) : (unsigned long long)id.z;
+            key_hi[o + k] = (net_key_id(id.x, n) << B) | net_key_id(id.y, n);
+            key_lo[o + k] = vertices ? ((net_key_id(id.z, n) << B) | net_key_id(id.w, n)) : net_key_id(id.z, n);
             src[o + k] = i;
         }
     }
@@ -177,10 +182,16 @@ void set_hex_table_network() {
     cudaMemcpyToSymbol(c_hex_n, &n, sizeof(int));
 }
 
+int net_key_bits(uint32_t n) {
+    int B = 1;
+    while (B < 32 && ((uint64_t)1 << B) <= (uint64_t)n) ++B;  // 2^B > n: ids 0..n-1 and NULL as n
+    return B;
+}
 void launch_net_keys(uint32_t V, const uint32_t* cnt, const uint32_t* off, const NetSlots& sl, int vertices,
-                     unsigned long long* key_hi, unsigned long long* key_lo, uint32_t* src, cudaStream_t s) {
-    int g = (int)(V < 148u * 16u ? (V > 0 ? V : 1) : 148u * 16u);
-    k_net_compact<<<g, 64, 0, s>>>(V, cnt, off, sl, vertices, key_hi, key_lo, src); count_launch();
+                     uint32_t n, unsigned long long* key_hi, unsigned long long* key_lo, uint32_t* src,
+                     cudaStream_t s) {
+    k_net_compact<<<gb(V), 256, 0, s>>>(V, cnt, off, sl, vertices, n, net_key_bits(n), key_hi, key_lo, src);
+    count_launch();
 }
 
 size_t net_sort_temp_bytes(uint32_t m) {
@@ -205,9 +216,11 @@ __global__ void k_gather_u32(uint32_t m, const uint32_t* __restrict__ idx, const
 }
 }  // namespace
 
-// Stable LSD sort of m keys (hi, lo): by lo, then by hi, carrying the dense index.  On
+// Stable LSD sort of m keys (hi, lo): by lo, then by hi, carrying the dense index; only
+// the low bits_lo / bits_hi bits of the words are sorted on (the rest are zero).  On
 // return hi_s/lo_s hold the sorted keys and order[i] the dense index of sorted element i.
-void net_sort(uint32_t m, const unsigned long long* hi, const unsigned long long* lo, NetSortBufs t, cudaStream_t s) {
+void net_sort(uint32_t m, const unsigned long long* hi, const unsigned long long* lo, int bits_hi, int bits_lo,
+              NetSortBufs t, cudaStream_t s) {
     if (m == 0) return;
     k_iota<<<gb(m), 256, 0, s>>>(m, t.idx_a); count_launch();
     cudaMemcpyAsync(t.key_a, lo, 8 * (size_t)m, cudaMemcpyDeviceToDevice, s);
@@ -215,7 +228,7 @@ void net_sort(uint32_t m, const unsigned long long* hi, const unsigned long long
     {
         cub::DoubleBuffer<unsigned long long> k(t.key_a, t.key_b);
         cub::DoubleBuffer<uint32_t> v(t.idx_a, t.idx_b);
-        cub::DeviceRadixSort::SortPairs(t.temp, tb, k, v, (int)m, 0, 64, s);
+        cub::DeviceRadixSort::SortPairs(t.temp, tb, k, v, (int)m, 0, bits_lo, s);
         count_launch();
         if (v.Current() != t.idx_a) cudaMemcpyAsync(t.idx_a, v.Current(), 4 * (size_t)m, cudaMemcpyDeviceToDevice, s);
     }
@@ -224,7 +237,7 @@ void net_sort(uint32_t m, const unsigned long long* hi, const unsigned long long
         tb = t.temp_bytes;
         cub::DoubleBuffer<unsigned long long> k(t.key_a, t.key_b);
         cub::DoubleBuffer<uint32_t> v(t.idx_a, t.idx_b);
-        cub::DeviceRadixSort::SortPairs(t.temp, tb, k, v, (int)m, 0, 64, s);
+        cub::DeviceRadixSort::SortPairs(t.temp, tb, k, v, (int)m, 0, bits_hi, s);
         count_launch();
         if (k.Current() != t.hi_s) cudaMemcpyAsync(t.hi_s, k.Current(), 8 * (size_t)m, cudaMemcpyDeviceToDevice, s);
         if (v.Current() != t.order) cudaMemcpyAsync(t.order, v.Current(), 4 * (size_t)m, cudaMemcpyDeviceToDevice, s);

@@ -365,11 +365,15 @@ void launch_net_elements_f32(const DevBufs& b, uint32_t P, const uint32_t* voff,
 // the pairs of ov_list through the serial contour (vt_contact64.cu); at most ov_cap
 void launch_net_serial(const DevBufs& b, const uint32_t* voff, NetSlots slots, cudaStream_t s);
 size_t net_slot_capacity();
-// dense keys of V pairs' elements (off = exclusive scan of cnt) and their element indices
+// dense keys of V pairs' elements (off = exclusive scan of cnt) and their element indices;
+// ids packed net_key_bits(n) bits each (NULL as n)
+int net_key_bits(uint32_t n);
 void launch_net_keys(uint32_t V, const uint32_t* cnt, const uint32_t* off, const NetSlots& slots, int vertices,
-                     unsigned long long* key_hi, unsigned long long* key_lo, uint32_t* src, cudaStream_t s);
+                     uint32_t n, unsigned long long* key_hi, unsigned long long* key_lo, uint32_t* src,
+                     cudaStream_t s);
 size_t net_sort_temp_bytes(uint32_t m);
-void net_sort(uint32_t m, const unsigned long long* hi, const unsigned long long* lo, NetSortBufs t, cudaStream_t s);
+void net_sort(uint32_t m, const unsigned long long* hi, const unsigned long long* lo, int bits_hi, int bits_lo,
+              NetSortBufs t, cudaStream_t s);
 // flags[i] = 1 for the first of each run of equal keys
 void launch_net_unique(uint32_t m, const NetSortBufs& t, uint32_t* flags, cudaStream_t s);
 // unique sorted elements (uoff = exclusive scan of the flags) to the output arrays
