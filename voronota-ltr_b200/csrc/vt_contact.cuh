@@ -400,6 +400,7 @@ struct ContourOut {
     Pt<T> q;
     int len;
     bool full;
+    bool unsure;  // a decision of the contour (not of the descriptor) fell in the band
     Sph<T> ic;
     V3<T> axis;
 };
@@ -827,6 +828,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
         co->q = q;
         co->len = len;
         co->full = !init;
+        co->unsure = __any_sync(kFull, d.unsure);
         co->ic = g.ic;
         co->axis = g.axis;
     }

@@ -23,7 +23,8 @@ namespace {
 constexpr int kWarps = VT_C32_WARPS;
 
 // One pair: the FP32 contour and the descriptor, written to the pair's outputs.
-template <bool FULL, bool XM>
+// REC: also record the pair's contour for the network (DevBufs::rec_*).
+template <bool FULL, bool XM, bool REC>
 __device__ __forceinline__ void contact_pair32(const DevBufs& b, uint32_t p, float band) {
     const int lane = threadIdx.x & 31;
     const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
@@ -47,7 +48,25 @@ __device__ __forceinline__ void contact_pair32(const DevBufs& b, uint32_t p, flo
         r.id = nid[e];
         return r;
     };
-    WarpContact r = contact_warp<float, true, FULL, XM>(g, (int)cnt, (int)(eb - off), nbf);
+    ContourOut<float> co;
+    WarpContact r = contact_warp<float, true, FULL, XM>(g, (int)cnt, (int)(eb - off), nbf, REC ? &co : nullptr);
+    if constexpr (REC) {
+        uint32_t base = kRecNone;
+        const int len = r.valid ? co.len : 0;
+        if (r.valid) {
+            if (lane == 0) base = atomicAdd(b.rec_count, (uint32_t)len);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if ((uint64_t)base + (uint64_t)len > (uint64_t)b.rec_cap) base = kRecNone;  // pool full: recompute
+            if (base != kRecNone && lane < len) {
+                b.rec_pts[base + lane] = make_float4(co.q.p.x, co.q.p.y, co.q.p.z, co.q.ang);
+                b.rec_ids[base + lane] = make_uint2(co.q.lid, co.q.rid);
+            }
+        }
+        if (lane == 0) {
+            b.rec_off[p] = base;
+            b.rec_meta[p] = ((uint32_t)len << 8) | (co.full ? 1u : 0u) | (r.merged ? 2u : 0u) | (co.unsure ? 4u : 0u);
+        }
+    }
     if (lane == 0) {
         uint8_t st = (r.valid ? kValid : 0) | (r.unsure ? kUnsure : 0) | (r.overflow ? kOverflow : 0);
         b.p_status[p] = st;
@@ -68,7 +87,7 @@ __device__ __forceinline__ void contact_pair32(const DevBufs& b, uint32_t p, flo
 // wave of resident blocks) whose warps take chunks of `chunk` consecutive pairs from the
 // work counter *queue (zero at launch), so that costly pairs do not leave a tail of idle
 // SMs.
-template <bool FULL, bool XM, int W>
+template <bool FULL, bool XM, bool REC, int W>
 __global__ void __launch_bounds__(W * 32, VT_C32_MINB * 4 / W)
     k_contact32(DevBufs b, uint32_t P, float band, uint32_t* queue, uint32_t chunk) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -85,7 +104,7 @@ __global__ void __launch_bounds__(W * 32, VT_C32_MINB * 4 / W)
             p = base;
             end = base + chunk < P ? base + chunk : P;
         }
-        contact_pair32<FULL, XM>(b, p, band);
+        contact_pair32<FULL, XM, REC>(b, p, band);
         p += step;
     }
 }
@@ -178,7 +197,7 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
 // points (the kept point's ids no longer define it), or has a vertex the snap cannot
 // place is listed for the FP64 element kernel instead.
 #ifndef VT_NET32_MINB
-#define VT_NET32_MINB 4
+#define VT_NET32_MINB 6  // 80 registers (a little spill) for 24 warps per SM: 10% faster than 4
 #endif
 __global__ void __launch_bounds__(kWarps * 32, VT_NET32_MINB)
     k_net_elements32(DevBufs b, uint32_t P, float band, const uint32_t* __restrict__ voff, NetSlots sl,
@@ -213,7 +232,31 @@ __global__ void __launch_bounds__(kWarps * 32, VT_NET32_MINB)
             return r;
         };
         ContourOut<float> co;
-        WarpContact r = contact_warp<float, true, false>(g, (int)cnt, (int)(eb - off), nbf, &co);
+        WarpContact r;
+        const uint32_t ro = b.rec_off ? b.rec_off[p] : kRecNone;
+        if (ro != kRecNone) {  // the contact kernel recorded this contour
+            const uint32_t meta = b.rec_meta[p];
+            co.len = (int)(meta >> 8);
+            co.full = (meta & 1u) != 0;
+            if (lane < co.len) {
+                const float4 q = b.rec_pts[ro + lane];
+                const uint2 ids = b.rec_ids[ro + lane];
+                co.q.p = {q.x, q.y, q.z};
+                co.q.ang = q.w;
+                co.q.lid = ids.x;
+                co.q.rid = ids.y;
+            } else {
+                co.q.p = {0.f, 0.f, 0.f};
+                co.q.ang = 0.f;
+                co.q.lid = co.q.rid = a;
+            }
+            r.valid = true;
+            r.overflow = false;
+            r.merged = (meta & 2u) != 0;
+            r.unsure = (meta & 4u) != 0;
+        } else {
+            r = contact_warp<float, true, false>(g, (int)cnt, (int)(eb - off), nbf, &co);
+        }
         bool fp64 = r.unsure || r.overflow || !r.valid || r.merged;
         const Sph<double> A = {{A4.x, A4.y, A4.z}, A4.w}, B = {{B4.x, B4.y, B4.z}, B4.w};
         const Sph<double> ic = intersection_circle(A, B);
@@ -327,14 +370,14 @@ void launch_adjoint_f32(const DevBufs& b, uint32_t P, const double* u_contact, c
     count_launch();
 }
 
-template <bool FULL, bool XM, int W>
+template <bool FULL, bool XM, bool REC, int W>
 void launch_c32_kernel(const DevBufs& b, uint32_t P, cudaStream_t s) {
     uint32_t* queue = b.c32_chunk > 0 ? b.c32_queue : nullptr;
     size_t g;
     if (queue) {
         static int blocks_per_sm = 0;  // resident blocks of this variant (per process)
         if (blocks_per_sm == 0)
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_contact32<FULL, XM, W>, W * 32, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_contact32<FULL, XM, REC, W>, W * 32, 0);
         int sms = 148;
         int dev = 0;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -345,18 +388,20 @@ void launch_c32_kernel(const DevBufs& b, uint32_t P, cudaStream_t s) {
         if (g > (size_t)148 * 16 * 32 / W) g = (size_t)148 * 16 * 32 / W;
     }
     if (g < 1) g = 1;
-    k_contact32<FULL, XM, W><<<(unsigned)g, W * 32, 0, s>>>(b, P, b.fp32_band, queue, (uint32_t)b.c32_chunk);
+    k_contact32<FULL, XM, REC, W><<<(unsigned)g, W * 32, 0, s>>>(b, P, b.fp32_band, queue, (uint32_t)b.c32_chunk);
     count_launch();
 }
 
 template <int W>
 void launch_c32(const DevBufs& b, uint32_t P, int full, cudaStream_t s) {
-    if (full && b.p_arcm)  // the updateable tessellation records arc moments
-        launch_c32_kernel<true, true, W>(b, P, s);
+    if (full && b.p_arcm)  // the updateable tessellation records arc and face moments
+        launch_c32_kernel<true, true, false, W>(b, P, s);
+    else if (full && b.rec_off)  // the network's element kernel reuses the contours
+        launch_c32_kernel<true, false, true, W>(b, P, s);
     else if (full)
-        launch_c32_kernel<true, false, W>(b, P, s);
+        launch_c32_kernel<true, false, false, W>(b, P, s);
     else
-        launch_c32_kernel<false, false, W>(b, P, s);
+        launch_c32_kernel<false, false, false, W>(b, P, s);
 }
 
 void launch_contact_f32(const DevBufs& b, uint32_t P, int full, cudaStream_t s) {

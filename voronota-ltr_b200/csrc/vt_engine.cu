@@ -167,6 +167,10 @@ struct vt_engine {
     DBuf<uint4> net_vids, net_eids, net_ov_vids, net_ov_eids;
     DBuf<double> net_vxyz, net_elen, net_ov_vxyz, net_ov_elen;
     DBuf<uint32_t> net_base, net_ov_list, net_fp64_list;
+    // FP32 contours recorded by the contact kernel for the element kernel (network calls)
+    DBuf<float4> rec_pts;
+    DBuf<uint2> rec_ids;
+    DBuf<uint32_t> rec_off, rec_meta;
     NetSlots net_slots{};
     DBuf<unsigned long long> net_hi, net_lo, net_ka, net_kb, net_hs, net_ls;
     DBuf<uint32_t> net_ia, net_ib, net_order;
@@ -669,6 +673,22 @@ struct vt_engine {
         b.serial_scratch = serial_scratch.p;
         b.serial_slots = serial_slots;
         const int full = contacts_only ? 0 : 1;
+        if (fp32 && network && !contacts_only && !batch && P > 0) {
+            // a pool of 3 points per candidate pair (valid pairs, about half, hold about 6);
+            // pairs past it are recomputed by the element kernel
+            const size_t cap = std::min<size_t>(3 * (size_t)P + 64, (size_t)0xfffffff0u);
+            rec_pts.ensure(cap);
+            rec_ids.ensure(cap);
+            rec_off.ensure(P);
+            rec_meta.ensure(P);
+            b.rec_pts = rec_pts.p;
+            b.rec_ids = rec_ids.p;
+            b.rec_off = rec_off.p;
+            b.rec_meta = rec_meta.p;
+            b.rec_count = words.p + 7;
+            b.rec_cap = (uint32_t)cap;
+            VT_CUDA(cudaMemsetAsync(b.rec_count, 0, sizeof(uint32_t), stream));
+        }
         if (P > 0) {
             if (fp32) {
                 t_begin(5);

@@ -37,6 +37,7 @@ enum PairStatus : uint8_t {
 constexpr int kSortCap = 256;       // neighbour list capacity of the warp sort buffer (longer
                                     // lists go through the block sort, without a limit)
 constexpr int kSerialCap = 256;     // contour capacity of the serial fallback
+constexpr uint32_t kRecNone = 0xffffffffu;  // a pair whose FP32 contour was not recorded
 
 // Host-visible bounding-box reduction result.
 struct BBox {
@@ -93,6 +94,18 @@ struct DevBufs {
     double* p_pv_a;
     double* p_pv_b;
     double* p_arcm;  // optional: first moments of each contact's arcs and area about a (6 per pair)
+    // optional (FP32 calls that build the network): the FP32 contact kernel records each
+    // valid pair's contour for the network's element kernel, which then need not
+    // recompute it.  rec_off[p]: first point in rec_pts / rec_ids, or kRecNone (not
+    // recorded: the element kernel recomputes the contour); rec_meta[p]: points << 8 |
+    // 1 uncut | 2 merged points | 4 an unsure contour decision; points are taken from a
+    // pool of rec_cap with the counter rec_count.
+    float4* rec_pts;  // x, y, z relative to a, arc angle
+    uint2* rec_ids;   // left id, right id
+    uint32_t* rec_off;
+    uint32_t* rec_meta;
+    uint32_t* rec_count;
+    uint32_t rec_cap;
     // recompute lists
     uint32_t* redo_list;
     uint32_t* d_redo_count;
