@@ -168,6 +168,7 @@ struct vt_engine {
     DBuf<double> net_vxyz, net_elen, net_ov_vxyz, net_ov_elen;
     DBuf<uint32_t> net_base, net_ov_list, net_fp64_list;
     // FP32 contours recorded by the contact kernel for the element kernel (network calls)
+    DBuf<uint32_t> hit_idx;  // the count pass's hits per ball, for the fill pass
     DBuf<float4> rec_pts;
     DBuf<uint2> rec_ids;
     DBuf<uint32_t> rec_off, rec_meta;
@@ -604,6 +605,8 @@ struct vt_engine {
         b.pair_off = pair_off.p;
         big_list.ensure(n + 1);
         b.big_list = big_list.p;
+        hit_idx.ensure((size_t)n * kHitCap);
+        b.hit_idx = hit_idx.p;
         b.d_big_count = words.p + 6;
         t_begin(3);
         launch_search_count(b, stream);

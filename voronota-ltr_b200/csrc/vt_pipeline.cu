@@ -198,6 +198,26 @@ __global__ void __launch_bounds__(kSearchWarps * 32, FILL ? 7 : 9) k_search(DevB
         }
         const double4 A4 = b.sph[i];
         const Sph<double> A = sph_of(A4);
+        // a row longer than the warp sort buffer is written unsorted to the CSR by the
+        // fill pass and sorted there by k_big_sort
+        const uint32_t row_cnt = FILL ? b.nb_cnt[row] : 0u;
+        const bool big = row_cnt > (uint32_t)kSortCap;
+        const uint32_t off = FILL ? b.nb_off[row] : 0u;
+        uint32_t hits = 0, np = 0;
+        bool hidden = false;
+        // fill pass of a row whose hits the count pass listed (at most kHitCap): read them
+        // instead of scanning the stencil again
+        if (FILL && b.hit_idx && row_cnt <= (uint32_t)kHitCap) {
+            if constexpr (FILL) {
+                for (uint32_t e = lane; e < row_cnt; e += 32) {
+                    const uint32_t idx = b.hit_idx[(size_t)row * kHitCap + e];
+                    s_val[w][e] = dist_to_ic_center(A, sph_of(b.c_pos[idx]));  // spheres_searcher.rs:312-316
+                    s_id[w][e] = b.c_id[idx];
+                    s_slot[w][e] = b.c_slot[idx];
+                }
+            }
+            hits = row_cnt;
+        } else {
         int cx = cell_coord(A4.x, g.ox, g.cell, g.dx), cy = cell_coord(A4.y, g.oy, g.cell, g.dy),
             cz = cell_coord(A4.z, g.oz, g.cell, g.dz);
         // stencil rows (y, z) of up to 2 half + 1 cells in x, one per lane; a row whose y and
@@ -231,13 +251,6 @@ __global__ void __launch_bounds__(kSearchWarps * 32, FILL ? 7 : 9) k_search(DevB
             if (lane >= o) incl += t;
         }
         const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-        // a row longer than the warp sort buffer is written unsorted to the CSR by the
-        // fill pass and sorted there by k_big_sort
-        const uint32_t row_cnt = FILL ? b.nb_cnt[row] : 0u;
-        const bool big = row_cnt > (uint32_t)kSortCap;
-        const uint32_t off = FILL ? b.nb_off[row] : 0u;
-        uint32_t hits = 0, np = 0;
-        bool hidden = false;
         for (uint32_t t0 = 0; t0 < total && !hidden; t0 += 32) {
             uint32_t t = t0 + lane;
             bool hit = false, hid = false;
@@ -254,8 +267,9 @@ __global__ void __launch_bounds__(kSearchWarps * 32, FILL ? 7 : 9) k_search(DevB
             const uint32_t r_end = __shfl_sync(0xffffffffu, incl, r);
             const uint32_t r_cnt = __shfl_sync(0xffffffffu, rcnt, r);
             const uint32_t r_beg = __shfl_sync(0xffffffffu, rbeg, r);
+            uint32_t idx = 0;
             if (t < total) {
-                uint32_t idx = r_beg + (t - (r_end - r_cnt));
+                idx = r_beg + (t - (r_end - r_cnt));
                 cid = b.c_id[idx];
                 if (cid != i) {
                     const Sph<double> C = sph_of(b.c_pos[idx]);
@@ -294,6 +308,8 @@ __global__ void __launch_bounds__(kSearchWarps * 32, FILL ? 7 : 9) k_search(DevB
                     }
                 }
             }
+            if (!FILL && hit && b.hit_idx && pos < (uint32_t)kHitCap)
+                b.hit_idx[(size_t)row * kHitCap + pos] = idx;  // for the fill pass
             if (!FILL) {  // pairs this ball generates (collect_collision_pairs, tessellation.rs:298-319)
                 const uint32_t bc = b.periodic ? cid % n : cid;
                 const bool gen = hit && !b.no_pairs && !same_group(b.groups, b.n_groups, i, bc) &&
@@ -302,6 +318,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32, FILL ? 7 : 9) k_search(DevB
             }
             hits += __popc(m);
         }
+        }  // stencil scan
         const uint32_t cnt = hidden ? 0 : hits;
         __syncwarp();
         if (!FILL) {

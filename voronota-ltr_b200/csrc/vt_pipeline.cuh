@@ -38,6 +38,7 @@ constexpr int kSortCap = 256;       // neighbour list capacity of the warp sort 
                                     // lists go through the block sort, without a limit)
 constexpr int kSerialCap = 256;     // contour capacity of the serial fallback
 constexpr uint32_t kRecNone = 0xffffffffu;  // a pair whose FP32 contour was not recorded
+constexpr int kHitCap = 64;  // hits per row the count pass lists for the fill pass
 
 // Host-visible bounding-box reduction result.
 struct BBox {
@@ -73,6 +74,9 @@ struct DevBufs {
     uint32_t* c_slot;
     // CSR
     uint32_t* nb_cnt;
+    // optional: kHitCap grid indices per search row, the hits the count pass found (rows
+    // with more hits are scanned again by the fill pass)
+    uint32_t* hit_idx;
     uint32_t* nb_npair;
     uint8_t* excluded;
     uint32_t* nb_off;

@@ -198,7 +198,7 @@ struct vt_updateable {
     DBuf<double4> sph, gsph, c_pos, changed_ball;
     DBuf<uint32_t> slot_id, gslot_id, cell_count, cell_start, cell_cursor, c_id, c_slot;
     DBuf<BBox> bbox_parts, bbox;
-    DBuf<uint32_t> img_cnt, img_off, scan_tmp, words, big_rows;
+    DBuf<uint32_t> img_cnt, img_off, scan_tmp, words, big_rows, hit_idx;
     DBuf<uint64_t> ids_in;
     DBuf<double> src_in;
     DBuf<uint32_t> flags, flags_off, mark, row_of, list1, more_list, nflags, noff;
@@ -417,6 +417,8 @@ struct vt_updateable {
         b.nb_off = L.off.p;
         big_rows.ensure(rows + 1);
         b.big_list = big_rows.p;
+        hit_idx.ensure((size_t)rows * kHitCap);
+        b.hit_idx = hit_idx.p;
         b.d_big_count = w(kWBig);
         launch_search_count(b, stream);
         ensure_scan(rows + 1);
