@@ -589,11 +589,15 @@ struct vt_updateable {
         tmp_k.ensure(mmax);
         ensure_scan(n + 1);
         scan_u32(tot_cnt.p, next_tab.off.p, n, scan_tmp.p, stream);
-        if (!fresh) launch_table_copy_kept(n, mk, old, next_tab.ref(), stream);
+        // with the adjoint off the coefficients are stale until a full computation: not
+        // copied (the adjoints are refused meanwhile)
+        TableRef nref = next_tab.ref();
+        if (!adjoint) nref.gA = nref.gB = nref.vA = nref.vB = nullptr;
+        if (!fresh) launch_table_copy_kept(n, mk, old, nref, stream);
         if (P) {
             zero(cursor.p, (size_t)n * 4);
-            launch_table_scatter_new(nc_ref(), d_nc, P, next_tab.ref(), keep_cnt.p, cursor.p, tmp_k.p, stream);
-            launch_table_write_new(n, nc_ref(), next_tab.ref(), keep_cnt.p, new_cnt.p, tmp_k.p, w(kWErr), stream);
+            launch_table_scatter_new(nc_ref(), d_nc, P, nref, keep_cnt.p, cursor.p, tmp_k.p, stream);
+            launch_table_write_new(n, nc_ref(), nref, keep_cnt.p, new_cnt.p, tmp_k.p, w(kWErr), stream);
         }
         S.tab.swap(next_tab);
         S.tab.M = 0;  // known after finish()
@@ -674,7 +678,9 @@ struct vt_updateable {
             launch_contact_serial(b, P2, 1, stream);
         }
         extract_new(b, P2);
-        if (P2) launch_table_update(nc_ref(), keep_off.p + P2, P2, S.tab.ref(), w(kWErr), stream);
+        TableRef tref = S.tab.ref();
+        if (!adjoint) tref.gA = tref.gB = tref.vA = tref.vB = nullptr;
+        if (P2) launch_table_update(nc_ref(), keep_off.p + P2, P2, tref, w(kWErr), stream);
         launch_table_cells(aff2.p, noff2.p + n, A2, S.tab.ref(), sph.p, S.excl.p, S.cell_flag.p, S.cell_sas.p,
                            S.cell_vol.p, 0.f, nullptr, stream);
     }
