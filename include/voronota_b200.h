@@ -216,6 +216,11 @@ int vt_engine_device_outputs(const vt_engine* e, vt_device_outputs* out);
  * NULL (no such term); d_grad: n x 4 doubles, overwritten. */
 int vt_engine_grad_device(vt_engine* e, const double* d_w_sas, const double* d_v_volume, const double* d_u_contact,
                           double* d_grad);
+/* Whether later FP32+fixup computations of the engine keep each contact's FP32 contour
+ * (about 24 bytes per contour point in device memory) so that vt_engine_grad_device reads
+ * it instead of recomputing it (no counterpart in the reference; off by default; vt_grad
+ * and the torch.autograd front end turn it on for their forward). */
+int vt_engine_set_keep_contours(vt_engine* e, int on);
 /* Forward (as vt_compute_tessellation, no groups) + adjoint on host arrays; u_contact
  * must have num_contacts = the tessellation's contact count entries. */
 int vt_grad(const double* xyzr, uint64_t n, double probe, const double* periodic_box9, int precision,

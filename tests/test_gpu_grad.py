@@ -236,6 +236,37 @@ def test_periodic_volume_adjoint():
         _check_fd(g[i, c], lambda b: _loss_gpu(b, 1.4, w, upair, box, v=v), balls, i, c)
 
 
+@pytest.mark.parametrize("periodic", [False, True])
+def test_kept_contours_give_the_same_adjoint(periodic):
+    """An FP32 forward that keeps its contours lets the adjoint skip their recomputation;
+    the gradient is the one the recomputing adjoint gives."""
+    import torch
+
+    if periodic:
+        balls, side = W.periodic_box_balls(3000, seed=42)
+        box = V.parse_periodic_box({"corners": [(0.0, 0.0, 0.0), (side, side, side)]})
+    else:
+        balls, box = W.lattice_balls(4000, 42), None
+    n = len(balls)
+    rng = np.random.default_rng(43)
+    d = torch.from_numpy(balls).cuda()
+    w = torch.from_numpy(rng.uniform(0.0, 1.0, n)).cuda()
+    v = torch.from_numpy(rng.uniform(0.0, 1.0, n)).cuda()
+    grads = []
+    for keep in (False, True):
+        e = V.Engine()
+        e.set_keep_contours(keep)
+        e.compute_device(d.data_ptr(), n, 1.4, box, precision="fp32")
+        r = e.download()
+        u = torch.from_numpy(np.random.default_rng(44).normal(0.0, 1.0, len(r.id_a))).cuda()
+        g = torch.empty((n, 4), dtype=torch.float64, device="cuda")
+        e.grad_device(w.data_ptr(), u.data_ptr(), g.data_ptr(), v.data_ptr())
+        torch.cuda.synchronize()
+        grads.append(g.cpu().numpy())
+        e.close()
+    assert np.allclose(grads[0], grads[1], rtol=1e-12, atol=1e-12)
+
+
 def test_torch_autograd_matches_c_abi():
     import torch
 

@@ -109,6 +109,36 @@ __global__ void __launch_bounds__(W * 32, VT_C32_MINB * 4 / W)
     }
 }
 
+// The FP32 contour the contact kernel of the same call recorded for pair p
+// (DevBufs::rec_*), filled in as the warp computation returns it (one point per lane);
+// false when none was recorded (the caller recomputes it).
+__device__ __forceinline__ bool recorded_contour(const DevBufs& b, uint32_t p, uint32_t a, ContourOut<float>& co,
+                                                 WarpContact& r) {
+    const uint32_t ro = b.rec_off ? b.rec_off[p] : kRecNone;
+    if (ro == kRecNone) return false;
+    const int lane = threadIdx.x & 31;
+    const uint32_t meta = b.rec_meta[p];
+    co.len = (int)(meta >> 8);
+    co.full = (meta & 1u) != 0;
+    if (lane < co.len) {
+        const float4 q = b.rec_pts[ro + lane];
+        const uint2 ids = b.rec_ids[ro + lane];
+        co.q.p = {q.x, q.y, q.z};
+        co.q.ang = q.w;
+        co.q.lid = ids.x;
+        co.q.rid = ids.y;
+    } else {
+        co.q.p = {0.f, 0.f, 0.f};
+        co.q.ang = 0.f;
+        co.q.lid = co.q.rid = a;
+    }
+    r.valid = true;
+    r.overflow = false;
+    r.merged = (meta & 2u) != 0;
+    r.unsure = (meta & 4u) != 0;
+    return true;
+}
+
 // FP32 adjoint: the contour recomputed in FP32 (relative to a), the gradient formed in
 // double from its points; pairs whose recomputation is unsure or overflows are listed for
 // the FP64 adjoint.
@@ -146,7 +176,9 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
             return r;
         };
         ContourOut<float> co;
-        WarpContact r = contact_warp<float, true, false>(g, (int)cnt, (int)(eb - off), nbf, &co);
+        WarpContact r;
+        if (!recorded_contour(b, p, a, co, r))
+            r = contact_warp<float, true, false>(g, (int)cnt, (int)(eb - off), nbf, &co);
         if (r.unsure || r.overflow) {
             if (lane == 0) b.redo_list[atomicAdd(b.d_redo_count, 1u)] = p;
             continue;
@@ -233,30 +265,8 @@ __global__ void __launch_bounds__(kWarps * 32, VT_NET32_MINB)
         };
         ContourOut<float> co;
         WarpContact r;
-        const uint32_t ro = b.rec_off ? b.rec_off[p] : kRecNone;
-        if (ro != kRecNone) {  // the contact kernel recorded this contour
-            const uint32_t meta = b.rec_meta[p];
-            co.len = (int)(meta >> 8);
-            co.full = (meta & 1u) != 0;
-            if (lane < co.len) {
-                const float4 q = b.rec_pts[ro + lane];
-                const uint2 ids = b.rec_ids[ro + lane];
-                co.q.p = {q.x, q.y, q.z};
-                co.q.ang = q.w;
-                co.q.lid = ids.x;
-                co.q.rid = ids.y;
-            } else {
-                co.q.p = {0.f, 0.f, 0.f};
-                co.q.ang = 0.f;
-                co.q.lid = co.q.rid = a;
-            }
-            r.valid = true;
-            r.overflow = false;
-            r.merged = (meta & 2u) != 0;
-            r.unsure = (meta & 4u) != 0;
-        } else {
+        if (!recorded_contour(b, p, a, co, r))
             r = contact_warp<float, true, false>(g, (int)cnt, (int)(eb - off), nbf, &co);
-        }
         bool fp64 = r.unsure || r.overflow || !r.valid || r.merged;
         const Sph<double> A = {{A4.x, A4.y, A4.z}, A4.w}, B = {{B4.x, B4.y, B4.z}, B4.w};
         const Sph<double> ic = intersection_circle(A, B);

@@ -167,7 +167,9 @@ struct vt_engine {
     DBuf<uint4> net_vids, net_eids, net_ov_vids, net_ov_eids;
     DBuf<double> net_vxyz, net_elen, net_ov_vxyz, net_ov_elen;
     DBuf<uint32_t> net_base, net_ov_list, net_fp64_list;
-    // FP32 contours recorded by the contact kernel for the element kernel (network calls)
+    // FP32 contours recorded by the contact kernel for the network's element kernel and
+    // the adjoint (network calls, and calls with keep_contours set)
+    bool keep_contours = false;
     DBuf<uint32_t> hit_idx;  // the count pass's hits per ball, for the fill pass
     DBuf<float4> rec_pts;
     DBuf<uint2> rec_ids;
@@ -676,7 +678,7 @@ struct vt_engine {
         b.serial_scratch = serial_scratch.p;
         b.serial_slots = serial_slots;
         const int full = contacts_only ? 0 : 1;
-        if (fp32 && network && !contacts_only && !batch && P > 0) {
+        if (fp32 && (network || keep_contours) && !contacts_only && !batch && P > 0) {
             // a pool of 3 points per candidate pair (valid pairs, about half, hold about 6);
             // pairs past it are recomputed by the element kernel
             const size_t cap = std::min<size_t>(3 * (size_t)P + 64, (size_t)0xfffffff0u);
@@ -1208,7 +1210,10 @@ int vt_grad(const double* xyzr, uint64_t n, double probe, const double* periodic
             double* grad_out) {
     if (n && !grad_out) return VT_ERR_INVALID;
     return with_default_engine([&](vt_engine* e) -> int {
+        const bool keep = e->keep_contours;
+        e->keep_contours = true;  // the adjoint reads the forward's FP32 contours
         int st = host_compute(e, xyzr, n, probe, periodic_box9, nullptr, 0, precision, 0);
+        e->keep_contours = keep;
         if (st != VT_OK) return st;
         if (n == 0) return VT_OK;
         if (u_contact && num_contacts != e->stats.num_contacts) {
@@ -1369,6 +1374,11 @@ void vt_solvent_free(vt_solvent_result* r) { delete r; }
 int vt_engine_set_fp32_min_pairs(vt_engine* e, uint64_t min_pairs) {
     if (!e) return VT_ERR_INVALID;
     e->fp32_min_pairs = min_pairs;
+    return VT_OK;
+}
+int vt_engine_set_keep_contours(vt_engine* e, int on) {
+    if (!e) return VT_ERR_INVALID;
+    e->keep_contours = on != 0;
     return VT_OK;
 }
 int vt_engine_set_network(vt_engine* e, int on) {

@@ -172,6 +172,7 @@ def library():
     L.vt_batch_free.argtypes = [_vp]
     L.vt_batch_free.restype = None
     L.vt_engine_grad_device.argtypes = [_vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.vt_engine_set_keep_contours.argtypes = [_vp, ctypes.c_int]
     L.vt_engine_autotune_device.argtypes = [_vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double, _f64p,
                                             ctypes.c_int, _u64p, ctypes.c_uint64]
     L.vt_engine_get_tuning.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
@@ -620,6 +621,11 @@ class Engine:
         """FP32 mode runs the FP32 contact kernel only from this many candidate pairs
         (default 2048; FP64 below); 0 forces the FP32 kernel."""
         _check(self._L.vt_engine_set_fp32_min_pairs(self._h, int(min_pairs)))
+
+    def set_keep_contours(self, on: bool = True):
+        """Later FP32 computations keep their contours for grad_device (faster adjoint,
+        about 24 bytes of device memory per contour point)."""
+        _check(self._L.vt_engine_set_keep_contours(self._h, 1 if on else 0))
 
     def set_network(self, on: bool = True):
         """Later compute calls also build the tessellation network (with_cell_vertices)."""

@@ -24,6 +24,7 @@ class _Tessellation(torch.autograd.Function):
         n = x.shape[0]
         eng = Engine(x.device.index or 0)
         eng.set_stream(torch.cuda.current_stream(x.device).cuda_stream)
+        eng.set_keep_contours(True)  # backward reads the forward's contours
         pb = None if periodic_box is None else parse_periodic_box(periodic_box)
         eng.compute_device(x.data_ptr(), n, probe, pb, precision=precision)
         r = eng.download()
