@@ -102,17 +102,37 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """Bytes per contact-kernel launch from the committed ncu summary, if present."""
+def profiled_value(key):
+    """A figure of the contact kernel's committed ncu summary (per launch on the 100k
+    lattice), if present: traffic_bytes_per_launch, warp_instructions_per_launch."""
     path = os.path.join(ROOT, "profiles", "contact_kernel_fp32_100k.md")
     try:
         with open(path) as f:
             for line in f:
-                if line.startswith("traffic_bytes_per_launch:"):
+                if line.startswith(key + ":"):
                     return float(line.split(":", 1)[1].strip())
     except OSError:
         pass
     return None
+
+
+def profiled_traffic():
+    """Bytes per contact-kernel launch from the committed ncu summary, if present."""
+    return profiled_value("traffic_bytes_per_launch")
+
+
+def issue_roofline(kernel_ms, sm_mhz, n_balls):
+    """The contact kernel's instruction-issue roofline: the warp instructions of one launch
+    (ncu, committed summary; valid for the 100k lattice it was measured on) over its
+    CUDA-event time, against one instruction per cycle on each of the 4 schedulers of the
+    148 SMs at the sampled SM clock."""
+    inst = profiled_value("warp_instructions_per_launch")
+    if inst is None or not kernel_ms or n_balls != 100_000:
+        return None
+    peak = 148 * 4 * (sm_mhz or 1965.0) * 1e6
+    achieved = inst / (kernel_ms * 1e-3)
+    return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "warp instructions/s",
+            "frac": achieved / peak, "instructions_source": "profiles/contact_kernel_fp32_100k.md (ncu)"}
 
 
 class ClockSampler:
@@ -906,6 +926,7 @@ def run_ours(args):
                          "frac": achieved / peak, "traffic": traffic, "kernel": "k_contact32",
                          "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": fp32["contact_ms"],
                          "peak_source": peak_kind},
+            "issue_roofline": issue_roofline(fp32["contact_ms"], (fp32["clocks"] or {}).get("sm_mhz"), args.n),
             "cpu_baseline": cpu,
             "clocks": fp32["clocks"],
             "gpu_launches": fp32["launches"],
