@@ -512,13 +512,13 @@ def contacts_only_leg(args, rank, torch, V, R, balls):
     eng = V.Engine()
     eng.set_stream(stream.cuda_stream)
 
-    def timed(precision, contacts_only, reps=7):
+    def timed(precision, contacts_only, reps=7, grouped=True):
         ts = []
         for k in range(reps + 2):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            eng.compute_device(d.data_ptr(), n, PROBE, None, dg.data_ptr(), n, precision=precision,
-                               contacts_only=contacts_only)
+            eng.compute_device(d.data_ptr(), n, PROBE, None, dg.data_ptr() if grouped else 0, n if grouped else 0,
+                               precision=precision, contacts_only=contacts_only)
             e1.record(stream)
             e1.synchronize()
             if k >= 2:
@@ -531,9 +531,13 @@ def contacts_only_leg(args, rank, torch, V, R, balls):
         tc = timed(prec, True)
         res[prec] = eng.download()
         tf = timed(prec, False)
+        tc0 = timed(prec, True, grouped=False)
+        tf0 = timed(prec, False, grouped=False)
         out[prec] = {"ms_contacts_only": tc, "ms_tessellation_same_groups": tf,
                      "balls_per_s_contacts_only": R.world * n / (tc * 1e-3),
-                     "contacts_only_over_tessellation": tc / tf, "contacts": int(len(res[prec].id_a))}
+                     "contacts_only_over_tessellation": tc / tf, "contacts": int(len(res[prec].id_a)),
+                     "no_groups": {"ms_contacts_only": tc0, "ms_tessellation": tf0,
+                                   "contacts_only_over_tessellation": tc0 / tf0}}
     eng.close()
     if rank == 0 and not args.no_cpu:
         import oracle as O

@@ -239,6 +239,15 @@ def test_fp32_large_lattice_pair_set_and_totals():
     assert stats["rel_sas"] <= 1e-6
 
 
+def test_fp32_million_ball_lattice():
+    """A 1,000,000-ball lattice through the FP32+fixup path: the pair set, central bits and
+    cells of the oracle's, the totals within 1e-6 relative."""
+    balls = W.lattice_balls(1_000_000, 5)
+    O.set_threads(0)
+    stats = compare(gpu(balls, 1.4, precision="fp32"), O.compute(balls, 1.4), "fp32")
+    assert stats["rel_sas"] <= 1e-6 and stats["rel_vol"] <= 1e-6
+
+
 def test_fp64_large_lattice():
     """The 100k-ball drop-in configuration through the plain FP64 path."""
     balls = W.lattice_balls(100000, 0)
