@@ -89,7 +89,9 @@ def _allowance(balls, probe, s):
     return 1e-7 * float((4 * np.pi * R[exposed] ** 2).sum()), 1e-7 * float((4 * np.pi * R[exposed] ** 3 / 3).sum())
 
 
-@pytest.mark.parametrize("k", [k for k in range(CASES) if k % 5 != 0][:16])
+# 53, 56 and 72: FP32 trajectories whose refresh of uncertain cells once gave a
+# contact-less neighbour (not affected by the update) a detached cell
+@pytest.mark.parametrize("k", [k for k in range(CASES) if k % 5 != 0][:16] + [53, 56, 72])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_random_trajectory(k, precision, fixed_grid):
     """update_with_changed on a random trajectory: each step moves a random subset (1 ball

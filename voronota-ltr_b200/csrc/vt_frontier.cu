@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(kWarps * 32)
     k_table_cells(const uint32_t* __restrict__ list, const uint32_t* __restrict__ count, TableRef T,
                   const double4* __restrict__ sph, const uint8_t* __restrict__ excl, uint8_t* __restrict__ cell_flag,
                   double* __restrict__ cell_sas, double* __restrict__ cell_vol, float cell_band,
-                  uint8_t* __restrict__ unsure) {
+                  uint8_t* __restrict__ unsure, int keep_empty) {
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     const uint32_t m = *count;
     for (uint32_t t = blockIdx.x * kWarps + wp; t < m; t += gridDim.x * kWarps) {
@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(kWarps * 32)
         sneg = wsum(sneg);
         ppos = wsum(ppos);
         pneg = wsum(pneg);
-        if (lane == 0) {
+        if (lane == 0 && !(keep_empty && e == s)) {
             const uint32_t cnt = e - s;
             const double r = sph[i].w;
             uint8_t flag = 0;
@@ -667,9 +667,9 @@ void launch_table_write_new(uint32_t n, const NewContacts& nc, TableRef nw, cons
 }
 void launch_table_cells(const uint32_t* list, const uint32_t* count, uint32_t max_count, TableRef tab,
                         const double4* sph, const uint8_t* excl, uint8_t* cell_flag, double* cell_sas,
-                        double* cell_vol, float cell_band, uint8_t* unsure, cudaStream_t s) {
+                        double* cell_vol, float cell_band, uint8_t* unsure, cudaStream_t s, int keep_empty) {
     k_table_cells<<<gw(max_count), kWarps * 32, 0, s>>>(list, count, tab, sph, excl, cell_flag, cell_sas, cell_vol,
-                                                        cell_band, unsure);
+                                                        cell_band, unsure, keep_empty);
     count_launch();
 }
 void launch_table_update(const NewContacts& nc, const uint32_t* nc_count, uint32_t max_nc, TableRef tab,

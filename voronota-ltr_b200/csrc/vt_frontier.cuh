@@ -142,9 +142,11 @@ void launch_table_write_new(uint32_t n, const NewContacts& nc, TableRef nw, cons
 // Cells of the listed balls from their table entries (recompute_cells_for_affected,
 // updateable.rs:691-727).  cell_band > 0: balls with an uncertain compute_sas branch
 // get unsure[i] = 1.
+// keep_empty: a listed ball without table entries keeps its cell state (the FP64 refresh of
+// uncertain cells, whose neighbours need not be affected by the operation).
 void launch_table_cells(const uint32_t* list, const uint32_t* count, uint32_t max_count, TableRef tab,
                         const double4* sph, const uint8_t* excl, uint8_t* cell_flag, double* cell_sas,
-                        double* cell_vol, float cell_band, uint8_t* unsure, cudaStream_t s);
+                        double* cell_vol, float cell_band, uint8_t* unsure, cudaStream_t s, int keep_empty = 0);
 // Contact-table bit: a recomputed contact found no entry to overwrite (launch_table_update).
 constexpr uint32_t kErrRefresh = 128u;
 // Overwrites the values of the existing entries (same canonical ids) of every contact in

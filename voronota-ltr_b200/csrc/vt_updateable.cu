@@ -681,8 +681,11 @@ struct vt_updateable {
         TableRef tref = S.tab.ref();
         if (!adjoint) tref.gA = tref.gB = tref.vA = tref.vB = nullptr;
         if (P2) launch_table_update(nc_ref(), keep_off.p + P2, P2, tref, w(kWErr), stream);
+        // the refreshed balls' neighbours need not be affected by this operation: a ball
+        // without contacts keeps the cell state its last computation gave it (the
+        // reference's detached rule applies to affected balls only, updateable.rs:711-719)
         launch_table_cells(aff2.p, noff2.p + n, A2, S.tab.ref(), sph.p, S.excl.p, S.cell_flag.p, S.cell_sas.p,
-                           S.cell_vol.p, 0.f, nullptr, stream);
+                           S.cell_vol.p, 0.f, nullptr, stream, 1);
     }
 
     // update_using_affected (updateable.rs:476-514) for the involved balls (mark != 0),
