@@ -139,6 +139,71 @@ __device__ __forceinline__ bool recorded_contour(const DevBufs& b, uint32_t p, u
     return true;
 }
 
+// Double spheres of a's neighbours by id, for the vertex placement and the adjoint (up to
+// three lookups per contour point).  A per-warp open-addressing table in shared memory
+// (id -> sphere slot, multiplicative hashing with linear probing, filled once per ball a:
+// a warp's consecutive pairs mostly share a) answers a lookup in a probe or two, where a
+// scan of the list costs about one iteration per list entry on the slowest lane; lists
+// longer than kIdTabMax are scanned.  Ids are distinct within a list and below
+// 0xffffffff (the host bounds them by 27 n), the table's empty key.
+constexpr int kIdTabBits = 7, kIdTabSize = 1 << kIdTabBits;
+constexpr uint32_t kIdTabMax = 96, kIdTabEmpty = 0xffffffffu;
+struct IdTab {
+    uint32_t key[kIdTabSize];
+    uint32_t slot[kIdTabSize];
+};
+__device__ __forceinline__ uint32_t idtab_hash(uint32_t id) { return (id * 0x9E3779B1u) >> (32 - kIdTabBits); }
+
+struct NbSpheres {
+    IdTab* t;
+    const double4* sph;
+    const uint32_t* nid;
+    const uint32_t* nslot;
+    uint32_t cnt;
+    uint32_t tab_a;  // the ball whose list the table holds (kIdTabEmpty: none yet)
+    bool hashed;
+    // warp-collective: make lookups refer to ball a's list
+    __device__ __forceinline__ void bind(uint32_t a, const uint32_t* nid_, const uint32_t* nslot_, uint32_t cnt_) {
+        nid = nid_;
+        nslot = nslot_;
+        cnt = cnt_;
+        hashed = cnt <= kIdTabMax;
+        if (!hashed || tab_a == a) return;
+        const int lane = threadIdx.x & 31;
+        __syncwarp();  // lookups into the previous list are done
+        for (int k = lane; k < kIdTabSize; k += 32) t->key[k] = kIdTabEmpty;
+        __syncwarp();
+        for (uint32_t e = lane; e < cnt; e += 32) {
+            const uint32_t id = nid[e];
+            uint32_t pos = idtab_hash(id);
+            for (int probe = 0; probe < kIdTabSize; ++probe) {  // cnt < kIdTabSize: a free key exists
+                if (atomicCAS(&t->key[pos], kIdTabEmpty, id) == kIdTabEmpty) {
+                    t->slot[pos] = nslot[e];
+                    break;
+                }
+                pos = (pos + 1) & (kIdTabSize - 1);
+            }
+        }
+        __syncwarp();
+        tab_a = a;
+    }
+    __device__ __forceinline__ double4 operator()(uint32_t c) const {
+        if (hashed) {
+            uint32_t pos = idtab_hash(c);
+            for (int probe = 0; probe < kIdTabSize; ++probe) {
+                const uint32_t k = t->key[pos];
+                if (k == c) return sph[t->slot[pos]];
+                if (k == kIdTabEmpty) break;
+                pos = (pos + 1) & (kIdTabSize - 1);
+            }
+        } else {
+            for (uint32_t e = 0; e < cnt; ++e)
+                if (nid[e] == c) return sph[nslot[e]];
+        }
+        return make_double4(0.0, 0.0, 0.0, 0.0);
+    }
+};
+
 // FP32 adjoint: the contour recomputed in FP32 (relative to a), the gradient formed in
 // double from its points; pairs whose recomputation is unsure or overflows are listed for
 // the FP64 adjoint.
@@ -146,79 +211,82 @@ template <bool VOL>
 __global__ void __launch_bounds__(kWarps * 32, 4)
     k_adjoint32(DevBufs b, uint32_t P, float band, const double* __restrict__ u_contact,
                 const double* __restrict__ w_eff, const double* __restrict__ v_eff, double* __restrict__ grad) {
+    __shared__ IdTab tabs[kWarps];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t n = b.n;
-    for (uint32_t p = blockIdx.x * kWarps + w; p < P; p += gridDim.x * kWarps) {
-        if (!(b.p_status[p] & kValid)) continue;
-        const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
-        const uint32_t bid = b.nb_id[eb];
-        AdjPair G;
-        if (!adjoint_weights(b, p, a, bid, u_contact, w_eff, v_eff, G)) continue;
-        const uint32_t off = b.nb_off[a], cnt = b.nb_cnt[a];
-        const double4 A4 = b.sph[a], B4 = b.sph[b.nb_slot[eb]];
-        PairGeom<float> g;
-        const float Ra = (float)A4.w;
-        const float4 rb = b.nb_rel[eb];
-        g.A = {{0.f, 0.f, 0.f}, Ra};
-        g.B = {{rb.x, rb.y, rb.z}, rb.w};
-        g.a_id = a;
-        g.b_id = bid;
-        g.S = Ra + rb.w;
-        g.e0 = band * g.S;
-        const float4* rel = b.nb_rel + off;
-        const uint32_t* nid = b.nb_id + off;
-        const uint32_t* nslot = b.nb_slot + off;
-        auto nbf = [&](int e) {
-            Nb<float> r;
-            float4 v = rel[e];
-            r.s = {{v.x, v.y, v.z}, v.w};
-            r.id = nid[e];
-            return r;
-        };
-        ContourOut<float> co;
-        WarpContact r;
-        if (!recorded_contour(b, p, a, co, r))
-            r = contact_warp<float, true, false>(g, (int)cnt, (int)(eb - off), nbf, &co);
-        if (r.unsure || r.overflow) {
-            if (lane == 0) b.redo_list[atomicAdd(b.d_redo_count, 1u)] = p;
-            continue;
+    NbSpheres sphere_of{&tabs[w], b.sph, nullptr, nullptr, 0, kIdTabEmpty, false};
+    // chunks of 32 consecutive pairs per warp: one coalesced status read per chunk, and
+    // consecutive pairs share ball a (one table fill)
+    for (size_t c0 = ((size_t)blockIdx.x * kWarps + w) * 32; c0 < P; c0 += (size_t)gridDim.x * kWarps * 32) {
+        unsigned todo = __ballot_sync(kFull, c0 + lane < P && (b.p_status[c0 + lane] & kValid));
+        while (todo) {
+            const uint32_t p = (uint32_t)c0 + (uint32_t)(__ffs(todo) - 1);
+            todo &= todo - 1;
+            const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
+            const uint32_t bid = b.nb_id[eb];
+            AdjPair G;
+            if (!adjoint_weights(b, p, a, bid, u_contact, w_eff, v_eff, G)) continue;
+            const uint32_t off = b.nb_off[a], cnt = b.nb_cnt[a];
+            const double4 A4 = b.sph[a], B4 = b.sph[b.nb_slot[eb]];
+            PairGeom<float> g;
+            const float Ra = (float)A4.w;
+            const float4 rb = b.nb_rel[eb];
+            g.A = {{0.f, 0.f, 0.f}, Ra};
+            g.B = {{rb.x, rb.y, rb.z}, rb.w};
+            g.a_id = a;
+            g.b_id = bid;
+            g.S = Ra + rb.w;
+            g.e0 = band * g.S;
+            const float4* rel = b.nb_rel + off;
+            const uint32_t* nid = b.nb_id + off;
+            const uint32_t* nslot = b.nb_slot + off;
+            auto nbf = [&](int e) {
+                Nb<float> r;
+                float4 v = rel[e];
+                r.s = {{v.x, v.y, v.z}, v.w};
+                r.id = nid[e];
+                return r;
+            };
+            ContourOut<float> co;
+            WarpContact r;
+            if (!recorded_contour(b, p, a, co, r))
+                r = contact_warp<float, true, false>(g, (int)cnt, (int)(eb - off), nbf, &co);
+            if (r.unsure || r.overflow) {
+                if (lane == 0) b.redo_list[atomicAdd(b.d_redo_count, 1u)] = p;
+                continue;
+            }
+            if (!r.valid) continue;  // no contact, decided outside the band
+            const Sph<double> A = {{A4.x, A4.y, A4.z}, A4.w}, B = {{B4.x, B4.y, B4.z}, B4.w};
+            const Sph<double> ic = intersection_circle(A, B);
+            G.pa = A.c;
+            G.pb = B.c;
+            G.Ra = A.r;
+            G.Rb = B.r;
+            G.q = ic.c;
+            G.rho = ic.r;
+            G.axis = normalize(B.c - A.c);
+            G.a = a;
+            G.bid = bid;
+            const int len = co.len;
+            const int nx = len > 0 ? (lane + 1 < len ? lane + 1 : 0) : 0;
+            if (!co.full) sphere_of.bind(a, nid, nslot, cnt);
+            // the FP32 topology with FP64 vertices and arc angles
+            V3<double> y = widen(co.q.p);
+            if (!co.full && lane < len) y = snap_vertex(G, y, co.q.lid, co.q.rid, sphere_of);
+            const V3<double> P0 = A.c + y;
+            const V3<double> P1 = mk<double>(__shfl_sync(kFull, P0.x, nx), __shfl_sync(kFull, P0.y, nx),
+                                             __shfl_sync(kFull, P0.z, nx));
+            const uint32_t nlid = __shfl_sync(kFull, co.q.lid, nx);
+            double ang = 0.0;
+            if (!co.full && lane < len && co.q.rid == a && nlid == a && co.q.ang > 0.f) {
+                const V3<double> v1 = P0 - G.q, v2 = P1 - G.q;
+                ang = atan2(dot(cross(v1, v2), G.axis), dot(v1, v2));
+                if (ang < 0.0) ang += kTau;
+                // a nearly full or nearly empty arc keeps the FP32 branch of the angle
+                if (fabs((double)co.q.ang - ang) > 1.0) ang = (double)co.q.ang;
+            }
+            adjoint_pair<VOL>(G, co.full, len, P0, P1, ang, co.q.rid, nlid, sphere_of, grad, n);
         }
-        if (!r.valid) continue;  // no contact, decided outside the band
-        const Sph<double> A = {{A4.x, A4.y, A4.z}, A4.w}, B = {{B4.x, B4.y, B4.z}, B4.w};
-        const Sph<double> ic = intersection_circle(A, B);
-        G.pa = A.c;
-        G.pb = B.c;
-        G.Ra = A.r;
-        G.Rb = B.r;
-        G.q = ic.c;
-        G.rho = ic.r;
-        G.axis = normalize(B.c - A.c);
-        G.a = a;
-        G.bid = bid;
-        const int len = co.len;
-        const int nx = len > 0 ? (lane + 1 < len ? lane + 1 : 0) : 0;
-        const double4* sph = b.sph;
-        auto sphere_of = [&](uint32_t c) {
-            for (uint32_t e = 0; e < cnt; ++e)
-                if (nid[e] == c) return sph[nslot[e]];
-            return make_double4(0.0, 0.0, 0.0, 0.0);
-        };
-        // the FP32 topology with FP64 vertices and arc angles
-        V3<double> y = widen(co.q.p);
-        if (!co.full && lane < len) y = snap_vertex(G, y, co.q.lid, co.q.rid, sphere_of);
-        const V3<double> P0 = A.c + y;
-        const V3<double> P1 = mk<double>(__shfl_sync(kFull, P0.x, nx), __shfl_sync(kFull, P0.y, nx),
-                                         __shfl_sync(kFull, P0.z, nx));
-        const uint32_t nlid = __shfl_sync(kFull, co.q.lid, nx);
-        double ang = 0.0;
-        if (!co.full && lane < len && co.q.rid == a && nlid == a && co.q.ang > 0.f) {
-            const V3<double> v1 = P0 - G.q, v2 = P1 - G.q;
-            ang = atan2(dot(cross(v1, v2), G.axis), dot(v1, v2));
-            if (ang < 0.0) ang += kTau;
-            // a nearly full or nearly empty arc keeps the FP32 branch of the angle
-            if (fabs((double)co.q.ang - ang) > 1.0) ang = (double)co.q.ang;
-        }
-        adjoint_pair<VOL>(G, co.full, len, P0, P1, ang, co.q.rid, nlid, sphere_of, grad, n);
     }
 }
 
@@ -234,125 +302,135 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
 __global__ void __launch_bounds__(kWarps * 32, VT_NET32_MINB)
     k_net_elements32(DevBufs b, uint32_t P, float band, const uint32_t* __restrict__ voff, NetSlots sl,
                      uint32_t* __restrict__ fp64_list, uint32_t* __restrict__ fp64_count) {
+    __shared__ IdTab tabs[kWarps];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t n = b.n;
     const int periodic = b.periodic;
-    for (uint32_t p = blockIdx.x * kWarps + w; p < P; p += gridDim.x * kWarps) {
-        const uint32_t slot = voff[p];
-        if (voff[p + 1] == slot) continue;  // no contact
-        const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
-        const uint32_t bid = b.nb_id[eb];
-        const uint32_t off = b.nb_off[a], cnt = b.nb_cnt[a];
-        const double4 A4 = b.sph[a], B4 = b.sph[b.nb_slot[eb]];
-        PairGeom<float> g;
-        const float Ra = (float)A4.w;
-        const float4 rb = b.nb_rel[eb];
-        g.A = {{0.f, 0.f, 0.f}, Ra};
-        g.B = {{rb.x, rb.y, rb.z}, rb.w};
-        g.a_id = a;
-        g.b_id = bid;
-        g.S = Ra + rb.w;
-        g.e0 = band * g.S;
-        const float4* rel = b.nb_rel + off;
-        const uint32_t* nid = b.nb_id + off;
-        const uint32_t* nslot = b.nb_slot + off;
-        auto nbf = [&](int e) {
-            Nb<float> r;
-            float4 v = rel[e];
-            r.s = {{v.x, v.y, v.z}, v.w};
-            r.id = nid[e];
-            return r;
-        };
-        ContourOut<float> co;
-        WarpContact r;
-        if (!recorded_contour(b, p, a, co, r))
-            r = contact_warp<float, true, false>(g, (int)cnt, (int)(eb - off), nbf, &co);
-        bool fp64 = r.unsure || r.overflow || !r.valid || r.merged;
-        const Sph<double> A = {{A4.x, A4.y, A4.z}, A4.w}, B = {{B4.x, B4.y, B4.z}, B4.w};
-        const Sph<double> ic = intersection_circle(A, B);
-        const uint32_t base = slot * (uint32_t)kNetSlot;
-        if (!fp64 && co.full) {  // an uncut contact: one SAS edge, no vertex
-            if (lane == 0) {
-                sl.e_ids[base] = net_edge_ids(a, bid, kNetNull, periodic, n);
-                sl.e_len[base] = kTau * ic.r;
-                sl.v_cnt[slot] = 0;
-                sl.e_cnt[slot] = 1;
-                sl.base[slot] = base;
-            }
-            continue;
+    NbSpheres sphere_of{&tabs[w], b.sph, nullptr, nullptr, 0, kIdTabEmpty, false};
+    // chunks of 32 consecutive pairs per warp: one coalesced read of the slot offsets per
+    // chunk, and consecutive pairs share ball a (one table fill)
+    for (size_t c0 = ((size_t)blockIdx.x * kWarps + w) * 32; c0 < P; c0 += (size_t)gridDim.x * kWarps * 32) {
+        uint32_t vo = 0, vn = 0;
+        if (c0 + lane < P) {
+            vo = voff[c0 + lane];
+            vn = voff[c0 + lane + 1];
         }
-        const int len = co.len;
-        V3<double> P0 = mk<double>(0, 0, 0), P1 = P0;
-        double ang = 0.0;
-        bool arc = false;
-        if (!fp64) {
-            AdjPair G;
-            G.pa = A.c;
-            G.pb = B.c;
-            G.Ra = A.r;
-            G.Rb = B.r;
-            G.q = ic.c;
-            G.rho = ic.r;
-            G.axis = normalize(B.c - A.c);
-            G.a = a;
-            G.bid = bid;
-            const double4* sph = b.sph;
-            auto sphere_of = [&](uint32_t c) {
-                for (uint32_t e = 0; e < cnt; ++e)
-                    if (nid[e] == c) return sph[nslot[e]];
-                return make_double4(0.0, 0.0, 0.0, 0.0);
+        unsigned todo = __ballot_sync(kFull, vn != vo);  // pairs with a contact
+        while (todo) {
+            const int k = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const uint32_t p = (uint32_t)c0 + (uint32_t)k;
+            const uint32_t slot = __shfl_sync(kFull, vo, k);
+            const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
+            const uint32_t bid = b.nb_id[eb];
+            const uint32_t off = b.nb_off[a], cnt = b.nb_cnt[a];
+            const double4 A4 = b.sph[a], B4 = b.sph[b.nb_slot[eb]];
+            PairGeom<float> g;
+            const float Ra = (float)A4.w;
+            const float4 rb = b.nb_rel[eb];
+            g.A = {{0.f, 0.f, 0.f}, Ra};
+            g.B = {{rb.x, rb.y, rb.z}, rb.w};
+            g.a_id = a;
+            g.b_id = bid;
+            g.S = Ra + rb.w;
+            g.e0 = band * g.S;
+            const float4* rel = b.nb_rel + off;
+            const uint32_t* nid = b.nb_id + off;
+            const uint32_t* nslot = b.nb_slot + off;
+            auto nbf = [&](int e) {
+                Nb<float> r;
+                float4 v = rel[e];
+                r.s = {{v.x, v.y, v.z}, v.w};
+                r.id = nid[e];
+                return r;
             };
-            bool ok = true;
-            V3<double> y = widen(co.q.p);
-            if (lane < len) y = snap_vertex(G, y, co.q.lid, co.q.rid, sphere_of, &ok);
-            P0 = A.c + y;
-            const int nx = len > 0 ? (lane + 1 < len ? lane + 1 : 0) : 0;
-            P1 = mk<double>(__shfl_sync(kFull, P0.x, nx), __shfl_sync(kFull, P0.y, nx), __shfl_sync(kFull, P0.z, nx));
-            const uint32_t nlid = __shfl_sync(kFull, co.q.lid, nx);
-            arc = lane < len && co.q.rid == a;
-            if (arc && nlid == a && co.q.ang > 0.f) {
-                const V3<double> v1 = P0 - G.q, v2 = P1 - G.q;
-                ang = atan2(dot(cross(v1, v2), G.axis), dot(v1, v2));
-                if (ang < 0.0) ang += kTau;
-                if (fabs((double)co.q.ang - ang) > 1e-3) ok = false;  // the 0 / 2 pi branch is unclear
+            ContourOut<float> co;
+            WarpContact r;
+            if (!recorded_contour(b, p, a, co, r))
+                r = contact_warp<float, true, false>(g, (int)cnt, (int)(eb - off), nbf, &co);
+            bool fp64 = r.unsure || r.overflow || !r.valid || r.merged;
+            const Sph<double> A = {{A4.x, A4.y, A4.z}, A4.w}, B = {{B4.x, B4.y, B4.z}, B4.w};
+            const Sph<double> ic = intersection_circle(A, B);
+            const uint32_t base = slot * (uint32_t)kNetSlot;
+            if (!fp64 && co.full) {  // an uncut contact: one SAS edge, no vertex
+                if (lane == 0) {
+                    sl.e_ids[base] = net_edge_ids(a, bid, kNetNull, periodic, n);
+                    sl.e_len[base] = kTau * ic.r;
+                    sl.v_cnt[slot] = 0;
+                    sl.e_cnt[slot] = 1;
+                    sl.base[slot] = base;
+                }
+                continue;
             }
-            // elements with equal ids inside one contour (arcs of one contact, both ends of
-            // an arc cut by the same ball): the network keeps the first in contour order,
-            // which the FP64 contour decides
-            const bool on = lane < len;
-            const uint32_t third = arc ? kNetNull : co.q.rid;
-            const uint32_t vl = co.q.lid == a ? kNetNull : co.q.lid;
-            const unsigned long long ek = on ? (unsigned long long)third : (1ull << 40) + lane;
-            const unsigned long long vk = on ? ((unsigned long long)vl << 32 | third) : (1ull << 63) + lane;
-            // both matches on every lane: a collective that some lanes skip (a short-circuit
-            // ||) pairs the warp's later collectives wrongly
-            const unsigned me = __match_any_sync(kFull, ek), mv = __match_any_sync(kFull, vk);
-            const bool dup = __popc(me) > 1 || __popc(mv) > 1;
-            fp64 = __any_sync(kFull, !ok || dup);
-        }
-        if (fp64) {
+            const int len = co.len;
+            V3<double> P0 = mk<double>(0, 0, 0), P1 = P0;
+            double ang = 0.0;
+            bool arc = false;
+            if (!fp64) {
+                AdjPair G;
+                G.pa = A.c;
+                G.pb = B.c;
+                G.Ra = A.r;
+                G.Rb = B.r;
+                G.q = ic.c;
+                G.rho = ic.r;
+                G.axis = normalize(B.c - A.c);
+                G.a = a;
+                G.bid = bid;
+                sphere_of.bind(a, nid, nslot, cnt);
+                bool ok = true;
+                V3<double> y = widen(co.q.p);
+                if (lane < len) y = snap_vertex(G, y, co.q.lid, co.q.rid, sphere_of, &ok);
+                P0 = A.c + y;
+                const int nx = len > 0 ? (lane + 1 < len ? lane + 1 : 0) : 0;
+                P1 = mk<double>(__shfl_sync(kFull, P0.x, nx), __shfl_sync(kFull, P0.y, nx),
+                                __shfl_sync(kFull, P0.z, nx));
+                const uint32_t nlid = __shfl_sync(kFull, co.q.lid, nx);
+                arc = lane < len && co.q.rid == a;
+                if (arc && nlid == a && co.q.ang > 0.f) {
+                    const V3<double> v1 = P0 - G.q, v2 = P1 - G.q;
+                    ang = atan2(dot(cross(v1, v2), G.axis), dot(v1, v2));
+                    if (ang < 0.0) ang += kTau;
+                    if (fabs((double)co.q.ang - ang) > 1e-3) ok = false;  // the 0 / 2 pi branch is unclear
+                }
+                // elements with equal ids inside one contour (arcs of one contact, both ends of
+                // an arc cut by the same ball): the network keeps the first in contour order,
+                // which the FP64 contour decides
+                const bool on = lane < len;
+                const uint32_t third = arc ? kNetNull : co.q.rid;
+                const uint32_t vl = co.q.lid == a ? kNetNull : co.q.lid;
+                const unsigned long long ek = on ? (unsigned long long)third : (1ull << 40) + lane;
+                const unsigned long long vk = on ? ((unsigned long long)vl << 32 | third) : (1ull << 63) + lane;
+                // both matches on every lane: a collective that some lanes skip (a short-circuit
+                // ||) pairs the warp's later collectives wrongly
+                const unsigned me = __match_any_sync(kFull, ek), mv = __match_any_sync(kFull, vk);
+                const bool dup = __popc(me) > 1 || __popc(mv) > 1;
+                fp64 = __any_sync(kFull, !ok || dup);
+            }
+            if (fp64) {
+                if (lane == 0) {
+                    sl.v_cnt[slot] = 0;
+                    sl.e_cnt[slot] = 0;
+                    sl.base[slot] = base;
+                    fp64_list[atomicAdd(fp64_count, 1u)] = p;
+                }
+                continue;
+            }
+            if (lane < len) {
+                const Pt<float>& cp = co.q;
+                sl.e_ids[base + lane] = net_edge_ids(a, bid, arc ? kNetNull : cp.rid, periodic, n);
+                sl.e_len[base + lane] = arc ? ang * ic.r : norm(P1 - P0);
+                sl.v_ids[base + lane] =
+                    net_vertex_ids(a, bid, cp.lid == a ? kNetNull : cp.lid, arc ? kNetNull : cp.rid, periodic, n);
+                sl.v_xyz[3 * (size_t)(base + lane)] = P0.x;
+                sl.v_xyz[3 * (size_t)(base + lane) + 1] = P0.y;
+                sl.v_xyz[3 * (size_t)(base + lane) + 2] = P0.z;
+            }
             if (lane == 0) {
-                sl.v_cnt[slot] = 0;
-                sl.e_cnt[slot] = 0;
+                sl.v_cnt[slot] = (uint32_t)len;
+                sl.e_cnt[slot] = (uint32_t)len;
                 sl.base[slot] = base;
-                fp64_list[atomicAdd(fp64_count, 1u)] = p;
             }
-            continue;
-        }
-        if (lane < len) {
-            const Pt<float>& cp = co.q;
-            sl.e_ids[base + lane] = net_edge_ids(a, bid, arc ? kNetNull : cp.rid, periodic, n);
-            sl.e_len[base + lane] = arc ? ang * ic.r : norm(P1 - P0);
-            sl.v_ids[base + lane] =
-                net_vertex_ids(a, bid, cp.lid == a ? kNetNull : cp.lid, arc ? kNetNull : cp.rid, periodic, n);
-            sl.v_xyz[3 * (size_t)(base + lane)] = P0.x;
-            sl.v_xyz[3 * (size_t)(base + lane) + 1] = P0.y;
-            sl.v_xyz[3 * (size_t)(base + lane) + 2] = P0.z;
-        }
-        if (lane == 0) {
-            sl.v_cnt[slot] = (uint32_t)len;
-            sl.e_cnt[slot] = (uint32_t)len;
-            sl.base[slot] = base;
         }
     }
 }
@@ -361,7 +439,7 @@ __global__ void __launch_bounds__(kWarps * 32, VT_NET32_MINB)
 
 void launch_net_elements_f32(const DevBufs& b, uint32_t P, const uint32_t* voff, NetSlots sl, uint32_t* fp64_list,
                              uint32_t* fp64_count, cudaStream_t s) {
-    size_t g = (P + kWarps - 1) / kWarps;
+    size_t g = ((size_t)P + 32 * kWarps - 1) / (32 * kWarps);
     if (g < 1) g = 1;
     if (g > 148 * 64) g = 148 * 64;
     k_net_elements32<<<(unsigned)g, kWarps * 32, 0, s>>>(b, P, b.fp32_band, voff, sl, fp64_list, fp64_count);
@@ -370,7 +448,7 @@ void launch_net_elements_f32(const DevBufs& b, uint32_t P, const uint32_t* voff,
 
 void launch_adjoint_f32(const DevBufs& b, uint32_t P, const double* u_contact, const double* w_eff,
                         const double* v_eff, double* grad, cudaStream_t s) {
-    size_t g = (P + kWarps - 1) / kWarps;
+    size_t g = ((size_t)P + 32 * kWarps - 1) / (32 * kWarps);
     if (g < 1) g = 1;
     if (g > 148 * 64) g = 148 * 64;
     if (v_eff)
