@@ -162,8 +162,7 @@ struct vt_engine {
     // tessellation network (with_cell_vertices) of the last call
     bool network = false;
     uint64_t net_nv = 0, net_ne = 0;
-    DBuf<uint32_t> net_flags, net_voff, net_vcnt, net_ecnt, net_off_v, net_off_e, net_src, net_src2, net_uflags,
-        net_uoff;
+    DBuf<uint32_t> net_flags, net_voff, net_vcnt, net_ecnt, net_off_v, net_off_e;
     DBuf<uint4> net_vids, net_eids, net_ov_vids, net_ov_eids;
     DBuf<double> net_vxyz, net_elen, net_ov_vxyz, net_ov_elen;
     DBuf<uint32_t> net_base, net_ov_list, net_fp64_list;
@@ -175,46 +174,40 @@ struct vt_engine {
     DBuf<uint2> rec_ids;
     DBuf<uint32_t> rec_off, rec_meta;
     NetSlots net_slots{};
-    DBuf<unsigned long long> net_hi, net_lo, net_ka, net_kb, net_hs, net_ls;
-    DBuf<uint32_t> net_ia, net_ib, net_order;
-    DBuf<uint8_t> net_temp;
+    DBuf<uint32_t> net_bcnt, net_boff, net_bcur, net_bucnt, net_buoff, net_big, net_bsrc;
+    DBuf<unsigned long long> net_k1, net_k2;
     DBuf<uint32_t> out_net_vid, out_net_eid;
     DBuf<double> out_net_vxyz, out_net_elen;
 
-    // one element type: sort the dense keys, keep the first of equal ids, gather
-    uint64_t net_unique(uint32_t m, int vertices) {
+    // one element type (m elements of V pairs): bucket by first id, sort the buckets, keep
+    // the first of equal ids, gather
+    uint64_t net_unique(uint32_t V, const uint32_t* cnt, const uint32_t* off, uint32_t m, int vertices) {
         if (m == 0) return 0;
-        net_ka.ensure(m);
-        net_kb.ensure(m);
-        net_hs.ensure(m);
-        net_ls.ensure(m);
-        net_ia.ensure(m);
-        net_ib.ensure(m);
-        net_order.ensure(m);
-        const size_t tb = net_sort_temp_bytes(m);
-        net_temp.ensure(tb);
-        NetSortBufs t{net_ka.p, net_kb.p, net_hs.p, net_ls.p, net_ia.p, net_ib.p, net_order.p, net_temp.p, tb};
-        const int B = net_key_bits(bufs.n);
-        net_sort(m, net_hi.p, net_lo.p, 2 * B, vertices ? 2 * B : B, t, stream);
-        net_uflags.ensure(m + 1);
-        net_uoff.ensure(m + 2);
-        launch_net_unique(m, t, net_uflags.p, stream);
-        ensure_scan(m + 1);
-        scan_u32(net_uflags.p, net_uoff.p, m, scan_tmp.p, stream);
-        VT_CUDA(cudaMemcpyAsync(h_words + 15, net_uoff.p + m, 4, cudaMemcpyDeviceToHost, stream));
+        const uint32_t n = (uint32_t)bufs.n, NB = n + 1;
+        net_bcnt.ensure(NB);
+        net_boff.ensure(NB + 1);
+        net_bcur.ensure(NB);
+        net_bucnt.ensure(NB);
+        net_buoff.ensure(NB + 1);
+        net_big.ensure(NB + 1);
+        net_k1.ensure(m);
+        net_k2.ensure(m);
+        net_bsrc.ensure(m);
+        NetBuckets t{net_bcnt.p, net_boff.p, net_bcur.p, net_bucnt.p, net_buoff.p, net_big.p,
+                     net_k1.p,   net_k2.p,   net_bsrc.p};
+        ensure_scan(NB + 1);
+        launch_net_dedup(V, cnt, off, net_slots, vertices, n, t, scan_tmp.p, stream);
+        VT_CUDA(cudaMemcpyAsync(h_words + 15, net_buoff.p + NB, 4, cudaMemcpyDeviceToHost, stream));
         sync();
         const uint32_t U = h_words[15];
-        net_src2.ensure(m);
         if (vertices) {
             out_net_vid.ensure(4 * (size_t)U + 4);
             out_net_vxyz.ensure(3 * (size_t)U + 3);
-            launch_net_gather(m, net_uoff.p, net_order.p, net_src.p, net_src2.p, net_slots, 1, out_net_vid.p,
-                              out_net_vxyz.p, stream);
+            launch_net_dedup_gather(n, t, net_slots, 1, out_net_vid.p, out_net_vxyz.p, stream);
         } else {
             out_net_eid.ensure(3 * (size_t)U + 3);
             out_net_elen.ensure((size_t)U + 1);
-            launch_net_gather(m, net_uoff.p, net_order.p, net_src.p, net_src2.p, net_slots, 0, out_net_eid.p,
-                              out_net_elen.p, stream);
+            launch_net_dedup_gather(n, t, net_slots, 0, out_net_eid.p, out_net_elen.p, stream);
         }
         return U;
     }
@@ -277,18 +270,8 @@ struct vt_engine {
         VT_CUDA(cudaMemcpyAsync(h_words + 14, net_off_e.p + V, 4, cudaMemcpyDeviceToHost, stream));
         sync();
         const uint32_t Mv = h_words[13], Me = h_words[14];
-        const uint32_t mmax = std::max(Mv, Me) + 1;
-        net_hi.ensure(mmax);
-        net_lo.ensure(mmax);
-        net_src.ensure(mmax);
-        if (Mv) {
-            launch_net_keys(V, net_vcnt.p, net_off_v.p, sl, 1, b.n, net_hi.p, net_lo.p, net_src.p, stream);
-            net_nv = net_unique(Mv, 1);
-        }
-        if (Me) {
-            launch_net_keys(V, net_ecnt.p, net_off_e.p, sl, 0, b.n, net_hi.p, net_lo.p, net_src.p, stream);
-            net_ne = net_unique(Me, 0);
-        }
+        net_nv = net_unique(V, net_vcnt.p, net_off_v.p, Mv, 1);
+        net_ne = net_unique(V, net_ecnt.p, net_off_e.p, Me, 0);
         return VT_OK;
     }
 

@@ -8,13 +8,12 @@
 //      right id with a's id as NULL), position; an uncut contact emits one SAS edge; a
 //      contour that outgrows the warp is listed for the serial kernel (vt_contact64.cu);
 //   2. ids are taken mod n for periodic images and sorted within the element;
-//   3. elements are compacted, stably sorted by their ids (radix sort on two key words,
-//      low word first; an id takes B = bits(n) bits with NULL mapped to n, so it still
-//      sorts after every ball id, and a word holds two ids: 2B bits instead of 64) and
-//      deduplicated keeping the first of equal ids, i.e. the first in pair and contour
-//      order (the reference sorts unstably and keeps an unspecified one).
-#include <cub/cub.cuh>
-
+//   3. elements are put in id order and deduplicated keeping the first of equal ids, i.e.
+//      the first in pair and contour order (the reference sorts unstably and keeps an
+//      unspecified one): bucketed by their first id (a counting pass, a scan, a scatter),
+//      each bucket sorted by (remaining ids, dense index) -- a warp's bitonic sort in
+//      registers for buckets of up to 128 elements, a block's otherwise -- and the first of
+//      each run of equal ids kept.  NULL (0xffffffff) sorts after every ball id.
 #include "vt_contact.cuh"
 #include "vt_pipeline.cuh"
 
@@ -109,56 +108,6 @@ __global__ void __launch_bounds__(kWarps * 32)
     }
 }
 
-// dense arrays: key words (hi, lo) and the element's index; thread per pair.  An id
-// takes B bits, NULL (0xffffffff) becoming n, above every ball id.
-__device__ __forceinline__ unsigned long long net_key_id(uint32_t id, uint32_t n) {
-    return id == kNetNull ? (unsigned long long)n : (unsigned long long)id;
-}
-__global__ void k_net_compact(uint32_t V, const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ off,
-                              NetSlots sl, int vertices, uint32_t n, int B, unsigned long long* __restrict__ key_hi,
-                              unsigned long long* __restrict__ key_lo, uint32_t* __restrict__ src) {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
-        const uint32_t c = cnt[v], o = off[v], base = sl.base[v];
-        for (uint32_t k = 0; k < c; ++k) {
-            const uint32_t i = base + k;
-            const uint4 id = vertices ? net_vid(sl, i) : net_eid(sl, i);
-            key_hi[o + k] = (net_key_id(id.x, n) << B) | net_key_id(id.y, n);
-            key_lo[o + k] = vertices ? ((net_key_id(id.z, n) << B) | net_key_id(id.w, n)) : net_key_id(id.z, n);
-            src[o + k] = i;
-        }
-    }
-}
-__global__ void k_first_flags(const unsigned long long* __restrict__ hi, const unsigned long long* __restrict__ lo,
-                              uint32_t m, uint32_t* __restrict__ flags) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
-        flags[i] = (i == 0 || hi[i] != hi[i - 1] || lo[i] != lo[i - 1]) ? 1u : 0u;
-}
-__global__ void k_net_gather_v(uint32_t m, const uint32_t* __restrict__ uoff, const uint32_t* __restrict__ src,
-                               NetSlots sl, uint32_t* __restrict__ out_ids, double* __restrict__ out_xyz) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-        if (uoff[i + 1] == uoff[i]) continue;
-        const uint32_t o = uoff[i], s = src[i];
-        const uint4 id = net_vid(sl, s);
-        out_ids[4 * (size_t)o] = id.x;
-        out_ids[4 * (size_t)o + 1] = id.y;
-        out_ids[4 * (size_t)o + 2] = id.z;
-        out_ids[4 * (size_t)o + 3] = id.w;
-        for (int k = 0; k < 3; ++k) out_xyz[3 * (size_t)o + k] = net_vxyz(sl, s, k);
-    }
-}
-__global__ void k_net_gather_e(uint32_t m, const uint32_t* __restrict__ uoff, const uint32_t* __restrict__ src,
-                               NetSlots sl, uint32_t* __restrict__ out_ids, double* __restrict__ out_len) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-        if (uoff[i + 1] == uoff[i]) continue;
-        const uint32_t o = uoff[i], s = src[i];
-        const uint4 id = net_eid(sl, s);
-        out_ids[3 * (size_t)o] = id.x;
-        out_ids[3 * (size_t)o + 1] = id.y;
-        out_ids[3 * (size_t)o + 2] = id.z;
-        out_len[o] = net_elen(sl, s);
-    }
-}
-
 int gb(size_t n) { return grid_blocks(n, 256, 148 * 16); }
 
 }  // namespace
@@ -182,81 +131,309 @@ void set_hex_table_network() {
     cudaMemcpyToSymbol(c_hex_n, &n, sizeof(int));
 }
 
-int net_key_bits(uint32_t n) {
-    int B = 1;
-    while (B < 32 && ((uint64_t)1 << B) <= (uint64_t)n) ++B;  // 2^B > n: ids 0..n-1 and NULL as n
-    return B;
-}
-void launch_net_keys(uint32_t V, const uint32_t* cnt, const uint32_t* off, const NetSlots& sl, int vertices,
-                     uint32_t n, unsigned long long* key_hi, unsigned long long* key_lo, uint32_t* src,
-                     cudaStream_t s) {
-    k_net_compact<<<gb(V), 256, 0, s>>>(V, cnt, off, sl, vertices, n, net_key_bits(n), key_hi, key_lo, src);
-    count_launch();
-}
-
-size_t net_sort_temp_bytes(uint32_t m) {
-    size_t bytes = 0;
-    cub::DoubleBuffer<unsigned long long> k(nullptr, nullptr);
-    cub::DoubleBuffer<uint32_t> v(nullptr, nullptr);
-    cub::DeviceRadixSort::SortPairs(nullptr, bytes, k, v, (int)(m > 0 ? m : 1));
-    return bytes + 256;
-}
-
+// ---- deduplication: bucket by the first id, sort each bucket, keep the first of equal ids ----
 namespace {
-__global__ void k_iota(uint32_t m, uint32_t* __restrict__ out) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) out[i] = i;
+
+constexpr int kBigSmem = 2048;  // bucket size the block sort holds in shared memory
+
+__device__ __forceinline__ uint4 net_ids(const NetSlots& sl, uint32_t i, int vertices) {
+    return vertices ? net_vid(sl, i) : net_eid(sl, i);
 }
-__global__ void k_gather_u64(uint32_t m, const uint32_t* __restrict__ idx, const unsigned long long* __restrict__ in,
-                             unsigned long long* __restrict__ out) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) out[i] = in[idx[i]];
+__device__ __forceinline__ uint32_t net_bucket(uint32_t id0, uint32_t n) { return id0 < n ? id0 : n; }
+
+// The counting (FILL = false) and scatter (FILL = true) passes, lanes over the dense
+// elements: a warp takes 32 consecutive pair slots, whose elements are the dense range
+// [off[v0], off[v0 + 32]), and finds each lane's slot by a shuffle binary search over the
+// slots' offsets (coalesced reads, every lane busy although a contour has ~5 vertices).
+// Lanes of one bucket share one atomic; the scatter places them in lane order after it.
+template <bool FILL>
+__global__ void k_nb_pass(uint32_t V, const uint32_t* __restrict__ off, NetSlots sl, int vertices, uint32_t n,
+                          NetBuckets t) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t wpb = blockDim.x >> 5;
+    const uint32_t groups = (V + 31) / 32;
+    for (uint32_t g = blockIdx.x * wpb + (threadIdx.x >> 5); g < groups; g += gridDim.x * wpb) {
+        const uint32_t v0 = g * 32, v = v0 + lane;
+        const uint32_t o = v < V ? off[v] : 0xffffffffu;  // non-decreasing over the lanes
+        const uint32_t base = v < V ? sl.base[v] : 0u;
+        const uint32_t d0 = __shfl_sync(kFull, o, 0);
+        const uint32_t d1 = off[v0 + 32 < V ? v0 + 32 : V];
+        for (uint32_t j0 = d0; j0 < d1; j0 += 32) {
+            const uint32_t j = j0 + lane;  // dense index
+            const bool on = j < d1;
+            int L = 0;  // the last slot whose offset is <= j
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1)
+                if (__shfl_sync(kFull, o, L + step) <= j) L += step;
+            const uint32_t e = __shfl_sync(kFull, base, L) + (j - __shfl_sync(kFull, o, L));
+            uint4 id = make_uint4(0u, 0u, 0u, 0u);
+            uint32_t bk = 0xffffffffu;
+            if (on) {
+                id = net_ids(sl, e, vertices);
+                bk = net_bucket(id.x, n);
+            }
+            const unsigned grp = __match_any_sync(kFull, bk);
+            const int leader = __ffs(grp) - 1;
+            uint32_t r = 0;
+            if (on && lane == leader) r = atomicAdd(FILL ? &t.cur[bk] : &t.cnt[bk], (uint32_t)__popc(grp));
+            if constexpr (FILL) {
+                r = __shfl_sync(kFull, r, leader);
+                if (on) {
+                    const uint32_t pos = t.off[bk] + r + (uint32_t)__popc(grp & ((1u << lane) - 1u));
+                    t.k1[pos] = (unsigned long long)id.y << 32 | id.z;
+                    t.k2[pos] = vertices ? ((unsigned long long)id.w << 32 | j) : (unsigned long long)j;
+                    t.src[pos] = e;
+                }
+            }
+        }
+    }
 }
-__global__ void k_gather_u32(uint32_t m, const uint32_t* __restrict__ idx, const uint32_t* __restrict__ in,
-                             uint32_t* __restrict__ out) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) out[i] = in[idx[i]];
+
+// (x1, x2) < (y1, y2) lexicographically
+__device__ __forceinline__ bool key_less(unsigned long long x1, unsigned long long x2, unsigned long long y1,
+                                         unsigned long long y2) {
+    return x1 < y1 || (x1 == y1 && x2 < y2);
 }
+// equal ids: k1 and, for vertices, the high word of k2 (the low word is the dense index)
+__device__ __forceinline__ bool same_ids(unsigned long long x1, unsigned long long x2, unsigned long long y1,
+                                         unsigned long long y2, int vertices) {
+    return x1 == y1 && (!vertices || (x2 >> 32) == (y2 >> 32));
+}
+
+// Bitonic sort of the N = 32 E elements a warp holds in registers, element index
+// i = 32 r + lane in register r: distances below 32 exchange through shuffles, larger
+// ones between a thread's own registers.  Elements past the bucket hold the largest key.
+template <int E>
+__device__ __forceinline__ void warp_bitonic(unsigned long long (&x1)[E], unsigned long long (&x2)[E],
+                                             uint32_t (&s)[E]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 2; k <= 32 * E; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j >= 32) {
+#pragma unroll
+                for (int r = 0; r < E; ++r) {
+                    const int r2 = r ^ (j >> 5);
+                    if (r2 < r) continue;
+                    const bool up = ((32 * r + lane) & k) == 0;  // this block ascending
+                    if (up ? key_less(x1[r2], x2[r2], x1[r], x2[r]) : key_less(x1[r], x2[r], x1[r2], x2[r2])) {
+                        const unsigned long long t1 = x1[r], t2 = x2[r];
+                        const uint32_t ts = s[r];
+                        x1[r] = x1[r2];
+                        x2[r] = x2[r2];
+                        s[r] = s[r2];
+                        x1[r2] = t1;
+                        x2[r2] = t2;
+                        s[r2] = ts;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < E; ++r) {
+                    const unsigned long long y1 = __shfl_xor_sync(kFull, x1[r], j), y2 = __shfl_xor_sync(kFull, x2[r], j);
+                    const uint32_t ys = __shfl_xor_sync(kFull, s[r], j);
+                    const int i = 32 * r + lane;
+                    const bool keep_min = ((i & j) == 0) == ((i & k) == 0);
+                    if (keep_min ? key_less(y1, y2, x1[r], x2[r]) : key_less(x1[r], x2[r], y1, y2)) {
+                        x1[r] = y1;
+                        x2[r] = y2;
+                        s[r] = ys;
+                    }
+                }
+            }
+        }
+    }
+}
+
+// One bucket of c <= 32 E elements at o: sorted in registers, then the first of each run
+// of equal ids written, in order, to the start of the bucket's src range.
+template <int E>
+__device__ __forceinline__ void warp_bucket(NetBuckets& t, uint32_t bk, uint32_t o, uint32_t c, int vertices) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long x1[E], x2[E];
+    uint32_t s[E];
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        const uint32_t i = 32 * r + lane;
+        x1[r] = x2[r] = ~0ull;
+        s[r] = 0;
+        if (i < c) {
+            x1[r] = t.k1[o + i];
+            x2[r] = t.k2[o + i];
+            s[r] = t.src[o + i];
+        }
+    }
+    if (c > 1) warp_bitonic<E>(x1, x2, s);
+    uint32_t u = 0;
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        const uint32_t i = 32 * r + lane;
+        unsigned long long p1 = __shfl_up_sync(kFull, x1[r], 1), p2 = __shfl_up_sync(kFull, x2[r], 1);
+        if (r > 0) {  // lane 0's predecessor is lane 31 of the previous register
+            const unsigned long long q1 = __shfl_sync(kFull, x1[r > 0 ? r - 1 : 0], 31);
+            const unsigned long long q2 = __shfl_sync(kFull, x2[r > 0 ? r - 1 : 0], 31);
+            if (lane == 0) {
+                p1 = q1;
+                p2 = q2;
+            }
+        }
+        const bool first = i < c && (i == 0 || !same_ids(p1, p2, x1[r], x2[r], vertices));
+        const unsigned fm = __ballot_sync(kFull, first);
+        if (first) t.src[o + u + __popc(fm & ((1u << lane) - 1u))] = s[r];
+        u += (uint32_t)__popc(fm);
+    }
+    if (lane == 0) t.ucnt[bk] = u;
+}
+
+// warp per bucket of at most kWarpSort elements (1, 2 or 4 per lane); larger buckets are
+// listed for k_nb_sort_big
+constexpr uint32_t kWarpSort = 128;
+__global__ void k_nb_sort_small(uint32_t NB, int vertices, NetBuckets t) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t wpb = blockDim.x >> 5;
+    for (uint32_t bk = blockIdx.x * wpb + (threadIdx.x >> 5); bk < NB; bk += gridDim.x * wpb) {
+        const uint32_t o = t.off[bk], c = t.off[bk + 1] - o;
+        if (c <= 32)
+            warp_bucket<1>(t, bk, o, c, vertices);
+        else if (c <= 64)
+            warp_bucket<2>(t, bk, o, c, vertices);
+        else if (c <= kWarpSort)
+            warp_bucket<4>(t, bk, o, c, vertices);
+        else if (lane == 0)
+            t.big[atomicAdd(t.big + NB, 1u)] = bk;
+    }
+}
+
+// One bitonic sort of c elements by (k1, k2) across a block, all comparators ascending
+// (each merge starts by comparing mirrored positions), so that positions past c act as
+// the largest keys and are never touched: sorts any c in place.
+__device__ void block_bitonic(unsigned long long* k1, unsigned long long* k2, uint32_t* src, uint32_t c) {
+    uint32_t N = 1;
+    while (N < c) N <<= 1;
+    for (uint32_t k = 2; k <= N; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t q = threadIdx.x; q < N / 2; q += blockDim.x) {
+                const uint32_t i = (q / j) * 2 * j + (q % j);
+                const uint32_t l = j == (k >> 1) ? (i ^ (k - 1)) : (i + j);
+                if (l < c && key_less(k1[l], k2[l], k1[i], k2[i])) {
+                    const unsigned long long t1 = k1[i], t2 = k2[i];
+                    const uint32_t ts = src[i];
+                    k1[i] = k1[l];
+                    k2[i] = k2[l];
+                    src[i] = src[l];
+                    k1[l] = t1;
+                    k2[l] = t2;
+                    src[l] = ts;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// block per listed bucket of more than kWarpSort elements: sorted in shared memory up to
+// kBigSmem elements, in place in global memory beyond; then warp 0 writes the first of
+// each run of equal ids to the start of the bucket's src range (positions at or before
+// the one being read, so the in-place form reads every element before it is overwritten).
+__global__ void __launch_bounds__(256) k_nb_sort_big(uint32_t NB, int vertices, NetBuckets t) {
+    __shared__ unsigned long long s1[kBigSmem], s2[kBigSmem];
+    __shared__ uint32_t ss[kBigSmem];
+    const uint32_t count = t.big[NB];
+    const int lane = threadIdx.x & 31;
+    for (uint32_t it = blockIdx.x; it < count; it += gridDim.x) {
+        const uint32_t bk = t.big[it];
+        const uint32_t o = t.off[bk], c = t.off[bk + 1] - o;
+        unsigned long long *K1 = t.k1 + o, *K2 = t.k2 + o;
+        uint32_t* S = t.src + o;
+        if (c <= (uint32_t)kBigSmem) {
+            for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+                s1[i] = K1[i];
+                s2[i] = K2[i];
+                ss[i] = S[i];
+            }
+            __syncthreads();
+            K1 = s1;
+            K2 = s2;
+            S = ss;
+        }
+        block_bitonic(K1, K2, S, c);
+        if (threadIdx.x < 32) {
+            uint32_t u = 0;
+            unsigned long long q1 = 0, q2 = 0;
+            for (uint32_t base = 0; base < c; base += 32) {
+                const uint32_t j = base + lane;
+                const bool in = j < c;
+                const unsigned long long x1 = in ? K1[j] : ~0ull, x2 = in ? K2[j] : ~0ull;
+                const uint32_t s = in ? S[j] : 0u;
+                unsigned long long p1 = __shfl_up_sync(kFull, x1, 1), p2 = __shfl_up_sync(kFull, x2, 1);
+                if (lane == 0) {
+                    p1 = q1;
+                    p2 = q2;
+                }
+                const bool first = in && (j == 0 || !same_ids(p1, p2, x1, x2, vertices));
+                const unsigned fm = __ballot_sync(kFull, first);
+                if (first) t.src[o + u + __popc(fm & ((1u << lane) - 1u))] = s;
+                u += (uint32_t)__popc(fm);
+                q1 = __shfl_sync(kFull, x1, 31);
+                q2 = __shfl_sync(kFull, x2, 31);
+            }
+            if (lane == 0) t.ucnt[bk] = u;
+        }
+        __syncthreads();
+    }
+}
+
+// warp per bucket: its unique elements to the output, at uoff[bucket]
+__global__ void k_nb_gather(uint32_t NB, NetBuckets t, NetSlots sl, int vertices, uint32_t* __restrict__ out_ids,
+                            double* __restrict__ out_vals) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t wpb = blockDim.x >> 5;
+    for (uint32_t bk = blockIdx.x * wpb + (threadIdx.x >> 5); bk < NB; bk += gridDim.x * wpb) {
+        const uint32_t u = t.ucnt[bk], o = t.off[bk], uo = t.uoff[bk];
+        for (uint32_t j = lane; j < u; j += 32) {
+            const uint32_t s = t.src[o + j];
+            const size_t w = (size_t)uo + j;
+            if (vertices) {
+                const uint4 id = net_vid(sl, s);
+                out_ids[4 * w] = id.x;
+                out_ids[4 * w + 1] = id.y;
+                out_ids[4 * w + 2] = id.z;
+                out_ids[4 * w + 3] = id.w;
+                for (int k = 0; k < 3; ++k) out_vals[3 * w + k] = net_vxyz(sl, s, k);
+            } else {
+                const uint4 id = net_eid(sl, s);
+                out_ids[3 * w] = id.x;
+                out_ids[3 * w + 1] = id.y;
+                out_ids[3 * w + 2] = id.z;
+                out_vals[w] = net_elen(sl, s);
+            }
+        }
+    }
+}
+
+int gw(size_t items) { return grid_blocks(items, 8, 148 * 32); }  // 8 warps per 256-thread block
+
 }  // namespace
 
-// Stable LSD sort of m keys (hi, lo): by lo, then by hi, carrying the dense index; only
-// the low bits_lo / bits_hi bits of the words are sorted on (the rest are zero).  On
-// return hi_s/lo_s hold the sorted keys and order[i] the dense index of sorted element i.
-void net_sort(uint32_t m, const unsigned long long* hi, const unsigned long long* lo, int bits_hi, int bits_lo,
-              NetSortBufs t, cudaStream_t s) {
-    if (m == 0) return;
-    k_iota<<<gb(m), 256, 0, s>>>(m, t.idx_a); count_launch();
-    cudaMemcpyAsync(t.key_a, lo, 8 * (size_t)m, cudaMemcpyDeviceToDevice, s);
-    size_t tb = t.temp_bytes;
-    {
-        cub::DoubleBuffer<unsigned long long> k(t.key_a, t.key_b);
-        cub::DoubleBuffer<uint32_t> v(t.idx_a, t.idx_b);
-        cub::DeviceRadixSort::SortPairs(t.temp, tb, k, v, (int)m, 0, bits_lo, s);
-        count_launch();
-        if (v.Current() != t.idx_a) cudaMemcpyAsync(t.idx_a, v.Current(), 4 * (size_t)m, cudaMemcpyDeviceToDevice, s);
-    }
-    k_gather_u64<<<gb(m), 256, 0, s>>>(m, t.idx_a, hi, t.key_a); count_launch();
-    {
-        tb = t.temp_bytes;
-        cub::DoubleBuffer<unsigned long long> k(t.key_a, t.key_b);
-        cub::DoubleBuffer<uint32_t> v(t.idx_a, t.idx_b);
-        cub::DeviceRadixSort::SortPairs(t.temp, tb, k, v, (int)m, 0, bits_hi, s);
-        count_launch();
-        if (k.Current() != t.hi_s) cudaMemcpyAsync(t.hi_s, k.Current(), 8 * (size_t)m, cudaMemcpyDeviceToDevice, s);
-        if (v.Current() != t.order) cudaMemcpyAsync(t.order, v.Current(), 4 * (size_t)m, cudaMemcpyDeviceToDevice, s);
-    }
-    k_gather_u64<<<gb(m), 256, 0, s>>>(m, t.order, lo, t.lo_s); count_launch();
+void launch_net_dedup(uint32_t V, const uint32_t* cnt, const uint32_t* off, const NetSlots& sl, int vertices,
+                      uint32_t n, NetBuckets t, uint32_t* scan_tmp, cudaStream_t s) {
+    const uint32_t NB = n + 1;
+    cudaMemsetAsync(t.cnt, 0, 4 * (size_t)NB, s);
+    cudaMemsetAsync(t.cur, 0, 4 * (size_t)NB, s);
+    cudaMemsetAsync(t.big + NB, 0, 4, s);
+    const size_t groups = ((size_t)V + 31) / 32;
+    k_nb_pass<false><<<gw(groups), 256, 0, s>>>(V, off, sl, vertices, n, t); count_launch();
+    scan_u32(t.cnt, t.off, NB, scan_tmp, s);
+    k_nb_pass<true><<<gw(groups), 256, 0, s>>>(V, off, sl, vertices, n, t); count_launch();
+    k_nb_sort_small<<<gw(NB), 256, 0, s>>>(NB, vertices, t); count_launch();
+    k_nb_sort_big<<<148 * 4, 256, 0, s>>>(NB, vertices, t); count_launch();
+    scan_u32(t.ucnt, t.uoff, NB, scan_tmp, s);
 }
-
-void launch_net_unique(uint32_t m, const NetSortBufs& t, uint32_t* flags, cudaStream_t s) {
-    k_first_flags<<<gb(m), 256, 0, s>>>(t.hi_s, t.lo_s, m, flags); count_launch();
-}
-void launch_net_gather(uint32_t m, const uint32_t* uoff, const uint32_t* order, const uint32_t* src_dense,
-                       uint32_t* src_tmp, const NetSlots& sl, int vertices, uint32_t* out_ids, double* out_vals,
-                       cudaStream_t s) {
-    k_gather_u32<<<gb(m), 256, 0, s>>>(m, order, src_dense, src_tmp); count_launch();
-    if (vertices)
-        k_net_gather_v<<<gb(m), 256, 0, s>>>(m, uoff, src_tmp, sl, out_ids, out_vals);
-    else
-        k_net_gather_e<<<gb(m), 256, 0, s>>>(m, uoff, src_tmp, sl, out_ids, out_vals);
-    count_launch();
+void launch_net_dedup_gather(uint32_t n, const NetBuckets& t, const NetSlots& sl, int vertices, uint32_t* out_ids,
+                             double* out_vals, cudaStream_t s) {
+    const uint32_t NB = n + 1;
+    k_nb_gather<<<gw(NB), 256, 0, s>>>(NB, t, sl, vertices, out_ids, out_vals); count_launch();
 }
 
 }  // namespace vt

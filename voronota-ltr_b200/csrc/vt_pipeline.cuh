@@ -365,11 +365,18 @@ __device__ __forceinline__ uint4 net_vertex_ids(uint32_t a, uint32_t b, uint32_t
     net_cswap(v1, v2);
     return make_uint4(v0, v1, v2, v3);
 }
-struct NetSortBufs {
-    unsigned long long *key_a, *key_b, *hi_s, *lo_s;
-    uint32_t *idx_a, *idx_b, *order;
-    void* temp;
-    size_t temp_bytes;
+// Deduplication buffers of one element type (m elements, n + 1 buckets by first id).
+struct NetBuckets {
+    uint32_t* cnt;   // [n + 1] elements per bucket
+    uint32_t* off;   // [n + 2] exclusive scan of cnt
+    uint32_t* cur;   // [n + 1] fill cursors
+    uint32_t* ucnt;  // [n + 1] distinct elements per bucket
+    uint32_t* uoff;  // [n + 2] exclusive scan of ucnt
+    uint32_t* big;   // [n + 2] buckets too large for a warp's sort; [n + 1] is their count
+    unsigned long long* k1;  // [m] ids 1 and 2 of the element
+    unsigned long long* k2;  // [m] vertices: id 3 and the dense index; edges: the dense index
+    uint32_t* src;   // [m] element index in the slot arrays; after the sort each bucket's range
+                     // starts with its distinct elements in id order
 };
 void launch_valid_flags(const DevBufs& b, uint32_t P, uint32_t* flags, cudaStream_t s);
 // FP64 elements of every valid pair, or (list != null) of the *count pairs listed
@@ -382,21 +389,15 @@ void launch_net_elements_f32(const DevBufs& b, uint32_t P, const uint32_t* voff,
 // the pairs of ov_list through the serial contour (vt_contact64.cu); at most ov_cap
 void launch_net_serial(const DevBufs& b, const uint32_t* voff, NetSlots slots, cudaStream_t s);
 size_t net_slot_capacity();
-// dense keys of V pairs' elements (off = exclusive scan of cnt) and their element indices;
-// ids packed net_key_bits(n) bits each (NULL as n)
-int net_key_bits(uint32_t n);
-void launch_net_keys(uint32_t V, const uint32_t* cnt, const uint32_t* off, const NetSlots& slots, int vertices,
-                     uint32_t n, unsigned long long* key_hi, unsigned long long* key_lo, uint32_t* src,
-                     cudaStream_t s);
-size_t net_sort_temp_bytes(uint32_t m);
-void net_sort(uint32_t m, const unsigned long long* hi, const unsigned long long* lo, int bits_hi, int bits_lo,
-              NetSortBufs t, cudaStream_t s);
-// flags[i] = 1 for the first of each run of equal keys
-void launch_net_unique(uint32_t m, const NetSortBufs& t, uint32_t* flags, cudaStream_t s);
-// unique sorted elements (uoff = exclusive scan of the flags) to the output arrays
-void launch_net_gather(uint32_t m, const uint32_t* uoff, const uint32_t* order, const uint32_t* src_dense,
-                       uint32_t* src_tmp, const NetSlots& slots, int vertices, uint32_t* out_ids, double* out_vals,
-                       cudaStream_t s);
+// The distinct elements of V pairs (off = exclusive scan of cnt, the dense order: pair
+// then contour order) in id order, keeping the first in dense order of equal ids:
+// elements bucketed by their first id (ids are sorted within an element), each bucket
+// sorted by (the other ids, dense index); t.uoff[n + 1] is the distinct count.
+void launch_net_dedup(uint32_t V, const uint32_t* cnt, const uint32_t* off, const NetSlots& slots, int vertices,
+                      uint32_t n, NetBuckets t, uint32_t* scan_tmp, cudaStream_t s);
+// the distinct elements to the output arrays (ids, and positions or lengths)
+void launch_net_dedup_gather(uint32_t n, const NetBuckets& t, const NetSlots& slots, int vertices,
+                             uint32_t* out_ids, double* out_vals, cudaStream_t s);
 
 // ---- contact kernels (vt_contact64.cu / vt_contact32.cu) ----
 // mode: 0 = all pairs; 1 = pairs listed in redo_list (count on device)
