@@ -135,6 +135,10 @@ int vt_engine_compute_host(vt_engine* e, const double* xyzr, uint64_t n, double 
 int vt_engine_download(vt_engine* e, vt_result** out);
 /* Engine calls also build the tessellation network (on) or not (off, the default). */
 int vt_engine_set_network(vt_engine* e, int on);
+/* The network's vertex deduplication packs the three ids after the first into one 64-bit
+ * key while 3 bits(n) <= 64 (fewer than 2^21 balls) and uses two words beyond; on: always
+ * two words (the same results; lets tests cover that form on small inputs). */
+int vt_engine_set_network_wide_keys(vt_engine* e, int on);
 
 typedef struct vt_stats {
     uint64_t num_balls, num_slots, num_entries, num_pairs, num_contacts, num_cells;

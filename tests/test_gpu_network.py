@@ -140,3 +140,38 @@ def test_fp32_network_after_larger_calls():
     balls, side = W.periodic_box_balls(3000, 0.033, 1.52, seed=9)
     for _ in range(2):
         check_network(balls, 1.4, "fp32", periodic_box={"corners": [(0, 0, 0), (side, side, side)]})
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_large_deduplication_buckets(prec):
+    """The big ball (id 0) among a lattice's small balls: its cell's vertices and edges all
+    fall into the bucket of id 0, several thousand elements (the block sort in global
+    memory); the sunflower's two large balls give buckets of ~1,400 (the block sort in
+    shared memory)."""
+    from common import big_ball_in_lattice
+    check_network(big_ball_in_lattice(), 1.4, prec)
+    check_network(sunflower(120, rr=0.12, rho=3.3), 0.5, prec)
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_deduplication_key_forms(prec):
+    """The vertex deduplication keys: three ids packed into one word (below 2^21 balls) and
+    the two-word form (taken from 2^21 balls on, forced here) give the same network."""
+    from common import big_ball_in_lattice
+    import torch
+    pballs, side = W.periodic_box_balls(3000, 0.033, 1.52, seed=9)
+    for balls, probe, box in [(W.lattice_balls(4000, 2), 1.4, None), (big_ball_in_lattice(), 1.4, None),
+                              (pballs, 1.4, {"corners": [(0, 0, 0), (side, side, side)]})]:
+        out = []
+        for wide in (False, True):
+            e = V.Engine()
+            e.set_network(True)
+            e.set_network_wide_keys(wide)
+            d = torch.from_numpy(np.ascontiguousarray(balls, dtype=np.float64)).cuda()
+            e.compute_device(d.data_ptr(), len(balls), probe, periodic_box=box, precision=prec)
+            out.append(e.download())
+            e.close()
+        a, b = out
+        assert len(a.vertex_ids) > 0
+        assert np.array_equal(a.vertex_ids, b.vertex_ids) and np.array_equal(a.vertex_xyz, b.vertex_xyz)
+        assert np.array_equal(a.edge_ids, b.edge_ids) and np.array_equal(a.edge_length, b.edge_length)

@@ -161,6 +161,7 @@ struct vt_engine {
     }
     // tessellation network (with_cell_vertices) of the last call
     bool network = false;
+    bool net_wide_keys = false;  // force the two-word vertex keys of the deduplication
     uint64_t net_nv = 0, net_ne = 0;
     DBuf<uint32_t> net_flags, net_voff, net_vcnt, net_ecnt, net_off_v, net_off_e;
     DBuf<uint4> net_vids, net_eids, net_ov_vids, net_ov_eids;
@@ -174,14 +175,14 @@ struct vt_engine {
     DBuf<uint2> rec_ids;
     DBuf<uint32_t> rec_off, rec_meta;
     NetSlots net_slots{};
-    DBuf<uint32_t> net_bcnt, net_boff, net_bcur, net_bucnt, net_buoff, net_big, net_bsrc;
+    DBuf<uint32_t> net_bcnt, net_boff, net_bcur, net_bucnt, net_buoff, net_big, net_bidx, net_bsrcd;
     DBuf<unsigned long long> net_k1, net_k2;
     DBuf<uint32_t> out_net_vid, out_net_eid;
     DBuf<double> out_net_vxyz, out_net_elen;
 
     // one element type (m elements of V pairs): bucket by first id, sort the buckets, keep
     // the first of equal ids, gather
-    uint64_t net_unique(uint32_t V, const uint32_t* cnt, const uint32_t* off, uint32_t m, int vertices) {
+    uint64_t net_unique(uint32_t V, const uint32_t* off, uint32_t m, int vertices) {
         if (m == 0) return 0;
         const uint32_t n = (uint32_t)bufs.n, NB = n + 1;
         net_bcnt.ensure(NB);
@@ -191,12 +192,14 @@ struct vt_engine {
         net_buoff.ensure(NB + 1);
         net_big.ensure(NB + 1);
         net_k1.ensure(m);
-        net_k2.ensure(m);
-        net_bsrc.ensure(m);
+        const bool wide = vertices && (net_wide_keys || 3 * net_key_bits(n) > 64);
+        net_k2.ensure(wide ? m : 1);  // the wide key form only
+        net_bidx.ensure(m);
+        net_bsrcd.ensure(m);
         NetBuckets t{net_bcnt.p, net_boff.p, net_bcur.p, net_bucnt.p, net_buoff.p, net_big.p,
-                     net_k1.p,   net_k2.p,   net_bsrc.p};
+                     net_k1.p,   net_k2.p,   net_bidx.p, net_bsrcd.p};
         ensure_scan(NB + 1);
-        launch_net_dedup(V, cnt, off, net_slots, vertices, n, t, scan_tmp.p, stream);
+        launch_net_dedup(V, off, net_slots, vertices, wide ? 1 : 0, n, t, scan_tmp.p, stream);
         VT_CUDA(cudaMemcpyAsync(h_words + 15, net_buoff.p + NB, 4, cudaMemcpyDeviceToHost, stream));
         sync();
         const uint32_t U = h_words[15];
@@ -270,8 +273,8 @@ struct vt_engine {
         VT_CUDA(cudaMemcpyAsync(h_words + 14, net_off_e.p + V, 4, cudaMemcpyDeviceToHost, stream));
         sync();
         const uint32_t Mv = h_words[13], Me = h_words[14];
-        net_nv = net_unique(V, net_vcnt.p, net_off_v.p, Mv, 1);
-        net_ne = net_unique(V, net_ecnt.p, net_off_e.p, Me, 0);
+        net_nv = net_unique(V, net_off_v.p, Mv, 1);
+        net_ne = net_unique(V, net_off_e.p, Me, 0);
         return VT_OK;
     }
 
@@ -1367,6 +1370,11 @@ int vt_engine_set_keep_contours(vt_engine* e, int on) {
 int vt_engine_set_network(vt_engine* e, int on) {
     if (!e) return VT_ERR_INVALID;
     e->network = on != 0;
+    return VT_OK;
+}
+int vt_engine_set_network_wide_keys(vt_engine* e, int on) {
+    if (!e) return VT_ERR_INVALID;
+    e->net_wide_keys = on != 0;
     return VT_OK;
 }
 uint64_t vt_result_num_vertices(const vt_result* r) { return r ? r->net_vxyz.size() / 3 : 0; }

@@ -140,14 +140,83 @@ __device__ __forceinline__ uint4 net_ids(const NetSlots& sl, uint32_t i, int ver
     return vertices ? net_vid(sl, i) : net_eid(sl, i);
 }
 __device__ __forceinline__ uint32_t net_bucket(uint32_t id0, uint32_t n) { return id0 < n ? id0 : n; }
+__device__ __forceinline__ unsigned long long net_key_id(uint32_t id, uint32_t n) {
+    return id == kNetNull ? (unsigned long long)n : (unsigned long long)id;  // NULL after every ball id
+}
+
+// A bucket element: the ids after the first and the element's dense index j (pair then
+// contour order), ordered by (ids, j).  Narrow form (WIDE = false): the ids packed B bits
+// each into k1, NULL as n (2^B > n): edges always, vertices while 3 B <= 64.  Wide form:
+// k1 = id1 << 32 | id2, k2 = id3.
+template <bool WIDE>
+struct NbKey {
+    unsigned long long k1, k2;
+    uint32_t j;
+    __device__ __forceinline__ static NbKey pad() { return {~0ull, ~0ull, 0xffffffffu}; }
+    __device__ __forceinline__ bool less(const NbKey& o) const {
+        if (k1 != o.k1) return k1 < o.k1;
+        if (WIDE && k2 != o.k2) return k2 < o.k2;
+        return j < o.j;
+    }
+    __device__ __forceinline__ bool same_ids(const NbKey& o) const { return k1 == o.k1 && (!WIDE || k2 == o.k2); }
+    __device__ __forceinline__ NbKey xor_lane(int m) const {
+        NbKey r;
+        r.k1 = __shfl_xor_sync(kFull, k1, m);
+        r.k2 = WIDE ? __shfl_xor_sync(kFull, k2, m) : 0ull;
+        r.j = __shfl_xor_sync(kFull, j, m);
+        return r;
+    }
+    __device__ __forceinline__ NbKey from_lane(int src) const {
+        NbKey r;
+        r.k1 = __shfl_sync(kFull, k1, src);
+        r.k2 = WIDE ? __shfl_sync(kFull, k2, src) : 0ull;
+        r.j = __shfl_sync(kFull, j, src);
+        return r;
+    }
+    __device__ __forceinline__ NbKey up_lane() const {
+        NbKey r;
+        r.k1 = __shfl_up_sync(kFull, k1, 1);
+        r.k2 = WIDE ? __shfl_up_sync(kFull, k2, 1) : 0ull;
+        r.j = __shfl_up_sync(kFull, j, 1);
+        return r;
+    }
+    __device__ __forceinline__ static NbKey load(const unsigned long long* k1s, const unsigned long long* k2s,
+                                                 const uint32_t* js, uint32_t i) {
+        return {k1s[i], WIDE ? k2s[i] : 0ull, js[i]};
+    }
+    __device__ __forceinline__ void store(unsigned long long* k1s, unsigned long long* k2s, uint32_t* js,
+                                          uint32_t i) const {
+        k1s[i] = k1;
+        if (WIDE) k2s[i] = k2;
+        js[i] = j;
+    }
+};
+
+// The key of an element with sorted ids id (first id already the bucket)
+template <bool WIDE>
+__device__ __forceinline__ NbKey<WIDE> nb_key(uint4 id, int vertices, uint32_t n, int B, uint32_t j) {
+    NbKey<WIDE> k;
+    k.j = j;
+    k.k2 = 0ull;
+    if (WIDE) {  // vertices only
+        k.k1 = (unsigned long long)id.y << 32 | id.z;
+        k.k2 = id.w;
+    } else if (vertices) {
+        k.k1 = (net_key_id(id.y, n) << (2 * B)) | (net_key_id(id.z, n) << B) | net_key_id(id.w, n);
+    } else {
+        k.k1 = (net_key_id(id.y, n) << B) | net_key_id(id.z, n);
+    }
+    return k;
+}
 
 // The counting (FILL = false) and scatter (FILL = true) passes, lanes over the dense
 // elements: a warp takes 32 consecutive pair slots, whose elements are the dense range
 // [off[v0], off[v0 + 32]), and finds each lane's slot by a shuffle binary search over the
 // slots' offsets (coalesced reads, every lane busy although a contour has ~5 vertices).
-// Lanes of one bucket share one atomic; the scatter places them in lane order after it.
-template <bool FILL>
-__global__ void k_nb_pass(uint32_t V, const uint32_t* __restrict__ off, NetSlots sl, int vertices, uint32_t n,
+// Lanes of one bucket share one atomic; the scatter places them in lane order after it,
+// and records each element's slot index by dense index for the gather.
+template <bool FILL, bool WIDE>
+__global__ void k_nb_pass(uint32_t V, const uint32_t* __restrict__ off, NetSlots sl, int vertices, uint32_t n, int B,
                           NetBuckets t) {
     const int lane = threadIdx.x & 31;
     const uint32_t wpb = blockDim.x >> 5;
@@ -180,32 +249,19 @@ __global__ void k_nb_pass(uint32_t V, const uint32_t* __restrict__ off, NetSlots
                 r = __shfl_sync(kFull, r, leader);
                 if (on) {
                     const uint32_t pos = t.off[bk] + r + (uint32_t)__popc(grp & ((1u << lane) - 1u));
-                    t.k1[pos] = (unsigned long long)id.y << 32 | id.z;
-                    t.k2[pos] = vertices ? ((unsigned long long)id.w << 32 | j) : (unsigned long long)j;
-                    t.src[pos] = e;
+                    nb_key<WIDE>(id, vertices, n, B, j).store(t.k1, t.k2, t.idx, pos);
+                    t.srcd[j] = e;
                 }
             }
         }
     }
 }
 
-// (x1, x2) < (y1, y2) lexicographically
-__device__ __forceinline__ bool key_less(unsigned long long x1, unsigned long long x2, unsigned long long y1,
-                                         unsigned long long y2) {
-    return x1 < y1 || (x1 == y1 && x2 < y2);
-}
-// equal ids: k1 and, for vertices, the high word of k2 (the low word is the dense index)
-__device__ __forceinline__ bool same_ids(unsigned long long x1, unsigned long long x2, unsigned long long y1,
-                                         unsigned long long y2, int vertices) {
-    return x1 == y1 && (!vertices || (x2 >> 32) == (y2 >> 32));
-}
-
 // Bitonic sort of the N = 32 E elements a warp holds in registers, element index
 // i = 32 r + lane in register r: distances below 32 exchange through shuffles, larger
-// ones between a thread's own registers.  Elements past the bucket hold the largest key.
-template <int E>
-__device__ __forceinline__ void warp_bitonic(unsigned long long (&x1)[E], unsigned long long (&x2)[E],
-                                             uint32_t (&s)[E]) {
+// ones between a thread's own registers.  Elements past the bucket hold the padding key.
+template <bool WIDE, int E>
+__device__ __forceinline__ void warp_bitonic(NbKey<WIDE> (&x)[E]) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int k = 2; k <= 32 * E; k <<= 1) {
@@ -217,70 +273,49 @@ __device__ __forceinline__ void warp_bitonic(unsigned long long (&x1)[E], unsign
                     const int r2 = r ^ (j >> 5);
                     if (r2 < r) continue;
                     const bool up = ((32 * r + lane) & k) == 0;  // this block ascending
-                    if (up ? key_less(x1[r2], x2[r2], x1[r], x2[r]) : key_less(x1[r], x2[r], x1[r2], x2[r2])) {
-                        const unsigned long long t1 = x1[r], t2 = x2[r];
-                        const uint32_t ts = s[r];
-                        x1[r] = x1[r2];
-                        x2[r] = x2[r2];
-                        s[r] = s[r2];
-                        x1[r2] = t1;
-                        x2[r2] = t2;
-                        s[r2] = ts;
+                    if (up ? x[r2].less(x[r]) : x[r].less(x[r2])) {
+                        const NbKey<WIDE> tmp = x[r];
+                        x[r] = x[r2];
+                        x[r2] = tmp;
                     }
                 }
             } else {
 #pragma unroll
                 for (int r = 0; r < E; ++r) {
-                    const unsigned long long y1 = __shfl_xor_sync(kFull, x1[r], j), y2 = __shfl_xor_sync(kFull, x2[r], j);
-                    const uint32_t ys = __shfl_xor_sync(kFull, s[r], j);
+                    const NbKey<WIDE> y = x[r].xor_lane(j);
                     const int i = 32 * r + lane;
                     const bool keep_min = ((i & j) == 0) == ((i & k) == 0);
-                    if (keep_min ? key_less(y1, y2, x1[r], x2[r]) : key_less(x1[r], x2[r], y1, y2)) {
-                        x1[r] = y1;
-                        x2[r] = y2;
-                        s[r] = ys;
-                    }
+                    if (keep_min ? y.less(x[r]) : x[r].less(y)) x[r] = y;
                 }
             }
         }
     }
 }
 
-// One bucket of c <= 32 E elements at o: sorted in registers, then the first of each run
-// of equal ids written, in order, to the start of the bucket's src range.
-template <int E>
-__device__ __forceinline__ void warp_bucket(NetBuckets& t, uint32_t bk, uint32_t o, uint32_t c, int vertices) {
+// One bucket of c <= 32 E elements at o: sorted in registers, then the dense index of the
+// first of each run of equal ids written, in order, to the start of the bucket's range.
+template <bool WIDE, int E>
+__device__ __forceinline__ void warp_bucket(NetBuckets& t, uint32_t bk, uint32_t o, uint32_t c) {
     const int lane = threadIdx.x & 31;
-    unsigned long long x1[E], x2[E];
-    uint32_t s[E];
+    NbKey<WIDE> x[E];
 #pragma unroll
     for (int r = 0; r < E; ++r) {
         const uint32_t i = 32 * r + lane;
-        x1[r] = x2[r] = ~0ull;
-        s[r] = 0;
-        if (i < c) {
-            x1[r] = t.k1[o + i];
-            x2[r] = t.k2[o + i];
-            s[r] = t.src[o + i];
-        }
+        x[r] = i < c ? NbKey<WIDE>::load(t.k1, t.k2, t.idx, o + i) : NbKey<WIDE>::pad();
     }
-    if (c > 1) warp_bitonic<E>(x1, x2, s);
+    if (c > 1) warp_bitonic<WIDE, E>(x);
     uint32_t u = 0;
 #pragma unroll
     for (int r = 0; r < E; ++r) {
         const uint32_t i = 32 * r + lane;
-        unsigned long long p1 = __shfl_up_sync(kFull, x1[r], 1), p2 = __shfl_up_sync(kFull, x2[r], 1);
+        NbKey<WIDE> p = x[r].up_lane();
         if (r > 0) {  // lane 0's predecessor is lane 31 of the previous register
-            const unsigned long long q1 = __shfl_sync(kFull, x1[r > 0 ? r - 1 : 0], 31);
-            const unsigned long long q2 = __shfl_sync(kFull, x2[r > 0 ? r - 1 : 0], 31);
-            if (lane == 0) {
-                p1 = q1;
-                p2 = q2;
-            }
+            const NbKey<WIDE> q = x[r > 0 ? r - 1 : 0].from_lane(31);
+            if (lane == 0) p = q;
         }
-        const bool first = i < c && (i == 0 || !same_ids(p1, p2, x1[r], x2[r], vertices));
+        const bool first = i < c && (i == 0 || !p.same_ids(x[r]));
         const unsigned fm = __ballot_sync(kFull, first);
-        if (first) t.src[o + u + __popc(fm & ((1u << lane) - 1u))] = s[r];
+        if (first) t.idx[o + u + __popc(fm & ((1u << lane) - 1u))] = x[r].j;
         u += (uint32_t)__popc(fm);
     }
     if (lane == 0) t.ucnt[bk] = u;
@@ -289,26 +324,28 @@ __device__ __forceinline__ void warp_bucket(NetBuckets& t, uint32_t bk, uint32_t
 // warp per bucket of at most kWarpSort elements (1, 2 or 4 per lane); larger buckets are
 // listed for k_nb_sort_big
 constexpr uint32_t kWarpSort = 128;
-__global__ void k_nb_sort_small(uint32_t NB, int vertices, NetBuckets t) {
+template <bool WIDE>
+__global__ void k_nb_sort_small(uint32_t NB, NetBuckets t) {
     const int lane = threadIdx.x & 31;
     const uint32_t wpb = blockDim.x >> 5;
     for (uint32_t bk = blockIdx.x * wpb + (threadIdx.x >> 5); bk < NB; bk += gridDim.x * wpb) {
         const uint32_t o = t.off[bk], c = t.off[bk + 1] - o;
         if (c <= 32)
-            warp_bucket<1>(t, bk, o, c, vertices);
+            warp_bucket<WIDE, 1>(t, bk, o, c);
         else if (c <= 64)
-            warp_bucket<2>(t, bk, o, c, vertices);
+            warp_bucket<WIDE, 2>(t, bk, o, c);
         else if (c <= kWarpSort)
-            warp_bucket<4>(t, bk, o, c, vertices);
+            warp_bucket<WIDE, 4>(t, bk, o, c);
         else if (lane == 0)
             t.big[atomicAdd(t.big + NB, 1u)] = bk;
     }
 }
 
-// One bitonic sort of c elements by (k1, k2) across a block, all comparators ascending
-// (each merge starts by comparing mirrored positions), so that positions past c act as
-// the largest keys and are never touched: sorts any c in place.
-__device__ void block_bitonic(unsigned long long* k1, unsigned long long* k2, uint32_t* src, uint32_t c) {
+// One bitonic sort of c elements across a block, all comparators ascending (each merge
+// starts by comparing mirrored positions), so that positions past c act as the largest
+// keys and are never touched: sorts any c in place.
+template <bool WIDE>
+__device__ void block_bitonic(unsigned long long* k1, unsigned long long* k2, uint32_t* js, uint32_t c) {
     uint32_t N = 1;
     while (N < c) N <<= 1;
     for (uint32_t k = 2; k <= N; k <<= 1) {
@@ -316,15 +353,12 @@ __device__ void block_bitonic(unsigned long long* k1, unsigned long long* k2, ui
             for (uint32_t q = threadIdx.x; q < N / 2; q += blockDim.x) {
                 const uint32_t i = (q / j) * 2 * j + (q % j);
                 const uint32_t l = j == (k >> 1) ? (i ^ (k - 1)) : (i + j);
-                if (l < c && key_less(k1[l], k2[l], k1[i], k2[i])) {
-                    const unsigned long long t1 = k1[i], t2 = k2[i];
-                    const uint32_t ts = src[i];
-                    k1[i] = k1[l];
-                    k2[i] = k2[l];
-                    src[i] = src[l];
-                    k1[l] = t1;
-                    k2[l] = t2;
-                    src[l] = ts;
+                if (l < c) {
+                    const NbKey<WIDE> a = NbKey<WIDE>::load(k1, k2, js, i), b = NbKey<WIDE>::load(k1, k2, js, l);
+                    if (b.less(a)) {
+                        b.store(k1, k2, js, i);
+                        a.store(k1, k2, js, l);
+                    }
                 }
             }
             __syncthreads();
@@ -333,50 +367,44 @@ __device__ void block_bitonic(unsigned long long* k1, unsigned long long* k2, ui
 }
 
 // block per listed bucket of more than kWarpSort elements: sorted in shared memory up to
-// kBigSmem elements, in place in global memory beyond; then warp 0 writes the first of
-// each run of equal ids to the start of the bucket's src range (positions at or before
-// the one being read, so the in-place form reads every element before it is overwritten).
-__global__ void __launch_bounds__(256) k_nb_sort_big(uint32_t NB, int vertices, NetBuckets t) {
-    __shared__ unsigned long long s1[kBigSmem], s2[kBigSmem];
-    __shared__ uint32_t ss[kBigSmem];
+// kBigSmem elements, in place in global memory beyond; then warp 0 writes the dense index
+// of the first of each run of equal ids to the start of the bucket's range (positions at
+// or before the one being read, so the in-place form reads every element before it is
+// overwritten).
+template <bool WIDE>
+__global__ void __launch_bounds__(256) k_nb_sort_big(uint32_t NB, NetBuckets t) {
+    __shared__ unsigned long long s1[kBigSmem], s2[WIDE ? kBigSmem : 1];
+    __shared__ uint32_t sj[kBigSmem];
     const uint32_t count = t.big[NB];
     const int lane = threadIdx.x & 31;
     for (uint32_t it = blockIdx.x; it < count; it += gridDim.x) {
         const uint32_t bk = t.big[it];
         const uint32_t o = t.off[bk], c = t.off[bk + 1] - o;
-        unsigned long long *K1 = t.k1 + o, *K2 = t.k2 + o;
-        uint32_t* S = t.src + o;
+        unsigned long long *K1 = t.k1 + o, *K2 = WIDE ? t.k2 + o : nullptr;
+        uint32_t* J = t.idx + o;
         if (c <= (uint32_t)kBigSmem) {
-            for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
-                s1[i] = K1[i];
-                s2[i] = K2[i];
-                ss[i] = S[i];
-            }
+            for (uint32_t i = threadIdx.x; i < c; i += blockDim.x)
+                NbKey<WIDE>::load(K1, K2, J, i).store(s1, s2, sj, i);
             __syncthreads();
             K1 = s1;
             K2 = s2;
-            S = ss;
+            J = sj;
         }
-        block_bitonic(K1, K2, S, c);
+        block_bitonic<WIDE>(K1, K2, J, c);
         if (threadIdx.x < 32) {
             uint32_t u = 0;
-            unsigned long long q1 = 0, q2 = 0;
+            NbKey<WIDE> q = NbKey<WIDE>::pad();
             for (uint32_t base = 0; base < c; base += 32) {
-                const uint32_t j = base + lane;
-                const bool in = j < c;
-                const unsigned long long x1 = in ? K1[j] : ~0ull, x2 = in ? K2[j] : ~0ull;
-                const uint32_t s = in ? S[j] : 0u;
-                unsigned long long p1 = __shfl_up_sync(kFull, x1, 1), p2 = __shfl_up_sync(kFull, x2, 1);
-                if (lane == 0) {
-                    p1 = q1;
-                    p2 = q2;
-                }
-                const bool first = in && (j == 0 || !same_ids(p1, p2, x1, x2, vertices));
+                const uint32_t i = base + lane;
+                const bool in = i < c;
+                const NbKey<WIDE> x = in ? NbKey<WIDE>::load(K1, K2, J, i) : NbKey<WIDE>::pad();
+                NbKey<WIDE> p = x.up_lane();
+                if (lane == 0) p = q;
+                const bool first = in && (i == 0 || !p.same_ids(x));
                 const unsigned fm = __ballot_sync(kFull, first);
-                if (first) t.src[o + u + __popc(fm & ((1u << lane) - 1u))] = s;
+                if (first) t.idx[o + u + __popc(fm & ((1u << lane) - 1u))] = x.j;
                 u += (uint32_t)__popc(fm);
-                q1 = __shfl_sync(kFull, x1, 31);
-                q2 = __shfl_sync(kFull, x2, 31);
+                q = x.from_lane(31);
             }
             if (lane == 0) t.ucnt[bk] = u;
         }
@@ -384,7 +412,7 @@ __global__ void __launch_bounds__(256) k_nb_sort_big(uint32_t NB, int vertices, 
     }
 }
 
-// warp per bucket: its unique elements to the output, at uoff[bucket]
+// warp per bucket: its distinct elements to the output, at uoff[bucket]
 __global__ void k_nb_gather(uint32_t NB, NetBuckets t, NetSlots sl, int vertices, uint32_t* __restrict__ out_ids,
                             double* __restrict__ out_vals) {
     const int lane = threadIdx.x & 31;
@@ -392,7 +420,7 @@ __global__ void k_nb_gather(uint32_t NB, NetBuckets t, NetSlots sl, int vertices
     for (uint32_t bk = blockIdx.x * wpb + (threadIdx.x >> 5); bk < NB; bk += gridDim.x * wpb) {
         const uint32_t u = t.ucnt[bk], o = t.off[bk], uo = t.uoff[bk];
         for (uint32_t j = lane; j < u; j += 32) {
-            const uint32_t s = t.src[o + j];
+            const uint32_t s = t.srcd[t.idx[o + j]];
             const size_t w = (size_t)uo + j;
             if (vertices) {
                 const uint4 id = net_vid(sl, s);
@@ -414,21 +442,38 @@ __global__ void k_nb_gather(uint32_t NB, NetBuckets t, NetSlots sl, int vertices
 
 int gw(size_t items) { return grid_blocks(items, 8, 148 * 32); }  // 8 warps per 256-thread block
 
+template <bool WIDE>
+void dedup_kernels(uint32_t V, const uint32_t* off, const NetSlots& sl, int vertices, uint32_t n, int B,
+                   NetBuckets t, uint32_t* scan_tmp, cudaStream_t s) {
+    const uint32_t NB = n + 1;
+    const size_t groups = ((size_t)V + 31) / 32;
+    k_nb_pass<false, WIDE><<<gw(groups), 256, 0, s>>>(V, off, sl, vertices, n, B, t); count_launch();
+    scan_u32(t.cnt, t.off, NB, scan_tmp, s);
+    k_nb_pass<true, WIDE><<<gw(groups), 256, 0, s>>>(V, off, sl, vertices, n, B, t); count_launch();
+    k_nb_sort_small<WIDE><<<gw(NB), 256, 0, s>>>(NB, t); count_launch();
+    k_nb_sort_big<WIDE><<<148 * 4, 256, 0, s>>>(NB, t); count_launch();
+    scan_u32(t.ucnt, t.uoff, NB, scan_tmp, s);
+}
+
 }  // namespace
 
-void launch_net_dedup(uint32_t V, const uint32_t* cnt, const uint32_t* off, const NetSlots& sl, int vertices,
-                      uint32_t n, NetBuckets t, uint32_t* scan_tmp, cudaStream_t s) {
+int net_key_bits(uint32_t n) {
+    int B = 1;
+    while (B < 32 && ((uint64_t)1 << B) <= (uint64_t)n) ++B;  // 2^B > n: ids 0..n-1 and NULL as n
+    return B;
+}
+
+void launch_net_dedup(uint32_t V, const uint32_t* off, const NetSlots& sl, int vertices, int wide, uint32_t n,
+                      NetBuckets t, uint32_t* scan_tmp, cudaStream_t s) {
     const uint32_t NB = n + 1;
     cudaMemsetAsync(t.cnt, 0, 4 * (size_t)NB, s);
     cudaMemsetAsync(t.cur, 0, 4 * (size_t)NB, s);
     cudaMemsetAsync(t.big + NB, 0, 4, s);
-    const size_t groups = ((size_t)V + 31) / 32;
-    k_nb_pass<false><<<gw(groups), 256, 0, s>>>(V, off, sl, vertices, n, t); count_launch();
-    scan_u32(t.cnt, t.off, NB, scan_tmp, s);
-    k_nb_pass<true><<<gw(groups), 256, 0, s>>>(V, off, sl, vertices, n, t); count_launch();
-    k_nb_sort_small<<<gw(NB), 256, 0, s>>>(NB, vertices, t); count_launch();
-    k_nb_sort_big<<<148 * 4, 256, 0, s>>>(NB, vertices, t); count_launch();
-    scan_u32(t.ucnt, t.uoff, NB, scan_tmp, s);
+    const int B = net_key_bits(n);
+    if (vertices && (wide || 3 * B > 64))
+        dedup_kernels<true>(V, off, sl, vertices, n, B, t, scan_tmp, s);
+    else
+        dedup_kernels<false>(V, off, sl, vertices, n, B, t, scan_tmp, s);
 }
 void launch_net_dedup_gather(uint32_t n, const NetBuckets& t, const NetSlots& sl, int vertices, uint32_t* out_ids,
                              double* out_vals, cudaStream_t s) {

@@ -373,11 +373,14 @@ struct NetBuckets {
     uint32_t* ucnt;  // [n + 1] distinct elements per bucket
     uint32_t* uoff;  // [n + 2] exclusive scan of ucnt
     uint32_t* big;   // [n + 2] buckets too large for a warp's sort; [n + 1] is their count
-    unsigned long long* k1;  // [m] ids 1 and 2 of the element
-    unsigned long long* k2;  // [m] vertices: id 3 and the dense index; edges: the dense index
-    uint32_t* src;   // [m] element index in the slot arrays; after the sort each bucket's range
-                     // starts with its distinct elements in id order
+    unsigned long long* k1;  // [m] by bucket position: the ids after the first (packed)
+    unsigned long long* k2;  // [m] the third of them when three do not fit one word
+    uint32_t* idx;   // [m] by bucket position: the dense index; after the sort each bucket's
+                     // range starts with its distinct elements' dense indices in id order
+    uint32_t* srcd;  // [m] by dense index: the element's index in the slot arrays
 };
+// bits of an id in the packed keys: 2^B > n (ids 0..n-1, NULL as n)
+int net_key_bits(uint32_t n);
 void launch_valid_flags(const DevBufs& b, uint32_t P, uint32_t* flags, cudaStream_t s);
 // FP64 elements of every valid pair, or (list != null) of the *count pairs listed
 void launch_net_elements(const DevBufs& b, uint32_t P, const uint32_t* voff, NetSlots slots, const uint32_t* list,
@@ -389,12 +392,13 @@ void launch_net_elements_f32(const DevBufs& b, uint32_t P, const uint32_t* voff,
 // the pairs of ov_list through the serial contour (vt_contact64.cu); at most ov_cap
 void launch_net_serial(const DevBufs& b, const uint32_t* voff, NetSlots slots, cudaStream_t s);
 size_t net_slot_capacity();
-// The distinct elements of V pairs (off = exclusive scan of cnt, the dense order: pair
-// then contour order) in id order, keeping the first in dense order of equal ids:
+// The distinct elements of V pairs (off = exclusive scan of the pairs' element counts,
+// the dense order: pair then contour order) in id order, keeping the first in dense order of equal ids:
 // elements bucketed by their first id (ids are sorted within an element), each bucket
 // sorted by (the other ids, dense index); t.uoff[n + 1] is the distinct count.
-void launch_net_dedup(uint32_t V, const uint32_t* cnt, const uint32_t* off, const NetSlots& slots, int vertices,
-                      uint32_t n, NetBuckets t, uint32_t* scan_tmp, cudaStream_t s);
+// wide: the two-word vertex keys (taken anyway when three ids need more than 64 bits)
+void launch_net_dedup(uint32_t V, const uint32_t* off, const NetSlots& slots, int vertices, int wide, uint32_t n,
+                      NetBuckets t, uint32_t* scan_tmp, cudaStream_t s);
 // the distinct elements to the output arrays (ids, and positions or lengths)
 void launch_net_dedup_gather(uint32_t n, const NetBuckets& t, const NetSlots& slots, int vertices,
                              uint32_t* out_ids, double* out_vals, cudaStream_t s);

@@ -105,6 +105,7 @@ def library():
     L.vt_result_vertices.argtypes = [_vp, _u32p, _f64p]
     L.vt_result_edges.argtypes = [_vp, _u32p, _f64p]
     L.vt_engine_set_network.argtypes = [_vp, ctypes.c_int]
+    L.vt_engine_set_network_wide_keys.argtypes = [_vp, ctypes.c_int]
     L.vt_engine_set_fp32_min_pairs.argtypes = [_vp, ctypes.c_uint64]
     L.vt_compute_solvent_spheres.argtypes = [_f64p, ctypes.c_uint64, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                              _f64p, ctypes.c_int, ctypes.POINTER(_vp)]
@@ -630,6 +631,11 @@ class Engine:
     def set_network(self, on: bool = True):
         """Later compute calls also build the tessellation network (with_cell_vertices)."""
         _check(self._L.vt_engine_set_network(self._h, 1 if on else 0))
+
+    def set_network_wide_keys(self, on: bool = True):
+        """The network's vertex deduplication in its two-word key form, which it takes by
+        itself from 2^21 balls on (same results)."""
+        _check(self._L.vt_engine_set_network_wide_keys(self._h, 1 if on else 0))
 
     def set_timing(self, on: bool = True):
         _check(self._L.vt_engine_set_timing(self._h, 1 if on else 0))
