@@ -185,13 +185,13 @@ __device__ __forceinline__ float plane_offset(V3<float> p, V3<float> n) {
 __device__ __forceinline__ float plane_side(V3<float> n, float h, V3<float> x) {  // n . x - h
     return __fmaf_rn(n.z, x.z, __fmaf_rn(n.y, x.y, __fmaf_rn(n.x, x.x, -h)));
 }
-__device__ __forceinline__ int halfspace_h(Dec<float, true>& d, V3<float> n, float h, V3<float> x, float tol) {
-    const float sd = plane_side(n, h, x);
-    d.band(sd - (float)kEps, tol);
-    d.band(sd + (float)kEps, tol);
-    if (sd - (float)kEps > 0.f) return 1;
-    if (sd + (float)kEps < 0.f) return -1;
-    return 0;
+// mark_contour's test halfspace >= 0 (on the plane or outside): its one decision is
+// sd + kEps < 0, so only that margin is banded (halfspace's 0 / 1 boundary at sd = kEps
+// cannot change the mark).
+__device__ __forceinline__ bool outside_or_on_h(Dec<float, true>& d, V3<float> n, float h, V3<float> x, float tol) {
+    const float m = plane_side(n, h, x) + (float)kEps;
+    d.band(m, tol);
+    return !(m < 0.f);
 }
 __device__ __forceinline__ V3<float> plane_segment_h(Dec<float, true>& d, V3<float> n, float h, V3<float> a,
                                                      V3<float> b, float E) {
@@ -479,7 +479,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             // mark_contour (contact.rs:506-521)
             bool out;
             if constexpr (F)
-                out = lane < len && halfspace_h(d, PN, PC.x, q.p, e0) >= 0;
+                out = lane < len && outside_or_on_h(d, PN, PC.x, q.p, e0);
             else
                 out = lane < len && halfspace(d, PC, PN, q.p, e0) >= 0;
             unsigned om = __ballot_sync(kFull, out);
