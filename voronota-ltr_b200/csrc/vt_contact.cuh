@@ -172,6 +172,14 @@ struct PairGeom {
 // Ratio of an intersection's sensitivity to its inputs beyond which the construction is
 // treated as ill-conditioned (the point could be off by more than E).
 constexpr float kCondMax = 64.f;
+// The FP32 cut loop's planes of one pass of 32 neighbours (unit normal, offset), per warp
+// in shared memory; the kernels that run the FP32 contour have at most kPlaneWarps warps
+// per block.
+constexpr int kPlaneWarps = 8;
+__device__ __forceinline__ float4* warp_planes() {
+    __shared__ float4 s_planes[kPlaneWarps][32];
+    return s_planes[threadIdx.x >> 5];
+}
 
 // FP32 forms with the plane given by its unit normal n and offset h = n . p: the side of
 // x (halfspace_of_point_unit, geometry.rs:118-131, with the same kEps margin and band)
@@ -458,14 +466,26 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             break;
         }
         unsigned cutmask = __ballot_sync(kFull, cls == kCut);
+        // FP32: the pass's cutting planes go to shared memory once, and each cut candidate
+        // reads its plane as one broadcast 16-byte load instead of four shuffles (blocks of
+        // at most kPlaneWarps warps; the previous pass's reads end at the first __syncwarp)
+        if constexpr (F) {
+            __syncwarp();
+            if (cls == kCut) warp_planes()[lane] = make_float4(pn.x, pn.y, pn.z, pc.x);
+            __syncwarp();
+        }
         while (cutmask) {
             int j = __ffs(cutmask) - 1;
             cutmask &= cutmask - 1;
-            V3<T> PC, PN = shfl_v3(pn, j);
-            if constexpr (F)
-                PC.x = __shfl_sync(kFull, pc.x, j);  // the plane offset
-            else
+            V3<T> PC, PN;
+            if constexpr (F) {
+                const float4 pl = warp_planes()[j];
+                PN = {pl.x, pl.y, pl.z};
+                PC.x = pl.w;  // the plane offset
+            } else {
+                PN = shfl_v3(pn, j);
                 PC = shfl_v3(pc, j);
+            }
             if (!init) {
                 len = init_contour(q, lane, g.a_id, g.ic, g.axis, (float)e0);
                 init = true;
