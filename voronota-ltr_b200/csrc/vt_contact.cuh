@@ -173,11 +173,11 @@ struct PairGeom {
 // treated as ill-conditioned (the point could be off by more than E).
 constexpr float kCondMax = 64.f;
 // The FP32 cut loop's planes of one pass of 32 neighbours (unit normal, offset), per warp
-// in shared memory; the kernels that run the FP32 contour have at most kPlaneWarps warps
-// per block.
+// in shared memory, for blocks of at most PW warps.
 constexpr int kPlaneWarps = 8;
+template <int PW>
 __device__ __forceinline__ float4* warp_planes() {
-    __shared__ float4 s_planes[kPlaneWarps][32];
+    __shared__ float4 s_planes[PW][32];
     return s_planes[threadIdx.x >> 5];
 }
 
@@ -413,8 +413,9 @@ struct ContourOut {
     V3<T> axis;
 };
 
-// XM: compile in the first moments (computed and written when g.xm_out is set).
-template <typename T, bool F, bool FULL, bool XM = false, typename NbFn>
+// XM: compile in the first moments (computed and written when g.xm_out is set).  PW: the
+// warps per block of the calling kernel (FP32).
+template <typename T, bool F, bool FULL, bool XM = false, int PW = kPlaneWarps, typename NbFn>
 __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn nb, ContourOut<T>* co = nullptr) {
     const int lane = threadIdx.x & 31;
     PairGeom<T> g = g0;
@@ -467,11 +468,11 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
         }
         unsigned cutmask = __ballot_sync(kFull, cls == kCut);
         // FP32: the pass's cutting planes go to shared memory once, and each cut candidate
-        // reads its plane as one broadcast 16-byte load instead of four shuffles (blocks of
-        // at most kPlaneWarps warps; the previous pass's reads end at the first __syncwarp)
+        // reads its plane as one broadcast 16-byte load instead of four shuffles (the
+        // previous pass's reads end at the first __syncwarp)
         if constexpr (F) {
             __syncwarp();
-            if (cls == kCut) warp_planes()[lane] = make_float4(pn.x, pn.y, pn.z, pc.x);
+            if (cls == kCut) warp_planes<PW>()[lane] = make_float4(pn.x, pn.y, pn.z, pc.x);
             __syncwarp();
         }
         while (cutmask) {
@@ -479,7 +480,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             cutmask &= cutmask - 1;
             V3<T> PC, PN;
             if constexpr (F) {
-                const float4 pl = warp_planes()[j];
+                const float4 pl = warp_planes<PW>()[j];
                 PN = {pl.x, pl.y, pl.z};
                 PC.x = pl.w;  // the plane offset
             } else {

@@ -24,7 +24,7 @@ constexpr int kWarps = VT_C32_WARPS;
 
 // One pair: the FP32 contour and the descriptor, written to the pair's outputs.
 // REC: also record the pair's contour for the network (DevBufs::rec_*).
-template <bool FULL, bool XM, bool REC>
+template <bool FULL, bool XM, bool REC, int W>
 __device__ __forceinline__ void contact_pair32(const DevBufs& b, uint32_t p, float band) {
     const int lane = threadIdx.x & 31;
     const uint32_t a = b.pair_a[p], eb = b.pair_e[p];
@@ -49,7 +49,7 @@ __device__ __forceinline__ void contact_pair32(const DevBufs& b, uint32_t p, flo
         return r;
     };
     ContourOut<float> co;
-    WarpContact r = contact_warp<float, true, FULL, XM>(g, (int)cnt, (int)(eb - off), nbf, REC ? &co : nullptr);
+    WarpContact r = contact_warp<float, true, FULL, XM, W>(g, (int)cnt, (int)(eb - off), nbf, REC ? &co : nullptr);
     if constexpr (REC) {
         uint32_t base = kRecNone;
         const int len = r.valid ? co.len : 0;
@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(W * 32, VT_C32_MINB * 4 / W)
             p = base;
             end = base + chunk < P ? base + chunk : P;
         }
-        contact_pair32<FULL, XM, REC>(b, p, band);
+        contact_pair32<FULL, XM, REC, W>(b, p, band);
         p += step;
     }
 }
@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
             ContourOut<float> co;
             WarpContact r;
             if (!recorded_contour(b, p, a, co, r))
-                r = contact_warp<float, true, false>(g, (int)cnt, (int)(eb - off), nbf, &co);
+                r = contact_warp<float, true, false, false, kWarps>(g, (int)cnt, (int)(eb - off), nbf, &co);
             if (r.unsure || r.overflow) {
                 if (lane == 0) b.redo_list[atomicAdd(b.d_redo_count, 1u)] = p;
                 continue;
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(kWarps * 32, VT_NET32_MINB)
             ContourOut<float> co;
             WarpContact r;
             if (!recorded_contour(b, p, a, co, r))
-                r = contact_warp<float, true, false>(g, (int)cnt, (int)(eb - off), nbf, &co);
+                r = contact_warp<float, true, false, false, kWarps>(g, (int)cnt, (int)(eb - off), nbf, &co);
             bool fp64 = r.unsure || r.overflow || !r.valid || r.merged;
             const Sph<double> A = {{A4.x, A4.y, A4.z}, A4.w}, B = {{B4.x, B4.y, B4.z}, B4.w};
             const Sph<double> ic = intersection_circle(A, B);
