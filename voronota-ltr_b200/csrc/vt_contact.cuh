@@ -93,7 +93,8 @@ template <typename T>
 __device__ __forceinline__ V3<T> shfl_v3(V3<T> v, int src) {
     return {__shfl_sync(kFull, v.x, src), __shfl_sync(kFull, v.y, src), __shfl_sync(kFull, v.z, src)};
 }
-// The same for the cut loop, where no point carries an arc angle yet (all 0).
+// The same for the cut loop and the restriction to the circle, where no point carries an
+// arc angle yet (all 0).
 template <typename T>
 __device__ __forceinline__ Pt<T> shfl_pt_flat(const Pt<T>& q, int src) {
     Pt<T> r;
@@ -101,6 +102,26 @@ __device__ __forceinline__ Pt<T> shfl_pt_flat(const Pt<T>& q, int src) {
     r.lid = __shfl_sync(kFull, q.lid, src);
     r.rid = __shfl_sync(kFull, q.rid, src);
     r.ang = 0;
+    return r;
+}
+// Gathers of only the fields a site reads (the others zero): position and left id (the
+// next point in the restriction and the arc angles), position and arc angle (the solid
+// angle's turn terms).
+template <typename T>
+__device__ __forceinline__ Pt<T> shfl_pt_pl(const Pt<T>& q, int src) {
+    Pt<T> r;
+    r.p = shfl_v3(q.p, src);
+    r.lid = __shfl_sync(kFull, q.lid, src);
+    r.rid = 0;
+    r.ang = 0;
+    return r;
+}
+template <typename T>
+__device__ __forceinline__ Pt<T> shfl_pt_pa(const Pt<T>& q, int src) {
+    Pt<T> r;
+    r.p = shfl_v3(q.p, src);
+    r.lid = r.rid = 0;
+    r.ang = __shfl_sync(kFull, q.ang, src);
     return r;
 }
 
@@ -621,7 +642,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
         unsigned outm = __ballot_sync(kFull, lane < len && !in);
         if (outm != 0) {
             int nx = lane + 1 < len ? lane + 1 : 0;
-            Pt<T> v = shfl_pt(q, nx);
+            Pt<T> v = shfl_pt_pl(q, nx);  // its position and left id are read
             bool v_in = __shfl_sync(kFull, in, nx);
             int k = 0;
             Pt<T> i1, i2;
@@ -752,16 +773,16 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             j = j > 31 ? 31 : j;
             int s = __shfl_sync(kFull, pos, j);
             int off = lane - s;
-            Pt<T> sp = shfl_pt(q, j);
-            Pt<T> s1 = shfl_pt(i1, j);
-            Pt<T> s2 = shfl_pt(i2, j);
+            Pt<T> sp = shfl_pt_flat(q, j);
+            Pt<T> s1 = shfl_pt_flat(i1, j);
+            Pt<T> s2 = shfl_pt_flat(i2, j);
             bool sin_ = __shfl_sync(kFull, in, j);
             Pt<T> outp = off == 0 ? (sin_ ? sp : s1) : (off == 1 ? (sin_ ? s1 : s2) : s2);
             if (lane < L) q = outp;
             len = L;
             // arc angles (contact.rs:741-754)
             int nx2 = lane + 1 < len ? lane + 1 : 0;
-            Pt<T> v2 = shfl_pt(q, nx2);
+            Pt<T> v2 = shfl_pt_pl(q, nx2);
             T a = 0;
             if (lane < len && q.rid == g.a_id && v2.lid == g.a_id) {
                 T tol_dir = 0;
@@ -782,7 +803,8 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             }
         }
         int nx = lane + 1 < len ? lane + 1 : 0;
-        Pt<T> v = shfl_pt(q, nx);
+        Pt<T> v;
+        v.p = shfl_v3(q.p, nx);  // the next point's position only
         // calculate_contour_area (contact.rs:773-793)
         on = lane < len;
         V3<T> pp = on ? q.p : mk<T>(0, 0, 0);
@@ -857,10 +879,12 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
         // construct_contact_descriptor (contact.rs:357-381)
         int pvl = lane > 0 ? lane - 1 : (len > 0 ? len - 1 : 0);
         int nxl = len > 0 ? (lane + 1 < len ? lane + 1 : 0) : 0;
-        Pt<T> p0 = shfl_pt(q, pvl);
-        Pt<T> p2 = shfl_pt(q, nxl);
-        T ea0 = 0;
-        if constexpr (F) ea0 = __shfl_sync(kFull, ang_err, pvl);
+        // the neighbouring points of the FP64 solid angles (position and arc angle of the
+        // previous, position of the next) and, with the moments, the next point's position
+        Pt<T> p0 = q, p2 = q;
+        if constexpr (!F) p0 = shfl_pt_pa(q, pvl);
+        if constexpr (!F || XM) p2.p = shfl_v3(q.p, nxl);
+        const T ea0 = 0;
         // one inlined copy of the solid angle for both sides.  FP64: side a, then side b.
         // FP32: a contour of at most 16 points (almost all) computes both sides at once,
         // lanes 0-15 side a and lanes 16-31 side b on the same points; longer ones take two
@@ -874,7 +898,9 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                 const int L = split ? (lane & 15) : lane;
                 const int pv = L > 0 ? L - 1 : (len > 0 ? len - 1 : 0);
                 const int nx = len > 0 ? (L + 1 < len ? L + 1 : 0) : 0;
-                const Pt<T> m1 = shfl_pt(q, L), m0 = shfl_pt(q, pv), m2 = shfl_pt(q, nx);
+                const Pt<T> m1 = shfl_pt_pa(q, L), m0 = shfl_pt_pa(q, pv);
+                Pt<T> m2 = m1;
+                m2.p = shfl_v3(q.p, nx);
                 const T e1 = __shfl_sync(kFull, ang_err, L), em = __shfl_sync(kFull, ang_err, pv);
                 const Sph<T> s0 = side ? g.B : g.A, s1 = side ? g.A : g.B;
                 const double v = solid_angle(d, s0, s1, g.ic, m0, m1, m2, L < len, len, e0, em, e1, split);
