@@ -622,6 +622,8 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
     T sum_arc = 0, area = 0;
     T area_tol = 0;  // FP32: band of the area <= 0 test (an uncut circle is far from it)
     V3<T> bary = mk<T>(0, 0, 0);
+    T tri = 0;                          // this lane's triangle (bary, point, next point) area
+    V3<T> vnext = mk<T>(0, 0, 0);       // the next point's position
     bool on = false;
     T ang_err = 0;  // FP32: bound on this lane's arc-angle error
     if (!init) {  // contact.rs:311-314
@@ -815,6 +817,8 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
             if (q.ang > (T)0) t2 = g.ic.r * g.ic.r * (q.ang - sin(q.ang)) * (T)0.5;
         }
         area = lsum2(t, t2, len);
+        tri = t;
+        vnext = v.p;
         if constexpr (F) {
             // moving each vertex by at most |d| changes the polygon area by at most |d| times
             // the perimeter and an arc segment by at most 2 r |d|: the band of area <= 0
@@ -880,10 +884,10 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
         int pvl = lane > 0 ? lane - 1 : (len > 0 ? len - 1 : 0);
         int nxl = len > 0 ? (lane + 1 < len ? lane + 1 : 0) : 0;
         // the neighbouring points of the FP64 solid angles (position and arc angle of the
-        // previous, position of the next) and, with the moments, the next point's position
+        // previous, position of the next)
         Pt<T> p0 = q, p2 = q;
         if constexpr (!F) p0 = shfl_pt_pa(q, pvl);
-        if constexpr (!F || XM) p2.p = shfl_v3(q.p, nxl);
+        if constexpr (!F) p2.p = shfl_v3(q.p, nxl);
         const T ea0 = 0;
         // one inlined copy of the solid angle for both sides.  FP64: side a, then side b.
         // FP32: a contour of at most 16 points (almost all) computes both sides at once,
@@ -952,10 +956,12 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
                     ak = qa * area;
                 }
             } else if (on) {
-                const V3<T> bw = bary - g.A.c, pk = q.p - g.A.c, pn = p2.p - g.A.c;
-                ak = (bw + pk + pn) * ((T)0.5 * norm(cross(pk - bw, pn - bw)) / (T)3);
+                // the triangle's area is the one the contour area summed
+                const V3<T> bw = bary - g.A.c, pk = q.p - g.A.c, pn = vnext - g.A.c;
+                ak = (bw + pk + pn) * (tri / (T)3);
                 if (q.ang > (T)0 && rho > (T)0) {
-                    const V3<T> e1 = (q.p - g.ic.c) / rho, e2 = (p2.p - g.ic.c) / rho;
+                    const T ir = (T)1 / rho;
+                    const V3<T> e1 = (q.p - g.ic.c) * ir, e2 = (vnext - g.ic.c) * ir;
                     const V3<T> f = cross(g.axis, e1);
                     const T ct = dot(e2, e1), st = dot(e2, f);
                     const V3<T> m = e1 * st + f * ((T)1 - ct);
