@@ -6,6 +6,8 @@
 // Every fuzzy decision is evaluated with an uncertainty band (vt_geom.cuh, Dec<float,
 // true>); a pair with any decision inside its band is marked unsure and recomputed by
 // the FP64 kernel, as is a pair whose contour outgrew the warp.
+// the FP32 kernels' double helpers stay inline (vt_geom.cuh)
+#define VT_FP32_UNIT 1
 #include "vt_adjoint.cuh"
 #include "vt_contact.cuh"
 #include "vt_pipeline.cuh"

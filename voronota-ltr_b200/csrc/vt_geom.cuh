@@ -65,6 +65,14 @@ template <typename T>
 __device__ __forceinline__ V3<T> normalize(V3<T> a) {
     return a / norm(a);
 }
+#ifndef VT_FP32_UNIT
+// FP64: normalize out of line (one copy).  Inlined at each of its call sites (a square root
+// and three divisions, with their slow paths, at about fifteen places) the FP64 contour's
+// code outgrew the instruction cache: the FP64 contact kernel stalled on instruction fetch
+// (5.6 cycles per issued instruction) and took 16.7 ms at the 100k lattice, 12.0 ms with
+// this copy.  The FP32 contact unit, whose double code is on its hot path, keeps it inline.
+static __device__ __noinline__ V3<double> normalize(V3<double> a) { return a / norm(a); }
+#endif
 template <typename T>
 __device__ __forceinline__ V3<T> cross(V3<T> a, V3<T> b) {
     return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
