@@ -321,6 +321,85 @@ __device__ __forceinline__ void warp_bucket(NetBuckets& t, uint32_t bk, uint32_t
     if (lane == 0) t.ucnt[bk] = u;
 }
 
+// The per-warp hash table of warp_bucket_distinct (256 slots: keys, smallest dense index),
+// for blocks of at most 8 warps.
+__device__ __forceinline__ unsigned long long* warp_hash_keys() {
+    __shared__ unsigned long long s_keys[8][256];
+    return s_keys[threadIdx.x >> 5];
+}
+__device__ __forceinline__ uint32_t* warp_hash_first() {
+    __shared__ uint32_t s_first[8][256];
+    return s_first[threadIdx.x >> 5];
+}
+
+// Narrow keys, a bucket of 33 to 32 E elements: most of a bucket repeats (a vertex sits
+// in up to six contours, an edge in three), so the warp first keeps each id tuple's first
+// occurrence (the smallest dense index) through an open-addressing table in shared memory
+// (twice as many slots as elements, multiplicative hashing, linear probing), then sorts
+// only those, one per lane, and writes their dense indices in id order.  Returns false,
+// having written nothing, when more than 32 distinct tuples remain.
+template <int E>
+__device__ __forceinline__ bool warp_bucket_distinct(NetBuckets& t, uint32_t bk, uint32_t o, uint32_t c) {
+    const int lane = threadIdx.x & 31;
+    constexpr int bits = E <= 2 ? 7 : 8;
+    constexpr uint32_t T = 1u << bits;
+    unsigned long long* hk = warp_hash_keys();
+    uint32_t* hj = warp_hash_first();
+    __syncwarp();  // the previous bucket's reads of the table are done
+    for (uint32_t k = lane; k < T; k += 32) {
+        hk[k] = ~0ull;
+        hj[k] = 0xffffffffu;
+    }
+    __syncwarp();
+    NbKey<false> x[E];
+    uint32_t slot[E];
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        const uint32_t i = 32 * r + lane;
+        slot[r] = 0;
+        x[r] = NbKey<false>::pad();
+        if (i < c) {
+            x[r] = NbKey<false>::load(t.k1, t.k2, t.idx, o + i);
+            uint32_t h = (uint32_t)((x[r].k1 * 0x9E3779B97F4A7C15ull) >> (64 - bits));
+            for (uint32_t probe = 0; probe < T; ++probe) {  // T > 2 c: a free slot exists
+                const unsigned long long prev = atomicCAS(&hk[h], ~0ull, x[r].k1);
+                if (prev == ~0ull || prev == x[r].k1) break;
+                h = (h + 1) & (T - 1);
+            }
+            atomicMin(&hj[h], x[r].j);
+            slot[r] = h;
+        }
+    }
+    __syncwarp();
+    bool rep[E];
+    uint32_t U = 0;
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        rep[r] = 32 * r + lane < c && hj[slot[r]] == x[r].j;
+        U += (uint32_t)__popc(__ballot_sync(kFull, rep[r]));
+    }
+    if (U > 32) return false;
+    __syncwarp();  // all reads of the table done: its first 32 slots take the survivors
+    uint32_t base = 0;
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        const unsigned m = __ballot_sync(kFull, rep[r]);
+        if (rep[r]) {
+            const uint32_t at = base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+            hk[at] = x[r].k1;
+            hj[at] = x[r].j;
+        }
+        base += (uint32_t)__popc(m);
+    }
+    __syncwarp();
+    NbKey<false> y[1];
+    y[0] = (uint32_t)lane < U ? NbKey<false>{hk[lane], 0ull, hj[lane]} : NbKey<false>::pad();
+    if (U > 1) warp_bitonic<false, 1>(y);
+    if ((uint32_t)lane < U) t.idx[o + lane] = y[0].j;
+    if (lane == 0) t.ucnt[bk] = U;
+    return true;
+}
+
 // warp per bucket of at most kWarpSort elements (1, 2 or 4 per lane); larger buckets are
 // listed for k_nb_sort_big
 constexpr uint32_t kWarpSort = 128;
@@ -330,14 +409,21 @@ __global__ void k_nb_sort_small(uint32_t NB, NetBuckets t) {
     const uint32_t wpb = blockDim.x >> 5;
     for (uint32_t bk = blockIdx.x * wpb + (threadIdx.x >> 5); bk < NB; bk += gridDim.x * wpb) {
         const uint32_t o = t.off[bk], c = t.off[bk + 1] - o;
-        if (c <= 32)
+        if (c <= 32) {
             warp_bucket<WIDE, 1>(t, bk, o, c);
-        else if (c <= 64)
-            warp_bucket<WIDE, 2>(t, bk, o, c);
-        else if (c <= kWarpSort)
-            warp_bucket<WIDE, 4>(t, bk, o, c);
-        else if (lane == 0)
+        } else if (c <= kWarpSort) {
+            bool done = false;
+            if constexpr (!WIDE)
+                done = c <= 64 ? warp_bucket_distinct<2>(t, bk, o, c) : warp_bucket_distinct<4>(t, bk, o, c);
+            if (!done) {
+                if (c <= 64)
+                    warp_bucket<WIDE, 2>(t, bk, o, c);
+                else
+                    warp_bucket<WIDE, 4>(t, bk, o, c);
+            }
+        } else if (lane == 0) {
             t.big[atomicAdd(t.big + NB, 1u)] = bk;
+        }
     }
 }
 
