@@ -436,8 +436,17 @@ struct ContourOut {
 
 // XM: compile in the first moments (computed and written when g.xm_out is set).  PW: the
 // warps per block of the calling kernel (FP32).
-template <typename T, bool F, bool FULL, bool XM = false, int PW = kPlaneWarps, typename NbFn>
-__device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn nb, ContourOut<T>* co = nullptr) {
+// rec(q, len, full, unsure, merged), when given, is called by the whole warp once the
+// contour of a valid contact is final, before the descriptor: a caller that records the
+// contour stores it there, so that none of it stays live through the descriptor code.
+struct NoContourRecord {
+    template <typename P>
+    __device__ __forceinline__ void operator()(const P&, int, bool, bool, bool) const {}
+};
+template <typename T, bool F, bool FULL, bool XM = false, int PW = kPlaneWarps, typename NbFn,
+          typename RecFn = NoContourRecord>
+__device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn nb, ContourOut<T>* co = nullptr,
+                                    RecFn rec = RecFn()) {
     const int lane = threadIdx.x & 31;
     PairGeom<T> g = g0;
     const T e0 = g.e0;
@@ -879,6 +888,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
         co->ic = g.ic;
         co->axis = g.axis;
     }
+    rec(q, len, !init, __any_sync(kFull, d.unsure), res.merged);
     if (FULL) {
         // construct_contact_descriptor (contact.rs:357-381)
         int pvl = lane > 0 ? lane - 1 : (len > 0 ? len - 1 : 0);

@@ -50,24 +50,30 @@ __device__ __forceinline__ void contact_pair32(const DevBufs& b, uint32_t p, flo
         r.id = nid[e];
         return r;
     };
-    ContourOut<float> co;
-    WarpContact r = contact_warp<float, true, FULL, XM, W>(g, (int)cnt, (int)(eb - off), nbf, REC ? &co : nullptr);
+    WarpContact r;
     if constexpr (REC) {
-        uint32_t base = kRecNone;
-        const int len = r.valid ? co.len : 0;
-        if (r.valid) {
+        // the contour of a valid contact goes to the pool as soon as it is final
+        auto record = [&](const Pt<float>& q, int len, bool full, bool unsure, bool merged) {
+            uint32_t base = 0;
             if (lane == 0) base = atomicAdd(b.rec_count, (uint32_t)len);
             base = __shfl_sync(0xffffffffu, base, 0);
             if ((uint64_t)base + (uint64_t)len > (uint64_t)b.rec_cap) base = kRecNone;  // pool full: recompute
             if (base != kRecNone && lane < len) {
-                b.rec_pts[base + lane] = make_float4(co.q.p.x, co.q.p.y, co.q.p.z, co.q.ang);
-                b.rec_ids[base + lane] = make_uint2(co.q.lid, co.q.rid);
+                b.rec_pts[base + lane] = make_float4(q.p.x, q.p.y, q.p.z, q.ang);
+                b.rec_ids[base + lane] = make_uint2(q.lid, q.rid);
             }
+            if (lane == 0) {
+                b.rec_off[p] = base;
+                b.rec_meta[p] = ((uint32_t)len << 8) | (full ? 1u : 0u) | (merged ? 2u : 0u) | (unsure ? 4u : 0u);
+            }
+        };
+        r = contact_warp<float, true, FULL, XM, W>(g, (int)cnt, (int)(eb - off), nbf, nullptr, record);
+        if (!r.valid && lane == 0) {  // no contact: nothing recorded
+            b.rec_off[p] = kRecNone;
+            b.rec_meta[p] = 0u;
         }
-        if (lane == 0) {
-            b.rec_off[p] = base;
-            b.rec_meta[p] = ((uint32_t)len << 8) | (co.full ? 1u : 0u) | (r.merged ? 2u : 0u) | (co.unsure ? 4u : 0u);
-        }
+    } else {
+        r = contact_warp<float, true, FULL, XM, W>(g, (int)cnt, (int)(eb - off), nbf);
     }
     if (lane == 0) {
         uint8_t st = (r.valid ? kValid : 0) | (r.unsure ? kUnsure : 0) | (r.overflow ? kOverflow : 0);
