@@ -890,6 +890,54 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
     }
     rec(q, len, !init, __any_sync(kFull, d.unsure), res.merged);
     if (FULL) {
+        // the moments first: they need the contour, its area and its triangles but not
+        // the solid angles, whose code then runs without them in registers
+        if (XM && g.xm_out) {
+            // integral of (x - a) over the arcs: an arc of angle t from e1 (unit, from the
+            // circle centre) around the axis contributes (q - a) rho t + rho^2 (sin t e1 +
+            // (1 - cos t) axis x e1), with cos t = e1.e2, sin t = e2.(axis x e1).
+            // integral of (x - a) over the area: the triangles (bary, p_k, p_k+1) of the
+            // area sum contribute their area times their centroid; the circular segment of
+            // an arc its area rho^2 (t - sin t) / 2 at q plus rho^3 (1 - cos t) / 6 (sin t e1
+            // + (1 - cos t) axis x e1) (the segment's centroid lies 4 rho sin^3(t/2) /
+            // (3 (t - sin t)) from q along the arc's bisector); sin t and cos t come from the
+            // arc's end points, as for the arcs' moment
+            // Formed in the contour's own precision (the FP32 kernel's coordinates are
+            // relative to a, so the moments carry no large offsets), one lane per contour
+            // point, then summed over the warp and widened.
+            const T rho = g.ic.r;
+            const V3<T> qa = g.ic.c - g.A.c;
+            V3<T> xk = mk<T>(0, 0, 0), ak = mk<T>(0, 0, 0);
+            if (!init) {
+                if (lane == 0) {
+                    xk = qa * ((T)kTau * rho);
+                    ak = qa * area;
+                }
+            } else if (on) {
+                // the triangle's area is the one the contour area summed
+                const V3<T> bw = bary - g.A.c, pk = q.p - g.A.c, pn = vnext - g.A.c;
+                ak = (bw + pk + pn) * (tri / (T)3);
+                if (q.ang > (T)0 && rho > (T)0) {
+                    const T ir = (T)1 / rho;
+                    const V3<T> e1 = (q.p - g.ic.c) * ir, e2 = (vnext - g.ic.c) * ir;
+                    const V3<T> f = cross(g.axis, e1);
+                    const T ct = dot(e2, e1), st = dot(e2, f);
+                    const V3<T> m = e1 * st + f * ((T)1 - ct);
+                    xk = qa * (rho * q.ang) + m * (rho * rho);
+                    ak = ak + qa * ((T)0.5 * rho * rho * (q.ang - st)) + m * (rho * rho * rho * ((T)1 - ct) / (T)6);
+                }
+            }
+            const T s0 = wsum(xk.x), s1 = wsum(xk.y), s2 = wsum(xk.z);
+            const T s3 = wsum(ak.x), s4 = wsum(ak.y), s5 = wsum(ak.z);
+            if (lane == 0) {
+                g.xm_out[0] = (double)s0;
+                g.xm_out[1] = (double)s1;
+                g.xm_out[2] = (double)s2;
+                g.xm_out[3] = (double)s3;
+                g.xm_out[4] = (double)s4;
+                g.xm_out[5] = (double)s5;
+            }
+        }
         // construct_contact_descriptor (contact.rs:357-381)
         int pvl = lane > 0 ? lane - 1 : (len > 0 ? len - 1 : 0);
         int nxl = len > 0 ? (lane + 1 < len ? lane + 1 : 0) : 0;
@@ -943,52 +991,6 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
         } else {
             res.pv_a = (double)(norm(g.ic.c - g.A.c) * area / (T)3 * sign_a);
             res.pv_b = (double)(norm(g.ic.c - g.B.c) * area / (T)3 * sign_b);
-        }
-        if (XM && g.xm_out) {
-            // integral of (x - a) over the arcs: an arc of angle t from e1 (unit, from the
-            // circle centre) around the axis contributes (q - a) rho t + rho^2 (sin t e1 +
-            // (1 - cos t) axis x e1), with cos t = e1.e2, sin t = e2.(axis x e1).
-            // integral of (x - a) over the area: the triangles (bary, p_k, p_k+1) of the
-            // area sum contribute their area times their centroid; the circular segment of
-            // an arc its area rho^2 (t - sin t) / 2 at q plus rho^3 (1 - cos t) / 6 (sin t e1
-            // + (1 - cos t) axis x e1) (the segment's centroid lies 4 rho sin^3(t/2) /
-            // (3 (t - sin t)) from q along the arc's bisector); sin t and cos t come from the
-            // arc's end points, as for the arcs' moment
-            // Formed in the contour's own precision (the FP32 kernel's coordinates are
-            // relative to a, so the moments carry no large offsets), one lane per contour
-            // point, then summed over the warp and widened.
-            const T rho = g.ic.r;
-            const V3<T> qa = g.ic.c - g.A.c;
-            V3<T> xk = mk<T>(0, 0, 0), ak = mk<T>(0, 0, 0);
-            if (!init) {
-                if (lane == 0) {
-                    xk = qa * ((T)kTau * rho);
-                    ak = qa * area;
-                }
-            } else if (on) {
-                // the triangle's area is the one the contour area summed
-                const V3<T> bw = bary - g.A.c, pk = q.p - g.A.c, pn = vnext - g.A.c;
-                ak = (bw + pk + pn) * (tri / (T)3);
-                if (q.ang > (T)0 && rho > (T)0) {
-                    const T ir = (T)1 / rho;
-                    const V3<T> e1 = (q.p - g.ic.c) * ir, e2 = (vnext - g.ic.c) * ir;
-                    const V3<T> f = cross(g.axis, e1);
-                    const T ct = dot(e2, e1), st = dot(e2, f);
-                    const V3<T> m = e1 * st + f * ((T)1 - ct);
-                    xk = qa * (rho * q.ang) + m * (rho * rho);
-                    ak = ak + qa * ((T)0.5 * rho * rho * (q.ang - st)) + m * (rho * rho * rho * ((T)1 - ct) / (T)6);
-                }
-            }
-            const T s0 = wsum(xk.x), s1 = wsum(xk.y), s2 = wsum(xk.z);
-            const T s3 = wsum(ak.x), s4 = wsum(ak.y), s5 = wsum(ak.z);
-            if (lane == 0) {
-                g.xm_out[0] = (double)s0;
-                g.xm_out[1] = (double)s1;
-                g.xm_out[2] = (double)s2;
-                g.xm_out[3] = (double)s3;
-                g.xm_out[4] = (double)s4;
-                g.xm_out[5] = (double)s5;
-            }
         }
     }
     res.unsure = __any_sync(kFull, d.unsure);
