@@ -436,12 +436,13 @@ struct ContourOut {
 
 // XM: compile in the first moments (computed and written when g.xm_out is set).  PW: the
 // warps per block of the calling kernel (FP32).
-// rec(q, len, full, unsure, merged), when given, is called by the whole warp once the
-// contour of a valid contact is final, before the descriptor: a caller that records the
-// contour stores it there, so that none of it stays live through the descriptor code.
+// rec(q, len, full, unsure, res), when given, is called by the whole warp once the contour
+// of a valid contact and its area, arc length and centrality (in res) are final, before
+// the descriptor: a caller stores there what it keeps of them, so that none of it stays
+// live through the descriptor code.
 struct NoContourRecord {
-    template <typename P>
-    __device__ __forceinline__ void operator()(const P&, int, bool, bool, bool) const {}
+    template <typename P, typename R>
+    __device__ __forceinline__ void operator()(const P&, int, bool, bool, const R&) const {}
 };
 template <typename T, bool F, bool FULL, bool XM = false, int PW = kPlaneWarps, typename NbFn,
           typename RecFn = NoContourRecord>
@@ -888,7 +889,7 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
         co->ic = g.ic;
         co->axis = g.axis;
     }
-    rec(q, len, !init, __any_sync(kFull, d.unsure), res.merged);
+    rec(q, len, !init, __any_sync(kFull, d.unsure), res);
     if (FULL) {
         // the moments first: they need the contour, its area and its triangles but not
         // the solid angles, whose code then runs without them in registers

@@ -50,10 +50,16 @@ __device__ __forceinline__ void contact_pair32(const DevBufs& b, uint32_t p, flo
         r.id = nid[e];
         return r;
     };
-    WarpContact r;
-    if constexpr (REC) {
-        // the contour of a valid contact goes to the pool as soon as it is final
-        auto record = [&](const Pt<float>& q, int len, bool full, bool unsure, bool merged) {
+    // the contact's area, arc length and centrality (and with REC its contour, into the
+    // pool) are stored as soon as they are final, so that they are not kept in registers
+    // through the descriptor code
+    auto on_final = [&](const Pt<float>& q, int len, bool full, bool unsure, const WarpContact& rr) {
+        if (lane == 0) {
+            b.p_area[p] = rr.area;
+            b.p_arc[p] = rr.arc;
+            b.p_central[p] = rr.central ? 1 : 0;
+        }
+        if constexpr (REC) {
             uint32_t base = 0;
             if (lane == 0) base = atomicAdd(b.rec_count, (uint32_t)len);
             base = __shfl_sync(0xffffffffu, base, 0);
@@ -64,23 +70,24 @@ __device__ __forceinline__ void contact_pair32(const DevBufs& b, uint32_t p, flo
             }
             if (lane == 0) {
                 b.rec_off[p] = base;
-                b.rec_meta[p] = ((uint32_t)len << 8) | (full ? 1u : 0u) | (merged ? 2u : 0u) | (unsure ? 4u : 0u);
+                b.rec_meta[p] =
+                    ((uint32_t)len << 8) | (full ? 1u : 0u) | (rr.merged ? 2u : 0u) | (unsure ? 4u : 0u);
             }
-        };
-        r = contact_warp<float, true, FULL, XM, W>(g, (int)cnt, (int)(eb - off), nbf, nullptr, record);
-        if (!r.valid && lane == 0) {  // no contact: nothing recorded
+        }
+    };
+    const WarpContact r = contact_warp<float, true, FULL, XM, W>(g, (int)cnt, (int)(eb - off), nbf, nullptr, on_final);
+    if (!r.valid && lane == 0) {  // no contact: zero outputs, nothing recorded
+        b.p_area[p] = 0.0;
+        b.p_arc[p] = 0.0;
+        b.p_central[p] = 0;
+        if constexpr (REC) {
             b.rec_off[p] = kRecNone;
             b.rec_meta[p] = 0u;
         }
-    } else {
-        r = contact_warp<float, true, FULL, XM, W>(g, (int)cnt, (int)(eb - off), nbf);
     }
     if (lane == 0) {
         uint8_t st = (r.valid ? kValid : 0) | (r.unsure ? kUnsure : 0) | (r.overflow ? kOverflow : 0);
         b.p_status[p] = st;
-        b.p_area[p] = r.valid ? r.area : 0.0;
-        b.p_arc[p] = r.valid ? r.arc : 0.0;
-        b.p_central[p] = r.valid && r.central ? 1 : 0;
         b.p_sa_a[p] = r.valid ? r.sa_a : 0.0;
         b.p_sa_b[p] = r.valid ? r.sa_b : 0.0;
         b.p_pv_a[p] = r.valid ? r.pv_a : 0.0;
