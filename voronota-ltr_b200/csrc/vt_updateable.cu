@@ -645,10 +645,9 @@ struct vt_updateable {
     // FP32 updates: an affected ball whose compute_sas branch is uncertain on its FP32 sums
     // (cell_from_sums' bands) has every contact recomputed in FP64, the table entries kept
     // from earlier operations included (their FP32 values take part in the same sums), and
-    // then the cells of the ball and its neighbours are recomputed.  The uncertain balls
-    // are marked 2 and their neighbours 1; the pairs with an end marked 2 are recomputed,
-    // and their FP64 values replace the entries' values in place, so the table keeps the
-    // reference's entry order.
+    // then its cell is recomputed.  The uncertain balls are marked 2 and their neighbours
+    // 1; the pairs with an end marked 2 are recomputed, and their FP64 values replace the
+    // entries' values in place, so the table keeps the reference's entry order.
     void refresh_unsure_cells(UState& S, const uint32_t* d_count, uint32_t A) {
         const uint32_t n = S.n;
         ulist.ensure(A + 1);
@@ -681,10 +680,16 @@ struct vt_updateable {
         TableRef tref = S.tab.ref();
         if (!adjoint) tref.gA = tref.gB = tref.vA = tref.vB = nullptr;
         if (P2) launch_table_update(nc_ref(), keep_off.p + P2, P2, tref, w(kWErr), stream);
-        // the refreshed balls' neighbours need not be affected by this operation: a ball
-        // without contacts keeps the cell state its last computation gave it (the
-        // reference's detached rule applies to affected balls only, updateable.rs:711-719)
-        launch_table_cells(aff2.p, noff2.p + n, A2, S.tab.ref(), sph.p, S.excl.p, S.cell_flag.p, S.cell_sas.p,
+        // only the uncertain balls' cells are recomputed: all their contacts are FP64 now.
+        // Their neighbours keep the cells they have: an affected neighbour was decided
+        // outside the band in the first pass (one pair moving from its FP32 to its FP64
+        // value stays within it), and a neighbour this operation does not affect keeps its
+        // cell in the reference too, while a recomputation could mix FP64 entries with FP32
+        // ones this operation wrote for its affected neighbours and, near a threshold, flip
+        // its exposure.  A ball without contacts keeps the cell state its last computation
+        // gave it (the reference's detached rule applies to affected balls only,
+        // updateable.rs:711-719).
+        launch_table_cells(ulist.p, w(kWUnsure), U, S.tab.ref(), sph.p, S.excl.p, S.cell_flag.p, S.cell_sas.p,
                            S.cell_vol.p, 0.f, nullptr, stream, 1);
     }
 
