@@ -205,7 +205,12 @@ __device__ __forceinline__ void cell_from_sums(uint32_t count, double arc, doubl
     *unsure = false;
     if (cell_band > 0.f && arc > 0.0) {
         double tol_sa = (double)cell_band * count;
-        if (fabs(spos - sneg) <= tol_sa + 1e-10) *unsure = true;
+        // which sum dominates (the centre inside or outside its own cell): decided only by
+        // cells whose centre is close to the cell's boundary, rare, and there the FP32
+        // solid angles' error (float vertices, about E / distance per contour point) once
+        // exceeded tol_sa (a nearly engulfed ball, 5 contacts); the wider band costs
+        // almost no recomputation
+        if (fabs(spos - sneg) <= 8.0 * tol_sa + 1e-10) *unsure = true;
         // a nearly buried ball (positive dominance, 4 pi - (spos - sneg) about 0): the
         // sign of its SAS area, i.e. whether it is exposed at all, is within the band
         if (spos > sneg && fabs(fma(4.0, kPiD, -(spos - sneg))) <= tol_sa) *unsure = true;
