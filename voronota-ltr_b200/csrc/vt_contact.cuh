@@ -632,8 +632,8 @@ __device__ WarpContact contact_warp(const PairGeom<T>& g0, int cnt, int kb, NbFn
     T sum_arc = 0, area = 0;
     T area_tol = 0;  // FP32: band of the area <= 0 test (an uncut circle is far from it)
     V3<T> bary = mk<T>(0, 0, 0);
-    T tri = 0;                          // this lane's triangle (bary, point, next point) area
-    V3<T> vnext = mk<T>(0, 0, 0);       // the next point's position
+    T tri = 0;                     // this lane's triangle (bary, point, next point) area
+    V3<T> vnext = mk<T>(0, 0, 0);  // the next point's position
     bool on = false;
     T ang_err = 0;  // FP32: bound on this lane's arc-angle error
     if (!init) {  // contact.rs:311-314
