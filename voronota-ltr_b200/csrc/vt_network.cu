@@ -2,18 +2,23 @@
 // edges of the radical tessellation, deduplicated (contact.rs:119-177,
 // tessellation.rs:334-401).
 //
-//   1. every valid pair's contour is recomputed in FP64 (warp per pair) and emits one edge
-//      per contour segment -- ids (a, b, the cutting neighbour or NULL on an arc), length
-//      of the chord or arc -- and one vertex per contour point -- ids (a, b, left id,
-//      right id with a's id as NULL), position; an uncut contact emits one SAS edge; a
-//      contour that outgrows the warp is listed for the serial kernel (vt_contact64.cu);
+//   1. every valid pair emits one edge per contour segment -- ids (a, b, the cutting
+//      neighbour or NULL on an arc), length of the chord or arc -- and one vertex per
+//      contour point -- ids (a, b, left id, right id with a's id as NULL), position; an
+//      uncut contact emits one SAS edge.  FP64 mode recomputes the contours here in FP64
+//      (warp per pair); FP32 mode takes the contours the contact kernel recorded and
+//      places their vertices in double (k_net_elements32, vt_contact32.cu), and the pairs
+//      that kernel cannot settle come here.  A contour that outgrows the warp is listed
+//      for the serial kernel (vt_contact64.cu);
 //   2. ids are taken mod n for periodic images and sorted within the element;
 //   3. elements are put in id order and deduplicated keeping the first of equal ids, i.e.
 //      the first in pair and contour order (the reference sorts unstably and keeps an
 //      unspecified one): bucketed by their first id (a counting pass, a scan, a scatter),
-//      each bucket sorted by (remaining ids, dense index) -- a warp's bitonic sort in
-//      registers for buckets of up to 128 elements, a block's otherwise -- and the first of
-//      each run of equal ids kept.  NULL (0xffffffff) sorts after every ball id.
+//      each bucket reduced to its distinct id tuples (first occurrence, through a hash
+//      table, for buckets of more than 32 elements) and sorted by (remaining ids, dense
+//      index) -- a warp's bitonic sort in registers for buckets of up to 128 elements, a
+//      block's otherwise.  The remaining ids are packed into one 64-bit key (NULL as n,
+//      after every ball id) or, for vertices of 2^21 balls and more, two.
 #include "vt_contact.cuh"
 #include "vt_pipeline.cuh"
 
